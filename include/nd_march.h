@@ -1,0 +1,229 @@
+/* nd_march.h - C ABI of the B200 distance-estimator sphere-tracing pass.
+ *
+ * This header is the drop-in boundary between NumericDream's host code and the
+ * CUDA kernels.  It is plain C (no CUDA or torch types) so that Zig can import it
+ * with addTranslateC exactly like the reference's own translate-C shims
+ * (build.zig:379-423, e.g. src/bindings/webgpu_shim.h), and Python with ctypes.
+ *
+ * What each entry point replaces in the reference:
+ *   nd_formula_register / nd_formula_find
+ *       FractalRenderer.rebuild / rebuildAsync  (src/gpu/fractal_renderer.zig:2927, :2951)
+ *       + assembleShaderSource (fractal_renderer.zig:725-760) + stampFormulaCodes (:2882):
+ *       a formula source becomes an integer formula code.  Formula files are
+ *       translated from WGSL to CUDA at build time; registering a source looks up
+ *       its compiled code by the source hash, as CodeTable.find does (:585-590).
+ *   nd_formula_params
+ *       formula.parseFormulaParams / CustomParam  (src/app/formula.zig:6-13, :147-157)
+ *   nd_view_desc
+ *       the per-view part of `Uniforms` (fractal_renderer.zig:228-346): camera
+ *       basis, resolution, tile_scale/tile_bias (tileTransform :852-863), max_steps,
+ *       max_dist, epsilon_coefficient/floor, refine_fast/hq, march_verify,
+ *       high_quality, and one FractalInstance (code, params, orbit trap).
+ *   nd_march_forward
+ *       FractalRenderer.renderToImage -> renderTile -> drawSlot(fs_simple)
+ *       (fractal_renderer.zig:3548, :3741-3828; template.wgsl:4522-4538): march every
+ *       pixel of every view and write the G-buffer (frag_out, template.wgsl:3768-3774:
+ *       depth = t or 0 on a miss, normal xyz with w = hit).
+ *   nd_last_stats
+ *       the hot-spot DE-evaluation counter (template.wgsl:363-378) and the wavefront
+ *       per-pass profile (src/gpu/wavefront.zig:280-411), as totals.
+ *   nd_autotune, nd_graph_*
+ *       no reference counterpart; the reference picks sub-tile sizes by a pacing
+ *       heuristic (ExportPacer, fractal_renderer.zig:991) instead.
+ *   nd_march_backward
+ *       no reference counterpart (the reference has no gradients).
+ *
+ * Conventions: every call returns an nd_status and never aborts.  The caller owns
+ * every buffer; G-buffer pointers are DEVICE pointers, descriptors are HOST
+ * pointers.  Work is enqueued on the given CUDA stream (a cudaStream_t passed as
+ * void*, NULL = legacy default stream) and is asynchronous with respect to the
+ * host unless the call says otherwise.  A context is not thread-safe; distinct
+ * contexts are.
+ */
+#ifndef ND_MARCH_H
+#define ND_MARCH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ND_ABI_VERSION 1
+#define ND_MAX_PARAMS 16          /* fractal_renderer.zig:47 */
+#define ND_PARAM_NAME_LEN 24      /* CustomParam.name [24:0]u8, formula.zig:7 */
+
+typedef int32_t nd_status;
+enum {
+  ND_OK = 0,
+  ND_ERR_INVALID = 1,      /* bad argument or descriptor */
+  ND_ERR_COMPILE = 2,      /* formula source rejected or not compiled into this build */
+  ND_ERR_OOM = 3,          /* device allocation failed */
+  ND_ERR_TIMEOUT = 4,      /* the device watchdog stopped a launch */
+  ND_ERR_CUDA = 5,         /* any other CUDA error */
+  ND_ERR_UNSUPPORTED = 6,  /* valid request this build cannot serve */
+  ND_ERR_NOT_FOUND = 7     /* unknown formula name or id */
+};
+
+typedef int32_t nd_formula_id;
+typedef struct nd_ctx nd_ctx;
+typedef struct nd_graph nd_graph;
+
+/* One @param slider (CustomParam, src/app/formula.zig:6-13). */
+typedef struct nd_param_info {
+  char name[ND_PARAM_NAME_LEN];
+  float min_value;
+  float max_value;
+  float default_value;
+  int32_t integral;
+} nd_param_info;
+
+/* Orbit trap of one instance (OrbitTrap template.wgsl:1207-1214, enums
+ * src/app/scene_state.zig:134-189) and its colour-strip mapping
+ * (orbit_trap_to_strip template.wgsl:2025-2035). */
+enum { ND_TRAP_POINT = 0, ND_TRAP_SPHERE = 1, ND_TRAP_BOX = 2, ND_TRAP_CROSS = 3, ND_TRAP_TORUS = 4 };
+enum { ND_TRAP_MIN = 0, ND_TRAP_MAX = 1, ND_TRAP_AVERAGE = 2, ND_TRAP_LAST = 3, ND_TRAP_ITERATION = 4 };
+typedef struct nd_trap_desc {
+  float center[3];
+  int32_t shape;
+  float box[3];
+  int32_t mode;
+  float radius;
+  float tube;
+  float span;     /* strip mapping: x = v / max(span, 1e-4) + offset */
+  float offset;
+  int32_t repeat; /* 0 clamp, 1 repeat, 2 mirror */
+  int32_t reserved;
+} nd_trap_desc;
+
+enum { ND_NORMAL_TETRA = 0, ND_NORMAL_CENTRAL = 1 };
+
+/* One view: a camera, a frame (or a tile of it) and one fractal instance. */
+typedef struct nd_view_desc {
+  double cam_pos[3];      /* ray origin, FP64 (u.camera_pos) */
+  double fwd[3];          /* u.camera_forward */
+  double right[3];        /* u.camera_right, already scaled by tan(fov_y/2) */
+  double up[3];           /* u.camera_up, already scaled by tan(fov_y/2) */
+  int32_t width;          /* full frame size: aspect = width / height */
+  int32_t height;
+  int32_t tile_x;         /* rendered rectangle of the frame (tileTransform) */
+  int32_t tile_y;
+  int32_t tile_w;
+  int32_t tile_h;
+  nd_formula_id formula;  /* from nd_formula_find / nd_formula_register */
+  int32_t spp;            /* primary rays per pixel; 1 = pixel centre, >1 = jittered */
+  uint64_t seed;          /* jitter seed (counter-based, per ray) */
+  float params[ND_MAX_PARAMS]; /* packed @param values (packParams, formula.zig:104) */
+  nd_trap_desc trap;
+  int32_t max_steps;      /* u.max_steps */
+  float max_dist;         /* u.max_dist (24 in the reference UI) */
+  float eps_coef;         /* u.epsilon_coefficient: eps(t) = coef * t + floor */
+  float eps_floor;        /* u.epsilon_floor */
+  int32_t refine_budget;  /* u.refine_fast or u.refine_hq (bisection / verify budget) */
+  int32_t march_verify;   /* u.march_verify */
+  int32_t high_quality;   /* u.high_quality */
+  float hq_footprint_px;  /* u.hq_footprint_budget_px */
+  int32_t normal_mode;    /* ND_NORMAL_TETRA (template.wgsl:1783) or ND_NORMAL_CENTRAL */
+  float normal_h_coef;    /* central differences: h = coef * t (0 -> eps(t)) */
+  int32_t shadow;         /* 1: one shadow ray per hit toward light_dir */
+  float light_dir[3];     /* direction TO a LIGHT_GLOBAL light (normalised by the library) */
+  float shadow_k;         /* soft-shadow sharpness k */
+  float step_safety;      /* instance step safety, clamped to [0.001, 1] */
+  int32_t flags;          /* reserved, 0 */
+  int32_t reserved[3];
+} nd_view_desc;
+
+/* G-buffer of one forward call.  Rays of view v occupy [ray_offset(v), +rays(v)),
+ * views in call order; rays(v) = spp * tile_w * tile_h and the ray index inside a
+ * view is sample * tile_w * tile_h + y * tile_w + x.  Every pointer may be NULL
+ * except depth. */
+typedef struct nd_gbuffer {
+  float* depth;       /* t at the hit, 0 on a miss (R32F depth target) */
+  float* normal;      /* 4 floats per ray: unit normal, w = 1 on a hit */
+  float* trap;        /* orbit-trap value of the DE evaluation at the hit point */
+  uint32_t* steps;    /* probe steps (MarchResult.steps; max_steps on a miss) */
+  uint32_t* iters;    /* formula iterations that changed the carry, at the hit */
+  float* shade;       /* Lambert grey level (simple_geometry, template.wgsl:4492) */
+  float* shadow;      /* shadow-ray visibility in [0, 1] (1 without a shadow ray) */
+  double* depth64;    /* t in FP64 */
+  uint32_t* evals;    /* DE evaluations spent on this ray */
+} nd_gbuffer;
+
+enum { ND_KERNEL_AUTO = 0, ND_KERNEL_PLAIN = 1, ND_KERNEL_PERSISTENT = 2 };
+
+typedef struct nd_march_opts {
+  int32_t kernel;            /* ND_KERNEL_* */
+  int32_t block;             /* threads per block (0 = tuned default) */
+  int32_t blocks_per_sm;     /* persistent kernel residency (0 = tuned default) */
+  int32_t refill_threshold;  /* persistent: refill a warp once this many lanes idle (0 = default) */
+  int32_t de_precision;      /* 32 (default) or 64: float type of the DE itself */
+  int32_t watchdog_ms;       /* device watchdog per launch (0 = 10000 ms) */
+  int32_t reserved[2];
+} nd_march_opts;
+
+typedef struct nd_stats {
+  uint64_t rays;
+  uint64_t de_evals;        /* all DE evaluations: probes, bisection, normals, shadows */
+  uint64_t march_evals;     /* primary march probes + refinement */
+  uint64_t normal_evals;
+  uint64_t shadow_evals;
+  uint64_t hits;
+  uint64_t refills;         /* persistent kernel: warp refills */
+  uint32_t timeouts;        /* watchdog expiries */
+  uint32_t kernel;          /* kernel that ran (ND_KERNEL_PLAIN / _PERSISTENT) */
+} nd_stats;
+
+typedef struct nd_tune_result {
+  int32_t block;
+  int32_t blocks_per_sm;
+  int32_t refill_threshold;
+  int32_t kernel;
+  double rays_per_s;
+} nd_tune_result;
+
+/* ---- library ---- */
+int32_t nd_abi_version(void);
+const char* nd_status_string(nd_status s);
+
+/* ---- formulas (build-time translated) ---- */
+nd_status nd_formula_count(int32_t* n);
+nd_status nd_formula_find(const char* name, nd_formula_id* out);
+nd_status nd_formula_name(nd_formula_id id, char* out, size_t out_len);
+nd_status nd_formula_register(const char* wgsl_src, size_t len, nd_formula_id* out, char* err, size_t err_len);
+nd_status nd_formula_params(nd_formula_id id, nd_param_info* out, int32_t* n);
+nd_status nd_view_defaults(nd_formula_id id, nd_view_desc* out);
+
+/* ---- context ---- */
+nd_status nd_ctx_create(int32_t device, nd_ctx** out);
+nd_status nd_ctx_destroy(nd_ctx* ctx);
+nd_status nd_last_error(const nd_ctx* ctx, char* out, size_t out_len);
+nd_status nd_last_stats(nd_ctx* ctx, nd_stats* out); /* synchronises the last forward's stream */
+
+/* ---- marching ---- */
+nd_status nd_count_rays(const nd_view_desc* views, int32_t nviews, int64_t* total);
+nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews,
+                           const nd_march_opts* opts, const nd_gbuffer* out, void* stream);
+nd_status nd_autotune(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews,
+                      const nd_gbuffer* scratch_out, nd_tune_result* result);
+nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews,
+                           const nd_march_opts* opts, const nd_gbuffer* out, void* stream, nd_graph** graph);
+nd_status nd_graph_launch(nd_graph* graph, void* stream);
+nd_status nd_graph_destroy(nd_graph* graph);
+
+/* DE of view->formula (with view->params and view->trap) at n points: pts is a
+ * DEVICE array of 3n doubles; de, trap (nullable) and iters (nullable) are DEVICE
+ * arrays of n.  Each point runs the formula wrapper of the reference (carry =
+ * (pos, 1), de_iterations() x de_step with the orbit trap, de_finalize;
+ * fractal_renderer.zig:490-512) in FP32 (de_precision 32) or FP64 (64). */
+nd_status nd_de_points(nd_ctx* ctx, const nd_view_desc* view, int64_t n, const double* pts, double* de,
+                       double* trap, uint32_t* iters, int32_t de_precision, void* stream);
+
+/* Size of a public struct by name ("nd_view_desc", ...), for binding layout checks. */
+size_t nd_sizeof(const char* name);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ND_MARCH_H */

@@ -1,0 +1,151 @@
+"""ctypes mirror of include/nd_march.h and helpers to fill its descriptors.
+
+The structures here must match the C header byte for byte; ``check_layout`` is
+called by the tests and compares sizes and offsets against the values the C
+library reports for itself.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+ND_MAX_PARAMS = 16
+ND_PARAM_NAME_LEN = 24
+
+ND_OK, ND_ERR_INVALID, ND_ERR_COMPILE, ND_ERR_OOM, ND_ERR_TIMEOUT, ND_ERR_CUDA, ND_ERR_UNSUPPORTED, ND_ERR_NOT_FOUND = range(8)
+STATUS_NAMES = ["ND_OK", "ND_ERR_INVALID", "ND_ERR_COMPILE", "ND_ERR_OOM", "ND_ERR_TIMEOUT", "ND_ERR_CUDA",
+                "ND_ERR_UNSUPPORTED", "ND_ERR_NOT_FOUND"]
+
+ND_TRAP_POINT, ND_TRAP_SPHERE, ND_TRAP_BOX, ND_TRAP_CROSS, ND_TRAP_TORUS = range(5)
+ND_TRAP_MIN, ND_TRAP_MAX, ND_TRAP_AVERAGE, ND_TRAP_LAST, ND_TRAP_ITERATION = range(5)
+ND_NORMAL_TETRA, ND_NORMAL_CENTRAL = 0, 1
+ND_KERNEL_AUTO, ND_KERNEL_PLAIN, ND_KERNEL_PERSISTENT = 0, 1, 2
+
+
+class nd_param_info(C.Structure):
+    _fields_ = [("name", C.c_char * ND_PARAM_NAME_LEN), ("min_value", C.c_float), ("max_value", C.c_float),
+                ("default_value", C.c_float), ("integral", C.c_int32)]
+
+
+class nd_trap_desc(C.Structure):
+    _fields_ = [("center", C.c_float * 3), ("shape", C.c_int32), ("box", C.c_float * 3), ("mode", C.c_int32),
+                ("radius", C.c_float), ("tube", C.c_float), ("span", C.c_float), ("offset", C.c_float),
+                ("repeat", C.c_int32), ("reserved", C.c_int32)]
+
+
+class nd_view_desc(C.Structure):
+    _fields_ = [
+        ("cam_pos", C.c_double * 3), ("fwd", C.c_double * 3), ("right", C.c_double * 3), ("up", C.c_double * 3),
+        ("width", C.c_int32), ("height", C.c_int32), ("tile_x", C.c_int32), ("tile_y", C.c_int32),
+        ("tile_w", C.c_int32), ("tile_h", C.c_int32), ("formula", C.c_int32), ("spp", C.c_int32),
+        ("seed", C.c_uint64), ("params", C.c_float * ND_MAX_PARAMS), ("trap", nd_trap_desc),
+        ("max_steps", C.c_int32), ("max_dist", C.c_float), ("eps_coef", C.c_float), ("eps_floor", C.c_float),
+        ("refine_budget", C.c_int32), ("march_verify", C.c_int32), ("high_quality", C.c_int32),
+        ("hq_footprint_px", C.c_float), ("normal_mode", C.c_int32), ("normal_h_coef", C.c_float),
+        ("shadow", C.c_int32), ("light_dir", C.c_float * 3), ("shadow_k", C.c_float), ("step_safety", C.c_float),
+        ("flags", C.c_int32), ("reserved", C.c_int32 * 3),
+    ]
+
+
+class nd_gbuffer(C.Structure):
+    _fields_ = [("depth", C.c_void_p), ("normal", C.c_void_p), ("trap", C.c_void_p), ("steps", C.c_void_p),
+                ("iters", C.c_void_p), ("shade", C.c_void_p), ("shadow", C.c_void_p), ("depth64", C.c_void_p),
+                ("evals", C.c_void_p)]
+
+
+class nd_march_opts(C.Structure):
+    _fields_ = [("kernel", C.c_int32), ("block", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("refill_threshold", C.c_int32), ("de_precision", C.c_int32), ("watchdog_ms", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
+
+
+class nd_stats(C.Structure):
+    _fields_ = [("rays", C.c_uint64), ("de_evals", C.c_uint64), ("march_evals", C.c_uint64),
+                ("normal_evals", C.c_uint64), ("shadow_evals", C.c_uint64), ("hits", C.c_uint64),
+                ("refills", C.c_uint64), ("timeouts", C.c_uint32), ("kernel", C.c_uint32)]
+
+
+class nd_tune_result(C.Structure):
+    _fields_ = [("block", C.c_int32), ("blocks_per_sm", C.c_int32), ("refill_threshold", C.c_int32),
+                ("kernel", C.c_int32), ("rays_per_s", C.c_double)]
+
+
+def _sub(a, b):
+    return [a[i] - b[i] for i in range(3)]
+
+
+def _cross(a, b):
+    return [a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]]
+
+
+def _norm(a):
+    n = math.sqrt(sum(x * x for x in a))
+    return [x / n for x in a]
+
+
+def look_at(pos, target=(0.0, 0.0, 0.0), world_up=(0.0, 1.0, 0.0), fov_y_deg=60.0):
+    """Camera basis as FreeCamera builds it (src/app/camera.zig:98-112):
+    forward = normalize(target - pos), right = normalize(forward x up),
+    up = normalize(right x forward); right and up are then scaled by tan(fov/2)
+    (the reference has no FOV knob: |up| = 1 is a 90 degree vertical FOV)."""
+    f = _norm(_sub(target, pos))
+    r = _norm(_cross(f, list(world_up)))
+    u = _norm(_cross(r, f))
+    s = math.tan(math.radians(fov_y_deg) * 0.5)
+    return f, [x * s for x in r], [x * s for x in u]
+
+
+def make_view(formula: int, width: int, height: int, cam_pos, target=(0.0, 0.0, 0.0), fov_y_deg=60.0,
+              params=None, world_up=(0.0, 1.0, 0.0), **kw) -> nd_view_desc:
+    """A view with the reference's render defaults (RenderSettingsState and
+    MarchPrecision, src/app/render_precision.zig:3-30: max_steps 256, max_dist 24,
+    epsilon 5e-4 * t + 5e-5, refine_fast 4), overridable by keyword."""
+    v = nd_view_desc()
+    v.cam_pos[:] = [float(x) for x in cam_pos]
+    f, r, u = look_at(list(cam_pos), list(target), world_up, fov_y_deg)
+    v.fwd[:] = f
+    v.right[:] = r
+    v.up[:] = u
+    v.width, v.height = width, height
+    v.tile_x, v.tile_y, v.tile_w, v.tile_h = 0, 0, width, height
+    v.formula = formula
+    v.spp = 1
+    v.seed = 0
+    if params is not None:
+        for i, p in enumerate(params[:ND_MAX_PARAMS]):
+            v.params[i] = p
+    v.trap.shape = ND_TRAP_POINT
+    v.trap.mode = ND_TRAP_MIN
+    v.trap.radius = 1.0
+    v.trap.box[:] = [1.0, 1.0, 1.0]
+    v.trap.span = 1.5
+    v.max_steps = 256
+    v.max_dist = 24.0
+    v.eps_coef = 5e-4
+    v.eps_floor = 5e-5
+    v.refine_budget = 4
+    v.march_verify = 0
+    v.high_quality = 0
+    v.hq_footprint_px = 2.0
+    v.normal_mode = ND_NORMAL_TETRA
+    v.normal_h_coef = 0.0
+    v.shadow = 0
+    v.shadow_k = 16.0
+    v.step_safety = 1.0
+    for k, val in kw.items():
+        if k == "trap":
+            for tk, tv in val.items():
+                if isinstance(tv, (list, tuple)):
+                    getattr(v.trap, tk)[:] = tv
+                else:
+                    setattr(v.trap, tk, tv)
+        elif isinstance(val, (list, tuple)):
+            getattr(v, k)[:] = list(val)
+        else:
+            setattr(v, k, val)
+    return v
+
+
+def rays_of(v: nd_view_desc) -> int:
+    return int(v.spp) * int(v.tile_w) * int(v.tile_h)

@@ -1,0 +1,163 @@
+// The DE helper library that formula plugins call, plus the orbit trap and the
+// per-formula iteration wrapper.  Host and device; templated on the float type T.
+//
+// Every function here has the behaviour of the WGSL function of the same name in
+// NumericDream's shader template (src/gpu/shaders/template.wgsl, line numbers
+// below), because formula files call these names and must see the same results.
+#pragma once
+
+#include "nd_wgsl.h"
+
+namespace ndw {
+
+// template.wgsl:57-70 constants used by the helpers
+template <class T> ND_HD_INLINE T k_epsilon() { return T(1e-4); }
+template <class T> ND_HD_INLINE T k_epsilon_fine() { return T(1e-6); }
+
+// template.wgsl:945-951: reflect each component beyond +-limit back inside.
+template <class T> ND_HD_INLINE v3<T> box_fold(v3<T> z, T limit) {
+  return clamp(z, v3<T>(-limit), v3<T>(limit)) * T(2) - z;
+}
+
+// template.wgsl:953-971: sphere inversion with a floor; radii are squared.
+template <class T> ND_HD_INLINE v4<T> sphere_fold(v3<T> z, T dr, T min_radius2, T fixed_radius2) {
+  const T r2 = dot(z, z);
+  if (r2 < min_radius2) {
+    const T t = fixed_radius2 / min_radius2;
+    return v4<T>(z * t, dr * t);
+  } else if (r2 < fixed_radius2) {
+    const T t = fixed_radius2 / r2;
+    return v4<T>(z * t, dr * t);
+  }
+  return v4<T>(z, dr);
+}
+
+// template.wgsl:973-985: inversion in the sphere |d|^2 < radius2 around center.
+template <class T> ND_HD_INLINE v4<T> sphere_invert_offset(v3<T> z, T dr, v3<T> center, T radius2) {
+  const v3<T> d = z - center;
+  const T r2 = max(dot(d, d), k_epsilon_fine<T>());
+  if (r2 < radius2) {
+    const T t = radius2 / r2;
+    return v4<T>(center + d * t, dr * t);
+  }
+  return v4<T>(z, dr);
+}
+
+// template.wgsl:987-991: wrap into the cube of side `cell` centred at the origin.
+template <class T> ND_HD_INLINE v3<T> lattice_wrap(v3<T> p, T cell) {
+  return p - round(p / cell) * cell;
+}
+
+// template.wgsl:993-997
+template <class T> ND_HD_INLINE T de_finalize_scaled(IterCarry<T> c) { return length(c.z) / abs(c.dr); }
+// template.wgsl:999-1003
+template <class T> ND_HD_INLINE T de_finalize_plain(IterCarry<T> c) { return length(c.z) / c.dr; }
+
+// template.wgsl:1005-1010: 0.5 log(r) r / dr, capped at r; r and dr floored.
+template <class T> ND_HD_INLINE T bulb_log_escape(IterCarry<T> c) {
+  const T r = length(c.z);
+  const T est = T(0.5) * log(max(r, k_epsilon_fine<T>())) * r / max(c.dr, k_epsilon_fine<T>());
+  return min(est, r);
+}
+
+// template.wgsl:1013 (BULB_BAILOUT) and 1019-1031: one Mandelbulb power step in
+// spherical coordinates (theta from +z, phi = atan2(y, x)); no-op once r > 2.
+template <class T> ND_HD_INLINE IterCarry<T> bulb_power_step(IterCarry<T> c, v3<T> add, T power) {
+  const T r = length(c.z);
+  if (r > T(2)) return c;
+  const T theta = acos(clamp(c.z.z / r, T(-1), T(1))) * power;
+  const T phi = atan2(c.z.y, c.z.x) * power;
+  const T rp = pow(r, power - T(1));
+  const T zr = rp * r;
+  const T dr = rp * power * c.dr + T(1);
+  const T st = sin(theta);
+  const v3<T> z = v3<T>(st * cos(phi), st * sin(phi), cos(theta)) * zr + add;
+  return IterCarry<T>{z, dr};
+}
+
+// template.wgsl:1033-1055: abs then sort components so that x >= y >= z.
+template <class T> ND_HD_INLINE v3<T> sort_desc_abs(v3<T> z) {
+  v3<T> v = abs(z);
+  if (v.x < v.y) { const T t = v.x; v.x = v.y; v.y = t; }
+  if (v.x < v.z) { const T t = v.x; v.x = v.z; v.z = t; }
+  if (v.y < v.z) { const T t = v.y; v.y = v.z; v.z = t; }
+  return v;
+}
+
+// template.wgsl:1057-1077: mirrors across x+y=0, x+z=0, y+z=0 in that order.
+template <class T> ND_HD_INLINE v3<T> tetra_fold(v3<T> z) {
+  v3<T> v = z;
+  if (v.x + v.y < T(0)) { const T t = -v.y; v.y = -v.x; v.x = t; }
+  if (v.x + v.z < T(0)) { const T t = -v.z; v.z = -v.x; v.x = t; }
+  if (v.y + v.z < T(0)) { const T t = -v.z; v.z = -v.y; v.y = t; }
+  return v;
+}
+
+// template.wgsl:1079-1083
+template <class T> ND_HD_INLINE T wrap_angle(T a, T period) { return a - period * floor(a / period); }
+
+// template.wgsl:1392-1408: right-handed rotations, columns as in the WGSL mat3x3f.
+template <class T> ND_HD_INLINE m3<T> rot_x(T a) {
+  const T c = cos(a), s = sin(a);
+  return m3<T>(v3<T>(T(1), T(0), T(0)), v3<T>(T(0), c, s), v3<T>(T(0), -s, c));
+}
+template <class T> ND_HD_INLINE m3<T> rot_y(T a) {
+  const T c = cos(a), s = sin(a);
+  return m3<T>(v3<T>(c, T(0), -s), v3<T>(T(0), T(1), T(0)), v3<T>(s, T(0), c));
+}
+template <class T> ND_HD_INLINE m3<T> rot_z(T a) {
+  const T c = cos(a), s = sin(a);
+  return m3<T>(v3<T>(c, s, T(0)), v3<T>(-s, c, T(0)), v3<T>(T(0), T(0), T(1)));
+}
+
+// template.wgsl:1085-1093: rot_z * (rot_y * (rot_x * z)) with angles in degrees;
+// identity when all three angles are exactly zero.
+template <class T> ND_HD_INLINE v3<T> rotate_xyz_deg(v3<T> z, v3<T> deg) {
+  if (deg.x == T(0) && deg.y == T(0) && deg.z == T(0)) return z;
+  const v3<T> a = radians(deg);
+  return mul(rot_z(a.z), mul(rot_y(a.y), mul(rot_x(a.x), z)));
+}
+
+// template.wgsl:1095-1098
+template <class T> ND_HD_INLINE int32_t primitive_de_iterations() { return 1; }
+
+// template.wgsl:1100-1109: rescale z by 1/size and 1/|dr|; dr becomes 1/size.
+template <class T> ND_HD_INLINE IterCarry<T> primitive_de_step(IterCarry<T> c, T size) {
+  const T unit_dr = T(1) / max(size, k_epsilon<T>());
+  const T f = unit_dr / max(abs(c.dr), k_epsilon_fine<T>());
+  return IterCarry<T>{c.z * f, unit_dr};
+}
+
+// template.wgsl:1648-1706: smooth combine family; k <= 1e-4 is the hard operation.
+template <class T> ND_HD_INLINE T smin(T a, T b, T k) {
+  if (k <= T(0.0001)) return min(a, b);
+  const T h = clamp(T(0.5) + T(0.5) * (b - a) / k, T(0), T(1));
+  return mix(b, a, h) - k * h * (T(1) - h);
+}
+template <class T> ND_HD_INLINE T smax(T a, T b, T k) {
+  if (k <= T(0.0001)) return max(a, b);
+  const T h = clamp(T(0.5) - T(0.5) * (b - a) / k, T(0), T(1));
+  return mix(b, a, h) + k * h * (T(1) - h);
+}
+template <class T> ND_HD_INLINE T ssub(T cut, T base, T k) {
+  if (k <= T(0.0001)) return max(-cut, base);
+  const T h = clamp(T(0.5) - T(0.5) * (base + cut) / k, T(0), T(1));
+  return mix(base, -cut, h) + k * h * (T(1) - h);
+}
+template <class T> ND_HD_INLINE T smin_lin(T a, T b, T k) {
+  if (k <= T(0.0001)) return min(a, b);
+  return min(b - max(k - a, T(0)), a - max(k - b, T(0)));
+}
+template <class T> ND_HD_INLINE T smin_nlin(T a, T b, T k) {
+  if (k <= T(0.0001)) return min(a, b);
+  const T ra = max(k - a, T(0));
+  const T rb = max(k - b, T(0));
+  return min(b - ra * (k - rb) / k, a - rb * (k - ra) / k);
+}
+template <class T> ND_HD_INLINE T smix(T a, T b, T k) {
+  if (k <= T(0.0001)) return min(a, b);
+  const T h = clamp(T(0.5) + T(0.5) * (b - a) / k, T(0), T(1));
+  return mix(b, a, h);
+}
+
+}  // namespace ndw

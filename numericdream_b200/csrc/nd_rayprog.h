@@ -1,0 +1,538 @@
+// The ray program of the sphere-tracing pass, shared by the CUDA kernels
+// (nd_kernels.cuh) and by the host op-counting build (nd_opcount.cpp).
+//
+// Work model.  A launch covers a list of views; every (view, sample, pixel) is one
+// work item ("ray") with a global index; views are concatenated in call order and
+// the G-buffer is indexed by that global index.
+//
+// Ray program.  The march of one ray is the reference's march_to
+// (src/gpu/shaders/template.wgsl:1859-1963) followed by estimate_normal
+// (tpl:1783-1804, or 6-tap central differences), the orbit trap of the DE
+// evaluation at the hit (formula_N, src/gpu/fractal_renderer.zig:490-512) and an
+// opaque soft shadow (visibility_march / shadow_factor, tpl:2282-2375).  In the
+// persistent kernel the whole program is a state machine that spends exactly one DE
+// evaluation per loop iteration, so all live lanes of a warp evaluate the DE
+// together whatever phase (probe, bisection, normal tap, shadow step) each is in;
+// lanes that finish are refilled with new rays once enough of them are idle.
+//
+// Precision: the DE runs in T (float by default); the ray origin, direction, t,
+// the bisection interval and the normal/shadow sample positions are double.
+#pragma once
+
+#include <stdint.h>
+
+#include "nd_helpers.h"
+#include "../../include/nd_march.h"
+
+#if defined(__CUDACC__)
+#define ND_DEV_INLINE __host__ __device__ __forceinline__
+#else
+#define ND_DEV_INLINE inline
+#endif
+
+namespace nd {
+
+// Correctly rounded arithmetic that the compiler may not contract into FMAs.
+#if defined(__CUDA_ARCH__)
+ND_DEV_INLINE float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+ND_DEV_INLINE float rn_add(float a, float b) { return __fadd_rn(a, b); }
+ND_DEV_INLINE double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+ND_DEV_INLINE double rn_add(double a, double b) { return __dadd_rn(a, b); }
+ND_DEV_INLINE double fma_d(double a, double b, double c) { return __fma_rn(a, b, c); }
+#else
+// host builds of this header are compiled with -ffp-contract=off
+ND_DEV_INLINE float rn_mul(float a, float b) { return a * b; }
+ND_DEV_INLINE float rn_add(float a, float b) { return a + b; }
+ND_DEV_INLINE double rn_mul(double a, double b) { return a * b; }
+ND_DEV_INLINE double rn_add(double a, double b) { return a + b; }
+ND_DEV_INLINE double fma_d(double a, double b, double c) { return ::fma(a, b, c); }
+#endif
+
+constexpr int kMaxIterations = 4096;   // watchdog cap on de_iterations()
+constexpr int kShadowMaxSteps = 40;    // SHADOW_MAX_STEPS tpl:2353
+constexpr double kShadowBias = 0.004;  // SHADOW_BIAS tpl:2344
+constexpr double kShadowHitEps = 0.0005;
+constexpr double kShadowMinStep = 0.001;
+constexpr double kSimpleAmbient = 0.18;  // SIMPLE_AMBIENT tpl:4418
+
+// Per-view record the kernels read (built on the host from nd_view_desc).
+struct DevView {
+  double org[3];
+  double fwd[3];
+  double right[3];
+  double up[3];
+  double uright[3];     // unit right / up for the camera-mounted key light
+  double uup[3];
+  double light[3];      // unit direction to the light (shadow / Lambert)
+  double aspect;
+  double footprint;     // hq_footprint_px * 2 / height
+  double max_dist;
+  int64_t ray_offset;   // first work-item index of this view inside its launch
+  int64_t out_offset;   // first G-buffer index of this view
+  int64_t rays;
+  uint64_t seed;
+  float params[ND_MAX_PARAMS];
+  nd_trap_desc trap;
+  float eps_coef, eps_floor, normal_h_coef, shadow_k, factor;
+  int32_t width, height, tile_x, tile_y, tile_w, tile_h, spp;
+  int32_t max_steps, refine, verify, hq, normal_mode, shadow, use_light;
+  int32_t code;         // formula index inside the kernel's formula set
+  int32_t max_samples;  // max_steps * (1 + refine budget) + bisect budget
+};
+
+struct Stats {
+  unsigned long long rays, de_evals, march_evals, normal_evals, shadow_evals, hits, refills;
+  unsigned int timeouts, pad;
+};
+
+struct LaunchArgs {
+  const DevView* views;       // device
+  int32_t nviews;
+  int64_t total_rays;
+  nd_gbuffer out;             // device pointers
+  unsigned long long* counter;  // persistent work counter (zeroed before launch)
+  Stats* stats;
+  int32_t refill_threshold;
+  int64_t deadline_ns;        // watchdog budget (globaltimer units)
+};
+
+// --------------------------------------------------------------- orbit trap
+// OrbitTrap accumulator: tpl:1227-1289.
+template <class T> struct TrapAcc {
+  T x, y, z, w;
+};
+
+template <class T> ND_HD_INLINE T trap_distance(const nd_trap_desc& t, ndw::v3<T> z) {
+  using ndw::v3;
+  const v3<T> q = z - v3<T>(T(t.center[0]), T(t.center[1]), T(t.center[2]));
+  switch (t.shape) {
+    case ND_TRAP_SPHERE: return ndw::abs(ndw::length(q) - T(t.radius));
+    case ND_TRAP_BOX: {
+      const v3<T> e = ndw::abs(q) - v3<T>(T(t.box[0]), T(t.box[1]), T(t.box[2]));
+      return ndw::abs(ndw::length(ndw::max(e, v3<T>(T(0)))) + ndw::min(ndw::max(e.x, ndw::max(e.y, e.z)), T(0)));
+    }
+    case ND_TRAP_CROSS: return ndw::min(ndw::abs(q.x), ndw::min(ndw::abs(q.y), ndw::abs(q.z)));
+    case ND_TRAP_TORUS: {
+      const T a = ndw::sqrt(q.x * q.x + q.z * q.z) - T(t.radius);
+      return ndw::abs(ndw::sqrt(a * a + q.y * q.y) - T(t.tube));
+    }
+    default: return ndw::length(q);
+  }
+}
+
+template <class T> ND_HD_INLINE TrapAcc<T> trap_begin(const nd_trap_desc& t) {
+  const bool high = t.mode != ND_TRAP_MAX && t.mode != ND_TRAP_AVERAGE;
+  return TrapAcc<T>{high ? T(1e6) : T(0), T(0), T(0), T(1e6)};
+}
+
+template <class T>
+ND_HD_INLINE void trap_update(TrapAcc<T>& a, const nd_trap_desc& t, ndw::v3<T> z, bool changed, int it) {
+  const T d = trap_distance(t, z);
+  a.w = d;
+  if (t.mode == ND_TRAP_MAX) {
+    a.x = ndw::max(a.x, d);
+  } else if (t.mode == ND_TRAP_AVERAGE) {
+    if (changed) {
+      a.x += d;
+      a.y += T(1);
+    }
+  } else if (t.mode == ND_TRAP_ITERATION) {
+    if (d < a.x) {
+      a.x = d;
+      a.z = T(it);
+    }
+  } else {
+    a.x = ndw::min(a.x, d);
+  }
+}
+
+template <class T> ND_HD_INLINE T trap_finish(const TrapAcc<T>& a, const nd_trap_desc& t, int iters) {
+  if (t.mode == ND_TRAP_AVERAGE) return a.y > T(0.5) ? a.x / ndw::max(a.y, T(1)) : a.w;
+  if (t.mode == ND_TRAP_LAST) return a.w;
+  if (t.mode == ND_TRAP_ITERATION) return (a.z + T(1)) / T(iters > 1 ? iters : 1);
+  return a.x;
+}
+
+template <class T> struct DEOut {
+  T d;
+  T trap;
+  int iters;
+};
+
+// Parameter access for formula code: p[i] reads the view's packed params.
+template <class T> struct ParamRef {
+  const float* v;
+  ND_HD_INLINE T operator[](int i) const { return T(v[i]); }
+};
+
+// formula_N (fractal_renderer.zig:490-512) + the single-instance scene_de
+// (tpl:1611-1626, 1756-1779): identity instance transform, DE scaled by factor.
+template <class F, class T>
+ND_DEV_INLINE DEOut<T> formula_de(ndw::v3<T> pos, const float* params, const nd_trap_desc& trap,
+                                               float factor) {
+  const ParamRef<T> p{params};
+  ndw::IterCarry<T> c{pos, T(1)};
+  TrapAcc<T> acc = trap_begin<T>(trap);
+  int n = F::template iterations<T, ParamRef<T>>(p);
+  n = n < kMaxIterations ? n : kMaxIterations;
+  int changed = 0;
+  for (int it = 0; it < n; ++it) {
+    const ndw::v3<T> zp = c.z;
+    c = F::template step<T, ParamRef<T>>(c, pos, p);
+    const bool ch = (c.z.x != zp.x) | (c.z.y != zp.y) | (c.z.z != zp.z);
+    changed += ch ? 1 : 0;
+    trap_update(acc, trap, c.z, ch, it);
+  }
+  DEOut<T> o;
+  o.d = F::template finalize<T, ParamRef<T>>(c) * T(factor);
+  o.trap = trap_finish(acc, trap, n);
+  o.iters = changed;
+  return o;
+}
+
+// A compile-time list of formulas; code selects one (warp-uniform in practice,
+// because work items are ordered by view).
+template <class... Fs> struct FormulaSet;
+template <class F> struct FormulaSet<F> {
+  template <class T>
+  static ND_DEV_INLINE DEOut<T> de(int, ndw::v3<T> pos, const DevView& v) {
+    return formula_de<F, T>(pos, v.params, v.trap, v.factor);
+  }
+};
+template <class F, class G, class... Rest> struct FormulaSet<F, G, Rest...> {
+  template <class T>
+  static ND_DEV_INLINE DEOut<T> de(int code, ndw::v3<T> pos, const DevView& v) {
+    if (code == 0) return formula_de<F, T>(pos, v.params, v.trap, v.factor);
+    return FormulaSet<G, Rest...>::template de<T>(code - 1, pos, v);
+  }
+};
+
+// --------------------------------------------------------------- helpers
+ND_DEV_INLINE uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+struct D3 {
+  double x, y, z;
+};
+ND_DEV_INLINE D3 d3(double x, double y, double z) { return D3{x, y, z}; }
+ND_DEV_INLINE D3 fmadd(D3 o, D3 d, double t) {
+  return D3{fma_d(d.x, t, o.x), fma_d(d.y, t, o.y), fma_d(d.z, t, o.z)};
+}
+
+// eps(t) = coef * t + floor in the DE precision, without FMA contraction
+// (march_epsilon tpl:1813-1815).
+template <class T> ND_DEV_INLINE double march_eps(const DevView& v, double t) {
+  return double(rn_add(rn_mul(v.eps_coef, float(t)), v.eps_floor));
+}
+template <> ND_DEV_INLINE double march_eps<float>(const DevView& v, double t) {
+  return double(rn_add(rn_mul(v.eps_coef, float(t)), v.eps_floor));
+}
+template <> ND_DEV_INLINE double march_eps<double>(const DevView& v, double t) {
+  return rn_add(rn_mul(double(v.eps_coef), t), double(v.eps_floor));
+}
+
+// Primary ray of a work item: cs_wf_generate tpl:5120-5127 / fs_simple tpl:4523-4525
+// with the tile transform (fractal_renderer.zig:852-863) folded into frame pixels.
+ND_DEV_INLINE D3 ray_dir(const DevView& v, int64_t local) {
+  const int64_t npix = int64_t(v.tile_w) * v.tile_h;
+  const int64_t s = local / npix;
+  const int64_t pix = local - s * npix;
+  const int px = v.tile_x + int(pix % v.tile_w);
+  const int py = v.tile_y + int(pix / v.tile_w);
+  double jx = 0.5, jy = 0.5;
+  if (v.spp > 1) {
+    const uint64_t h = splitmix64(v.seed ^ splitmix64(uint64_t(local)));
+    jx = double(uint32_t(h) >> 8) * (1.0 / 16777216.0);
+    jy = double(uint32_t(h >> 32) >> 8) * (1.0 / 16777216.0);
+  }
+  const double ndc_x = 2.0 * (double(px) + jx) / double(v.width) - 1.0;
+  const double ndc_y = 1.0 - 2.0 * (double(py) + jy) / double(v.height);
+  const double ux = ndc_x * v.aspect, uy = -ndc_y;
+  double x = v.fwd[0] + v.right[0] * ux + v.up[0] * uy;
+  double y = v.fwd[1] + v.right[1] * ux + v.up[1] * uy;
+  double z = v.fwd[2] + v.right[2] * ux + v.up[2] * uy;
+  const double inv = 1.0 / sqrt(x * x + y * y + z * z);
+  return D3{x * inv, y * inv, z * inv};
+}
+
+template <class T> ND_DEV_INLINE ndw::v3<T> to_t(D3 p) { return ndw::v3<T>(T(p.x), T(p.y), T(p.z)); }
+
+// Tetrahedral tap directions (tetra_gradient tpl:1790-1804).
+ND_DEV_INLINE D3 tetra_k(int i) {
+  return i == 0 ? d3(1, -1, -1) : i == 1 ? d3(-1, -1, 1) : i == 2 ? d3(-1, 1, -1) : d3(1, 1, 1);
+}
+
+// Final per-ray outputs (frag_out tpl:3768-3774; simple_geometry tpl:4492-4507).
+struct RayResult {
+  double t;
+  float nx, ny, nz;
+  float trap;
+  float shade;
+  float shadow;
+  uint32_t steps, iters, evals;
+  bool hit;
+};
+
+ND_DEV_INLINE void write_result(const nd_gbuffer& g, int64_t r, const RayResult& o) {
+  // r is the G-buffer index (view out_offset + ray index inside the view)
+  g.depth[r] = o.hit ? float(o.t) : 0.0f;
+  if (g.normal) {
+    struct alignas(16) F4 {
+      float x, y, z, w;
+    };
+    reinterpret_cast<F4*>(g.normal)[r] = F4{o.nx, o.ny, o.nz, o.hit ? 1.0f : 0.0f};
+  }
+  if (g.trap) g.trap[r] = o.trap;
+  if (g.steps) g.steps[r] = o.steps;
+  if (g.iters) g.iters[r] = o.iters;
+  if (g.shade) g.shade[r] = o.shade;
+  if (g.shadow) g.shadow[r] = o.shadow;
+  if (g.depth64) g.depth64[r] = o.hit ? o.t : 0.0;
+  if (g.evals) g.evals[r] = o.evals;
+}
+
+// Lambert grey level with the camera-mounted key light of simple_geometry, or the
+// view's directional light (times the shadow visibility).
+ND_DEV_INLINE float lambert(const DevView& v, D3 dir, double nx, double ny, double nz, float vis) {
+  double kx, ky, kz;
+  if (v.use_light) {
+    kx = v.light[0]; ky = v.light[1]; kz = v.light[2];
+  } else {
+    kx = -dir.x + v.uup[0] * 0.45 - v.uright[0] * 0.35;
+    ky = -dir.y + v.uup[1] * 0.45 - v.uright[1] * 0.35;
+    kz = -dir.z + v.uup[2] * 0.45 - v.uright[2] * 0.35;
+    const double inv = 1.0 / sqrt(kx * kx + ky * ky + kz * kz);
+    kx *= inv; ky *= inv; kz *= inv;
+  }
+  const double lam = fmax(nx * kx + ny * ky + nz * kz, 0.0) * double(vis);
+  return float(kSimpleAmbient + (1.0 - kSimpleAmbient) * lam);
+}
+
+ND_DEV_INLINE int find_view(const DevView* views, int nviews, int64_t item) {
+  int lo = 0, hi = nviews - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (views[mid].ray_offset <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// --------------------------------------------------------------- the ray state machine
+enum Phase : int { PH_MARCH = 0, PH_NORMAL = 1, PH_SHADOW = 2, PH_DONE = 3 };
+
+template <class T> struct Lane {
+  int64_t item;   // global ray index, -1 when idle
+  int view;
+  int phase;
+  D3 dir;
+  // march_to state
+  double t, lo, hi;
+  int i, n, refines;
+  bool probing, bisecting, resolved;
+  // hit
+  float trap;
+  int iters;
+  // normal taps
+  int tap;
+  double gx, gy, gz;
+  // shadow
+  double nx, ny, nz, st, res;
+  int sstep;
+  uint32_t evals;
+  bool was_hit;
+  uint32_t ev_march, ev_normal, ev_shadow;
+
+  ND_DEV_INLINE void start(const DevView& v, int64_t it, int vidx) {
+    item = it;
+    view = vidx;
+    dir = ray_dir(v, it - v.ray_offset);
+    phase = PH_MARCH;
+    t = lo = hi = 0.0;
+    i = n = refines = 0;
+    probing = true;
+    bisecting = resolved = false;
+    trap = 0.0f;
+    iters = 0;
+    evals = 0;
+  }
+
+  ND_DEV_INLINE D3 hit_pos(const DevView& v) const {
+    return fmadd(d3(v.org[0], v.org[1], v.org[2]), dir, t);
+  }
+
+  // Position of this lane's next DE sample.
+  ND_DEV_INLINE D3 sample_pos(const DevView& v) const {
+    const D3 o = d3(v.org[0], v.org[1], v.org[2]);
+    if (phase == PH_MARCH) return fmadd(o, dir, probing ? t : 0.5 * (lo + hi));
+    const D3 p = fmadd(o, dir, t);
+    if (phase == PH_NORMAL) {
+      if (v.normal_mode == ND_NORMAL_CENTRAL) {
+        const double h = v.normal_h_coef > 0.0f ? double(v.normal_h_coef) * t : march_eps<T>(v, t);
+        const double s = (tap & 1) ? -h : h;
+        const int a = tap >> 1;
+        return d3(p.x + (a == 0 ? s : 0.0), p.y + (a == 1 ? s : 0.0), p.z + (a == 2 ? s : 0.0));
+      }
+      const double e = march_eps<T>(v, t);
+      return fmadd(p, tetra_k(tap), e);
+    }
+    // PH_SHADOW: origin = hit + n * bias, then along the light direction
+    const D3 so = fmadd(p, d3(nx, ny, nz), kShadowBias);
+    return fmadd(so, d3(v.light[0], v.light[1], v.light[2]), st);
+  }
+
+  ND_DEV_INLINE int normal_taps(const DevView& v) const {
+    return v.normal_mode == ND_NORMAL_CENTRAL ? 6 : 4;
+  }
+
+  ND_DEV_INLINE void finish(const DevView& v, const nd_gbuffer& g, bool hit, float vis, Stats* ls) {
+    RayResult r;
+    r.hit = hit;
+    r.t = t;
+    r.trap = hit ? trap : 0.0f;
+    r.iters = hit ? uint32_t(iters) : 0u;
+    r.steps = hit ? uint32_t(i) : uint32_t(v.max_steps);
+    r.evals = evals;
+    r.nx = hit ? float(nx) : 0.0f;
+    r.ny = hit ? float(ny) : 0.0f;
+    r.nz = hit ? float(nz) : 0.0f;
+    r.shadow = vis;
+    r.shade = hit ? lambert(v, dir, nx, ny, nz, vis) : 0.0f;
+    write_result(g, v.out_offset + (item - v.ray_offset), r);
+    was_hit = hit;
+    phase = PH_DONE;
+  }
+
+  // Enter the normal phase at hit distance t with the hit's DE output.
+  ND_DEV_INLINE void record_hit(const DEOut<T>& de) {
+    trap = float(de.trap);
+    iters = de.iters;
+  }
+
+  ND_DEV_INLINE void begin_normal() {
+    phase = PH_NORMAL;
+    tap = 0;
+    gx = gy = gz = 0.0;
+  }
+
+  // Consume one DE result.  Returns nothing; sets phase = PH_DONE when the ray is
+  // finished (its outputs are then written).
+  ND_DEV_INLINE void advance(const DevView& v, const DEOut<T>& de, const nd_gbuffer& g, Stats* ls) {
+    ++evals;
+    const double d = double(de.d);
+    if (phase == PH_MARCH) {
+      ++ev_march;
+      // one iteration of march_to's sample loop (tpl:1881-1960)
+      const int budget = v.refine;
+      const bool on_hit = v.verify == 0;
+      const int refine_budget = on_hit ? 0 : budget;
+      const int bisect_budget = on_hit ? budget : 0;
+      const double st = probing ? t : 0.5 * (lo + hi);
+      const double e = march_eps<T>(v, st);
+      ++n;
+      if (bisecting) {
+        if (d < e) {
+          hi = st;
+          record_hit(de);
+        } else {
+          lo = st;
+        }
+        ++refines;
+        if (hi - lo <= e || refines >= bisect_budget) {
+          t = hi;
+          begin_normal();
+        } else if (n >= v.max_samples) {
+          finish(v, g, false, 1.0f, ls);  // the loop of march_to ran out: a miss
+        }
+        return;
+      }
+      if (d < e) {
+        record_hit(de);
+        if (on_hit && bisect_budget > 0 && st - lo > e) {
+          bisecting = true;
+          probing = false;
+          hi = st;
+          refines = 0;
+          if (n >= v.max_samples) finish(v, g, false, 1.0f, ls);
+          return;
+        }
+        t = st;
+        begin_normal();
+        return;
+      }
+      if (probing) {
+        lo = t;
+        hi = t + d;
+        refines = 0;
+        resolved = false;
+        probing = false;
+      } else {
+        if (d >= hi - st) resolved = true;
+        else hi = st;
+        ++refines;
+      }
+      if (resolved || refines >= refine_budget) {
+        if (v.hq && !resolved && refine_budget > 0) hi = fmin(hi, lo + fmax(t, 1.0) * v.footprint);
+        t = hi;
+        ++i;
+        if (t > v.max_dist || i >= v.max_steps) {
+          finish(v, g, false, 1.0f, ls);
+          return;
+        }
+        probing = true;
+      }
+      if (n >= v.max_samples) finish(v, g, false, 1.0f, ls);
+      return;
+    }
+    if (phase == PH_NORMAL) {
+      ++ev_normal;
+      if (v.normal_mode == ND_NORMAL_CENTRAL) {
+        const double s = (tap & 1) ? -d : d;
+        const int a = tap >> 1;
+        if (a == 0) gx += s;
+        else if (a == 1) gy += s;
+        else gz += s;
+      } else {
+        const D3 k = tetra_k(tap);
+        gx += k.x * d;
+        gy += k.y * d;
+        gz += k.z * d;
+      }
+      ++tap;
+      if (tap < normal_taps(v)) return;
+      const double l = sqrt(gx * gx + gy * gy + gz * gz);
+      const double inv = l > 0.0 ? 1.0 / l : 0.0;
+      nx = gx * inv;
+      ny = gy * inv;
+      nz = gz * inv;
+      if (!v.shadow) {
+        finish(v, g, true, 1.0f, ls);
+        return;
+      }
+      phase = PH_SHADOW;
+      st = kShadowBias;
+      res = 1.0;
+      sstep = 0;
+      const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
+      if (steps <= 0 || st >= 2.0 * v.max_dist) finish(v, g, true, 1.0f, ls);
+      return;
+    }
+    // PH_SHADOW: one step of visibility_march (tpl:2294-2341), opaque scene
+    ++ev_shadow;
+    if (d < kShadowHitEps) {
+      finish(v, g, true, 0.0f, ls);
+      return;
+    }
+    res = fmin(res, double(v.shadow_k) * d / st);
+    st += fmax(d, kShadowMinStep);
+    ++sstep;
+    const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
+    if (sstep >= steps || st >= 2.0 * v.max_dist) finish(v, g, true, float(fmin(fmax(res, 0.0), 1.0)), ls);
+  }
+};
+
+}  // namespace nd

@@ -1,0 +1,737 @@
+// C-ABI implementation (include/nd_march.h): formula registry, contexts, view
+// validation, launch planning, statistics, autotuning and CUDA-graph capture.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "nd_registry.h"
+#include "nd_view.h"
+
+using nd::DevView;
+using nd::make_dev_view;
+using nd::KernelTable;
+using nd::LaunchArgs;
+using nd::LaunchConfig;
+using nd::LaunchFn;
+using nd::Stats;
+
+namespace {
+
+constexpr int kMaxViews = 1 << 16;
+constexpr int64_t kMaxRays = int64_t(1) << 40;
+
+const char* kStatusNames[] = {"ND_OK",          "ND_ERR_INVALID", "ND_ERR_COMPILE",     "ND_ERR_OOM",
+                              "ND_ERR_TIMEOUT", "ND_ERR_CUDA",    "ND_ERR_UNSUPPORTED", "ND_ERR_NOT_FOUND"};
+
+uint64_t fnv1a64(const char* s, size_t n) {
+  uint64_t h = 0xCBF29CE484222325ull;
+  for (size_t i = 0; i < n; ++i) {
+    h ^= uint8_t(s[i]);
+    h *= 0x100000001B3ull;
+  }
+  return h;
+}
+
+void copy_str(char* out, size_t out_len, const std::string& s) {
+  if (!out || out_len == 0) return;
+  const size_t n = std::min(out_len - 1, s.size());
+  memcpy(out, s.data(), n);
+  out[n] = 0;
+}
+
+// Per-(formula set) tuned launch parameters, filled by nd_autotune.
+struct Tuned {
+  int kernel = ND_KERNEL_PERSISTENT;
+  int blocks_per_sm = 0;
+  int refill_threshold = 8;
+};
+std::mutex g_tune_mu;
+std::map<std::string, Tuned> g_tuned;
+
+}  // namespace
+
+struct nd_ctx {
+  int device = 0;
+  int num_sms = 0;
+  std::string err;
+  DevView* d_views = nullptr;
+  int views_cap = 0;
+  unsigned long long* d_counters = nullptr;
+  int counters_cap = 0;
+  Stats* d_stats = nullptr;
+  DevView* h_views = nullptr;  // pinned staging
+  int h_views_cap = 0;
+  cudaStream_t last_stream = nullptr;
+  cudaEvent_t last_done = nullptr;
+  bool have_last = false;
+  int last_kernel = 0;
+  int64_t last_rays = 0;
+};
+
+struct nd_graph {
+  nd_ctx* ctx = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  DevView* d_views = nullptr;
+  unsigned long long* d_counters = nullptr;
+};
+
+namespace {
+
+nd_status fail(nd_ctx* ctx, nd_status s, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    ctx->err = buf;
+  }
+  return s;
+}
+
+nd_status cuda_fail(nd_ctx* ctx, cudaError_t e, const char* what) {
+  const nd_status s = (e == cudaErrorMemoryAllocation) ? ND_ERR_OOM : ND_ERR_CUDA;
+  return fail(ctx, s, "%s: %s", what, cudaGetErrorString(e));
+}
+
+bool finite(double x) { return x == x && x < 1e300 && x > -1e300; }
+
+nd_status validate_view(nd_ctx* ctx, const nd_view_desc& v, int idx) {
+  if (v.formula < 0 || v.formula >= nd_formula_entry_count)
+    return fail(ctx, ND_ERR_NOT_FOUND, "view %d: unknown formula id %d", idx, v.formula);
+  if (v.width <= 0 || v.height <= 0 || v.tile_w < 0 || v.tile_h < 0 || v.tile_x < 0 || v.tile_y < 0 ||
+      int64_t(v.tile_x) + v.tile_w > v.width || int64_t(v.tile_y) + v.tile_h > v.height)
+    return fail(ctx, ND_ERR_INVALID, "view %d: bad frame %dx%d / tile (%d,%d %dx%d)", idx, v.width, v.height,
+                v.tile_x, v.tile_y, v.tile_w, v.tile_h);
+  if (v.spp < 1 || v.spp > 4096) return fail(ctx, ND_ERR_INVALID, "view %d: spp %d out of [1, 4096]", idx, v.spp);
+  if (v.max_steps < 0 || v.max_steps > (1 << 20))
+    return fail(ctx, ND_ERR_INVALID, "view %d: max_steps %d out of range", idx, v.max_steps);
+  if (v.refine_budget < 0 || v.refine_budget > 4096)
+    return fail(ctx, ND_ERR_INVALID, "view %d: refine_budget %d out of range", idx, v.refine_budget);
+  for (int i = 0; i < 3; ++i)
+    if (!finite(v.cam_pos[i]) || !finite(v.fwd[i]) || !finite(v.right[i]) || !finite(v.up[i]))
+      return fail(ctx, ND_ERR_INVALID, "view %d: non-finite camera", idx);
+  for (int i = 0; i < ND_MAX_PARAMS; ++i)
+    if (!finite(v.params[i])) return fail(ctx, ND_ERR_INVALID, "view %d: param %d is not finite", idx, i);
+  if (!(v.max_dist > 0) || !finite(v.max_dist) || !finite(v.eps_coef) || !finite(v.eps_floor))
+    return fail(ctx, ND_ERR_INVALID, "view %d: bad max_dist/epsilon", idx);
+  if (v.normal_mode != ND_NORMAL_TETRA && v.normal_mode != ND_NORMAL_CENTRAL)
+    return fail(ctx, ND_ERR_INVALID, "view %d: bad normal_mode %d", idx, v.normal_mode);
+  if (v.shadow) {
+    const double l2 = double(v.light_dir[0]) * v.light_dir[0] + double(v.light_dir[1]) * v.light_dir[1] +
+                      double(v.light_dir[2]) * v.light_dir[2];
+    if (!(l2 > 0) || !finite(l2)) return fail(ctx, ND_ERR_INVALID, "view %d: shadow needs a light direction", idx);
+  }
+  return ND_OK;
+}
+
+template <class T> nd_status ensure_dev(nd_ctx* ctx, T** p, int* cap, int need, const char* what) {
+  if (*cap >= need) return ND_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  const int n = std::max(need, 64);
+  cudaError_t e = cudaMalloc((void**)p, sizeof(T) * size_t(n));
+  if (e != cudaSuccess) return cuda_fail(ctx, e, what);
+  *cap = n;
+  return ND_OK;
+}
+
+// A launch plan: one or more launches, each over a subset of the views with one
+// kernel table.
+struct Launch {
+  KernelTable table;
+  std::vector<int> views;  // indices into the caller's array
+  std::vector<int> codes;  // formula code of each view inside the table's set
+  int64_t rays = 0;
+  std::string key;         // tuning key
+};
+
+std::string set_key(const std::vector<int>& formulas) {
+  std::string k;
+  for (int f : formulas) {
+    k += nd_formula_entries[f].name;
+    k += "+";
+  }
+  return k;
+}
+
+nd_status plan(nd_ctx* ctx, const nd_view_desc* views, int nviews, std::vector<Launch>* out) {
+  std::vector<int> distinct;
+  for (int i = 0; i < nviews; ++i)
+    if (std::find(distinct.begin(), distinct.end(), views[i].formula) == distinct.end())
+      distinct.push_back(views[i].formula);
+  out->clear();
+  if (distinct.size() == 1) {
+    Launch L;
+    L.table = nd_formula_entries[distinct[0]].kernels();
+    for (int i = 0; i < nviews; ++i) {
+      L.views.push_back(i);
+      L.codes.push_back(0);
+    }
+    L.key = set_key(distinct);
+    out->push_back(L);
+    return ND_OK;
+  }
+  // one launch when a compiled group covers every formula of the batch
+  for (int g = 0; g < nd_group_entry_count; ++g) {
+    const nd::GroupEntry& G = nd_group_entries[g];
+    bool covers = true;
+    for (int f : distinct) {
+      bool in = false;
+      for (int m = 0; m < G.count; ++m) in |= G.members[m] == f;
+      covers &= in;
+    }
+    if (!covers) continue;
+    Launch L;
+    L.table = G.kernels();
+    // order the views by formula code so that warps stay formula-uniform
+    std::vector<int> order(nviews);
+    for (int i = 0; i < nviews; ++i) order[i] = i;
+    auto code_of = [&](int vi) {
+      for (int m = 0; m < G.count; ++m)
+        if (G.members[m] == views[vi].formula) return m;
+      return 0;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return code_of(a) < code_of(b); });
+    for (int vi : order) {
+      L.views.push_back(vi);
+      L.codes.push_back(code_of(vi));
+    }
+    L.key = std::string("group:") + G.name;
+    out->push_back(L);
+    return ND_OK;
+  }
+  // otherwise one launch per formula
+  for (int f : distinct) {
+    Launch L;
+    L.table = nd_formula_entries[f].kernels();
+    for (int i = 0; i < nviews; ++i)
+      if (views[i].formula == f) {
+        L.views.push_back(i);
+        L.codes.push_back(0);
+      }
+    L.key = set_key({f});
+    out->push_back(L);
+  }
+  return ND_OK;
+}
+
+LaunchFn pick(const KernelTable& t, int kernel, int prec, bool batched) {
+  if (prec == 64) {
+    if (kernel == ND_KERNEL_PLAIN) return batched ? t.plain_f64_batched : t.plain_f64;
+    return batched ? t.persistent_f64_batched : t.persistent_f64;
+  }
+  if (kernel == ND_KERNEL_PLAIN) return batched ? t.plain_f32_batched : t.plain_f32;
+  return batched ? t.persistent_f32_batched : t.persistent_f32;
+}
+
+Tuned tuned_for(const std::string& key) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tuned.find(key);
+  return it == g_tuned.end() ? Tuned() : it->second;
+}
+
+// Enqueue every launch of a forward call.  d_views / d_counters are device
+// buffers with room for nviews views and plans.size() counters; h_views is host
+// staging (pinned when owned by the context).  When views_ready is true the view
+// table is already on the device (graph replay).
+nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_march_opts* opts,
+                  const nd_gbuffer* out, cudaStream_t stream, const std::vector<Launch>& plans, DevView* d_views,
+                  DevView* h_views, unsigned long long* d_counters, bool copy_views, int* kernel_used) {
+  const int prec = (opts && opts->de_precision == 64) ? 64 : 32;
+  // global output offsets in call order
+  std::vector<int64_t> out_off(nviews + 1, 0);
+  for (int i = 0; i < nviews; ++i) out_off[i + 1] = out_off[i] + int64_t(views[i].spp) * views[i].tile_w * views[i].tile_h;
+  int base = 0;
+  for (size_t p = 0; p < plans.size(); ++p) {
+    const Launch& L = plans[p];
+    int64_t off = 0;
+    for (size_t k = 0; k < L.views.size(); ++k) {
+      const int vi = L.views[k];
+      h_views[base + k] = make_dev_view(views[vi], off, out_off[vi], L.codes[k]);
+      off += h_views[base + k].rays;
+    }
+    base += int(L.views.size());
+  }
+  if (copy_views && base > 0) {
+    cudaError_t e = cudaMemcpyAsync(d_views, h_views, sizeof(DevView) * size_t(base), cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy view table");
+  }
+  cudaError_t e = cudaMemsetAsync(ctx->d_stats, 0, sizeof(Stats), stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "clear stats");
+  e = cudaMemsetAsync(d_counters, 0, sizeof(unsigned long long) * plans.size(), stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "clear work counters");
+  base = 0;
+  int used = 0;
+  for (size_t p = 0; p < plans.size(); ++p) {
+    const Launch& L = plans[p];
+    const int nv = int(L.views.size());
+    int64_t rays = 0;
+    for (int k = 0; k < nv; ++k) rays += h_views[base + k].rays;
+    if (rays > 0) {
+      const Tuned tu = tuned_for(L.key);
+      int kernel = opts && opts->kernel ? opts->kernel : tu.kernel;
+      LaunchArgs a;
+      memset(&a, 0, sizeof(a));
+      a.views = d_views + base;
+      a.nviews = nv;
+      a.total_rays = rays;
+      a.out = *out;
+      a.counter = d_counters + p;
+      a.stats = ctx->d_stats;
+      a.refill_threshold = std::max(1, std::min(32, opts && opts->refill_threshold ? opts->refill_threshold : tu.refill_threshold));
+      const int wd = opts && opts->watchdog_ms > 0 ? opts->watchdog_ms : 10000;
+      a.deadline_ns = int64_t(wd) * 1000000;
+      LaunchConfig c;
+      c.kernel = kernel;
+      c.block = 128;
+      c.blocks_per_sm = opts && opts->blocks_per_sm ? opts->blocks_per_sm : tu.blocks_per_sm;
+      c.num_sms = ctx->num_sms;
+      const bool batched = nv > 1;
+      LaunchFn fn = pick(L.table, kernel, prec, batched);
+      e = fn(a, h_views[base], c, stream);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+      used = kernel;
+    }
+    base += nv;
+  }
+  if (kernel_used) *kernel_used = used;
+  return ND_OK;
+}
+
+nd_status prepare(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_gbuffer* out,
+                  std::vector<Launch>* plans, int64_t* total) {
+  if (!ctx) return ND_ERR_INVALID;
+  if (!views || nviews <= 0 || nviews > kMaxViews) return fail(ctx, ND_ERR_INVALID, "nviews %d out of range", nviews);
+  if (!out || !out->depth) return fail(ctx, ND_ERR_INVALID, "the G-buffer needs at least a depth pointer");
+  if ((out->normal && (uintptr_t(out->normal) & 15)) || (out->depth64 && (uintptr_t(out->depth64) & 7)) ||
+      (uintptr_t(out->depth) & 3))
+    return fail(ctx, ND_ERR_INVALID, "misaligned G-buffer pointer (normal needs 16 bytes)");
+  int64_t t = 0;
+  for (int i = 0; i < nviews; ++i) {
+    nd_status s = validate_view(ctx, views[i], i);
+    if (s != ND_OK) return s;
+    t += int64_t(views[i].spp) * views[i].tile_w * views[i].tile_h;
+    if (t > kMaxRays) return fail(ctx, ND_ERR_INVALID, "too many rays in one call");
+  }
+  *total = t;
+  return plan(ctx, views, nviews, plans);
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t nd_abi_version(void) { return ND_ABI_VERSION; }
+
+const char* nd_status_string(nd_status s) {
+  if (s < 0 || s > 7) return "ND_ERR_UNKNOWN";
+  return kStatusNames[s];
+}
+
+nd_status nd_formula_count(int32_t* n) {
+  if (!n) return ND_ERR_INVALID;
+  *n = nd_formula_entry_count;
+  return ND_OK;
+}
+
+nd_status nd_formula_find(const char* name, nd_formula_id* out) {
+  if (!name || !out) return ND_ERR_INVALID;
+  for (int i = 0; i < nd_formula_entry_count; ++i)
+    if (strcmp(nd_formula_entries[i].name, name) == 0) {
+      *out = i;
+      return ND_OK;
+    }
+  return ND_ERR_NOT_FOUND;
+}
+
+nd_status nd_formula_name(nd_formula_id id, char* out, size_t out_len) {
+  if (id < 0 || id >= nd_formula_entry_count) return ND_ERR_NOT_FOUND;
+  if (!out || out_len == 0) return ND_ERR_INVALID;
+  copy_str(out, out_len, nd_formula_entries[id].name);
+  return ND_OK;
+}
+
+// The reference compiles a formula source into the scene's shader module and
+// reports errors into FormulaState.formula_error (formula.zig:73-77, 170-181).
+// Here sources are compiled at build time; registering a source checks the
+// contract functions like missingContractFn and then finds the compiled code by
+// the source hash (CodeTable.find, fractal_renderer.zig:585-590).
+nd_status nd_formula_register(const char* src, size_t len, nd_formula_id* out, char* err, size_t err_len) {
+  if (!src || !out) {
+    copy_str(err, err_len, "null argument");
+    return ND_ERR_INVALID;
+  }
+  const std::string s(src, len);
+  const char* missing = nullptr;
+  if (s.find("fn de_step(") == std::string::npos)
+    missing = "fn de_step(carry: IterCarry, pos: vec3f, p: Params) -> IterCarry";
+  else if (s.find("fn de_finalize(") == std::string::npos)
+    missing = "fn de_finalize(carry: IterCarry) -> f32";
+  else if (s.find("fn de_iterations(") == std::string::npos)
+    missing = "fn de_iterations(p: Params) -> i32";
+  if (missing) {
+    copy_str(err, err_len, std::string("missing: ") + missing);
+    return ND_ERR_COMPILE;
+  }
+  const uint64_t h = fnv1a64(src, len);
+  for (int i = 0; i < nd_formula_entry_count; ++i)
+    if (nd_formula_entries[i].source_hash == h) {
+      *out = i;
+      copy_str(err, err_len, "");
+      return ND_OK;
+    }
+  copy_str(err, err_len,
+           "formula source is not compiled into this build: add the file to the build's formula directory "
+           "(ND_FORMULA_DIRS) and rebuild");
+  return ND_ERR_COMPILE;
+}
+
+nd_status nd_formula_params(nd_formula_id id, nd_param_info* out, int32_t* n) {
+  if (id < 0 || id >= nd_formula_entry_count) return ND_ERR_NOT_FOUND;
+  if (!n) return ND_ERR_INVALID;
+  const nd::FormulaEntry& f = nd_formula_entries[id];
+  if (out) {
+    for (int i = 0; i < f.nparams; ++i) {
+      memset(&out[i], 0, sizeof(nd_param_info));
+      copy_str(out[i].name, ND_PARAM_NAME_LEN, f.params[i].name);
+      out[i].min_value = f.params[i].min_value;
+      out[i].max_value = f.params[i].max_value;
+      out[i].default_value = f.params[i].default_value;
+      out[i].integral = f.params[i].integral;
+    }
+  }
+  *n = f.nparams;
+  return ND_OK;
+}
+
+// Defaults of the reference's render settings (render_precision.zig:3-30,
+// scene_state.zig:192-210) with the formula's @param defaults packed in.
+nd_status nd_view_defaults(nd_formula_id id, nd_view_desc* v) {
+  if (id < 0 || id >= nd_formula_entry_count) return ND_ERR_NOT_FOUND;
+  if (!v) return ND_ERR_INVALID;
+  memset(v, 0, sizeof(*v));
+  v->cam_pos[2] = -3.0;
+  v->fwd[2] = 1.0;
+  v->right[0] = 1.0;
+  v->up[1] = 1.0;
+  v->width = v->height = v->tile_w = v->tile_h = 256;
+  v->formula = id;
+  v->spp = 1;
+  const nd::FormulaEntry& f = nd_formula_entries[id];
+  for (int i = 0; i < f.nparams; ++i) v->params[i] = f.params[i].default_value;
+  v->trap.shape = ND_TRAP_POINT;
+  v->trap.mode = ND_TRAP_MIN;
+  v->trap.radius = 1.0f;
+  v->trap.box[0] = v->trap.box[1] = v->trap.box[2] = 1.0f;
+  v->trap.span = 1.5f;
+  v->max_steps = 256;
+  v->max_dist = 24.0f;
+  v->eps_coef = 5e-4f;
+  v->eps_floor = 5e-5f;
+  v->refine_budget = 4;
+  v->hq_footprint_px = 2.0f;
+  v->normal_mode = ND_NORMAL_TETRA;
+  v->shadow_k = 16.0f;
+  v->step_safety = 1.0f;
+  return ND_OK;
+}
+
+nd_status nd_ctx_create(int32_t device, nd_ctx** out) {
+  if (!out) return ND_ERR_INVALID;
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) return ND_ERR_CUDA;
+  if (device < 0 || device >= count) return ND_ERR_INVALID;
+  nd_ctx* ctx = new nd_ctx();
+  ctx->device = device;
+  e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_stats, sizeof(Stats));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_stats, 0, sizeof(Stats));
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->last_done, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    nd_ctx_destroy(ctx);
+    return e == cudaErrorMemoryAllocation ? ND_ERR_OOM : ND_ERR_CUDA;
+  }
+  *out = ctx;
+  return ND_OK;
+}
+
+nd_status nd_ctx_destroy(nd_ctx* ctx) {
+  if (!ctx) return ND_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->have_last) cudaEventSynchronize(ctx->last_done);
+  if (ctx->d_views) cudaFree(ctx->d_views);
+  if (ctx->d_counters) cudaFree(ctx->d_counters);
+  if (ctx->d_stats) cudaFree(ctx->d_stats);
+  if (ctx->h_views) cudaFreeHost(ctx->h_views);
+  if (ctx->last_done) cudaEventDestroy(ctx->last_done);
+  delete ctx;
+  return ND_OK;
+}
+
+nd_status nd_last_error(const nd_ctx* ctx, char* out, size_t out_len) {
+  if (!ctx) return ND_ERR_INVALID;
+  copy_str(out, out_len, ctx->err);
+  return ND_OK;
+}
+
+nd_status nd_count_rays(const nd_view_desc* views, int32_t nviews, int64_t* total) {
+  if (!views || !total || nviews < 0) return ND_ERR_INVALID;
+  int64_t t = 0;
+  for (int i = 0; i < nviews; ++i) {
+    if (views[i].spp < 0 || views[i].tile_w < 0 || views[i].tile_h < 0) return ND_ERR_INVALID;
+    t += int64_t(views[i].spp) * views[i].tile_w * views[i].tile_h;
+  }
+  *total = t;
+  return ND_OK;
+}
+
+nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_march_opts* opts,
+                           const nd_gbuffer* out, void* stream) {
+  std::vector<Launch> plans;
+  int64_t total = 0;
+  nd_status s = prepare(ctx, views, nviews, out, &plans, &total);
+  if (s != ND_OK) return s;
+  if (opts && opts->de_precision != 0 && opts->de_precision != 32 && opts->de_precision != 64)
+    return fail(ctx, ND_ERR_INVALID, "de_precision must be 32 or 64");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
+  cudaStream_t st = (cudaStream_t)stream;
+  // the staging buffer may still feed an earlier copy: wait for the last call
+  if (ctx->have_last) cudaEventSynchronize(ctx->last_done);
+  if ((s = ensure_dev(ctx, &ctx->d_views, &ctx->views_cap, nviews, "view table")) != ND_OK) return s;
+  if ((s = ensure_dev(ctx, &ctx->d_counters, &ctx->counters_cap, int(plans.size()), "work counters")) != ND_OK) return s;
+  if (ctx->h_views_cap < nviews) {
+    if (ctx->h_views) cudaFreeHost(ctx->h_views);
+    ctx->h_views = nullptr;
+    ctx->h_views_cap = 0;
+    e = cudaMallocHost((void**)&ctx->h_views, sizeof(DevView) * size_t(std::max(nviews, 64)));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "pinned view staging");
+    ctx->h_views_cap = std::max(nviews, 64);
+  }
+  int kernel = 0;
+  s = enqueue(ctx, views, nviews, opts, out, st, plans, ctx->d_views, ctx->h_views, ctx->d_counters, true, &kernel);
+  if (s != ND_OK) return s;
+  e = cudaEventRecord(ctx->last_done, st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "record event");
+  ctx->have_last = true;
+  ctx->last_stream = st;
+  ctx->last_kernel = kernel;
+  ctx->last_rays = total;
+  return ND_OK;
+}
+
+nd_status nd_last_stats(nd_ctx* ctx, nd_stats* out) {
+  if (!ctx || !out) return ND_ERR_INVALID;
+  memset(out, 0, sizeof(*out));
+  cudaSetDevice(ctx->device);
+  if (ctx->have_last) {
+    cudaError_t e = cudaEventSynchronize(ctx->last_done);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "synchronise");
+  }
+  Stats h;
+  cudaError_t e = cudaMemcpy(&h, ctx->d_stats, sizeof(Stats), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "read stats");
+  out->rays = h.rays;
+  out->de_evals = h.de_evals;
+  out->march_evals = h.march_evals;
+  out->normal_evals = h.normal_evals;
+  out->shadow_evals = h.shadow_evals;
+  out->hits = h.hits;
+  out->refills = h.refills;
+  out->timeouts = h.timeouts;
+  out->kernel = uint32_t(ctx->last_kernel);
+  if (h.timeouts) return fail(ctx, ND_ERR_TIMEOUT, "the device watchdog stopped %u warps", h.timeouts);
+  return ND_OK;
+}
+
+// Times every candidate launch configuration on the given views (writing into
+// scratch_out) and keeps the fastest for this formula set.
+nd_status nd_autotune(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_gbuffer* scratch_out,
+                      nd_tune_result* result) {
+  std::vector<Launch> plans;
+  int64_t total = 0;
+  nd_status s = prepare(ctx, views, nviews, scratch_out, &plans, &total);
+  if (s != ND_OK) return s;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st;
+  cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "stream");
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  struct Cand {
+    int kernel, per_sm, thr;
+  };
+  std::vector<Cand> cands;
+  cands.push_back({ND_KERNEL_PLAIN, 0, 1});
+  for (int per_sm : {0, 4, 8})
+    for (int thr : {1, 4, 8, 16, 24})
+      cands.push_back({ND_KERNEL_PERSISTENT, per_sm, thr});
+  double best = 1e30;
+  Cand bc = cands[1];
+  for (const Cand& c : cands) {
+    nd_march_opts o;
+    memset(&o, 0, sizeof(o));
+    o.kernel = c.kernel;
+    o.blocks_per_sm = c.per_sm;
+    o.refill_threshold = c.thr;
+    float ms = 0;
+    s = nd_march_forward(ctx, views, nviews, &o, scratch_out, st);  // warm-up
+    if (s != ND_OK) break;
+    cudaEventRecord(a, st);
+    s = nd_march_forward(ctx, views, nviews, &o, scratch_out, st);
+    if (s != ND_OK) break;
+    cudaEventRecord(b, st);
+    e = cudaEventSynchronize(b);
+    if (e != cudaSuccess) {
+      s = cuda_fail(ctx, e, "autotune run");
+      break;
+    }
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms < best) {
+      best = ms;
+      bc = c;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaStreamDestroy(st);
+  if (s != ND_OK) return s;
+  Tuned t;
+  t.kernel = bc.kernel;
+  t.blocks_per_sm = bc.per_sm;
+  t.refill_threshold = bc.thr;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (const Launch& L : plans) g_tuned[L.key] = t;
+  }
+  if (result) {
+    result->kernel = t.kernel;
+    result->block = 128;
+    result->blocks_per_sm = t.blocks_per_sm;
+    result->refill_threshold = t.refill_threshold;
+    result->rays_per_s = best > 0 ? double(total) / (best * 1e-3) : 0.0;
+  }
+  return ND_OK;
+}
+
+// Captures one forward call (work-counter and stats resets plus every launch)
+// into a CUDA graph.  The graph owns a device copy of the view table, so it can
+// be replayed while the caller changes its own descriptors.
+nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_march_opts* opts,
+                           const nd_gbuffer* out, void* stream, nd_graph** graph) {
+  if (!graph) return ND_ERR_INVALID;
+  *graph = nullptr;
+  std::vector<Launch> plans;
+  int64_t total = 0;
+  nd_status s = prepare(ctx, views, nviews, out, &plans, &total);
+  if (s != ND_OK) return s;
+  cudaSetDevice(ctx->device);
+  nd_graph* g = new nd_graph();
+  g->ctx = ctx;
+  cudaError_t e = cudaMalloc((void**)&g->d_views, sizeof(DevView) * size_t(nviews));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_counters, sizeof(unsigned long long) * plans.size());
+  if (e != cudaSuccess) {
+    nd_graph_destroy(g);
+    return cuda_fail(ctx, e, "graph buffers");
+  }
+  std::vector<DevView> hv(nviews);
+  // fill the host table (enqueue builds it) without launching: capture does both
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaStream_t cap;
+  e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    nd_graph_destroy(g);
+    return cuda_fail(ctx, e, "capture stream");
+  }
+  e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(cap);
+    nd_graph_destroy(g);
+    return cuda_fail(ctx, e, "begin capture");
+  }
+  s = enqueue(ctx, views, nviews, opts, out, cap, plans, g->d_views, hv.data(), g->d_counters, false, nullptr);
+  cudaGraph_t gr = nullptr;
+  e = cudaStreamEndCapture(cap, &gr);
+  cudaStreamDestroy(cap);
+  if (s != ND_OK || e != cudaSuccess) {
+    if (gr) cudaGraphDestroy(gr);
+    nd_graph_destroy(g);
+    return s != ND_OK ? s : cuda_fail(ctx, e, "end capture");
+  }
+  g->graph = gr;
+  e = cudaMemcpy(g->d_views, hv.data(), sizeof(DevView) * size_t(nviews), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, gr, 0);
+  if (e != cudaSuccess) {
+    nd_graph_destroy(g);
+    return cuda_fail(ctx, e, "instantiate graph");
+  }
+  (void)st;
+  *graph = g;
+  return ND_OK;
+}
+
+nd_status nd_graph_launch(nd_graph* g, void* stream) {
+  if (!g || !g->exec) return ND_ERR_INVALID;
+  cudaSetDevice(g->ctx->device);
+  cudaError_t e = cudaGraphLaunch(g->exec, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(g->ctx, e, "graph launch");
+  e = cudaEventRecord(g->ctx->last_done, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(g->ctx, e, "record event");
+  g->ctx->have_last = true;
+  return ND_OK;
+}
+
+nd_status nd_graph_destroy(nd_graph* g) {
+  if (!g) return ND_ERR_INVALID;
+  if (g->ctx) cudaSetDevice(g->ctx->device);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  if (g->d_views) cudaFree(g->d_views);
+  if (g->d_counters) cudaFree(g->d_counters);
+  delete g;
+  return ND_OK;
+}
+
+nd_status nd_de_points(nd_ctx* ctx, const nd_view_desc* view, int64_t n, const double* pts, double* de,
+                       double* trap, uint32_t* iters, int32_t de_precision, void* stream) {
+  if (!ctx || !view || n < 0 || (n > 0 && (!pts || !de))) return fail(ctx, ND_ERR_INVALID, "bad nd_de_points arguments");
+  if (view->formula < 0 || view->formula >= nd_formula_entry_count)
+    return fail(ctx, ND_ERR_NOT_FOUND, "unknown formula id %d", view->formula);
+  cudaSetDevice(ctx->device);
+  const DevView v = make_dev_view(*view, 0, 0, 0);
+  const KernelTable t = nd_formula_entries[view->formula].kernels();
+  const nd::DePointsFn fn = de_precision == 64 ? t.de_points_f64 : t.de_points_f32;
+  cudaError_t e = fn(v, n, pts, de, trap, iters, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "nd_de_points launch");
+  return ND_OK;
+}
+
+// Layout check for bindings: sizes of the public structs.
+size_t nd_sizeof(const char* name) {
+  if (!name) return 0;
+  const std::string n(name);
+  if (n == "nd_view_desc") return sizeof(nd_view_desc);
+  if (n == "nd_trap_desc") return sizeof(nd_trap_desc);
+  if (n == "nd_gbuffer") return sizeof(nd_gbuffer);
+  if (n == "nd_march_opts") return sizeof(nd_march_opts);
+  if (n == "nd_stats") return sizeof(nd_stats);
+  if (n == "nd_param_info") return sizeof(nd_param_info);
+  if (n == "nd_tune_result") return sizeof(nd_tune_result);
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,66 @@
+// Host-side construction of the kernels' per-view record from nd_view_desc.
+#pragma once
+
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+
+#include "nd_rayprog.h"
+
+namespace nd {
+
+inline DevView make_dev_view(const nd_view_desc& v, int64_t ray_offset, int64_t out_offset, int code) {
+  DevView d;
+  memset(&d, 0, sizeof(d));
+  auto unit = [](const double* a, double* out) {
+    const double n = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    for (int i = 0; i < 3; ++i) out[i] = n > 0 ? a[i] / n : 0.0;
+  };
+  for (int i = 0; i < 3; ++i) {
+    d.org[i] = v.cam_pos[i];
+    d.fwd[i] = v.fwd[i];
+    d.right[i] = v.right[i];
+    d.up[i] = v.up[i];
+  }
+  unit(v.right, d.uright);
+  unit(v.up, d.uup);
+  const double l[3] = {v.light_dir[0], v.light_dir[1], v.light_dir[2]};
+  unit(l, d.light);
+  d.use_light = (v.shadow || (l[0] * l[0] + l[1] * l[1] + l[2] * l[2]) > 0) ? 1 : 0;
+  d.aspect = double(v.width) / double(v.height);
+  d.footprint = double(v.hq_footprint_px) * 2.0 / std::max(double(v.height), 1.0);
+  d.max_dist = v.max_dist;
+  d.ray_offset = ray_offset;
+  d.out_offset = out_offset;
+  d.rays = int64_t(v.spp) * v.tile_w * v.tile_h;
+  d.seed = v.seed;
+  memcpy(d.params, v.params, sizeof(d.params));
+  d.trap = v.trap;
+  d.eps_coef = v.eps_coef;
+  d.eps_floor = v.eps_floor;
+  d.normal_h_coef = v.normal_h_coef;
+  d.shadow_k = v.shadow_k;
+  d.factor = std::min(std::max(v.step_safety, 0.001f), 1.0f);
+  d.width = v.width;
+  d.height = v.height;
+  d.tile_x = v.tile_x;
+  d.tile_y = v.tile_y;
+  d.tile_w = v.tile_w;
+  d.tile_h = v.tile_h;
+  d.spp = v.spp;
+  d.max_steps = v.max_steps;
+  d.refine = v.refine_budget;
+  d.verify = v.march_verify;
+  d.hq = v.high_quality;
+  d.normal_mode = v.normal_mode;
+  d.shadow = v.shadow;
+  d.code = code;
+  const int refine = v.march_verify ? v.refine_budget : 0;
+  const int bisect = v.march_verify ? 0 : v.refine_budget;
+  const int64_t ms = int64_t(v.max_steps) * (1 + refine) + bisect;
+  d.max_samples = int32_t(std::min<int64_t>(ms, 0x7fffffff));
+  return d;
+}
+
+}  // namespace nd

@@ -1,0 +1,340 @@
+"""Python host side over the C ABI (include/nd_march.h), through ctypes.
+
+This mirrors the reference's host interface for the sphere-tracing path:
+
+* ``FractalRenderer.rebuild(sources)`` stands where the reference's
+  ``FractalRenderer.rebuild`` (src/gpu/fractal_renderer.zig:2927) compiles a scene's
+  formula sources and stamps formula codes (``stampFormulaCodes``, :2882); errors are
+  raised as ``FormulaError`` carrying the message the reference would copy into
+  ``FormulaState.formula_error`` (src/app/formula.zig:73-77).
+* ``FractalRenderer.render(views)`` stands where ``renderToImage`` (:3548) marches
+  every pixel; it returns the G-buffer as torch tensors on the device.
+
+torch is used only for device memory and streams.  The library is the in-tree
+``libnd_march.so``; importing this module on a machine without it raises at once
+(there is no CPU fallback).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnd_march.so")
+
+# every entry point include/nd_march.h declares, with its ctypes signature
+_SIGNATURES = {
+    "nd_abi_version": (C.c_int32, []),
+    "nd_status_string": (C.c_char_p, [C.c_int32]),
+    "nd_formula_count": (C.c_int32, [C.POINTER(C.c_int32)]),
+    "nd_formula_find": (C.c_int32, [C.c_char_p, C.POINTER(C.c_int32)]),
+    "nd_formula_name": (C.c_int32, [C.c_int32, C.c_char_p, C.c_size_t]),
+    "nd_formula_register": (C.c_int32, [C.c_char_p, C.c_size_t, C.POINTER(C.c_int32), C.c_char_p, C.c_size_t]),
+    "nd_formula_params": (C.c_int32, [C.c_int32, C.POINTER(abi.nd_param_info), C.POINTER(C.c_int32)]),
+    "nd_view_defaults": (C.c_int32, [C.c_int32, C.POINTER(abi.nd_view_desc)]),
+    "nd_ctx_create": (C.c_int32, [C.c_int32, C.POINTER(C.c_void_p)]),
+    "nd_ctx_destroy": (C.c_int32, [C.c_void_p]),
+    "nd_last_error": (C.c_int32, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    "nd_last_stats": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_stats)]),
+    "nd_count_rays": (C.c_int32, [C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(C.c_int64)]),
+    "nd_march_forward": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32,
+                                     C.POINTER(abi.nd_march_opts), C.POINTER(abi.nd_gbuffer), C.c_void_p]),
+    "nd_autotune": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(abi.nd_gbuffer),
+                                C.POINTER(abi.nd_tune_result)]),
+    "nd_graph_capture": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32,
+                                     C.POINTER(abi.nd_march_opts), C.POINTER(abi.nd_gbuffer), C.c_void_p,
+                                     C.POINTER(C.c_void_p)]),
+    "nd_graph_launch": (C.c_int32, [C.c_void_p, C.c_void_p]),
+    "nd_graph_destroy": (C.c_int32, [C.c_void_p]),
+    "nd_sizeof": (C.c_size_t, [C.c_char_p]),
+    "nd_de_points": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int64, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+}
+
+_lib = None
+
+
+class NDError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        name = abi.STATUS_NAMES[status] if 0 <= status < len(abi.STATUS_NAMES) else f"status {status}"
+        super().__init__(f"{name}: {msg}" if msg else name)
+        self.status = status
+
+
+class FormulaError(NDError):
+    """A formula source the library cannot use (the reference's formula_error text)."""
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libnd_march.so (built in-tree by numericdream_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m numericdream_b200.build` "
+                          "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check_layout(lib=None):
+    """Compare the ctypes structure sizes with the library's own."""
+    lib = lib or load_library()
+    for name in ("nd_view_desc", "nd_trap_desc", "nd_gbuffer", "nd_march_opts", "nd_stats", "nd_param_info",
+                 "nd_tune_result"):
+        mine = C.sizeof(getattr(abi, name))
+        theirs = lib.nd_sizeof(name.encode())
+        if mine != theirs:
+            raise AssertionError(f"{name}: ctypes size {mine} != C size {theirs}")
+
+
+def formula_count() -> int:
+    n = C.c_int32()
+    load_library().nd_formula_count(C.byref(n))
+    return n.value
+
+
+def formula_name(fid: int) -> str:
+    buf = C.create_string_buffer(64)
+    st = load_library().nd_formula_name(fid, buf, 64)
+    if st != abi.ND_OK:
+        raise NDError(st, f"formula id {fid}")
+    return buf.value.decode()
+
+
+def formula_names() -> list:
+    return [formula_name(i) for i in range(formula_count())]
+
+
+def find_formula(name: str) -> int:
+    out = C.c_int32()
+    st = load_library().nd_formula_find(name.encode(), C.byref(out))
+    if st != abi.ND_OK:
+        raise NDError(st, f"formula {name!r} is not in this build")
+    return out.value
+
+
+def register_formula(source: str) -> int:
+    out = C.c_int32()
+    err = C.create_string_buffer(512)
+    data = source.encode("utf-8")
+    st = load_library().nd_formula_register(data, len(data), C.byref(out), err, 512)
+    if st != abi.ND_OK:
+        raise FormulaError(st, err.value.decode())
+    return out.value
+
+
+def formula_params(fid: int) -> list:
+    n = C.c_int32()
+    buf = (abi.nd_param_info * abi.ND_MAX_PARAMS)()
+    st = load_library().nd_formula_params(fid, buf, C.byref(n))
+    if st != abi.ND_OK:
+        raise NDError(st, f"formula id {fid}")
+    return [buf[i] for i in range(n.value)]
+
+
+def view_defaults(fid: int) -> abi.nd_view_desc:
+    v = abi.nd_view_desc()
+    st = load_library().nd_view_defaults(fid, C.byref(v))
+    if st != abi.ND_OK:
+        raise NDError(st)
+    return v
+
+
+def total_rays(views) -> int:
+    arr = (abi.nd_view_desc * len(views))(*views)
+    t = C.c_int64()
+    st = load_library().nd_count_rays(arr, len(views), C.byref(t))
+    if st != abi.ND_OK:
+        raise NDError(st)
+    return t.value
+
+
+@dataclass
+class GBuffer:
+    """Device G-buffer (torch tensors) for one forward call."""
+
+    depth: "object"
+    normal: "object" = None
+    trap: "object" = None
+    steps: "object" = None
+    iters: "object" = None
+    shade: "object" = None
+    shadow: "object" = None
+    depth64: "object" = None
+    evals: "object" = None
+
+    @staticmethod
+    def allocate(n: int, device="cuda", full: bool = True) -> "GBuffer":
+        import torch
+
+        g = GBuffer(depth=torch.empty(n, dtype=torch.float32, device=device))
+        if full:
+            g.normal = torch.empty((n, 4), dtype=torch.float32, device=device)
+            g.trap = torch.empty(n, dtype=torch.float32, device=device)
+            g.steps = torch.empty(n, dtype=torch.int32, device=device)
+            g.iters = torch.empty(n, dtype=torch.int32, device=device)
+            g.shade = torch.empty(n, dtype=torch.float32, device=device)
+            g.shadow = torch.empty(n, dtype=torch.float32, device=device)
+            g.depth64 = torch.empty(n, dtype=torch.float64, device=device)
+            g.evals = torch.empty(n, dtype=torch.int32, device=device)
+        return g
+
+    def as_abi(self) -> abi.nd_gbuffer:
+        g = abi.nd_gbuffer()
+        for f in ("depth", "normal", "trap", "steps", "iters", "shade", "shadow", "depth64", "evals"):
+            t = getattr(self, f)
+            setattr(g, f, None if t is None else t.data_ptr())
+        return g
+
+    def numpy(self) -> dict:
+        out = {}
+        for f in ("depth", "normal", "trap", "steps", "iters", "shade", "shadow", "depth64", "evals"):
+            t = getattr(self, f)
+            if t is not None:
+                out[f] = t.cpu().numpy()
+        return out
+
+
+def make_opts(kernel=abi.ND_KERNEL_AUTO, blocks_per_sm=0, refill_threshold=0, de_precision=32, watchdog_ms=0):
+    o = abi.nd_march_opts()
+    o.kernel, o.blocks_per_sm, o.refill_threshold = kernel, blocks_per_sm, refill_threshold
+    o.de_precision, o.watchdog_ms = de_precision, watchdog_ms
+    return o
+
+
+class Context:
+    """One nd_ctx on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        self.device = device
+        h = C.c_void_p()
+        st = self.lib.nd_ctx_create(device, C.byref(h))
+        if st != abi.ND_OK:
+            raise NDError(st, f"nd_ctx_create(device={device})")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            self.lib.nd_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def last_error(self) -> str:
+        buf = C.create_string_buffer(512)
+        self.lib.nd_last_error(self.handle, buf, 512)
+        return buf.value.decode()
+
+    def _check(self, st, what):
+        if st != abi.ND_OK:
+            raise NDError(st, f"{what}: {self.last_error()}")
+
+    def forward(self, views, gbuf: GBuffer, opts: abi.nd_march_opts | None = None, stream=None):
+        arr = (abi.nd_view_desc * len(views))(*views)
+        g = gbuf.as_abi()
+        s = None if stream is None else C.c_void_p(stream)
+        st = self.lib.nd_march_forward(self.handle, arr, len(views), C.byref(opts) if opts is not None else None,
+                                       C.byref(g), s)
+        self._check(st, "nd_march_forward")
+
+    def de_points(self, view: abi.nd_view_desc, pts, de_precision: int = 32):
+        """DE, trap and changed-iteration count of view's formula at points (torch, on device)."""
+        import torch
+
+        pts = torch.as_tensor(pts, dtype=torch.float64).reshape(-1, 3).contiguous().to(f"cuda:{self.device}")
+        n = pts.shape[0]
+        de = torch.empty(n, dtype=torch.float64, device=pts.device)
+        tr = torch.empty(n, dtype=torch.float64, device=pts.device)
+        it = torch.empty(n, dtype=torch.int32, device=pts.device)
+        st = self.lib.nd_de_points(self.handle, C.byref(view), n, pts.data_ptr(), de.data_ptr(), tr.data_ptr(),
+                                   it.data_ptr(), de_precision, None)
+        self._check(st, "nd_de_points")
+        torch.cuda.synchronize(pts.device)
+        return de.cpu().numpy(), tr.cpu().numpy(), it.cpu().numpy()
+
+    def stats(self) -> abi.nd_stats:
+        out = abi.nd_stats()
+        st = self.lib.nd_last_stats(self.handle, C.byref(out))
+        self._check(st, "nd_last_stats")
+        return out
+
+    def autotune(self, views, scratch: GBuffer) -> abi.nd_tune_result:
+        arr = (abi.nd_view_desc * len(views))(*views)
+        g = scratch.as_abi()
+        r = abi.nd_tune_result()
+        st = self.lib.nd_autotune(self.handle, arr, len(views), C.byref(g), C.byref(r))
+        self._check(st, "nd_autotune")
+        return r
+
+    def capture(self, views, gbuf: GBuffer, opts=None, stream=None) -> "Graph":
+        arr = (abi.nd_view_desc * len(views))(*views)
+        g = gbuf.as_abi()
+        h = C.c_void_p()
+        s = None if stream is None else C.c_void_p(stream)
+        st = self.lib.nd_graph_capture(self.handle, arr, len(views), C.byref(opts) if opts is not None else None,
+                                       C.byref(g), s, C.byref(h))
+        self._check(st, "nd_graph_capture")
+        return Graph(self, h)
+
+
+class Graph:
+    def __init__(self, ctx: Context, handle):
+        self.ctx, self.handle = ctx, handle
+
+    def launch(self, stream=None):
+        s = None if stream is None else C.c_void_p(stream)
+        st = self.ctx.lib.nd_graph_launch(self.handle, s)
+        self.ctx._check(st, "nd_graph_launch")
+
+    def close(self):
+        if self.handle:
+            self.ctx.lib.nd_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FractalRenderer:
+    """The reference's renderer surface for this path (rebuild + render)."""
+
+    def __init__(self, device: int = 0):
+        self.ctx = Context(device)
+        self.codes: list = []
+
+    def rebuild(self, sources) -> list:
+        """Register each formula source (WGSL text) or built-in name; returns codes."""
+        codes = []
+        for s in sources:
+            if "\n" in s or "fn " in s:
+                codes.append(register_formula(s))
+            else:
+                codes.append(find_formula(s))
+        self.codes = codes
+        return codes
+
+    def render(self, views, opts=None, full: bool = True, stream=None) -> GBuffer:
+        import torch
+
+        n = total_rays(views)
+        g = GBuffer.allocate(n, device=torch.device("cuda", self.ctx.device), full=full)
+        self.ctx.forward(views, g, opts, stream=stream)
+        return g

@@ -1,0 +1,134 @@
+"""Synthetic benchmark workloads for the sphere-tracing pass (seeded, no datasets).
+
+Five workloads, each a list of ``nd_view_desc`` (see include/nd_march.h):
+
+* ``mandelbulb_256``     Mandelbulb power 8, 12 iterations, bailout 2; 256x256 rays from
+                        (0, 0, -2.5) at the origin, 60 deg FOV; max 256 steps, eps 1e-4 t;
+                        central-difference normals h = 1e-4 t; sphere orbit trap.
+* ``mandelbox_1080p``    Mandelbox scale -1.5, fold limit 1, min radius 0.5 (r^2 0.25),
+                        fixed radius 1, 15 iterations; 1920x1080 x 4 jittered rays per
+                        pixel; max 512 steps, eps 5e-5 t; one directional shadow ray per
+                        hit, k = 16; box-shell orbit trap.
+* ``batched_64``         64 views, sides log-uniform in [64, 1024], formulas drawn from
+                        Mandelbulb (power U[4,10]), Mandelbox (scale U[-2,-1.2]), Menger
+                        (3-6 iterations), pseudo-Kleinian (box size U[0.8,1.2]); cameras
+                        on spheres of radius U[1.5,4] aimed at the origin; max 384 steps.
+* ``mandelbulb_512``     the differentiation workload's forward view (Lambert, one light).
+* ``deepzoom_4096``      Mandelbox scale -1.5, 30 iterations, 4096x4096 in 16 tiles of
+                        1024x1024, FOV 0.01 deg, camera 1e-5 from the surface.
+
+Values the workloads do not fix are the reference's render defaults
+(src/app/render_precision.zig:3-30): max_dist 24, eps floor 5e-5 unless stated,
+bisection refinement budget 4 (refine_fast), no verify pass.
+"""
+
+from __future__ import annotations
+
+import math
+import random
+
+from . import abi
+
+MANDELBULB = "mandelbrot"            # built-in formula (src/gpu/shaders/mandelbrot.wgsl)
+MANDELBOX = "amazingbox_box"
+MENGER = "menger3_ifs"
+PSEUDO_KLEINIAN = "pseudokleinian_kleinian"
+
+# default light of the shadowed workloads (unit direction TO the light)
+LIGHT_DIR = (0.4, 0.8, -0.45)
+
+
+def _ids(resolve):
+    return {n: resolve(n) for n in (MANDELBULB, MANDELBOX, MENGER, PSEUDO_KLEINIAN)}
+
+
+def mandelbox_params(scale=-1.5, iterations=15):
+    # Scale, MinRadius, FixedRadius, FoldingLimit, Iterations, RotX/Y/Z, CScale, JuliaX/Y/Z
+    return [scale, 0.5, 1.0, 1.0, float(iterations), 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0]
+
+
+def mandelbulb_params(power=8.0, iterations=12):
+    return [power, float(iterations)]
+
+
+def menger_params(iterations=4):
+    # Iterations, Scalex/y/z, Scale, RotX/Y/Z (formulas/menger3_ifs.wgsl defaults)
+    return [float(iterations), 1.0, 1.0, 1.0, 3.0, 0.0, 0.0, 0.0]
+
+
+def pseudo_kleinian_params(box_size=1.0):
+    # CenterX/Y/Z, Radius, CellSize, Iterations, CScale, JuliaX/Y/Z.  "Box size" is
+    # the lattice cube's half-width: CellSize = 2 * box size.
+    return [1.0, 1.0, 1.0, 1.0, 2.0 * box_size, 14.0, 1.0, 0.0, 0.0, 0.0]
+
+
+def mandelbulb_256(resolve, size=256):
+    fid = resolve(MANDELBULB)
+    v = abi.make_view(fid, size, size, (0.0, 0.0, -2.5), fov_y_deg=60.0, params=mandelbulb_params(8.0, 12),
+                      max_steps=256, eps_coef=1e-4, eps_floor=0.0, normal_mode=abi.ND_NORMAL_CENTRAL,
+                      normal_h_coef=1e-4, trap={"shape": abi.ND_TRAP_SPHERE, "radius": 1.0})
+    return [v]
+
+
+def reference_initial_camera():
+    """FreeCamera.initial (src/app/camera.zig:98-107): yaw 0.7, pitch 0.35, distance 3.2."""
+    yaw, pitch, dist = 0.7, 0.35, 3.2
+    cp = math.cos(pitch)
+    return (dist * cp * math.cos(yaw), dist * math.sin(pitch), dist * cp * math.sin(yaw))
+
+
+def mandelbox_1080p(resolve, width=1920, height=1080, spp=4, seed=1234):
+    fid = resolve(MANDELBOX)
+    # the reference camera has no FOV knob: |up| = 1, a 90 degree vertical FOV
+    v = abi.make_view(fid, width, height, reference_initial_camera(), fov_y_deg=90.0,
+                      params=mandelbox_params(-1.5, 15), spp=spp, seed=seed, max_steps=512, eps_coef=5e-5,
+                      eps_floor=0.0, normal_mode=abi.ND_NORMAL_CENTRAL, normal_h_coef=0.0, shadow=1,
+                      light_dir=list(LIGHT_DIR), shadow_k=16.0,
+                      trap={"shape": abi.ND_TRAP_BOX, "box": [1.0, 1.0, 1.0]})
+    return [v]
+
+
+def batched_64(resolve, nviews=64, seed=7, min_side=64, max_side=1024, max_steps=384):
+    rng = random.Random(seed)
+    ids = _ids(resolve)
+    kinds = [MANDELBULB, MANDELBOX, MENGER, PSEUDO_KLEINIAN]
+    views = []
+    for i in range(nviews):
+        w = int(round(math.exp(rng.uniform(math.log(min_side), math.log(max_side)))))
+        h = int(round(math.exp(rng.uniform(math.log(min_side), math.log(max_side)))))
+        kind = kinds[rng.randrange(4)]
+        if kind == MANDELBULB:
+            params = mandelbulb_params(rng.uniform(4.0, 10.0), 6)
+        elif kind == MANDELBOX:
+            params = mandelbox_params(rng.uniform(-2.0, -1.2), 12)
+        elif kind == MENGER:
+            params = menger_params(rng.randint(3, 6))
+        else:
+            params = pseudo_kleinian_params(rng.uniform(0.8, 1.2))
+        # uniform direction on the sphere, radius U[1.5, 4]
+        z = rng.uniform(-1.0, 1.0)
+        phi = rng.uniform(0.0, 2.0 * math.pi)
+        s = math.sqrt(max(0.0, 1.0 - z * z))
+        r = rng.uniform(1.5, 4.0)
+        pos = (r * s * math.cos(phi), r * s * math.sin(phi), r * z)
+        up = (0.0, 1.0, 0.0) if abs(pos[1]) < 0.99 * r else (1.0, 0.0, 0.0)
+        v = abi.make_view(ids[kind], w, h, pos, fov_y_deg=60.0, params=params, world_up=up,
+                          max_steps=max_steps, normal_mode=abi.ND_NORMAL_CENTRAL, normal_h_coef=1e-4,
+                          trap={"shape": abi.ND_TRAP_SPHERE, "radius": 1.0}, seed=seed * 1000 + i)
+        views.append(v)
+    return views
+
+
+def mandelbulb_512(resolve, power=8.0, yaw_deg=0.0, pitch_deg=0.0, dist=2.5, size=512):
+    """The differentiation workload's forward view: Lambert with one directional light."""
+    fid = resolve(MANDELBULB)
+    yaw, pitch = math.radians(yaw_deg), math.radians(pitch_deg)
+    pos = (dist * math.cos(pitch) * math.sin(yaw), dist * math.sin(pitch), -dist * math.cos(pitch) * math.cos(yaw))
+    v = abi.make_view(fid, size, size, pos, fov_y_deg=60.0, params=mandelbulb_params(power, 12), max_steps=256,
+                      eps_coef=1e-4, eps_floor=0.0, normal_mode=abi.ND_NORMAL_CENTRAL, normal_h_coef=1e-4,
+                      light_dir=list(LIGHT_DIR))
+    return [v]
+
+
+def rays(views) -> int:
+    return sum(abi.rays_of(v) for v in views)

@@ -1,0 +1,31 @@
+"""Build recipe for the CPU oracle (test infrastructure).
+
+Compiles oracle/oracle_capi.cpp into oracle/_build/liboracle.so with g++/OpenMP.
+Run directly (``python oracle/build_oracle.py``) or through ``__graft_entry__.build``.
+"""
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT_DIR = os.path.join(HERE, "_build")
+LIB = os.path.join(OUT_DIR, "liboracle.so")
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(HERE, "oracle_capi.cpp")
+    deps = [src, os.path.join(HERE, "oracle.hpp"), os.path.join(HERE, "..", "include", "nd_march.h")]
+    if not force and os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(d) for d in deps):
+        return LIB
+    os.makedirs(OUT_DIR, exist_ok=True)
+    # -ffp-contract=off keeps the oracle's float mode free of FMA contraction
+    cmd = ["g++", "-std=c++17", "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fopenmp", "-fPIC",
+           "-shared", src, "-o", LIB + ".tmp"]
+    subprocess.run(cmd, check=True)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv))

@@ -1,0 +1,522 @@
+// CPU oracle for the distance-estimator sphere-tracing pass.  TEST INFRASTRUCTURE:
+// only tests, the smoke check and bench.py's CPU-baseline leg use this code, as the
+// checker and the timed CPU baseline; the CUDA product never calls it.
+//
+// This is an independent, hand-written restatement of NumericDream's WGSL (the
+// reference app's src/gpu/shaders/template.wgsl, "tpl" below, and the formula
+// files), templated on the float type R: R = double is the FP64 oracle every error
+// figure is measured against, R = float mirrors the reference's own f32 arithmetic
+// and is the timed CPU baseline.  It shares no code with the CUDA library.
+//
+// Parity pinning: the reference ships no golden vectors, known-answer tests or
+// fixtures for this path, and it cannot run here (Zig, wgpu-native and a graphics
+// stack are all absent).  The formulas below are pinned instead (a) against the
+// reference's own formula sources, mechanically translated and compiled under
+// oracle/_ref (see build_ref.py), on fixed point sets committed as tests/golden
+// fixtures, and (b) against closed-form answers for the sphere and cube
+// primitives.  The march, normals and shadow logic are pinned only by (b) and by
+// reading: for those, parity with the reference is otherwise unpinned.
+#pragma once
+
+#include <stdint.h>
+#include <math.h>
+#include <string.h>
+#include <algorithm>
+#include <string>
+
+#include "../include/nd_march.h"
+
+namespace oracle {
+
+template <class R> struct V3 {
+  R x, y, z;
+  V3() : x(0), y(0), z(0) {}
+  V3(R a, R b, R c) : x(a), y(b), z(c) {}
+  explicit V3(R s) : x(s), y(s), z(s) {}
+  V3 operator+(V3 o) const { return V3(x + o.x, y + o.y, z + o.z); }
+  V3 operator-(V3 o) const { return V3(x - o.x, y - o.y, z - o.z); }
+  V3 operator*(R s) const { return V3(x * s, y * s, z * s); }
+  V3 operator/(R s) const { return V3(x / s, y / s, z / s); }
+  V3 operator-() const { return V3(-x, -y, -z); }
+};
+template <class R> R dot(V3<R> a, V3<R> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class R> R len(V3<R> a) { return std::sqrt(dot(a, a)); }
+template <class R> V3<R> norm(V3<R> a) { return a * (R(1) / len(a)); }
+template <class R> V3<R> vabs(V3<R> a) { return V3<R>(std::fabs(a.x), std::fabs(a.y), std::fabs(a.z)); }
+template <class R> V3<R> vmax(V3<R> a, R s) { return V3<R>(std::fmax(a.x, s), std::fmax(a.y, s), std::fmax(a.z, s)); }
+template <class R> V3<R> cross(V3<R> a, V3<R> b) {
+  return V3<R>(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+template <class R> R clampv(R x, R lo, R hi) { return std::fmin(std::fmax(x, lo), hi); }
+
+template <class R> struct Carry {
+  V3<R> z;
+  R dr;
+};
+
+// ------------------------------------------------------------------ formulas
+// Each formula: iterations(p), step(carry, pos, p), finalize(carry).
+
+// Built-in Mandelbulb: src/gpu/shaders/mandelbrot.wgsl:1-13 with bulb_power_step
+// (tpl:1019-1031, BULB_BAILOUT = 2 tpl:1013) and bulb_log_escape (tpl:1006-1010).
+template <class R> struct Mandelbulb {
+  static int iterations(const R* p) { return to_int(p[1]); }
+  static Carry<R> step(Carry<R> c, V3<R> pos, const R* p) {
+    const R power = p[0];
+    const R r = len(c.z);
+    if (r > R(2)) return c;
+    const R theta = std::acos(clampv(c.z.z / r, R(-1), R(1))) * power;
+    const R phi = std::atan2(c.z.y, c.z.x) * power;
+    const R rp = std::pow(r, power - R(1));
+    Carry<R> o;
+    o.dr = rp * power * c.dr + R(1);
+    const R zr = rp * r;
+    o.z = V3<R>(std::sin(theta) * std::cos(phi), std::sin(theta) * std::sin(phi), std::cos(theta)) * zr + pos;
+    return o;
+  }
+  static R finalize(Carry<R> c) {
+    const R r = len(c.z);
+    const R est = R(0.5) * std::log(std::fmax(r, R(1e-6))) * r / std::fmax(c.dr, R(1e-6));
+    return std::fmin(est, r);
+  }
+  static int to_int(R v) { return int(v); }
+};
+
+// Euler rotation in degrees about x, then y, then z (rotate_xyz_deg tpl:1085-1093,
+// rot_x/rot_y/rot_z tpl:1392-1408); identity when all angles are zero.
+template <class R> V3<R> rotate_deg(V3<R> z, R ax, R ay, R az) {
+  if (ax == R(0) && ay == R(0) && az == R(0)) return z;
+  const R k = R(0.017453292519943295);
+  R a = ax * k, b = ay * k, g = az * k;
+  // rot_x(a) * z
+  R c = std::cos(a), s = std::sin(a);
+  V3<R> v(z.x, c * z.y - s * z.z, s * z.y + c * z.z);
+  // rot_y(b) * v
+  c = std::cos(b); s = std::sin(b);
+  v = V3<R>(c * v.x + s * v.z, v.y, -s * v.x + c * v.z);
+  // rot_z(g) * v
+  c = std::cos(g); s = std::sin(g);
+  return V3<R>(c * v.x - s * v.y, s * v.x + c * v.y, v.z);
+}
+
+// Mandelbox: formulas/amazingbox_box.wgsl:13-36 with box_fold (tpl:949),
+// sphere_fold (tpl:959), de_finalize_scaled (tpl:993).
+template <class R> struct Mandelbox {
+  static int iterations(const R* p) { return int(p[4]); }
+  static Carry<R> step(Carry<R> c, V3<R> pos, const R* p) {
+    const R scale = p[0];
+    const R min_r2 = p[1] * p[1];
+    const R fixed_r2 = p[2] * p[2];
+    const R lim = p[3];
+    V3<R> z(clampv(c.z.x, -lim, lim) * R(2) - c.z.x, clampv(c.z.y, -lim, lim) * R(2) - c.z.y,
+            clampv(c.z.z, -lim, lim) * R(2) - c.z.z);
+    R dr = c.dr;
+    const R r2 = dot(z, z);
+    if (r2 < min_r2) {
+      const R t = fixed_r2 / min_r2;
+      z = z * t;
+      dr = dr * t;
+    } else if (r2 < fixed_r2) {
+      const R t = fixed_r2 / r2;
+      z = z * t;
+      dr = dr * t;
+    }
+    z = rotate_deg(z, p[5], p[6], p[7]);
+    z = z * scale + pos * p[8] + V3<R>(p[9], p[10], p[11]);
+    dr = dr * std::fabs(scale) + std::fmax(std::fabs(p[8]), R(1));
+    return Carry<R>{z, dr};
+  }
+  static R finalize(Carry<R> c) { return len(c.z) / std::fabs(c.dr); }
+};
+
+// Menger sponge: formulas/menger3_ifs.wgsl:9-28 with sort_desc_abs (tpl:1036).
+template <class R> struct Menger3 {
+  static int iterations(const R* p) { return int(p[0]); }
+  static Carry<R> step(Carry<R> c, V3<R>, const R* p) {
+    const R scale = p[4];
+    const V3<R> off(p[1], p[2], p[3]);
+    V3<R> v = vabs(c.z);
+    if (v.x < v.y) std::swap(v.x, v.y);
+    if (v.x < v.z) std::swap(v.x, v.z);
+    if (v.y < v.z) std::swap(v.y, v.z);
+    V3<R> z = rotate_deg(v, p[5], p[6], p[7]);
+    z = z * scale - off * (scale - R(1));
+    if (z.z < R(-0.5) * off.z * (scale - R(1))) z.z = z.z + off.z * (scale - R(1));
+    return Carry<R>{z, c.dr * scale};
+  }
+  static R finalize(Carry<R> c) {
+    const V3<R> q = vabs(c.z) - V3<R>(R(1));
+    return len(vmax(q, R(0))) / c.dr;
+  }
+};
+
+// Pseudo-Kleinian: formulas/pseudokleinian_kleinian.wgsl:11-33 with lattice_wrap
+// (tpl:987, round half to even) and sphere_invert_offset (tpl:975).
+template <class R> struct PseudoKleinian {
+  static int iterations(const R* p) { return int(p[5]); }
+  static R rne(R x) { return std::nearbyint(x); }
+  static Carry<R> step(Carry<R> c, V3<R> pos, const R* p) {
+    const V3<R> center(p[0], p[1], p[2]);
+    const R radius2 = p[3] * p[3];
+    const R cell = p[4];
+    V3<R> z(c.z.x - cell * rne(c.z.x / cell), c.z.y - cell * rne(c.z.y / cell), c.z.z - cell * rne(c.z.z / cell));
+    R dr = c.dr;
+    const V3<R> d = z - center;
+    const R r2 = std::fmax(dot(d, d), R(1e-6));
+    if (r2 < radius2) {
+      const R t = radius2 / r2;
+      z = center + d * t;
+      dr = dr * t;
+    }
+    z = z + pos * p[6] + V3<R>(p[7], p[8], p[9]);
+    dr = dr + std::fmax(std::fabs(p[6]), R(1));
+    return Carry<R>{z, dr};
+  }
+  static R finalize(Carry<R> c) { return len(c.z) / std::fabs(c.dr); }
+};
+
+// Primitives: formulas/sphere_primitive.wgsl, formulas/cube_primitive.wgsl with
+// primitive_de_step (tpl:1100-1109).
+template <class R> Carry<R> primitive_step(Carry<R> c, R size) {
+  const R unit = R(1) / std::fmax(size, R(1e-4));
+  const R f = unit / std::fmax(std::fabs(c.dr), R(1e-6));
+  return Carry<R>{c.z * f, unit};
+}
+template <class R> struct SpherePrim {
+  static int iterations(const R*) { return 1; }
+  static Carry<R> step(Carry<R> c, V3<R>, const R* p) { return primitive_step(c, p[0]); }
+  static R finalize(Carry<R> c) { return (len(c.z) - R(1)) / std::fmax(std::fabs(c.dr), R(1e-6)); }
+};
+template <class R> struct CubePrim {
+  static int iterations(const R*) { return 1; }
+  static Carry<R> step(Carry<R> c, V3<R>, const R* p) { return primitive_step(c, p[0]); }
+  static R finalize(Carry<R> c) {
+    const V3<R> q = vabs(c.z) - V3<R>(R(1));
+    const R outside = len(vmax(q, R(0)));
+    const R inside = std::fmin(std::fmax(q.x, std::fmax(q.y, q.z)), R(0));
+    return (outside + inside) / std::fmax(std::fabs(c.dr), R(1e-6));
+  }
+};
+
+enum FormulaKind { F_MANDELBULB = 0, F_MANDELBOX, F_MENGER3, F_PSEUDOKLEINIAN, F_SPHERE, F_CUBE, F_COUNT };
+
+inline int formula_index(const char* name) {
+  const std::string n(name ? name : "");
+  if (n == "mandelbrot") return F_MANDELBULB;
+  if (n == "amazingbox_box") return F_MANDELBOX;
+  if (n == "menger3_ifs") return F_MENGER3;
+  if (n == "pseudokleinian_kleinian") return F_PSEUDOKLEINIAN;
+  if (n == "sphere_primitive") return F_SPHERE;
+  if (n == "cube_primitive") return F_CUBE;
+  return -1;
+}
+
+// ------------------------------------------------------------------ orbit trap
+// OrbitTrap and its accumulator: tpl:1193-1289.
+template <class R> R trap_distance(const nd_trap_desc& t, V3<R> z) {
+  const V3<R> q = z - V3<R>(R(t.center[0]), R(t.center[1]), R(t.center[2]));
+  switch (t.shape) {
+    case ND_TRAP_SPHERE: return std::fabs(len(q) - R(t.radius));
+    case ND_TRAP_BOX: {
+      const V3<R> e = vabs(q) - V3<R>(R(t.box[0]), R(t.box[1]), R(t.box[2]));
+      return std::fabs(len(vmax(e, R(0))) + std::fmin(std::fmax(e.x, std::fmax(e.y, e.z)), R(0)));
+    }
+    case ND_TRAP_CROSS: return std::fmin(std::fabs(q.x), std::fmin(std::fabs(q.y), std::fabs(q.z)));
+    case ND_TRAP_TORUS: {
+      const R a = std::sqrt(q.x * q.x + q.z * q.z) - R(t.radius);
+      return std::fabs(std::sqrt(a * a + q.y * q.y) - R(t.tube));
+    }
+    default: return len(q);
+  }
+}
+
+template <class R> struct TrapAcc {
+  R x, y, z, w;
+};
+
+template <class R> TrapAcc<R> trap_begin(const nd_trap_desc& t) {
+  const bool high = t.mode != ND_TRAP_MAX && t.mode != ND_TRAP_AVERAGE;
+  return TrapAcc<R>{high ? R(1e6) : R(0), R(0), R(0), R(1e6)};
+}
+
+template <class R> void trap_update(TrapAcc<R>& a, const nd_trap_desc& t, V3<R> z, V3<R> zp, int it) {
+  const R d = trap_distance(t, z);
+  a.w = d;
+  if (t.mode == ND_TRAP_MAX) {
+    a.x = std::fmax(a.x, d);
+  } else if (t.mode == ND_TRAP_AVERAGE) {
+    if (z.x != zp.x || z.y != zp.y || z.z != zp.z) {
+      a.x += d;
+      a.y += R(1);
+    }
+  } else if (t.mode == ND_TRAP_ITERATION) {
+    if (d < a.x) {
+      a.x = d;
+      a.z = R(it);
+    }
+  } else {
+    a.x = std::fmin(a.x, d);
+  }
+}
+
+template <class R> R trap_finish(const TrapAcc<R>& a, const nd_trap_desc& t, int iters) {
+  if (t.mode == ND_TRAP_AVERAGE) return a.y > R(0.5) ? a.x / std::fmax(a.y, R(1)) : a.w;
+  if (t.mode == ND_TRAP_LAST) return a.w;
+  if (t.mode == ND_TRAP_ITERATION) return (a.z + R(1)) / R(std::max(iters, 1));
+  return a.x;
+}
+
+// ------------------------------------------------------------------ one DE evaluation
+template <class R> struct DE {
+  R d;
+  R trap;
+  int iters;  // iterations in which the carry changed
+};
+
+// The generated per-formula wrapper formula_N (fractal_renderer.zig:490-512) with
+// the single-instance scene_de (tpl:1756-1779): instance_local is the identity and
+// instance_de_factor = min(scale) * clamp(step_safety, 0.001, 1) (tpl:1611-1620).
+// Iteration counts are capped at 4096 (a build-wide watchdog cap).
+template <class R, class F> DE<R> formula_de(V3<R> pos, const R* p, const nd_trap_desc& trap, R factor) {
+  Carry<R> c{pos, R(1)};
+  TrapAcc<R> acc = trap_begin<R>(trap);
+  int n = F::iterations(p);
+  if (n > 4096) n = 4096;
+  int changed = 0;
+  for (int it = 0; it < n; ++it) {
+    const V3<R> zp = c.z;
+    c = F::step(c, pos, p);
+    if (c.z.x != zp.x || c.z.y != zp.y || c.z.z != zp.z) ++changed;
+    trap_update(acc, trap, c.z, zp, it);
+  }
+  DE<R> out;
+  out.d = F::finalize(c) * factor;
+  out.trap = trap_finish(acc, trap, n);
+  out.iters = changed;
+  return out;
+}
+
+template <class R> DE<R> eval_de(int kind, V3<R> pos, const R* p, const nd_trap_desc& trap, R factor) {
+  switch (kind) {
+    case F_MANDELBULB: return formula_de<R, Mandelbulb<R>>(pos, p, trap, factor);
+    case F_MANDELBOX: return formula_de<R, Mandelbox<R>>(pos, p, trap, factor);
+    case F_MENGER3: return formula_de<R, Menger3<R>>(pos, p, trap, factor);
+    case F_PSEUDOKLEINIAN: return formula_de<R, PseudoKleinian<R>>(pos, p, trap, factor);
+    case F_SPHERE: return formula_de<R, SpherePrim<R>>(pos, p, trap, factor);
+    default: return formula_de<R, CubePrim<R>>(pos, p, trap, factor);
+  }
+}
+
+// ------------------------------------------------------------------ per-ray result
+struct RayOut {
+  double depth;       // t at the hit, 0 on a miss
+  double normal[3];
+  int hit;
+  double trap;
+  uint32_t steps;
+  uint32_t iters;
+  double shade;
+  double shadow;
+  uint32_t evals;
+  double margin;      // smallest |d - eps| / eps over all hit decisions of the primary march
+};
+
+// Philox-free counter hash for jitter: SplitMix64 of (seed, ray) -> two floats in
+// [0, 1) with 24-bit resolution.  The CUDA library uses the same function.
+inline uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+inline void jitter2(uint64_t seed, uint64_t ray, double* jx, double* jy) {
+  const uint64_t h = splitmix64(seed ^ splitmix64(ray));
+  *jx = double(uint32_t(h) >> 8) * (1.0 / 16777216.0);
+  *jy = double(uint32_t(h >> 32) >> 8) * (1.0 / 16777216.0);
+}
+
+template <class R> struct Tracer {
+  const nd_view_desc& v;
+  int kind;
+  R p[ND_MAX_PARAMS];
+  R factor;
+  V3<double> org;
+  uint32_t evals = 0;
+  double de_scale = 1.0;  // every DE value is multiplied by this (stability probes)
+
+  Tracer(const nd_view_desc& view, int k) : v(view), kind(k) {
+    for (int i = 0; i < ND_MAX_PARAMS; ++i) p[i] = R(view.params[i]);
+    factor = R(std::min(std::max(double(view.step_safety), 0.001), 1.0));
+    org = V3<double>(view.cam_pos[0], view.cam_pos[1], view.cam_pos[2]);
+  }
+
+  DE<R> de_at(V3<double> pos) {
+    ++evals;
+    DE<R> o = eval_de<R>(kind, V3<R>(R(pos.x), R(pos.y), R(pos.z)), p, v.trap, factor);
+    if (de_scale != 1.0) o.d = R(double(o.d) * de_scale);
+    return o;
+  }
+
+  // march_epsilon: tpl:1813-1815
+  double eps(double t) const { return double(R(v.eps_coef) * R(t) + R(v.eps_floor)); }
+
+  // march_to: tpl:1859-1963, without the accelerator, warps, coarse mode and the
+  // overstep diagnostic (all off on this path).  t, lo, hi are kept in double.
+  void march(V3<double> dir, RayOut& o, DE<R>& hit_de) {
+    const int max_steps = v.max_steps;
+    const bool hq = v.high_quality != 0;
+    const int budget = std::max(v.refine_budget, 0);
+    const bool on_hit = v.march_verify == 0;
+    const int refine_budget = on_hit ? 0 : budget;
+    const int bisect_budget = on_hit ? budget : 0;
+    const double footprint = double(v.hq_footprint_px) * 2.0 / std::max(double(v.height), 1.0);
+    const double max_t = v.max_dist;
+    double t = 0, lo = 0, hi = 0;
+    int i = 0, refines = 0;
+    bool probing = true, bisecting = false, resolved = false;
+    o.margin = 1e30;
+    const long max_samples = long(max_steps) * (1 + refine_budget) + bisect_budget;
+    for (long n = 0; n < max_samples; ++n) {
+      const double st = probing ? t : 0.5 * (lo + hi);
+      const double e = eps(st);
+      const V3<double> pos = org + dir * st;
+      const DE<R> de = de_at(pos);
+      const double d = double(de.d);
+      o.margin = std::min(o.margin, std::fabs(d - e) / std::max(e, 1e-30));
+      if (bisecting) {
+        if (d < e) {
+          hi = st;
+          hit_de = de;
+        } else {
+          lo = st;
+        }
+        ++refines;
+        if (hi - lo <= e || refines >= bisect_budget) {
+          o.hit = 1; o.depth = hi; o.steps = uint32_t(i);
+          return;
+        }
+        continue;
+      }
+      if (d < e) {
+        if (on_hit && bisect_budget > 0 && st - lo > e) {
+          bisecting = true;
+          probing = false;
+          hi = st;
+          refines = 0;
+          hit_de = de;
+          continue;
+        }
+        o.hit = 1; o.depth = st; o.steps = uint32_t(i);
+        hit_de = de;
+        return;
+      }
+      if (probing) {
+        lo = t;
+        hi = t + d;
+        refines = 0;
+        resolved = false;
+        probing = false;
+      } else {
+        if (d >= hi - st) resolved = true;
+        else hi = st;
+        ++refines;
+      }
+      if (resolved || refines >= refine_budget) {
+        if (hq && !resolved && refine_budget > 0) hi = std::min(hi, lo + std::max(t, 1.0) * footprint);
+        t = hi;
+        ++i;
+        o.margin = std::min(o.margin, std::fabs(t - max_t) / max_t);
+        if (t > max_t || i >= max_steps) break;
+        probing = true;
+      }
+    }
+    o.hit = 0; o.depth = t; o.steps = uint32_t(max_steps);
+  }
+
+  // Normals: tetrahedral gradient with e = eps(t) (estimate_normal / tetra_gradient
+  // tpl:1783-1804), or 6-tap central differences with h = coef * t.
+  V3<double> normal(V3<double> pos, double t) {
+    V3<double> g(0.0);
+    if (v.normal_mode == ND_NORMAL_CENTRAL) {
+      const double h = v.normal_h_coef > 0 ? double(v.normal_h_coef) * t : eps(t);
+      for (int a = 0; a < 3; ++a) {
+        V3<double> k(0.0);
+        (a == 0 ? k.x : a == 1 ? k.y : k.z) = h;
+        const double dp = double(de_at(pos + k).d);
+        const double dm = double(de_at(pos - k).d);
+        (a == 0 ? g.x : a == 1 ? g.y : g.z) = dp - dm;
+      }
+    } else {
+      const double e = eps(t);
+      const V3<double> ks[4] = {V3<double>(1, -1, -1), V3<double>(-1, -1, 1), V3<double>(-1, 1, -1), V3<double>(1, 1, 1)};
+      for (int i = 0; i < 4; ++i) g = g + ks[i] * double(de_at(pos + ks[i] * e).d);
+    }
+    const double l = len(g);
+    return l > 0 ? g / l : g;
+  }
+
+  // Opaque soft shadow toward a LIGHT_GLOBAL light: shadow_factor tpl:2365-2375 and
+  // visibility_march tpl:2282-2342 with constants tpl:2344-2353 (bias 0.004, hit
+  // eps 5e-4, min step 1e-3, at most min(max_steps, 40) steps, light distance
+  // 2 * max_dist as light_sample_ex gives for LIGHT_GLOBAL, tpl:2187-2190).
+  double shadow(V3<double> pos, V3<double> n, V3<double> l) {
+    const V3<double> o = pos + n * 0.004;
+    const double light_dist = double(v.max_dist) * 2.0;
+    const int steps = std::min(v.max_steps, 40);
+    double t = 0.004, res = 1.0;
+    for (int i = 0; i < steps; ++i) {
+      if (t >= light_dist) break;
+      const double d = double(de_at(o + l * t).d);
+      if (d < 0.0005) return 0.0;
+      res = std::min(res, double(v.shadow_k) * d / t);
+      t += std::max(d, 0.001);
+    }
+    return clampv(res, 0.0, 1.0);
+  }
+
+  RayOut trace(int64_t ray) {
+    RayOut o;
+    memset(&o, 0, sizeof(o));
+    evals = 0;
+    const int64_t npix = int64_t(v.tile_w) * v.tile_h;
+    const int64_t s = ray / npix, pix = ray % npix;
+    const int px = v.tile_x + int(pix % v.tile_w), py = v.tile_y + int(pix / v.tile_w);
+    double jx = 0.5, jy = 0.5;
+    if (v.spp > 1) jitter2(v.seed, uint64_t(s * npix + pix), &jx, &jy);
+    // camera ray: cs_wf_generate tpl:5120-5127 and fs_simple tpl:4523-4525; the tile
+    // transform (fractal_renderer.zig:852-863) is folded into full-frame pixels.
+    const double ndc_x = 2.0 * (px + jx) / v.width - 1.0;
+    const double ndc_y = 1.0 - 2.0 * (py + jy) / v.height;
+    const double aspect = double(v.width) / double(v.height);
+    const double ux = ndc_x * aspect, uy = -ndc_y;
+    const V3<double> f(v.fwd[0], v.fwd[1], v.fwd[2]), r(v.right[0], v.right[1], v.right[2]),
+        u(v.up[0], v.up[1], v.up[2]);
+    const V3<double> dir = norm(f + r * ux + u * uy);
+    DE<R> hit_de{R(0), R(0), 0};
+    march(dir, o, hit_de);
+    o.shadow = 1.0;
+    if (!o.hit) {
+      o.depth = 0;
+      o.evals = evals;
+      return o;
+    }
+    o.trap = double(hit_de.trap);
+    o.iters = uint32_t(hit_de.iters);
+    const V3<double> pos = org + dir * o.depth;
+    const V3<double> n = normal(pos, o.depth);
+    o.normal[0] = n.x; o.normal[1] = n.y; o.normal[2] = n.z;
+    // simple_geometry (tpl:4492-4507): key light normalize(-dir + 0.45 up - 0.35 right)
+    // in camera space, or the view's directional light when one is given.
+    V3<double> key;
+    const V3<double> ld(v.light_dir[0], v.light_dir[1], v.light_dir[2]);
+    if (v.shadow || dot(ld, ld) > 0) key = norm(ld);
+    else key = norm(-dir + norm(u) * 0.45 - norm(r) * 0.35);
+    if (v.shadow) o.shadow = shadow(pos, n, key);
+    const double lam = std::max(dot(n, key), 0.0) * o.shadow;
+    o.shade = 0.18 + (1.0 - 0.18) * lam;
+    o.evals = evals;
+    return o;
+  }
+};
+
+}  // namespace oracle

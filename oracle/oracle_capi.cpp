@@ -1,0 +1,86 @@
+// C entry points of the CPU oracle (test infrastructure; see oracle.hpp).
+// Built as oracle/_build/liboracle.so by oracle/build_oracle.py; loaded with ctypes
+// by the tests and by bench.py's CPU-baseline leg only.
+#include <omp.h>
+#include <stdint.h>
+
+#include "oracle.hpp"
+
+using namespace oracle;
+
+extern "C" {
+
+int oracle_formula_index(const char* name) { return formula_index(name); }
+
+// DE (and trap, changed-iteration count) of a formula at n points, in FP64
+// (precision 64) or FP32 (precision 32).
+int oracle_de(const char* name, const float* params, const nd_trap_desc* trap, int precision, int64_t n,
+              const double* pts, double* de, double* trap_out, int32_t* iters) {
+  const int kind = formula_index(name);
+  if (kind < 0) return -1;
+  nd_trap_desc tz;
+  memset(&tz, 0, sizeof(tz));
+  const nd_trap_desc& t = trap ? *trap : tz;
+  for (int64_t i = 0; i < n; ++i) {
+    if (precision == 32) {
+      float p[ND_MAX_PARAMS];
+      for (int k = 0; k < ND_MAX_PARAMS; ++k) p[k] = params[k];
+      const DE<float> r = eval_de<float>(kind, V3<float>(float(pts[3 * i]), float(pts[3 * i + 1]), float(pts[3 * i + 2])), p, t, 1.0f);
+      de[i] = r.d;
+      if (trap_out) trap_out[i] = r.trap;
+      if (iters) iters[i] = r.iters;
+    } else {
+      double p[ND_MAX_PARAMS];
+      for (int k = 0; k < ND_MAX_PARAMS; ++k) p[k] = params[k];
+      const DE<double> r = eval_de<double>(kind, V3<double>(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]), p, t, 1.0);
+      de[i] = r.d;
+      if (trap_out) trap_out[i] = r.trap;
+      if (iters) iters[i] = r.iters;
+    }
+  }
+  return 0;
+}
+
+// Trace rays [first, first + n) of one view.  Outputs are indexed 0..n-1; any
+// output pointer may be NULL.  nthreads <= 0 uses every core.  de_scale multiplies
+// every DE value (1 for the plain march; 1 +- delta probes a ray's stability).
+// Returns -1 for an unknown formula name.
+int oracle_render(const nd_view_desc* view, const char* formula_name, int precision, int nthreads,
+                  int64_t first, int64_t n, float* depth, float* normal4, float* trap, uint32_t* steps,
+                  uint32_t* iters, float* shade, float* shadow, double* depth64, uint32_t* evals,
+                  double* margin, double de_scale) {
+  const int kind = formula_index(formula_name);
+  if (kind < 0) return -1;
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel num_threads(nthreads)
+  {
+    Tracer<float> tf(*view, kind);
+    Tracer<double> td(*view, kind);
+    tf.de_scale = de_scale;
+    td.de_scale = de_scale;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i) {
+      const RayOut o = precision == 32 ? tf.trace(first + i) : td.trace(first + i);
+      if (depth) depth[i] = float(o.depth);
+      if (depth64) depth64[i] = o.depth;
+      if (normal4) {
+        normal4[4 * i] = float(o.normal[0]);
+        normal4[4 * i + 1] = float(o.normal[1]);
+        normal4[4 * i + 2] = float(o.normal[2]);
+        normal4[4 * i + 3] = o.hit ? 1.0f : 0.0f;
+      }
+      if (trap) trap[i] = float(o.trap);
+      if (steps) steps[i] = o.steps;
+      if (iters) iters[i] = o.iters;
+      if (shade) shade[i] = float(o.shade);
+      if (shadow) shadow[i] = float(o.shadow);
+      if (evals) evals[i] = o.evals;
+      if (margin) margin[i] = o.margin;
+    }
+  }
+  return 0;
+}
+
+int oracle_max_threads(void) { return omp_get_max_threads(); }
+
+}  // extern "C"

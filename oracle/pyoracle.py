@@ -1,0 +1,87 @@
+"""ctypes front end of the CPU oracle (test infrastructure only; see oracle.hpp)."""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from numericdream_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "_build", "liboracle.so")
+        if not os.path.exists(path):
+            from . import build_oracle
+            build_oracle.build()
+        _LIB = C.CDLL(path)
+        _LIB.oracle_formula_index.argtypes = [C.c_char_p]
+        _LIB.oracle_de.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p]
+        _LIB.oracle_render.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_int64, C.c_int64] + [C.c_void_p] * 10 + [C.c_double]
+        _LIB.oracle_max_threads.restype = C.c_int
+    return _LIB
+
+
+def has_formula(name: str) -> bool:
+    return lib().oracle_formula_index(name.encode()) >= 0
+
+
+def max_threads() -> int:
+    return lib().oracle_max_threads()
+
+
+def de(name: str, params, pts, precision=64, trap: abi.nd_trap_desc | None = None):
+    pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    n = pts.shape[0]
+    prm = np.zeros(16, np.float32)
+    prm[: len(params)] = params
+    out = np.zeros(n, np.float64)
+    tr = np.zeros(n, np.float64)
+    it = np.zeros(n, np.int32)
+    rc = lib().oracle_de(name.encode(), prm.ctypes.data, C.addressof(trap) if trap is not None else None,
+                         precision, n, pts.ctypes.data, out.ctypes.data, tr.ctypes.data, it.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"oracle has no formula {name!r}")
+    return out, tr, it
+
+
+def render(view: abi.nd_view_desc, formula_name: str, precision=64, nthreads=0, first=0, n=None, de_scale=1.0):
+    """Trace rays [first, first+n) of one view; returns a dict of numpy arrays."""
+    total = abi.rays_of(view)
+    if n is None:
+        n = total - first
+    out = {
+        "depth": np.zeros(n, np.float32), "normal": np.zeros((n, 4), np.float32), "trap": np.zeros(n, np.float32),
+        "steps": np.zeros(n, np.uint32), "iters": np.zeros(n, np.uint32), "shade": np.zeros(n, np.float32),
+        "shadow": np.zeros(n, np.float32), "depth64": np.zeros(n, np.float64), "evals": np.zeros(n, np.uint32),
+        "margin": np.zeros(n, np.float64),
+    }
+    keys = ["depth", "normal", "trap", "steps", "iters", "shade", "shadow", "depth64", "evals", "margin"]
+    rc = lib().oracle_render(C.addressof(view), formula_name.encode(), precision, nthreads, first, n,
+                             *[out[k].ctypes.data for k in keys], de_scale)
+    if rc != 0:
+        raise ValueError(f"oracle has no formula {formula_name!r}")
+    return out
+
+
+STABILITY_DELTA = 1e-4
+
+
+def unstable_rays(view: abi.nd_view_desc, formula_name: str, delta: float = STABILITY_DELTA, nthreads=0):
+    """Rays whose FP64 outcome (hit/miss or probe-step count) changes when every DE
+    value is scaled by 1 - delta or 1 + delta: their integer outputs are not
+    determined at FP32 precision (the boundary-case policy)."""
+    base = render(view, formula_name, 64, nthreads)
+    lo = render(view, formula_name, 64, nthreads, de_scale=1.0 - delta)
+    hi = render(view, formula_name, 64, nthreads, de_scale=1.0 + delta)
+    h = [o["normal"][:, 3] > 0.5 for o in (base, lo, hi)]
+    unstable = (h[0] != h[1]) | (h[0] != h[2])
+    unstable |= (base["steps"] != lo["steps"]) | (base["steps"] != hi["steps"])
+    return unstable, base
