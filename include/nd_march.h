@@ -99,6 +99,10 @@ typedef struct nd_trap_desc {
 
 enum { ND_NORMAL_TETRA = 0, ND_NORMAL_CENTRAL = 1 };
 
+/* nd_view_desc.flags: ND_VIEW_DIR64 keeps ray directions in FP64 (set
+ * automatically when |right| or |up| < 1e-3, i.e. fields of view under ~0.1 deg). */
+enum { ND_VIEW_DIR64 = 1 };
+
 /* One view: a camera, a frame (or a tile of it) and one fractal instance. */
 typedef struct nd_view_desc {
   double cam_pos[3];      /* ray origin, FP64 (u.camera_pos) */
@@ -130,7 +134,7 @@ typedef struct nd_view_desc {
   float light_dir[3];     /* direction TO a LIGHT_GLOBAL light (normalised by the library) */
   float shadow_k;         /* soft-shadow sharpness k */
   float step_safety;      /* instance step safety, clamped to [0.001, 1] */
-  int32_t flags;          /* reserved, 0 */
+  int32_t flags;          /* ND_VIEW_* bits */
   int32_t reserved[3];
 } nd_view_desc;
 

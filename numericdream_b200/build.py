@@ -35,7 +35,7 @@ INCLUDE = os.path.join(ROOT, "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v", "--expt-relaxed-constexpr",
-           "-I", CSRC, "-I", INCLUDE, "-I", GEN]
+           "-I", CSRC, "-I", INCLUDE, "-I", GEN] + os.environ.get("ND_NVCC_EXTRA", "").split()
 
 # Mixed-formula batches run in ONE persistent launch when every formula of the
 # batch belongs to a compiled group.  The default group holds the four formulas

@@ -10,6 +10,10 @@
 
 namespace nd {
 
+#ifndef ND_PERSISTENT_MIN_BLOCKS
+#define ND_PERSISTENT_MIN_BLOCKS 1
+#endif
+
 __device__ __forceinline__ int64_t globaltimer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -39,30 +43,38 @@ __device__ __forceinline__ void flush_stats(Stats* s, unsigned long long rays, u
 }
 
 // --------------------------------------------------------------- plain kernel
-// One thread per ray, the reference's fragment-shader structure (fs_simple):
-// march to completion, then the normal taps, then the shadow ray.  No refill: a
-// warp runs until its slowest ray is done.
-template <class Set, class T, bool kBatched>
+// The reference's per-pixel program as a plain per-view launch: one thread per
+// ray, the march loop of march_to, then the normal taps of estimate_normal, then
+// the shadow loop of visibility_march, each loop running until its slowest lane
+// in the warp is done (fs_simple tpl:4522-4538 / simple_geometry tpl:4492-4507).
+template <class Set, class T, bool kDir64>
 __global__ void __launch_bounds__(128) plain_kernel(const __grid_constant__ LaunchArgs a,
-                                                    const __grid_constant__ DevView single) {
-  const int64_t item = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  const bool live = item < a.total_rays;
-  unsigned long long rays = 0, hits = 0;
-  Lane<T> L;
-  L.ev_march = L.ev_normal = L.ev_shadow = 0;
-  if (live) {
-    const int vi = kBatched ? find_view(a.views, a.nviews, item) : 0;
-    const DevView& v = kBatched ? a.views[vi] : single;
-    L.start(v, item, vi);
-    if (v.max_samples <= 0) L.finish(v, a.out, false, 1.0f, a.stats);
-    while (L.phase != PH_DONE) {
+                                                    const __grid_constant__ DevView v) {
+  const int64_t local = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;  // ray index inside the view
+  unsigned long long rays = 0, hits = 0, m = 0, nn = 0, sh = 0;
+  if (local < v.rays) {
+    Lane<T, kDir64> L;
+    L.start(v, int32_t(v.ray_offset + local), 0);
+    if (L.phase == PH_DONE) L.finish(v, a.out, 1.0f);
+    while (L.phase == PH_MARCH) {
       const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(L.sample_pos(v)), v);
-      L.advance(v, de, a.out, a.stats);
+      L.advance(v, de, a.out);
     }
+    m = L.evals;
+    while (L.phase == PH_NORMAL) {
+      const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(L.sample_pos(v)), v);
+      L.advance(v, de, a.out);
+    }
+    nn = L.evals - m;
+    while (L.phase == PH_SHADOW) {
+      const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(L.sample_pos(v)), v);
+      L.advance(v, de, a.out);
+    }
+    sh = L.evals - m - nn;
     rays = 1;
-    hits = L.was_hit ? 1 : 0;
+    hits = L.hit ? 1 : 0;
   }
-  flush_stats(a.stats, rays, L.ev_march, L.ev_normal, L.ev_shadow, hits, 0);
+  flush_stats(a.stats, rays, m, nn, sh, hits, 0);
 }
 
 // --------------------------------------------------------------- persistent kernel
@@ -71,65 +83,70 @@ __global__ void __launch_bounds__(128) plain_kernel(const __grid_constant__ Laun
 // lanes are idle (or all are), the first idle lane takes that many new ray
 // indices with ONE atomicAdd on the work counter and hands them out by
 // popc-prefix rank (the analogue of the reference's workgroup-aggregated queue
-// reservation wf_reserve, tpl:5083-5105).
-template <class Set, class T, bool kBatched>
-__global__ void __launch_bounds__(128) persistent_kernel(const __grid_constant__ LaunchArgs a,
+// reservation wf_reserve, tpl:5083-5105).  Whatever phase a lane is in, each pass
+// of the loop is one DE evaluation for every busy lane.
+template <class Set, class T, bool kDir64, bool kBatched>
+__global__ void __launch_bounds__(128, ND_PERSISTENT_MIN_BLOCKS) persistent_kernel(const __grid_constant__ LaunchArgs a,
                                                          const __grid_constant__ DevView single) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
-  Lane<T> L;
+  Lane<T, kDir64> L;
   L.item = -1;
   L.phase = PH_DONE;
-  L.ev_march = L.ev_normal = L.ev_shadow = 0;
-  unsigned long long rays = 0, hits = 0, refills = 0;
+  L.evals = 0;
+  L.hit = false;
+  uint32_t rays = 0, hits = 0, ev_m = 0, ev_n = 0, ev_s = 0, refills = 0;
   bool exhausted = false;
-  int vi = 0;
-  const int64_t t0 = __shfl_sync(full, globaltimer_ns(), 0);
+  const int64_t deadline = __shfl_sync(full, globaltimer_ns(), 0) + a.deadline_ns;
   int tick = 0;
+  const int32_t total = int32_t(a.total_rays);
   while (true) {
     if (L.phase == PH_DONE && L.item >= 0) {
       ++rays;
-      hits += L.was_hit ? 1 : 0;
+      hits += L.hit ? 1 : 0;
+      const uint32_t taps = L.hit ? normal_taps(kBatched ? a.views[L.view] : single) : 0u;
+      ev_m += L.mev;
+      ev_n += taps;
+      ev_s += L.evals - L.mev - taps;
       L.item = -1;
     }
     const unsigned idle = __ballot_sync(full, L.item < 0);
     if (!exhausted && idle != 0u && (__popc(idle) >= a.refill_threshold || idle == full)) {
       const int want = __popc(idle);
       const int leader = __ffs(idle) - 1;
-      unsigned long long base = 0;
-      if (lane == leader) base = atomicAdd(a.counter, (unsigned long long)want);
+      int32_t base = 0;
+      if (lane == leader) base = int32_t(atomicAdd(a.counter, (unsigned long long)want));
       base = __shfl_sync(full, base, leader);
       ++refills;
-      if (base + want >= (unsigned long long)a.total_rays) exhausted = true;
+      if (int64_t(base) + want >= int64_t(total)) exhausted = true;
       if (L.item < 0) {
-        const int64_t it = int64_t(base) + __popc(idle & lt_mask);
-        if (it < a.total_rays) {
-          vi = kBatched ? find_view(a.views, a.nviews, it) : 0;
-          const DevView& v = kBatched ? a.views[vi] : single;
-          L.start(v, it, vi);
-          if (v.max_samples <= 0) L.finish(v, a.out, false, 1.0f, a.stats);
+        const int32_t it = base + __popc(idle & lt_mask);
+        if (it < total && it >= 0) {
+          L.view = kBatched ? find_view(a.views, a.nviews, it) : 0;
+          const DevView& v = kBatched ? a.views[L.view] : single;
+          L.start(v, it, L.view);
+          if (L.phase == PH_DONE) L.finish(v, a.out, 1.0f);
         }
       }
-      if (__ballot_sync(full, L.item >= 0) == 0u) break;
-      continue;  // lanes finished at start re-enter the bookkeeping above
+      continue;  // lanes that finished at once go back through the bookkeeping
     }
     if (exhausted && idle == full) break;
     if (((++tick) & 63) == 0) {
       // lane 0's clock decides for the whole warp, so the exit stays warp-uniform
       const int64_t now = __shfl_sync(full, globaltimer_ns(), 0);
-      if (now - t0 > a.deadline_ns) {
+      if (now > deadline) {
         if (lane == 0) atomicAdd(&a.stats->timeouts, 1u);
         break;
       }
     }
     if (L.item >= 0) {
-      const DevView& v = kBatched ? a.views[vi] : single;
+      const DevView& v = kBatched ? a.views[L.view] : single;
       const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(L.sample_pos(v)), v);
-      L.advance(v, de, a.out, a.stats);
+      L.advance(v, de, a.out);
     }
   }
-  flush_stats(a.stats, rays, L.ev_march, L.ev_normal, L.ev_shadow, hits, refills);
+  flush_stats(a.stats, rays, ev_m, ev_n, ev_s, hits, refills);
 }
 
 // --------------------------------------------------------------- launchers
@@ -140,21 +157,22 @@ struct LaunchConfig {
   int num_sms;
 };
 
-template <class Set, class T, bool kBatched>
+template <class Set, class T, bool kDir64>
 cudaError_t launch_plain(const LaunchArgs& a, const DevView& single, const LaunchConfig& c, cudaStream_t s) {
   const int block = 128;
-  const int64_t grid = (a.total_rays + block - 1) / block;
+  const int64_t grid = (single.rays + block - 1) / block;
   if (grid <= 0) return cudaSuccess;
-  plain_kernel<Set, T, kBatched><<<unsigned(grid), block, 0, s>>>(a, single);
+  plain_kernel<Set, T, kDir64><<<unsigned(grid), block, 0, s>>>(a, single);
   return cudaGetLastError();
 }
 
-template <class Set, class T, bool kBatched>
+template <class Set, class T, bool kDir64, bool kBatched>
 cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const LaunchConfig& c, cudaStream_t s) {
   const int block = 128;
   int per_sm = c.blocks_per_sm;
   if (per_sm <= 0) {
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel<Set, T, kBatched>, block, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, persistent_kernel<Set, T, kDir64, kBatched>, block, 0);
     if (e != cudaSuccess) return e;
     if (per_sm <= 0) per_sm = 1;
   }
@@ -162,7 +180,7 @@ cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const 
   const int64_t needed = (a.total_rays + block - 1) / block;
   if (grid > needed) grid = needed;
   if (grid <= 0) return cudaSuccess;
-  persistent_kernel<Set, T, kBatched><<<unsigned(grid), block, 0, s>>>(a, single);
+  persistent_kernel<Set, T, kDir64, kBatched><<<unsigned(grid), block, 0, s>>>(a, single);
   return cudaGetLastError();
 }
 
@@ -194,23 +212,27 @@ cudaError_t launch_de_points(const DevView& v, int64_t n, const double* pts, dou
 
 typedef cudaError_t (*DePointsFn)(const DevView&, int64_t, const double*, double*, double*, uint32_t*, cudaStream_t);
 
-// Launchers of one formula set: [kernel][precision][batched].
+// Launchers of one formula set.  Plain launches take one view (kernel param);
+// persistent ones take one view (single) or a view table (batched).  "dir64" is
+// the deep-zoom variant with FP64 ray directions; FP64 DEs always use it.
 struct KernelTable {
-  LaunchFn plain_f32, plain_f32_batched, persistent_f32, persistent_f32_batched;
-  LaunchFn plain_f64, plain_f64_batched, persistent_f64, persistent_f64_batched;
+  LaunchFn plain_f32, plain_f32_dir64, plain_f64;
+  LaunchFn persistent_f32, persistent_f32_batched, persistent_f32_dir64, persistent_f32_dir64_batched;
+  LaunchFn persistent_f64, persistent_f64_batched;
   DePointsFn de_points_f32, de_points_f64;
 };
 
 template <class Set> KernelTable make_kernel_table() {
   KernelTable t;
   t.plain_f32 = &launch_plain<Set, float, false>;
-  t.plain_f32_batched = &launch_plain<Set, float, true>;
-  t.persistent_f32 = &launch_persistent<Set, float, false>;
-  t.persistent_f32_batched = &launch_persistent<Set, float, true>;
-  t.plain_f64 = &launch_plain<Set, double, false>;
-  t.plain_f64_batched = &launch_plain<Set, double, true>;
-  t.persistent_f64 = &launch_persistent<Set, double, false>;
-  t.persistent_f64_batched = &launch_persistent<Set, double, true>;
+  t.plain_f32_dir64 = &launch_plain<Set, float, true>;
+  t.plain_f64 = &launch_plain<Set, double, true>;
+  t.persistent_f32 = &launch_persistent<Set, float, false, false>;
+  t.persistent_f32_batched = &launch_persistent<Set, float, false, true>;
+  t.persistent_f32_dir64 = &launch_persistent<Set, float, true, false>;
+  t.persistent_f32_dir64_batched = &launch_persistent<Set, float, true, true>;
+  t.persistent_f64 = &launch_persistent<Set, double, true, false>;
+  t.persistent_f64_batched = &launch_persistent<Set, double, true, true>;
   t.de_points_f32 = &launch_de_points<Set, float>;
   t.de_points_f64 = &launch_de_points<Set, double>;
   return t;

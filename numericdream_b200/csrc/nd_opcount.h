@@ -93,13 +93,12 @@ inline void count_ray(const DevView& view, int64_t ray, ndw::OpCounts* out, uint
   g.depth = &depth;
   ndw::OpCounts& c = ndw::op_counts();
   const ndw::OpCounts before = c;
-  Lane<ndw::CF> L;
-  L.ev_march = L.ev_normal = L.ev_shadow = 0;
-  L.start(v, ray, 0);
-  if (v.max_samples <= 0) L.finish(v, g, false, 1.0f, nullptr);
+  Lane<ndw::CF, false> L;
+  L.start(v, int32_t(ray), 0);
+  if (L.phase == PH_DONE) L.finish(v, g, 1.0f);
   while (L.phase != PH_DONE) {
     const DEOut<ndw::CF> de = Set::template de<ndw::CF>(v.code, to_t<ndw::CF>(L.sample_pos(v)), v);
-    L.advance(v, de, g, nullptr);
+    L.advance(v, de, g);
   }
   out->add += c.add - before.add;
   out->mul += c.mul - before.mul;

@@ -78,6 +78,8 @@ struct DevView {
   int32_t max_steps, refine, verify, hq, normal_mode, shadow, use_light;
   int32_t code;         // formula index inside the kernel's formula set
   int32_t max_samples;  // max_steps * (1 + refine budget) + bisect budget
+  int32_t dir64;        // ray directions need FP64 (deep-zoom cameras)
+  int32_t pad;
 };
 
 struct Stats {
@@ -167,9 +169,16 @@ template <class T> struct ParamRef {
 
 // formula_N (fractal_renderer.zig:490-512) + the single-instance scene_de
 // (tpl:1611-1626, 1756-1779): identity instance transform, DE scaled by factor.
+//
+// de_step(carry, pos, p) is a pure function of its arguments (the contract gives it
+// no iteration index), so once one iteration returns its input carry unchanged
+// every later iteration would too, and the orbit-trap updates they would make
+// leave the accumulator as it is (min, max, last and iteration modes see the same
+// distance again; average mode only counts changed iterations).  The loop stops
+// at that fixed point, e.g. as soon as a Mandelbulb point has escaped
+// (bulb_power_step returns the carry unchanged once r > 2, tpl:1019-1023).
 template <class F, class T>
-ND_DEV_INLINE DEOut<T> formula_de(ndw::v3<T> pos, const float* params, const nd_trap_desc& trap,
-                                               float factor) {
+ND_DEV_INLINE DEOut<T> formula_de(ndw::v3<T> pos, const float* params, const nd_trap_desc& trap, float factor) {
   const ParamRef<T> p{params};
   ndw::IterCarry<T> c{pos, T(1)};
   TrapAcc<T> acc = trap_begin<T>(trap);
@@ -178,8 +187,10 @@ ND_DEV_INLINE DEOut<T> formula_de(ndw::v3<T> pos, const float* params, const nd_
   int changed = 0;
   for (int it = 0; it < n; ++it) {
     const ndw::v3<T> zp = c.z;
+    const T drp = c.dr;
     c = F::template step<T, ParamRef<T>>(c, pos, p);
     const bool ch = (c.z.x != zp.x) | (c.z.y != zp.y) | (c.z.z != zp.z);
+    if (!ch && !(c.dr != drp)) break;  // fixed point: nothing changes any more
     changed += ch ? 1 : 0;
     trap_update(acc, trap, c.z, ch, it);
   }
@@ -191,7 +202,7 @@ ND_DEV_INLINE DEOut<T> formula_de(ndw::v3<T> pos, const float* params, const nd_
 }
 
 // A compile-time list of formulas; code selects one (warp-uniform in practice,
-// because work items are ordered by view).
+// because batched views are ordered by formula).
 template <class... Fs> struct FormulaSet;
 template <class F> struct FormulaSet<F> {
   template <class T>
@@ -223,12 +234,23 @@ ND_DEV_INLINE D3 fmadd(D3 o, D3 d, double t) {
   return D3{fma_d(d.x, t, o.x), fma_d(d.y, t, o.y), fma_d(d.z, t, o.z)};
 }
 
+// Ray direction storage: float for ordinary cameras, double for deep-zoom
+// cameras whose neighbouring pixels differ by less than an FP32 ulp.
+template <bool kDir64> struct Dir;
+template <> struct Dir<false> {
+  float x, y, z;
+  ND_DEV_INLINE void set(D3 d) { x = float(d.x); y = float(d.y); z = float(d.z); }
+  ND_DEV_INLINE D3 get() const { return D3{double(x), double(y), double(z)}; }
+};
+template <> struct Dir<true> {
+  double x, y, z;
+  ND_DEV_INLINE void set(D3 d) { x = d.x; y = d.y; z = d.z; }
+  ND_DEV_INLINE D3 get() const { return D3{x, y, z}; }
+};
+
 // eps(t) = coef * t + floor in the DE precision, without FMA contraction
 // (march_epsilon tpl:1813-1815).
 template <class T> ND_DEV_INLINE double march_eps(const DevView& v, double t) {
-  return double(rn_add(rn_mul(v.eps_coef, float(t)), v.eps_floor));
-}
-template <> ND_DEV_INLINE double march_eps<float>(const DevView& v, double t) {
   return double(rn_add(rn_mul(v.eps_coef, float(t)), v.eps_floor));
 }
 template <> ND_DEV_INLINE double march_eps<double>(const DevView& v, double t) {
@@ -322,74 +344,65 @@ ND_DEV_INLINE int find_view(const DevView* views, int nviews, int64_t item) {
   return lo;
 }
 
-// --------------------------------------------------------------- the ray state machine
+// --------------------------------------------------------------- the ray program
 enum Phase : int { PH_MARCH = 0, PH_NORMAL = 1, PH_SHADOW = 2, PH_DONE = 3 };
 
-template <class T> struct Lane {
-  int64_t item;   // global ray index, -1 when idle
-  int view;
-  int phase;
-  D3 dir;
-  // march_to state
-  double t, lo, hi;
-  int i, n, refines;
-  bool probing, bisecting, resolved;
-  // hit
+// State of one ray in flight.  The fields are shared between the phases: in the
+// march a = lo and b = hi (march_to's bracket); in the shadow phase a = the
+// distance along the shadow ray and b = the soft-shadow factor res; g holds the
+// gradient sum during the normal taps and the unit normal after them; k counts
+// bisection refines, normal taps or shadow steps.
+template <class T, bool kDir64> struct Lane {
+  int32_t item;   // work-item index inside the launch, -1 when idle
+  int32_t view;
+  int32_t phase;
+  Dir<kDir64> dir;
+  double t, a, b;
+  float gx, gy, gz;
   float trap;
-  int iters;
-  // normal taps
-  int tap;
-  double gx, gy, gz;
-  // shadow
-  double nx, ny, nz, st, res;
-  int sstep;
+  int32_t i, n, k, iters;
   uint32_t evals;
-  bool was_hit;
-  uint32_t ev_march, ev_normal, ev_shadow;
+  uint32_t mev;   // evaluations the march used (set when the march ends)
+  bool probing, bisecting, resolved, hit;
 
-  ND_DEV_INLINE void start(const DevView& v, int64_t it, int vidx) {
+  ND_DEV_INLINE void start(const DevView& v, int32_t it, int32_t vidx) {
     item = it;
     view = vidx;
-    dir = ray_dir(v, it - v.ray_offset);
+    dir.set(ray_dir(v, int64_t(it) - v.ray_offset));
     phase = PH_MARCH;
-    t = lo = hi = 0.0;
-    i = n = refines = 0;
-    probing = true;
-    bisecting = resolved = false;
-    trap = 0.0f;
+    t = a = b = 0.0;
+    i = n = k = 0;
     iters = 0;
+    probing = true;
+    bisecting = resolved = hit = false;
+    trap = 0.0f;
     evals = 0;
-  }
-
-  ND_DEV_INLINE D3 hit_pos(const DevView& v) const {
-    return fmadd(d3(v.org[0], v.org[1], v.org[2]), dir, t);
+    mev = 0;
+    if (v.max_samples <= 0) phase = PH_DONE;  // march_to's loop never runs: a miss
   }
 
   // Position of this lane's next DE sample.
   ND_DEV_INLINE D3 sample_pos(const DevView& v) const {
     const D3 o = d3(v.org[0], v.org[1], v.org[2]);
-    if (phase == PH_MARCH) return fmadd(o, dir, probing ? t : 0.5 * (lo + hi));
-    const D3 p = fmadd(o, dir, t);
+    const D3 d = dir.get();
+    if (phase == PH_MARCH) return fmadd(o, d, probing ? t : 0.5 * (a + b));
+    const D3 p = fmadd(o, d, t);
     if (phase == PH_NORMAL) {
       if (v.normal_mode == ND_NORMAL_CENTRAL) {
         const double h = v.normal_h_coef > 0.0f ? double(v.normal_h_coef) * t : march_eps<T>(v, t);
-        const double s = (tap & 1) ? -h : h;
-        const int a = tap >> 1;
-        return d3(p.x + (a == 0 ? s : 0.0), p.y + (a == 1 ? s : 0.0), p.z + (a == 2 ? s : 0.0));
+        const double s = (k & 1) ? -h : h;
+        const int ax = k >> 1;
+        return d3(p.x + (ax == 0 ? s : 0.0), p.y + (ax == 1 ? s : 0.0), p.z + (ax == 2 ? s : 0.0));
       }
-      const double e = march_eps<T>(v, t);
-      return fmadd(p, tetra_k(tap), e);
+      return fmadd(p, tetra_k(k), march_eps<T>(v, t));
     }
     // PH_SHADOW: origin = hit + n * bias, then along the light direction
-    const D3 so = fmadd(p, d3(nx, ny, nz), kShadowBias);
-    return fmadd(so, d3(v.light[0], v.light[1], v.light[2]), st);
+    const D3 so = fmadd(p, d3(gx, gy, gz), kShadowBias);
+    return fmadd(so, d3(v.light[0], v.light[1], v.light[2]), a);
   }
 
-  ND_DEV_INLINE int normal_taps(const DevView& v) const {
-    return v.normal_mode == ND_NORMAL_CENTRAL ? 6 : 4;
-  }
-
-  ND_DEV_INLINE void finish(const DevView& v, const nd_gbuffer& g, bool hit, float vis, Stats* ls) {
+  ND_DEV_INLINE void finish(const DevView& v, const nd_gbuffer& g, float vis) {
+    if (!hit) mev = evals;
     RayResult r;
     r.hit = hit;
     r.t = t;
@@ -397,142 +410,132 @@ template <class T> struct Lane {
     r.iters = hit ? uint32_t(iters) : 0u;
     r.steps = hit ? uint32_t(i) : uint32_t(v.max_steps);
     r.evals = evals;
-    r.nx = hit ? float(nx) : 0.0f;
-    r.ny = hit ? float(ny) : 0.0f;
-    r.nz = hit ? float(nz) : 0.0f;
+    r.nx = hit ? gx : 0.0f;
+    r.ny = hit ? gy : 0.0f;
+    r.nz = hit ? gz : 0.0f;
     r.shadow = vis;
-    r.shade = hit ? lambert(v, dir, nx, ny, nz, vis) : 0.0f;
-    write_result(g, v.out_offset + (item - v.ray_offset), r);
-    was_hit = hit;
+    r.shade = hit ? lambert(v, dir.get(), gx, gy, gz, vis) : 0.0f;
+    write_result(g, v.out_offset + (int64_t(item) - v.ray_offset), r);
     phase = PH_DONE;
   }
 
-  // Enter the normal phase at hit distance t with the hit's DE output.
-  ND_DEV_INLINE void record_hit(const DEOut<T>& de) {
-    trap = float(de.trap);
-    iters = de.iters;
-  }
-
-  ND_DEV_INLINE void begin_normal() {
+  ND_DEV_INLINE void begin_normal(double at) {
+    mev = evals;
+    t = at;
+    hit = true;
     phase = PH_NORMAL;
-    tap = 0;
-    gx = gy = gz = 0.0;
+    k = 0;
+    gx = gy = gz = 0.0f;
   }
 
-  // Consume one DE result.  Returns nothing; sets phase = PH_DONE when the ray is
-  // finished (its outputs are then written).
-  ND_DEV_INLINE void advance(const DevView& v, const DEOut<T>& de, const nd_gbuffer& g, Stats* ls) {
+  // Consume one DE result; sets phase = PH_DONE (outputs written) when finished.
+  ND_DEV_INLINE void advance(const DevView& v, const DEOut<T>& de, const nd_gbuffer& g) {
     ++evals;
     const double d = double(de.d);
     if (phase == PH_MARCH) {
-      ++ev_march;
-      // one iteration of march_to's sample loop (tpl:1881-1960)
-      const int budget = v.refine;
+      // one pass of march_to's sample loop (tpl:1881-1960); a = lo, b = hi
       const bool on_hit = v.verify == 0;
-      const int refine_budget = on_hit ? 0 : budget;
-      const int bisect_budget = on_hit ? budget : 0;
-      const double st = probing ? t : 0.5 * (lo + hi);
+      const int refine_budget = on_hit ? 0 : v.refine;
+      const int bisect_budget = on_hit ? v.refine : 0;
+      const double st = probing ? t : 0.5 * (a + b);
       const double e = march_eps<T>(v, st);
       ++n;
       if (bisecting) {
         if (d < e) {
-          hi = st;
-          record_hit(de);
+          b = st;
+          trap = float(de.trap);
+          iters = de.iters;
         } else {
-          lo = st;
+          a = st;
         }
-        ++refines;
-        if (hi - lo <= e || refines >= bisect_budget) {
-          t = hi;
-          begin_normal();
-        } else if (n >= v.max_samples) {
-          finish(v, g, false, 1.0f, ls);  // the loop of march_to ran out: a miss
-        }
+        ++k;
+        if (b - a <= e || k >= bisect_budget) begin_normal(b);
+        else if (n >= v.max_samples) finish(v, g, 1.0f);  // march_to's loop ran out: a miss
         return;
       }
       if (d < e) {
-        record_hit(de);
-        if (on_hit && bisect_budget > 0 && st - lo > e) {
+        trap = float(de.trap);
+        iters = de.iters;
+        if (on_hit && bisect_budget > 0 && st - a > e) {
           bisecting = true;
           probing = false;
-          hi = st;
-          refines = 0;
-          if (n >= v.max_samples) finish(v, g, false, 1.0f, ls);
+          b = st;
+          k = 0;
+          if (n >= v.max_samples) finish(v, g, 1.0f);
           return;
         }
-        t = st;
-        begin_normal();
+        begin_normal(st);
         return;
       }
       if (probing) {
-        lo = t;
-        hi = t + d;
-        refines = 0;
+        a = t;
+        b = t + d;
+        k = 0;
         resolved = false;
         probing = false;
       } else {
-        if (d >= hi - st) resolved = true;
-        else hi = st;
-        ++refines;
+        if (d >= b - st) resolved = true;
+        else b = st;
+        ++k;
       }
-      if (resolved || refines >= refine_budget) {
-        if (v.hq && !resolved && refine_budget > 0) hi = fmin(hi, lo + fmax(t, 1.0) * v.footprint);
-        t = hi;
+      if (resolved || k >= refine_budget) {
+        if (v.hq && !resolved && refine_budget > 0) b = fmin(b, a + fmax(t, 1.0) * v.footprint);
+        t = b;
         ++i;
         if (t > v.max_dist || i >= v.max_steps) {
-          finish(v, g, false, 1.0f, ls);
+          finish(v, g, 1.0f);
           return;
         }
         probing = true;
       }
-      if (n >= v.max_samples) finish(v, g, false, 1.0f, ls);
+      if (n >= v.max_samples) finish(v, g, 1.0f);
       return;
     }
     if (phase == PH_NORMAL) {
-      ++ev_normal;
       if (v.normal_mode == ND_NORMAL_CENTRAL) {
-        const double s = (tap & 1) ? -d : d;
-        const int a = tap >> 1;
-        if (a == 0) gx += s;
-        else if (a == 1) gy += s;
+        const float s = float((k & 1) ? -d : d);
+        const int ax = k >> 1;
+        if (ax == 0) gx += s;
+        else if (ax == 1) gy += s;
         else gz += s;
       } else {
-        const D3 k = tetra_k(tap);
-        gx += k.x * d;
-        gy += k.y * d;
-        gz += k.z * d;
+        const D3 kk = tetra_k(k);
+        gx += float(kk.x * d);
+        gy += float(kk.y * d);
+        gz += float(kk.z * d);
       }
-      ++tap;
-      if (tap < normal_taps(v)) return;
-      const double l = sqrt(gx * gx + gy * gy + gz * gz);
-      const double inv = l > 0.0 ? 1.0 / l : 0.0;
-      nx = gx * inv;
-      ny = gy * inv;
-      nz = gz * inv;
-      if (!v.shadow) {
-        finish(v, g, true, 1.0f, ls);
+      ++k;
+      if (k < (v.normal_mode == ND_NORMAL_CENTRAL ? 6 : 4)) return;
+      const float l = sqrtf(gx * gx + gy * gy + gz * gz);
+      const float inv = l > 0.0f ? 1.0f / l : 0.0f;
+      gx *= inv;
+      gy *= inv;
+      gz *= inv;
+      const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
+      if (!v.shadow || steps <= 0 || kShadowBias >= 2.0 * v.max_dist) {
+        finish(v, g, 1.0f);
         return;
       }
       phase = PH_SHADOW;
-      st = kShadowBias;
-      res = 1.0;
-      sstep = 0;
-      const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
-      if (steps <= 0 || st >= 2.0 * v.max_dist) finish(v, g, true, 1.0f, ls);
+      a = kShadowBias;  // distance along the shadow ray
+      b = 1.0;          // res
+      k = 0;
       return;
     }
     // PH_SHADOW: one step of visibility_march (tpl:2294-2341), opaque scene
-    ++ev_shadow;
     if (d < kShadowHitEps) {
-      finish(v, g, true, 0.0f, ls);
+      finish(v, g, 0.0f);
       return;
     }
-    res = fmin(res, double(v.shadow_k) * d / st);
-    st += fmax(d, kShadowMinStep);
-    ++sstep;
+    b = fmin(b, double(v.shadow_k) * d / a);
+    a += fmax(d, kShadowMinStep);
+    ++k;
     const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
-    if (sstep >= steps || st >= 2.0 * v.max_dist) finish(v, g, true, float(fmin(fmax(res, 0.0), 1.0)), ls);
+    if (k >= steps || a >= 2.0 * v.max_dist) finish(v, g, float(fmin(fmax(b, 0.0), 1.0)));
   }
 };
+
+// Normal taps of a view (4 tetrahedral or 6 central-difference evaluations).
+ND_DEV_INLINE uint32_t normal_taps(const DevView& v) { return v.normal_mode == ND_NORMAL_CENTRAL ? 6u : 4u; }
 
 }  // namespace nd

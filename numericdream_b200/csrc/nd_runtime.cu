@@ -225,12 +225,10 @@ nd_status plan(nd_ctx* ctx, const nd_view_desc* views, int nviews, std::vector<L
   return ND_OK;
 }
 
-LaunchFn pick(const KernelTable& t, int kernel, int prec, bool batched) {
-  if (prec == 64) {
-    if (kernel == ND_KERNEL_PLAIN) return batched ? t.plain_f64_batched : t.plain_f64;
-    return batched ? t.persistent_f64_batched : t.persistent_f64;
-  }
-  if (kernel == ND_KERNEL_PLAIN) return batched ? t.plain_f32_batched : t.plain_f32;
+LaunchFn pick(const KernelTable& t, int kernel, int prec, bool batched, bool dir64) {
+  if (kernel == ND_KERNEL_PLAIN) return prec == 64 ? t.plain_f64 : (dir64 ? t.plain_f32_dir64 : t.plain_f32);
+  if (prec == 64) return batched ? t.persistent_f64_batched : t.persistent_f64;
+  if (dir64) return batched ? t.persistent_f32_dir64_batched : t.persistent_f32_dir64;
   return batched ? t.persistent_f32_batched : t.persistent_f32;
 }
 
@@ -285,6 +283,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       a.views = d_views + base;
       a.nviews = nv;
       a.total_rays = rays;
+      if (rays > int64_t(0x7fffffff)) return fail(ctx, ND_ERR_INVALID, "more than 2^31-1 rays in one launch");
       a.out = *out;
       a.counter = d_counters + p;
       a.stats = ctx->d_stats;
@@ -296,10 +295,21 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       c.block = 128;
       c.blocks_per_sm = opts && opts->blocks_per_sm ? opts->blocks_per_sm : tu.blocks_per_sm;
       c.num_sms = ctx->num_sms;
-      const bool batched = nv > 1;
-      LaunchFn fn = pick(L.table, kernel, prec, batched);
-      e = fn(a, h_views[base], c, stream);
-      if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+      bool dir64 = false;
+      for (int k = 0; k < nv; ++k) dir64 |= h_views[base + k].dir64 != 0;
+      if (kernel == ND_KERNEL_PLAIN) {
+        // the plain baseline: one launch per view, one thread per ray
+        for (int k = 0; k < nv; ++k) {
+          LaunchFn fn = pick(L.table, kernel, prec, false, h_views[base + k].dir64 != 0);
+          e = fn(a, h_views[base + k], c, stream);
+          if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+        }
+      } else {
+        const bool batched = nv > 1;
+        LaunchFn fn = pick(L.table, kernel, prec, batched, dir64);
+        e = fn(a, h_views[base], c, stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+      }
       used = kernel;
     }
     base += nv;

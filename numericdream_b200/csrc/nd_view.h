@@ -60,6 +60,11 @@ inline DevView make_dev_view(const nd_view_desc& v, int64_t ray_offset, int64_t 
   const int bisect = v.march_verify ? 0 : v.refine_budget;
   const int64_t ms = int64_t(v.max_steps) * (1 + refine) + bisect;
   d.max_samples = int32_t(std::min<int64_t>(ms, 0x7fffffff));
+  // FP64 ray directions when the camera's pixel footprint approaches an FP32 ulp
+  // (deep zoom) or when the view asks for them
+  const double rn = sqrt(v.right[0] * v.right[0] + v.right[1] * v.right[1] + v.right[2] * v.right[2]);
+  const double un = sqrt(v.up[0] * v.up[0] + v.up[1] * v.up[1] + v.up[2] * v.up[2]);
+  d.dir64 = ((v.flags & ND_VIEW_DIR64) != 0 || std::max(rn, un) < 1e-3) ? 1 : 0;
   return d;
 }
 

@@ -5,11 +5,14 @@ from __future__ import annotations
 import numpy as np
 
 
-def compare(gpu: dict, ref: dict) -> dict:
-    """Statistics of one G-buffer against an oracle run of the same rays."""
+def compare(gpu: dict, ref: dict, mask=None) -> dict:
+    """Statistics of one G-buffer against an oracle run of the same rays; the
+    depth/normal/trap errors are taken over rays both hit (and inside mask)."""
     gh = gpu["normal"][:, 3] > 0.5
     rh = ref["normal"][:, 3] > 0.5
     both = gh & rh
+    if mask is not None:
+        both = both & mask
     out = {"rays": int(gh.size), "hits_gpu": int(gh.sum()), "hits_ref": int(rh.sum()),
            "hit_mismatch": int((gh != rh).sum()),
            "steps_mismatch": int((gpu["steps"].astype(np.int64) != ref["steps"].astype(np.int64)).sum()),
@@ -57,4 +60,5 @@ def policy_check(gpu: dict, base64: dict, unstable, max_strict_frac=0.001, agg_t
     ok &= abs(out["hit_frac_gpu"] - out["hit_frac_f64"]) <= agg_tol
     ok &= abs(out["mean_steps_gpu"] - out["mean_steps_f64"]) <= agg_tol * max(out["mean_steps_f64"], 1.0)
     out["ok"] = bool(ok)
+    out["strict_mask"] = strict
     return out
