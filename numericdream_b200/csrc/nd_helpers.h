@@ -60,6 +60,14 @@ template <class T> ND_HD_INLINE T bulb_log_escape(IterCarry<T> c) {
   return min(est, r);
 }
 
+// sin and cos of one angle (one shared range reduction for f32/f64).
+template <class T> ND_HD_INLINE void sin_cos(T x, T& s, T& c) {
+  s = sin(x);
+  c = cos(x);
+}
+ND_HD_INLINE void sin_cos(float x, float& s, float& c) { sincosf(x, &s, &c); }
+ND_HD_INLINE void sin_cos(double x, double& s, double& c) { ::sincos(x, &s, &c); }
+
 // template.wgsl:1013 (BULB_BAILOUT) and 1019-1031: one Mandelbulb power step in
 // spherical coordinates (theta from +z, phi = atan2(y, x)); no-op once r > 2.
 template <class T> ND_HD_INLINE IterCarry<T> bulb_power_step(IterCarry<T> c, v3<T> add, T power) {
@@ -70,8 +78,10 @@ template <class T> ND_HD_INLINE IterCarry<T> bulb_power_step(IterCarry<T> c, v3<
   const T rp = pow(r, power - T(1));
   const T zr = rp * r;
   const T dr = rp * power * c.dr + T(1);
-  const T st = sin(theta);
-  const v3<T> z = v3<T>(st * cos(phi), st * sin(phi), cos(theta)) * zr + add;
+  T st, ct, sp, cp;
+  sin_cos(theta, st, ct);
+  sin_cos(phi, sp, cp);
+  const v3<T> z = v3<T>(st * cp, st * sp, ct) * zr + add;
   return IterCarry<T>{z, dr};
 }
 

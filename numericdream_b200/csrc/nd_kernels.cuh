@@ -6,13 +6,11 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "nd_rayprog.h"
 
 namespace nd {
-
-#ifndef ND_PERSISTENT_MIN_BLOCKS
-#define ND_PERSISTENT_MIN_BLOCKS 1
-#endif
 
 __device__ __forceinline__ int64_t globaltimer_ns() {
   uint64_t t;
@@ -42,13 +40,19 @@ __device__ __forceinline__ void flush_stats(Stats* s, unsigned long long rays, u
   }
 }
 
+// Residency the kernels are compiled for: 8 blocks of 128 threads per SM with an
+// FP32 DE (at most 64 registers per thread), 4 with an FP64 DE.
+template <class T> struct MinBlocks {
+  static constexpr int value = sizeof(T) == 4 ? 8 : 4;
+};
+
 // --------------------------------------------------------------- plain kernel
 // The reference's per-pixel program as a plain per-view launch: one thread per
 // ray, the march loop of march_to, then the normal taps of estimate_normal, then
 // the shadow loop of visibility_march, each loop running until its slowest lane
 // in the warp is done (fs_simple tpl:4522-4538 / simple_geometry tpl:4492-4507).
 template <class Set, class T, bool kDir64>
-__global__ void __launch_bounds__(128) plain_kernel(const __grid_constant__ LaunchArgs a,
+__global__ void __launch_bounds__(128, MinBlocks<T>::value) plain_kernel(const __grid_constant__ LaunchArgs a,
                                                     const __grid_constant__ DevView v) {
   const int64_t local = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;  // ray index inside the view
   unsigned long long rays = 0, hits = 0, m = 0, nn = 0, sh = 0;
@@ -80,14 +84,17 @@ __global__ void __launch_bounds__(128) plain_kernel(const __grid_constant__ Laun
 // --------------------------------------------------------------- persistent kernel
 // One resident grid; every warp keeps 32 rays in flight.  After each DE
 // evaluation the warp ballots its idle lanes; once at least refill_threshold
-// lanes are idle (or all are), the first idle lane takes that many new ray
-// indices with ONE atomicAdd on the work counter and hands them out by
-// popc-prefix rank (the analogue of the reference's workgroup-aggregated queue
-// reservation wf_reserve, tpl:5083-5105).  Whatever phase a lane is in, each pass
-// of the loop is one DE evaluation for every busy lane.
+// lanes are idle (or all are) it hands them the next ray indices by popc-prefix
+// rank.  The indices come from a warp-private run of `chunk` consecutive rays that
+// the warp takes from the global work counter with ONE atomicAdd whenever the run
+// is used up, so most refills touch no global atomic (the reference reserves
+// queue slots with workgroup-aggregated atomics instead, wf_reserve
+// tpl:5083-5105), and a warp keeps marching neighbouring pixels.  Whatever phase
+// a lane is in, each pass of the loop is one DE evaluation for every busy lane.
+
 template <class Set, class T, bool kDir64, bool kBatched>
-__global__ void __launch_bounds__(128, ND_PERSISTENT_MIN_BLOCKS) persistent_kernel(const __grid_constant__ LaunchArgs a,
-                                                         const __grid_constant__ DevView single) {
+__global__ void __launch_bounds__(128, MinBlocks<T>::value)
+    persistent_kernel(const __grid_constant__ LaunchArgs a, const __grid_constant__ DevView single) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
@@ -101,6 +108,8 @@ __global__ void __launch_bounds__(128, ND_PERSISTENT_MIN_BLOCKS) persistent_kern
   const int64_t deadline = __shfl_sync(full, globaltimer_ns(), 0) + a.deadline_ns;
   int tick = 0;
   const int32_t total = int32_t(a.total_rays);
+  int32_t wnext = 0, wend = 0;  // warp-uniform: taken but not yet started rays [wnext, wend)
+  const int thr = a.refill_threshold;
   while (true) {
     if (L.phase == PH_DONE && L.item >= 0) {
       ++rays;
@@ -112,26 +121,40 @@ __global__ void __launch_bounds__(128, ND_PERSISTENT_MIN_BLOCKS) persistent_kern
       L.item = -1;
     }
     const unsigned idle = __ballot_sync(full, L.item < 0);
-    if (!exhausted && idle != 0u && (__popc(idle) >= a.refill_threshold || idle == full)) {
-      const int want = __popc(idle);
-      const int leader = __ffs(idle) - 1;
-      int32_t base = 0;
-      if (lane == leader) base = int32_t(atomicAdd(a.counter, (unsigned long long)want));
-      base = __shfl_sync(full, base, leader);
-      ++refills;
-      if (int64_t(base) + want >= int64_t(total)) exhausted = true;
+    const int nidle = __popc(idle);
+    const bool have_work = !exhausted || wnext < wend;
+    if (have_work && nidle != 0 && (nidle >= thr || idle == full)) {
+      int avail = wend - wnext;
+      int32_t base = 0, nnew = 0;
+      if (avail < nidle && !exhausted) {
+        // enough whole runs to fill every idle lane
+        const int take = ((nidle - avail + a.chunk - 1) / a.chunk) * a.chunk;
+        if (lane == 0) base = int32_t(atomicAdd(a.counter, (unsigned long long)take));
+        base = __shfl_sync(full, base, 0);
+        ++refills;
+        nnew = base < total ? min(take, total - base) : 0;
+        if (int64_t(base) + take >= int64_t(total)) exhausted = true;
+      }
+      const int used = min(nidle, avail + nnew);
       if (L.item < 0) {
-        const int32_t it = base + __popc(idle & lt_mask);
-        if (it < total && it >= 0) {
+        const int r = __popc(idle & lt_mask);
+        if (r < used) {
+          const int32_t it = r < avail ? wnext + r : base + (r - avail);
           L.view = kBatched ? find_view(a.views, a.nviews, it) : 0;
           const DevView& v = kBatched ? a.views[L.view] : single;
           L.start(v, it, L.view);
           if (L.phase == PH_DONE) L.finish(v, a.out, 1.0f);
         }
       }
+      if (used <= avail) {
+        wnext += used;
+      } else {
+        wnext = base + (used - avail);
+        wend = base + nnew;
+      }
       continue;  // lanes that finished at once go back through the bookkeeping
     }
-    if (exhausted && idle == full) break;
+    if (!have_work && idle == full) break;
     if (((++tick) & 63) == 0) {
       // lane 0's clock decides for the whole warp, so the exit stays warp-uniform
       const int64_t now = __shfl_sync(full, globaltimer_ns(), 0);
@@ -180,7 +203,12 @@ cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const 
   const int64_t needed = (a.total_rays + block - 1) / block;
   if (grid > needed) grid = needed;
   if (grid <= 0) return cudaSuccess;
-  persistent_kernel<Set, T, kDir64, kBatched><<<unsigned(grid), block, 0, s>>>(a, single);
+  // runs of up to 64 rays per warp refill, but at least ~4 runs per warp so that
+  // small launches still spread over every warp
+  LaunchArgs b = a;
+  const int64_t warps = grid * (block / 32);
+  b.chunk = int32_t(std::max<int64_t>(1, std::min<int64_t>(64, a.total_rays / (warps * 4))));
+  persistent_kernel<Set, T, kDir64, kBatched><<<unsigned(grid), block, 0, s>>>(b, single);
   return cudaGetLastError();
 }
 

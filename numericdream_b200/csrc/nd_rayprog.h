@@ -95,6 +95,7 @@ struct LaunchArgs {
   unsigned long long* counter;  // persistent work counter (zeroed before launch)
   Stats* stats;
   int32_t refill_threshold;
+  int32_t chunk;              // rays a warp takes from the work counter at a time
   int64_t deadline_ns;        // watchdog budget (globaltimer units)
 };
 
