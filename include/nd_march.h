@@ -168,10 +168,11 @@ typedef struct nd_march_opts {
 
 typedef struct nd_stats {
   uint64_t rays;
-  uint64_t de_evals;        /* all DE evaluations: probes, bisection, normals, shadows */
+  uint64_t de_evals;        /* all DE evaluations: march, normals, shadows and trap pass */
   uint64_t march_evals;     /* primary march probes + refinement */
   uint64_t normal_evals;
   uint64_t shadow_evals;
+  uint64_t trap_evals;      /* one DE with the orbit trap per hit (when trap/iters are requested) */
   uint64_t hits;
   uint64_t refills;         /* persistent kernel: warp refills */
   uint32_t timeouts;        /* watchdog expiries */

@@ -59,20 +59,20 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value) plain_kernel(const _
   if (local < v.rays) {
     Lane<T, kDir64> L;
     L.start(v, int32_t(v.ray_offset + local), 0);
-    if (L.phase == PH_DONE) L.finish(v, a.out, 1.0f);
+    if (L.phase == PH_DONE) L.finish(v, a.out, a.t_hit, 1.0f);
     while (L.phase == PH_MARCH) {
       const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(L.sample_pos(v)), v);
-      L.advance(v, de, a.out);
+      L.advance(v, de, a.out, a.t_hit);
     }
     m = L.evals;
     while (L.phase == PH_NORMAL) {
       const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(L.sample_pos(v)), v);
-      L.advance(v, de, a.out);
+      L.advance(v, de, a.out, a.t_hit);
     }
     nn = L.evals - m;
     while (L.phase == PH_SHADOW) {
       const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(L.sample_pos(v)), v);
-      L.advance(v, de, a.out);
+      L.advance(v, de, a.out, a.t_hit);
     }
     sh = L.evals - m - nn;
     rays = 1;
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
           L.view = kBatched ? find_view(a.views, a.nviews, it) : 0;
           const DevView& v = kBatched ? a.views[L.view] : single;
           L.start(v, it, L.view);
-          if (L.phase == PH_DONE) L.finish(v, a.out, 1.0f);
+          if (L.phase == PH_DONE) L.finish(v, a.out, a.t_hit, 1.0f);
         }
       }
       if (used <= avail) {
@@ -166,10 +166,30 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     if (L.item >= 0) {
       const DevView& v = kBatched ? a.views[L.view] : single;
       const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(L.sample_pos(v)), v);
-      L.advance(v, de, a.out);
+      L.advance(v, de, a.out, a.t_hit);
     }
   }
   flush_stats(a.stats, rays, ev_m, ev_n, ev_s, hits, refills);
+}
+
+// --------------------------------------------------------------- trap pass
+// One thread per ray: the DE with the orbit trap at each hit point.  Coherent
+// (every hit costs exactly one evaluation), so it needs no refill.
+template <class Set, class T, bool kDir64, bool kBatched>
+__global__ void __launch_bounds__(128, MinBlocks<T>::value)
+    trap_kernel(const __grid_constant__ LaunchArgs a, const __grid_constant__ DevView single) {
+  const int64_t it = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (it >= a.total_rays) return;
+  const int vi = kBatched ? find_view(a.views, a.nviews, it) : 0;
+  const DevView& v = kBatched ? a.views[vi] : single;
+  const int64_t local = it - v.ray_offset;
+  const double t = a.t_hit[v.out_offset + local];
+  if (t < 0.0) {
+    if (a.out.trap) a.out.trap[v.out_offset + local] = 0.0f;
+    if (a.out.iters) a.out.iters[v.out_offset + local] = 0u;
+    return;
+  }
+  trap_at_hit<Set, T, kDir64>(v, local, t, a.out);
 }
 
 // --------------------------------------------------------------- launchers
@@ -214,6 +234,14 @@ cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const 
 
 typedef cudaError_t (*LaunchFn)(const LaunchArgs&, const DevView&, const LaunchConfig&, cudaStream_t);
 
+template <class Set, class T, bool kDir64, bool kBatched>
+cudaError_t launch_trap(const LaunchArgs& a, const DevView& single, const LaunchConfig&, cudaStream_t s) {
+  const int64_t grid = (a.total_rays + 127) / 128;
+  if (grid <= 0) return cudaSuccess;
+  trap_kernel<Set, T, kDir64, kBatched><<<unsigned(grid), 128, 0, s>>>(a, single);
+  return cudaGetLastError();
+}
+
 // DE of one formula at n points (the formula wrapper with its orbit trap), for
 // parity tests against fixed point sets.
 template <class Set, class T>
@@ -223,7 +251,7 @@ __global__ void __launch_bounds__(128) de_points_kernel(const __grid_constant__ 
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const ndw::v3<T> p = ndw::v3<T>(T(pts[3 * i]), T(pts[3 * i + 1]), T(pts[3 * i + 2]));
-  const DEOut<T> o = Set::template de<T>(v.code, p, v);
+  const DEOut<T> o = Set::template de<T, true>(v.code, p, v);
   de[i] = double(o.d);
   if (trap) trap[i] = double(o.trap);
   if (iters) iters[i] = uint32_t(o.iters);
@@ -247,6 +275,7 @@ struct KernelTable {
   LaunchFn plain_f32, plain_f32_dir64, plain_f64;
   LaunchFn persistent_f32, persistent_f32_batched, persistent_f32_dir64, persistent_f32_dir64_batched;
   LaunchFn persistent_f64, persistent_f64_batched;
+  LaunchFn trap_f32, trap_f32_batched, trap_f32_dir64, trap_f32_dir64_batched, trap_f64, trap_f64_batched;
   DePointsFn de_points_f32, de_points_f64;
 };
 
@@ -261,6 +290,12 @@ template <class Set> KernelTable make_kernel_table() {
   t.persistent_f32_dir64_batched = &launch_persistent<Set, float, true, true>;
   t.persistent_f64 = &launch_persistent<Set, double, true, false>;
   t.persistent_f64_batched = &launch_persistent<Set, double, true, true>;
+  t.trap_f32 = &launch_trap<Set, float, false, false>;
+  t.trap_f32_batched = &launch_trap<Set, float, false, true>;
+  t.trap_f32_dir64 = &launch_trap<Set, float, true, false>;
+  t.trap_f32_dir64_batched = &launch_trap<Set, float, true, true>;
+  t.trap_f64 = &launch_trap<Set, double, true, false>;
+  t.trap_f64_batched = &launch_trap<Set, double, true, true>;
   t.de_points_f32 = &launch_de_points<Set, float>;
   t.de_points_f64 = &launch_de_points<Set, double>;
   return t;

@@ -95,10 +95,15 @@ inline void count_ray(const DevView& view, int64_t ray, ndw::OpCounts* out, uint
   const ndw::OpCounts before = c;
   Lane<ndw::CF, false> L;
   L.start(v, int32_t(ray), 0);
-  if (L.phase == PH_DONE) L.finish(v, g, 1.0f);
+  if (L.phase == PH_DONE) L.finish(v, g, nullptr, 1.0f);
   while (L.phase != PH_DONE) {
     const DEOut<ndw::CF> de = Set::template de<ndw::CF>(v.code, to_t<ndw::CF>(L.sample_pos(v)), v);
-    L.advance(v, de, g);
+    L.advance(v, de, g, nullptr);
+  }
+  if (L.hit) {  // the trap pass: one DE with the orbit trap at the hit point
+    ++*evals;
+    g.trap = &depth;
+    trap_at_hit<Set, ndw::CF, false>(v, ray - v.ray_offset, L.t, g);
   }
   out->add += c.add - before.add;
   out->mul += c.mul - before.mul;

@@ -92,6 +92,7 @@ struct LaunchArgs {
   int32_t nviews;
   int64_t total_rays;
   nd_gbuffer out;             // device pointers
+  double* t_hit;              // FP64 hit distance per G-buffer slot (-1 on a miss), for the trap pass
   unsigned long long* counter;  // persistent work counter (zeroed before launch)
   Stats* stats;
   int32_t refill_threshold;
@@ -170,6 +171,9 @@ template <class T> struct ParamRef {
 
 // formula_N (fractal_renderer.zig:490-512) + the single-instance scene_de
 // (tpl:1611-1626, 1756-1779): identity instance transform, DE scaled by factor.
+// With kTrap the orbit trap and the count of iterations that changed the carry
+// are accumulated too; the march itself only needs the distance, so the kernels
+// evaluate the trap once per hit, at the hit point, in a separate pass.
 //
 // de_step(carry, pos, p) is a pure function of its arguments (the contract gives it
 // no iteration index), so once one iteration returns its input carry unchanged
@@ -178,11 +182,12 @@ template <class T> struct ParamRef {
 // distance again; average mode only counts changed iterations).  The loop stops
 // at that fixed point, e.g. as soon as a Mandelbulb point has escaped
 // (bulb_power_step returns the carry unchanged once r > 2, tpl:1019-1023).
-template <class F, class T>
+template <class F, class T, bool kTrap>
 ND_DEV_INLINE DEOut<T> formula_de(ndw::v3<T> pos, const float* params, const nd_trap_desc& trap, float factor) {
   const ParamRef<T> p{params};
   ndw::IterCarry<T> c{pos, T(1)};
-  TrapAcc<T> acc = trap_begin<T>(trap);
+  TrapAcc<T> acc;
+  if (kTrap) acc = trap_begin<T>(trap);
   int n = F::template iterations<T, ParamRef<T>>(p);
   n = n < kMaxIterations ? n : kMaxIterations;
   int changed = 0;
@@ -192,12 +197,14 @@ ND_DEV_INLINE DEOut<T> formula_de(ndw::v3<T> pos, const float* params, const nd_
     c = F::template step<T, ParamRef<T>>(c, pos, p);
     const bool ch = (c.z.x != zp.x) | (c.z.y != zp.y) | (c.z.z != zp.z);
     if (!ch && !(c.dr != drp)) break;  // fixed point: nothing changes any more
-    changed += ch ? 1 : 0;
-    trap_update(acc, trap, c.z, ch, it);
+    if (kTrap) {
+      changed += ch ? 1 : 0;
+      trap_update(acc, trap, c.z, ch, it);
+    }
   }
   DEOut<T> o;
   o.d = F::template finalize<T, ParamRef<T>>(c) * T(factor);
-  o.trap = trap_finish(acc, trap, n);
+  o.trap = kTrap ? trap_finish(acc, trap, n) : T(0);
   o.iters = changed;
   return o;
 }
@@ -206,16 +213,16 @@ ND_DEV_INLINE DEOut<T> formula_de(ndw::v3<T> pos, const float* params, const nd_
 // because batched views are ordered by formula).
 template <class... Fs> struct FormulaSet;
 template <class F> struct FormulaSet<F> {
-  template <class T>
+  template <class T, bool kTrap = false>
   static ND_DEV_INLINE DEOut<T> de(int, ndw::v3<T> pos, const DevView& v) {
-    return formula_de<F, T>(pos, v.params, v.trap, v.factor);
+    return formula_de<F, T, kTrap>(pos, v.params, v.trap, v.factor);
   }
 };
 template <class F, class G, class... Rest> struct FormulaSet<F, G, Rest...> {
-  template <class T>
+  template <class T, bool kTrap = false>
   static ND_DEV_INLINE DEOut<T> de(int code, ndw::v3<T> pos, const DevView& v) {
-    if (code == 0) return formula_de<F, T>(pos, v.params, v.trap, v.factor);
-    return FormulaSet<G, Rest...>::template de<T>(code - 1, pos, v);
+    if (code == 0) return formula_de<F, T, kTrap>(pos, v.params, v.trap, v.factor);
+    return FormulaSet<G, Rest...>::template de<T, kTrap>(code - 1, pos, v);
   }
 };
 
@@ -293,25 +300,24 @@ ND_DEV_INLINE D3 tetra_k(int i) {
 struct RayResult {
   double t;
   float nx, ny, nz;
-  float trap;
   float shade;
   float shadow;
-  uint32_t steps, iters, evals;
+  uint32_t steps, evals;
   bool hit;
 };
 
-ND_DEV_INLINE void write_result(const nd_gbuffer& g, int64_t r, const RayResult& o) {
+// Outputs of the march; t_hit (FP64 t on a hit, -1 on a miss) feeds the trap pass.
+ND_DEV_INLINE void write_result(const nd_gbuffer& g, double* t_hit, int64_t r, const RayResult& o) {
   // r is the G-buffer index (view out_offset + ray index inside the view)
   g.depth[r] = o.hit ? float(o.t) : 0.0f;
+  if (t_hit) t_hit[r] = o.hit ? o.t : -1.0;
   if (g.normal) {
     struct alignas(16) F4 {
       float x, y, z, w;
     };
     reinterpret_cast<F4*>(g.normal)[r] = F4{o.nx, o.ny, o.nz, o.hit ? 1.0f : 0.0f};
   }
-  if (g.trap) g.trap[r] = o.trap;
   if (g.steps) g.steps[r] = o.steps;
-  if (g.iters) g.iters[r] = o.iters;
   if (g.shade) g.shade[r] = o.shade;
   if (g.shadow) g.shadow[r] = o.shadow;
   if (g.depth64) g.depth64[r] = o.hit ? o.t : 0.0;
@@ -360,8 +366,7 @@ template <class T, bool kDir64> struct Lane {
   Dir<kDir64> dir;
   double t, a, b;
   float gx, gy, gz;
-  float trap;
-  int32_t i, n, k, iters;
+  int32_t i, n, k;
   uint32_t evals;
   uint32_t mev;   // evaluations the march used (set when the march ends)
   bool probing, bisecting, resolved, hit;
@@ -373,10 +378,8 @@ template <class T, bool kDir64> struct Lane {
     phase = PH_MARCH;
     t = a = b = 0.0;
     i = n = k = 0;
-    iters = 0;
     probing = true;
     bisecting = resolved = hit = false;
-    trap = 0.0f;
     evals = 0;
     mev = 0;
     if (v.max_samples <= 0) phase = PH_DONE;  // march_to's loop never runs: a miss
@@ -402,13 +405,11 @@ template <class T, bool kDir64> struct Lane {
     return fmadd(so, d3(v.light[0], v.light[1], v.light[2]), a);
   }
 
-  ND_DEV_INLINE void finish(const DevView& v, const nd_gbuffer& g, float vis) {
+  ND_DEV_INLINE void finish(const DevView& v, const nd_gbuffer& g, double* t_hit, float vis) {
     if (!hit) mev = evals;
     RayResult r;
     r.hit = hit;
     r.t = t;
-    r.trap = hit ? trap : 0.0f;
-    r.iters = hit ? uint32_t(iters) : 0u;
     r.steps = hit ? uint32_t(i) : uint32_t(v.max_steps);
     r.evals = evals;
     r.nx = hit ? gx : 0.0f;
@@ -416,7 +417,7 @@ template <class T, bool kDir64> struct Lane {
     r.nz = hit ? gz : 0.0f;
     r.shadow = vis;
     r.shade = hit ? lambert(v, dir.get(), gx, gy, gz, vis) : 0.0f;
-    write_result(g, v.out_offset + (int64_t(item) - v.ray_offset), r);
+    write_result(g, t_hit, v.out_offset + (int64_t(item) - v.ray_offset), r);
     phase = PH_DONE;
   }
 
@@ -430,7 +431,7 @@ template <class T, bool kDir64> struct Lane {
   }
 
   // Consume one DE result; sets phase = PH_DONE (outputs written) when finished.
-  ND_DEV_INLINE void advance(const DevView& v, const DEOut<T>& de, const nd_gbuffer& g) {
+  ND_DEV_INLINE void advance(const DevView& v, const DEOut<T>& de, const nd_gbuffer& g, double* t_hit) {
     ++evals;
     const double d = double(de.d);
     if (phase == PH_MARCH) {
@@ -444,25 +445,21 @@ template <class T, bool kDir64> struct Lane {
       if (bisecting) {
         if (d < e) {
           b = st;
-          trap = float(de.trap);
-          iters = de.iters;
         } else {
           a = st;
         }
         ++k;
         if (b - a <= e || k >= bisect_budget) begin_normal(b);
-        else if (n >= v.max_samples) finish(v, g, 1.0f);  // march_to's loop ran out: a miss
+        else if (n >= v.max_samples) finish(v, g, t_hit, 1.0f);  // march_to's loop ran out: a miss
         return;
       }
       if (d < e) {
-        trap = float(de.trap);
-        iters = de.iters;
         if (on_hit && bisect_budget > 0 && st - a > e) {
           bisecting = true;
           probing = false;
           b = st;
           k = 0;
-          if (n >= v.max_samples) finish(v, g, 1.0f);
+          if (n >= v.max_samples) finish(v, g, t_hit, 1.0f);
           return;
         }
         begin_normal(st);
@@ -484,12 +481,12 @@ template <class T, bool kDir64> struct Lane {
         t = b;
         ++i;
         if (t > v.max_dist || i >= v.max_steps) {
-          finish(v, g, 1.0f);
+          finish(v, g, t_hit, 1.0f);
           return;
         }
         probing = true;
       }
-      if (n >= v.max_samples) finish(v, g, 1.0f);
+      if (n >= v.max_samples) finish(v, g, t_hit, 1.0f);
       return;
     }
     if (phase == PH_NORMAL) {
@@ -514,7 +511,7 @@ template <class T, bool kDir64> struct Lane {
       gz *= inv;
       const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
       if (!v.shadow || steps <= 0 || kShadowBias >= 2.0 * v.max_dist) {
-        finish(v, g, 1.0f);
+        finish(v, g, t_hit, 1.0f);
         return;
       }
       phase = PH_SHADOW;
@@ -525,18 +522,35 @@ template <class T, bool kDir64> struct Lane {
     }
     // PH_SHADOW: one step of visibility_march (tpl:2294-2341), opaque scene
     if (d < kShadowHitEps) {
-      finish(v, g, 0.0f);
+      finish(v, g, t_hit, 0.0f);
       return;
     }
     b = fmin(b, double(v.shadow_k) * d / a);
     a += fmax(d, kShadowMinStep);
     ++k;
     const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
-    if (k >= steps || a >= 2.0 * v.max_dist) finish(v, g, float(fmin(fmax(b, 0.0), 1.0)));
+    if (k >= steps || a >= 2.0 * v.max_dist) finish(v, g, t_hit, float(fmin(fmax(b, 0.0), 1.0)));
   }
 };
 
 // Normal taps of a view (4 tetrahedral or 6 central-difference evaluations).
 ND_DEV_INLINE uint32_t normal_taps(const DevView& v) { return v.normal_mode == ND_NORMAL_CENTRAL ? 6u : 4u; }
+
+}  // namespace nd
+
+namespace nd {
+
+// The orbit trap and changed-iteration count at a ray's hit point: the formula
+// wrapper with its trap (formula_N) evaluated once at org + dir * t_hit.
+template <class Set, class T, bool kDir64>
+ND_DEV_INLINE void trap_at_hit(const DevView& v, int64_t local, double t, const nd_gbuffer& g) {
+  Dir<kDir64> dir;
+  dir.set(ray_dir(v, local));
+  const D3 p = fmadd(d3(v.org[0], v.org[1], v.org[2]), dir.get(), t);
+  const DEOut<T> de = Set::template de<T, true>(v.code, to_t<T>(p), v);
+  const int64_t r = v.out_offset + local;
+  if (g.trap) g.trap[r] = float(de.trap);
+  if (g.iters) g.iters[r] = uint32_t(de.iters);
+}
 
 }  // namespace nd

@@ -66,6 +66,9 @@ struct nd_ctx {
   unsigned long long* d_counters = nullptr;
   int counters_cap = 0;
   Stats* d_stats = nullptr;
+  double* d_thit = nullptr;    // FP64 hit distances for the trap pass
+  int64_t thit_cap = 0;
+  bool last_trap = false;
   DevView* h_views = nullptr;  // pinned staging
   int h_views_cap = 0;
   cudaStream_t last_stream = nullptr;
@@ -81,6 +84,8 @@ struct nd_graph {
   cudaGraphExec_t exec = nullptr;
   DevView* d_views = nullptr;
   unsigned long long* d_counters = nullptr;
+  double* d_thit = nullptr;
+  bool trap = false;
 };
 
 namespace {
@@ -244,7 +249,8 @@ Tuned tuned_for(const std::string& key) {
 // table is already on the device (graph replay).
 nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_march_opts* opts,
                   const nd_gbuffer* out, cudaStream_t stream, const std::vector<Launch>& plans, DevView* d_views,
-                  DevView* h_views, unsigned long long* d_counters, bool copy_views, int* kernel_used) {
+                  DevView* h_views, unsigned long long* d_counters, double* d_thit, bool copy_views,
+                  int* kernel_used) {
   const int prec = (opts && opts->de_precision == 64) ? 64 : 32;
   // global output offsets in call order
   std::vector<int64_t> out_off(nviews + 1, 0);
@@ -285,6 +291,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       a.total_rays = rays;
       if (rays > int64_t(0x7fffffff)) return fail(ctx, ND_ERR_INVALID, "more than 2^31-1 rays in one launch");
       a.out = *out;
+      a.t_hit = d_thit;
       a.counter = d_counters + p;
       a.stats = ctx->d_stats;
       a.refill_threshold = std::max(1, std::min(32, opts && opts->refill_threshold ? opts->refill_threshold : tu.refill_threshold));
@@ -309,6 +316,16 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
         LaunchFn fn = pick(L.table, kernel, prec, batched, dir64);
         e = fn(a, h_views[base], c, stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+      }
+      if (out->trap || out->iters) {
+        // orbit trap and iteration count at every hit point
+        const bool batched = nv > 1;
+        const nd::KernelTable& T = L.table;
+        LaunchFn tf = prec == 64 ? (batched ? T.trap_f64_batched : T.trap_f64)
+                                 : dir64 ? (batched ? T.trap_f32_dir64_batched : T.trap_f32_dir64)
+                                         : (batched ? T.trap_f32_batched : T.trap_f32);
+        e = tf(a, h_views[base], c, stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "trap pass launch");
       }
       used = kernel;
     }
@@ -485,6 +502,7 @@ nd_status nd_ctx_destroy(nd_ctx* ctx) {
   if (ctx->d_views) cudaFree(ctx->d_views);
   if (ctx->d_counters) cudaFree(ctx->d_counters);
   if (ctx->d_stats) cudaFree(ctx->d_stats);
+  if (ctx->d_thit) cudaFree(ctx->d_thit);
   if (ctx->h_views) cudaFreeHost(ctx->h_views);
   if (ctx->last_done) cudaEventDestroy(ctx->last_done);
   delete ctx;
@@ -523,6 +541,15 @@ nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
   if (ctx->have_last) cudaEventSynchronize(ctx->last_done);
   if ((s = ensure_dev(ctx, &ctx->d_views, &ctx->views_cap, nviews, "view table")) != ND_OK) return s;
   if ((s = ensure_dev(ctx, &ctx->d_counters, &ctx->counters_cap, int(plans.size()), "work counters")) != ND_OK) return s;
+  const bool want_trap = out->trap || out->iters;
+  if (want_trap && ctx->thit_cap < total) {
+    if (ctx->d_thit) cudaFree(ctx->d_thit);
+    ctx->d_thit = nullptr;
+    ctx->thit_cap = 0;
+    e = cudaMalloc((void**)&ctx->d_thit, sizeof(double) * size_t(total));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "hit-distance buffer");
+    ctx->thit_cap = total;
+  }
   if (ctx->h_views_cap < nviews) {
     if (ctx->h_views) cudaFreeHost(ctx->h_views);
     ctx->h_views = nullptr;
@@ -532,7 +559,8 @@ nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
     ctx->h_views_cap = std::max(nviews, 64);
   }
   int kernel = 0;
-  s = enqueue(ctx, views, nviews, opts, out, st, plans, ctx->d_views, ctx->h_views, ctx->d_counters, true, &kernel);
+  s = enqueue(ctx, views, nviews, opts, out, st, plans, ctx->d_views, ctx->h_views, ctx->d_counters,
+              want_trap ? ctx->d_thit : nullptr, true, &kernel);
   if (s != ND_OK) return s;
   e = cudaEventRecord(ctx->last_done, st);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "record event");
@@ -540,6 +568,7 @@ nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
   ctx->last_stream = st;
   ctx->last_kernel = kernel;
   ctx->last_rays = total;
+  ctx->last_trap = want_trap;
   return ND_OK;
 }
 
@@ -559,6 +588,8 @@ nd_status nd_last_stats(nd_ctx* ctx, nd_stats* out) {
   out->march_evals = h.march_evals;
   out->normal_evals = h.normal_evals;
   out->shadow_evals = h.shadow_evals;
+  out->trap_evals = ctx->last_trap ? h.hits : 0;
+  out->de_evals += out->trap_evals;
   out->hits = h.hits;
   out->refills = h.refills;
   out->timeouts = h.timeouts;
@@ -652,8 +683,10 @@ nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
   cudaSetDevice(ctx->device);
   nd_graph* g = new nd_graph();
   g->ctx = ctx;
+  g->trap = out->trap || out->iters;
   cudaError_t e = cudaMalloc((void**)&g->d_views, sizeof(DevView) * size_t(nviews));
   if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_counters, sizeof(unsigned long long) * plans.size());
+  if (e == cudaSuccess && g->trap) e = cudaMalloc((void**)&g->d_thit, sizeof(double) * size_t(std::max<int64_t>(total, 1)));
   if (e != cudaSuccess) {
     nd_graph_destroy(g);
     return cuda_fail(ctx, e, "graph buffers");
@@ -673,7 +706,8 @@ nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
     nd_graph_destroy(g);
     return cuda_fail(ctx, e, "begin capture");
   }
-  s = enqueue(ctx, views, nviews, opts, out, cap, plans, g->d_views, hv.data(), g->d_counters, false, nullptr);
+  s = enqueue(ctx, views, nviews, opts, out, cap, plans, g->d_views, hv.data(), g->d_counters, g->d_thit, false,
+              nullptr);
   cudaGraph_t gr = nullptr;
   e = cudaStreamEndCapture(cap, &gr);
   cudaStreamDestroy(cap);
@@ -702,6 +736,7 @@ nd_status nd_graph_launch(nd_graph* g, void* stream) {
   e = cudaEventRecord(g->ctx->last_done, (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(g->ctx, e, "record event");
   g->ctx->have_last = true;
+  g->ctx->last_trap = g->trap;
   return ND_OK;
 }
 
@@ -712,6 +747,7 @@ nd_status nd_graph_destroy(nd_graph* g) {
   if (g->graph) cudaGraphDestroy(g->graph);
   if (g->d_views) cudaFree(g->d_views);
   if (g->d_counters) cudaFree(g->d_counters);
+  if (g->d_thit) cudaFree(g->d_thit);
   delete g;
   return ND_OK;
 }

@@ -56,7 +56,8 @@ def test_c1_small_parity(ctx):
     print("vs oracle f64:", c64)
     n = c32["rays"]
     assert st.rays == n and st.timeouts == 0
-    assert st.de_evals == int(gp["evals"].astype(np.int64).sum())
+    assert st.de_evals == int(gp["evals"].astype(np.int64).sum()) + st.trap_evals
+    assert st.trap_evals == st.hits
     from oracle import pyoracle
 
     unstable, base = pyoracle.unstable_rays(views[0], "mandelbrot")
