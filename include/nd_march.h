@@ -216,6 +216,22 @@ nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
 nd_status nd_graph_launch(nd_graph* graph, void* stream);
 nd_status nd_graph_destroy(nd_graph* graph);
 
+/* Forward march that allocates nothing: no cudaMalloc, no cudaFree, no context.
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (a host whose allocator owns the device, a render thread where an
+ * allocation may synchronise the device, loops that must not allocate after
+ * start-up).  Runs the persistent kernel on the current device and the given
+ * stream; its scratch (view table, work counters, statistics) is a fixed array of
+ * about 28 KB inside the library, present on every GPU that loads it.
+ * Limits: at most 64 views and 2^31-1 rays per call; trap and iters outputs are
+ * not available here (they need per-ray scratch) and return ND_ERR_UNSUPPORTED.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  Every call shares the one array: calls
+ * that overlap on the GPU (different streams, or host threads) race, so serialise
+ * them.  views is a HOST array; the G-buffer pointers are DEVICE pointers. */
+nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t nviews, const nd_march_opts* opts,
+                                   const nd_gbuffer* out, void* stream);
+
 /* DE of view->formula (with view->params and view->trap) at n points: pts is a
  * DEVICE array of 3n doubles; de, trap (nullable) and iters (nullable) are DEVICE
  * arrays of n.  Each point runs the formula wrapper of the reference (carry =

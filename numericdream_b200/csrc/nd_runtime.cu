@@ -781,3 +781,190 @@ size_t nd_sizeof(const char* name) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Forward march without any allocation.
+//
+// Some callers cannot allocate device memory: code that runs inside a host
+// framework whose allocator owns all device memory (a renderer plug-in, a game
+// engine with a fixed budget), hosts that forbid cudaMalloc on their render thread
+// because it may synchronise the device, and embedded or real-time loops that must
+// not allocate after start-up.  nd_march_forward_noalloc serves them with the
+// persistent kernel and no context: its only scratch (the view table, the work
+// counters and the statistics block, about 28 KB) lives in the file-scope array
+// below, which the library's module brings with it on every GPU that loads the
+// library, until the process exits.
+namespace {
+
+constexpr int kNoAllocMaxViews = 64;  // views (and launches) per call
+
+struct NoAllocScratch {
+  DevView views[kNoAllocMaxViews];
+  unsigned long long counters[kNoAllocMaxViews];
+  Stats stats;
+};
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+NoAllocScratch* g_noalloc_ptr[kNoAllocMaxDevices] = {};  // device address per device
+int g_noalloc_sms[kNoAllocMaxDevices] = {};
+
+}  // namespace
+
+// The scratch array.  In host code this name is only a stand-in: its device
+// address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_nd_noalloc_scratch[sizeof(NoAllocScratch)];
+
+namespace {
+
+// First call on a device: look up the device address of the scratch array and
+// the SM count, with that device current.
+nd_status noalloc_setup(int dev, NoAllocScratch** ptr, int* sms) {
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return ND_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_nd_noalloc_scratch);
+    if (e != cudaSuccess || !p) return ND_ERR_CUDA;
+    int n = 0;
+    e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess || n <= 0) return ND_ERR_CUDA;
+    g_noalloc_sms[dev] = n;
+    g_noalloc_ptr[dev] = static_cast<NoAllocScratch*>(p);
+  }
+  *ptr = g_noalloc_ptr[dev];
+  *sms = g_noalloc_sms[dev];
+  return ND_OK;
+}
+
+}  // namespace
+
+extern "C" nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t nviews, const nd_march_opts* opts,
+                                              const nd_gbuffer* out, void* stream) {
+  if (!views || nviews <= 0 || !out || !out->depth) return ND_ERR_INVALID;
+  if (nviews > kNoAllocMaxViews) return ND_ERR_INVALID;
+  if (out->trap || out->iters) return ND_ERR_UNSUPPORTED;  // the trap pass needs per-ray scratch
+  if ((out->normal && (uintptr_t(out->normal) & 15)) || (out->depth64 && (uintptr_t(out->depth64) & 7)) ||
+      (uintptr_t(out->depth) & 3))
+    return ND_ERR_INVALID;
+  if (opts && opts->de_precision != 0 && opts->de_precision != 32 && opts->de_precision != 64) return ND_ERR_INVALID;
+  int64_t total = 0;
+  for (int i = 0; i < nviews; ++i) {
+    const nd_status s = validate_view(nullptr, views[i], i);
+    if (s != ND_OK) return s;
+    total += int64_t(views[i].spp) * views[i].tile_w * views[i].tile_h;
+    if (total > int64_t(0x7fffffff)) return ND_ERR_INVALID;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return ND_ERR_CUDA;
+  NoAllocScratch* scratch = nullptr;
+  int sms = 0;
+  nd_status s = noalloc_setup(dev, &scratch, &sms);
+  if (s != ND_OK) return s;
+
+  // plan without heap allocation: one launch when one formula or one compiled
+  // group covers the call, else one launch per formula; views grouped by launch
+  int order[kNoAllocMaxViews], codes[kNoAllocMaxViews], launch_of[kNoAllocMaxViews];
+  KernelTable tables[kNoAllocMaxViews];
+  int nlaunch = 0;
+  int distinct[kNoAllocMaxViews], ndistinct = 0;
+  for (int i = 0; i < nviews; ++i) {
+    bool seen = false;
+    for (int k = 0; k < ndistinct; ++k) seen |= distinct[k] == views[i].formula;
+    if (!seen) distinct[ndistinct++] = views[i].formula;
+  }
+  int group = -1;
+  if (ndistinct > 1) {
+    for (int g = 0; g < nd_group_entry_count && group < 0; ++g) {
+      bool covers = true;
+      for (int k = 0; k < ndistinct; ++k) {
+        bool in = false;
+        for (int m = 0; m < nd_group_entries[g].count; ++m) in |= nd_group_entries[g].members[m] == distinct[k];
+        covers &= in;
+      }
+      if (covers) group = g;
+    }
+  }
+  int nv = 0;
+  if (ndistinct == 1 || group >= 0) {
+    tables[0] = group >= 0 ? nd_group_entries[group].kernels() : nd_formula_entries[distinct[0]].kernels();
+    nlaunch = 1;
+    const int gcount = group >= 0 ? nd_group_entries[group].count : 1;
+    for (int m = 0; m < gcount; ++m)  // views ordered by formula code
+      for (int i = 0; i < nviews; ++i) {
+        const int code = group >= 0 ? m : 0;
+        const bool match = group >= 0 ? nd_group_entries[group].members[m] == views[i].formula : true;
+        if (!match) continue;
+        order[nv] = i;
+        codes[nv] = code;
+        launch_of[nv] = 0;
+        ++nv;
+      }
+  } else {
+    for (int k = 0; k < ndistinct; ++k) {
+      tables[nlaunch] = nd_formula_entries[distinct[k]].kernels();
+      for (int i = 0; i < nviews; ++i)
+        if (views[i].formula == distinct[k]) {
+          order[nv] = i;
+          codes[nv] = 0;
+          launch_of[nv] = nlaunch;
+          ++nv;
+        }
+      ++nlaunch;
+    }
+  }
+  if (nv != nviews) return ND_ERR_INVALID;
+
+  // view table: G-buffer offsets in call order, work-item offsets per launch
+  int64_t out_off[kNoAllocMaxViews + 1];
+  out_off[0] = 0;
+  for (int i = 0; i < nviews; ++i) out_off[i + 1] = out_off[i] + int64_t(views[i].spp) * views[i].tile_w * views[i].tile_h;
+  DevView host[kNoAllocMaxViews];
+  int first[kNoAllocMaxViews + 1];
+  int64_t rays[kNoAllocMaxViews];
+  for (int l = 0, k = 0; l < nlaunch; ++l) {
+    first[l] = k;
+    int64_t off = 0;
+    while (k < nv && launch_of[k] == l) {
+      host[k] = make_dev_view(views[order[k]], off, out_off[order[k]], codes[k]);
+      off += host[k].rays;
+      ++k;
+    }
+    rays[l] = off;
+  }
+  first[nlaunch] = nv;
+
+  cudaStream_t st = (cudaStream_t)stream;
+  // the host table is pageable: the copy returns once it has been staged
+  cudaError_t e = cudaMemcpyAsync(scratch->views, host, sizeof(DevView) * size_t(nv), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(scratch->counters, 0, sizeof(unsigned long long) * size_t(nlaunch), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(&scratch->stats, 0, sizeof(Stats), st);
+  if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? ND_ERR_OOM : ND_ERR_CUDA;
+  const int prec = (opts && opts->de_precision == 64) ? 64 : 32;
+  for (int l = 0; l < nlaunch; ++l) {
+    if (rays[l] <= 0) continue;
+    const int n = first[l + 1] - first[l];
+    bool dir64 = false;
+    for (int k = first[l]; k < first[l + 1]; ++k) dir64 |= host[k].dir64 != 0;
+    LaunchArgs a;
+    memset(&a, 0, sizeof(a));
+    a.views = scratch->views + first[l];
+    a.nviews = n;
+    a.total_rays = rays[l];
+    a.out = *out;
+    a.t_hit = nullptr;
+    a.counter = scratch->counters + l;
+    a.stats = &scratch->stats;
+    a.refill_threshold = std::max(1, std::min(32, opts && opts->refill_threshold ? opts->refill_threshold : 4));
+    a.deadline_ns = int64_t(opts && opts->watchdog_ms > 0 ? opts->watchdog_ms : 10000) * 1000000;
+    LaunchConfig c;
+    c.kernel = ND_KERNEL_PERSISTENT;
+    c.block = 128;
+    c.blocks_per_sm = opts ? opts->blocks_per_sm : 0;
+    c.num_sms = sms;
+    LaunchFn fn = pick(tables[l], ND_KERNEL_PERSISTENT, prec, n > 1, dir64);
+    e = fn(a, host[first[l]], c, st);
+    if (e != cudaSuccess) return ND_ERR_CUDA;
+  }
+  return ND_OK;
+}

@@ -1,0 +1,90 @@
+"""nd_march_forward_noalloc: the forward march for callers that cannot allocate
+device memory (a host whose allocator owns the device, a render thread where an
+allocation may synchronise the device).  It must give the same G-buffer as
+nd_march_forward with the same persistent kernel, call after call.
+
+This file is named to be collected last, so that a run stopping at the first
+failure has already run every other test.
+"""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from numericdream_b200 import abi, runtime, workloads
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("depth", "normal", "steps", "shade", "shadow", "depth64", "evals")
+
+
+def _noalloc(lib):
+    fn = lib.nd_march_forward_noalloc
+    fn.restype = C.c_int32
+    fn.argtypes = [C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(abi.nd_march_opts),
+                   C.POINTER(abi.nd_gbuffer), C.c_void_p]
+    return fn
+
+
+def _gbuf(n):
+    g = runtime.GBuffer.allocate(n)
+    g.trap = None  # the no-allocation entry point has no trap pass
+    g.iters = None
+    return g
+
+
+def _views_single():
+    fid = runtime.find_formula(workloads.MANDELBOX)
+    return [abi.make_view(fid, 96, 72, (2.2, 1.3, -3.1), fov_y_deg=60.0, params=workloads.mandelbox_params(-1.5, 12),
+                          max_steps=256, normal_mode=abi.ND_NORMAL_CENTRAL, normal_h_coef=1e-4, shadow=1,
+                          light_dir=list(workloads.LIGHT_DIR))]
+
+
+def _views_batched():
+    return workloads.batched_64(runtime.find_formula, nviews=6, min_side=24, max_side=64, seed=11)
+
+
+def test_noalloc_matches_forward_twice(ndlib):
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    ctx = runtime.Context(0)
+    fn = _noalloc(ndlib)
+    opts = runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, refill_threshold=4)
+    for views in (_views_single(), _views_batched()):
+        n = workloads.rays(views)
+        ref = _gbuf(n)
+        ctx.forward(views, ref, opts)
+        torch.cuda.synchronize()
+        want = ref.numpy()
+        for call in range(2):  # two calls in a row share the one scratch array
+            got_buf = _gbuf(n)
+            arr = (abi.nd_view_desc * len(views))(*views)
+            g = got_buf.as_abi()
+            st = fn(arr, len(views), C.byref(opts), C.byref(g), None)
+            assert st == abi.ND_OK, abi.STATUS_NAMES[st]
+            torch.cuda.synchronize()
+            got = got_buf.numpy()
+            for k in KEYS:
+                np.testing.assert_array_equal(got[k], want[k], err_msg=f"call {call}: {k} differs")
+    ctx.close()
+
+
+def test_noalloc_rejects_what_it_cannot_serve(ndlib):
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    fn = _noalloc(ndlib)
+    views = _views_single()
+    n = workloads.rays(views)
+    full = runtime.GBuffer.allocate(n)  # trap and iters requested
+    arr = (abi.nd_view_desc * 1)(*views)
+    g = full.as_abi()
+    assert fn(arr, 1, None, C.byref(g), None) == abi.ND_ERR_UNSUPPORTED
+    too_many = (abi.nd_view_desc * 65)(*([views[0]] * 65))
+    small = _gbuf(n * 65)
+    g2 = small.as_abi()
+    assert fn(too_many, 65, None, C.byref(g2), None) == abi.ND_ERR_INVALID
