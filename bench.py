@@ -1,25 +1,30 @@
 """Benchmark of the B200 sphere-tracing pass.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload batched_64|mandelbox_1080p|mandelbulb_256]
 
 A step is one forward march over the whole workload.  The default workload is the
-batched one (64 views of mixed formulas and uneven sizes in one persistent launch,
-replayed as a CUDA graph); the plain per-view launch of the same views is timed
-beside it.  Rank 0 prints one JSON line.
+batched one: 64 views of mixed formulas (Mandelbulb, Mandelbox, Menger,
+pseudo-Kleinian) and uneven sizes (log-uniform 64..1024 per side, 7.2 M rays) in one
+persistent launch plus the trap pass, replayed as a CUDA graph.  The plain per-view
+launch of the same views is timed beside it, and the 1080p x 4 spp Mandelbox frame
+with shadow rays is timed as a second workload.  Rank 0 prints one JSON line.
 
-value      rays/s of the batched persistent kernel, device time (CUDA events on the
-           launching stream), inputs resident; L2 is flushed between steps.
-e2e        the same metric through the public C ABI call with host view descriptors
-           and the G-buffer read back to pinned host memory every step.
-roofline   FP32-pipe roofline of the march kernel: algorithmic FLOPs per launch
-           (DE evaluations x FLOPs per evaluation of each formula, counted by the
-           op-counting instantiation of the same formula code) / kernel time.
-cpu_baseline  the oracle's FP32 march (same formulas, same march) on all host
-           cores over a bounded sample of the workload's rays.
+value         rays/s of the batched persistent march, device time (CUDA events on the
+              launching stream), inputs resident; L2 is flushed between steps.
+e2e           the same metric through the public C ABI call (nd_march_forward) with
+              host view descriptors and the G-buffer read back to pinned host memory.
+roofline      FP32-pipe roofline of the march kernel: algorithmic FLOPs per launch
+              (DE evaluations x FLOPs per evaluation, counted by running the same ray
+              program and formula code on the host with a counting float) / kernel
+              time, against the nominal FP32 FMA peak at the sampled SM clock.
+cpu_baseline  the oracle's FP32 march (same formulas, same march) on every host core
+              over a bounded, seeded sample of the workload's rays; the same sample in
+              FP64 gives the error figures against the GPU's output.
 
---impl reference times the CPU implementation of the path (the oracle's FP32
-march, every host thread) on the same workload and metric: the reference app
-itself only runs through WebGPU, which this machine cannot run.
+--impl reference times the CPU implementation of the path on the host cores: the
+reference app itself only runs through WebGPU, which this machine cannot run, so its
+march is timed as the oracle's FP32 restatement with every host thread.
 """
 
 from __future__ import annotations
@@ -27,6 +32,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import random
 import subprocess
 import sys
 import threading
@@ -38,6 +44,10 @@ if ROOT not in sys.path:
 
 METRIC = "Mrays/s & DE-evals/s on 1 B200, batched vs plain, at stated FP64 error"
 
+# DRAM bytes of one batched persistent launch (march kernel), from
+# ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum on this workload.
+NCU_TRAFFIC = {"batched_64": 412.7e6}
+
 
 def _dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -47,11 +57,12 @@ def _dist_env():
 
 
 class ClockSampler:
-    """Samples nvidia-smi SM clocks and throttle reasons while running."""
+    """Samples nvidia-smi SM clocks and throttle reasons while the timed work runs."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
@@ -83,18 +94,14 @@ class ClockSampler:
                 self.proc.kill()
         if self.thread is not None:
             self.thread.join(timeout=2)
-        return self.summary()
-
-    def summary(self):
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for s in self.samples:
             try:
                 sm.append(float(s[1]))
                 mx = float(s[2])
             except (ValueError, IndexError):
                 continue
-            for i, n in enumerate(names):
+            for i, n in enumerate(self.NAMES):
                 if len(s) > 5 + i and s[5 + i].lower().startswith("active"):
                     reasons.add(n)
         if not sm:
@@ -103,71 +110,103 @@ class ClockSampler:
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_views(name, resolve):
+def build_views(name, resolve, rank=0):
     from numericdream_b200 import workloads
 
     if name == "batched_64":
-        return workloads.batched_64(resolve)
+        return workloads.batched_64(resolve, seed=7 + 1000 * rank)
     if name == "mandelbox_1080p":
-        return workloads.mandelbox_1080p(resolve)
+        return workloads.mandelbox_1080p(resolve, seed=1234 + rank)
     if name == "mandelbulb_256":
         return workloads.mandelbulb_256(resolve)
     raise SystemExit(f"unknown workload {name}")
 
 
-def config_of(name, views):
+def config_of(name, views, ws):
     from numericdream_b200 import workloads
 
-    return {"workload": name, "views": len(views), "rays_per_step": workloads.rays(views),
-            "max_steps": int(views[0].max_steps), "de": "fp32", "t": "fp64",
-            "l2": "flushed between steps (256 MiB write)"}
+    return {"workload": name, "views": len(views), "rays_per_step_per_gpu": workloads.rays(views),
+            "max_steps": int(max(v.max_steps for v in views)), "de": "fp32 (fast math)", "t": "fp64",
+            "l2": "flushed between steps (256 MiB write)", "parallelism": f"shards{ws}" if ws > 1 else "single"}
 
 
-def cpu_sample(views, target_rays, seed=0):
-    """A bounded, seeded, evenly spread subset of (view, first ray, count) chunks."""
-    import random
-
+def cpu_sample(views, target_rays, seed=0, run=64):
+    """Seeded runs of `run` consecutive rays spread over every view: (view index, first, n)."""
     from numericdream_b200 import abi
 
     rng = random.Random(seed)
     total = sum(abi.rays_of(v) for v in views)
     frac = min(1.0, target_rays / max(total, 1))
-    chunks = []
-    for v in views:
+    out = []
+    for i, v in enumerate(views):
         n = abi.rays_of(v)
-        k = max(1, int(n * frac))
-        # contiguous runs of 64 rays spread over the view
-        runs = max(1, k // 64)
+        runs = max(1, int(n * frac) // run)
         for _ in range(runs):
-            first = rng.randrange(0, max(1, n - 64))
-            chunks.append((v, first, min(64, n - first)))
-    return chunks
+            first = rng.randrange(0, max(1, n - run))
+            out.append((i, first, min(run, n - first)))
+    return out
 
 
-def run_cpu(views, seconds_budget=15.0, nthreads=0):
-    """Time the oracle's FP32 march on all host cores over a bounded sample."""
+def run_cpu(views, seconds_budget=15.0, with_fp64=False):
+    """The oracle's FP32 march on all host cores over a bounded sample (timed), and
+    optionally the FP64 oracle on the same sample (for the error figures)."""
     from numericdream_b200 import runtime
     from oracle import pyoracle
 
-    cores = nthreads or pyoracle.max_threads()
-    probe = cpu_sample(views, 2048, seed=1)
+    cores = pyoracle.max_threads()
+    names = [runtime.formula_name(v.formula) for v in views]
     t0 = time.perf_counter()
     nr = 0
-    for v, first, n in probe:
-        pyoracle.render(v, runtime.formula_name(v.formula), precision=32, nthreads=cores, first=first, n=n)
+    for vi, first, n in cpu_sample(views, 2048, seed=1):
+        pyoracle.render(views[vi], names[vi], precision=32, first=first, n=n)
         nr += n
-    dt = max(time.perf_counter() - t0, 1e-6)
-    target = int(nr / dt * seconds_budget)
-    chunks = cpu_sample(views, max(target, 4096), seed=2)
+    rate = nr / max(time.perf_counter() - t0, 1e-6)
+    chunks = cpu_sample(views, max(int(rate * seconds_budget), 4096), seed=2)
     t0 = time.perf_counter()
-    rays = 0
-    evals = 0
-    for v, first, n in chunks:
-        o = pyoracle.render(v, runtime.formula_name(v.formula), precision=32, nthreads=cores, first=first, n=n)
+    rays = evals = 0
+    for vi, first, n in chunks:
+        o = pyoracle.render(views[vi], names[vi], precision=32, first=first, n=n)
         rays += n
         evals += int(o["evals"].astype("int64").sum())
     dt = time.perf_counter() - t0
-    return {"rays_per_s": rays / dt, "evals_per_s": evals / dt, "rays": rays, "seconds": dt, "cores": cores}
+    res = {"rays_per_s": rays / dt, "evals_per_s": evals / dt, "rays": rays, "seconds": dt, "cores": cores,
+           "chunks": chunks}
+    if with_fp64:
+        res["fp64"] = [pyoracle.render(views[vi], names[vi], precision=64, first=first, n=n)
+                       for vi, first, n in chunks[: max(1, len(chunks) // 4)]]
+    return res
+
+
+def error_stats(views, gbuf_np, cpu):
+    """GPU output against the FP64 oracle on the sampled rays (hits of both)."""
+    import numpy as np
+
+    from numericdream_b200 import abi
+
+    offs = [0]
+    for v in views:
+        offs.append(offs[-1] + abi.rays_of(v))
+    rel, ang, mism, n = [], [], 0, 0
+    for (vi, first, cnt), ref in zip(cpu["chunks"], cpu["fp64"]):
+        sl = slice(offs[vi] + first, offs[vi] + first + cnt)
+        gh = gbuf_np["normal"][sl, 3] > 0.5
+        rh = ref["normal"][:, 3] > 0.5
+        mism += int((gh != rh).sum())
+        n += cnt
+        both = gh & rh & (ref["depth64"] > 1e-3)
+        if both.any():
+            rel.append(np.abs(gbuf_np["depth64"][sl][both] - ref["depth64"][both]) / ref["depth64"][both])
+            a = gbuf_np["normal"][sl][both, :3].astype(np.float64)
+            b = ref["normal"][both, :3].astype(np.float64)
+            c = np.clip((a * b).sum(1) / np.maximum(np.linalg.norm(a, axis=1) * np.linalg.norm(b, axis=1), 1e-30), -1, 1)
+            ang.append(np.degrees(np.arccos(c)))
+    rel = np.concatenate(rel) if rel else np.zeros(1)
+    ang = np.concatenate(ang) if ang else np.zeros(1)
+    return {"sample_rays": n, "hit_mismatch_frac": mism / max(n, 1),
+            "depth_rel_p99": float(np.percentile(rel, 99)), "depth_rel_max": float(rel.max()),
+            "depth_rel_frac_over_1e-4": float((rel > 1e-4).mean()),
+            "normal_deg_p99": float(np.percentile(ang, 99)), "normal_deg_max": float(ang.max()),
+            "note": "all sampled rays incl. rounding-unstable ones; hits with t > 1e-3"}
 
 
 def reference_arm(args):
@@ -178,26 +217,27 @@ def reference_arm(args):
 
     try:
         runtime.load_library()
-        resolve = runtime.find_formula
     except ImportError as e:
         print(json.dumps({"impl": "reference", "unavailable": f"formula table not built: {e}"}))
         return 0
-    views = build_views(args.workload, resolve)
-    per = []
-    res = None
+    views = build_views(args.workload, runtime.find_formula)
+    per, res = [], None
+    budget = max(2.0, 60.0 / max(args.steps + args.warmup, 1))
     for i in range(args.warmup + args.steps):
-        res = run_cpu(views, seconds_budget=max(2.0, 60.0 / max(args.steps + args.warmup, 1)))
+        res = run_cpu(views, seconds_budget=budget)
         if i >= args.warmup:
             per.append(res)
     v = sum(r["rays_per_s"] for r in per) / len(per) / 1e6
     line = {"metric": METRIC, "value": v, "unit": "Mrays/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_of(args.workload, views),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_of(args.workload, views, 1),
             "de_evals_per_s": sum(r["evals_per_s"] for r in per) / len(per),
             "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": res["cores"], "kind": "port",
-                             "sample": f"{res['rays']} rays per step, seeded runs of 64 rays spread over all views"},
+                             "sample": f"{res['rays']} rays per step in seeded runs of 64 over all views"},
             "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "CPU FP32 restatement of the reference march (the reference runs only through WebGPU)"}
+            "note": "the reference's march restated on the CPU (FP32, all host threads); "
+                    "the reference app itself runs only through WebGPU, unavailable on this box"}
     print(json.dumps(line))
     return 0
 
@@ -210,7 +250,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched_64")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the second (1080p Mandelbox) workload")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -222,27 +262,18 @@ def main():
 
     ws, rank, local = _dist_env()
     if ws > 1:
-        import torch.distributed as dist
         import datetime
+
+        import torch.distributed as dist
 
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     ctx = runtime.Context(local)
-    views = build_views(args.workload, runtime.find_formula)
-    nrays = workloads.rays(views)
-    gbuf = runtime.GBuffer.allocate(nrays, device=dev)
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-
-    tune = None
-    if not args.no_autotune:
-        tune = ctx.autotune(views, gbuf)
-    opts = runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, blocks_per_sm=tune.blocks_per_sm if tune else 0,
-                             refill_threshold=tune.refill_threshold if tune else 8)
-    graph = ctx.capture(views, gbuf, opts, stream=sptr)
 
     def timed(fn, steps, warmup):
         with torch.cuda.stream(stream):
@@ -268,19 +299,33 @@ def main():
             torch.distributed.barrier()
         return total / steps
 
+    def run_workload(name, steps, warmup, tune=True):
+        views = build_views(name, runtime.find_formula, rank)
+        nrays = workloads.rays(views)
+        gbuf = runtime.GBuffer.allocate(nrays, device=dev)
+        tr = ctx.autotune(views, gbuf) if tune else None
+        opts = runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, blocks_per_sm=tr.blocks_per_sm if tr else 0,
+                                 refill_threshold=tr.refill_threshold if tr else 4)
+        graph = ctx.capture(views, gbuf, opts, stream=sptr)
+        ms_p = timed(lambda: graph.launch(sptr), steps, warmup)
+        st = ctx.stats()
+        plain_opts = runtime.make_opts(kernel=abi.ND_KERNEL_PLAIN)
+        ms_plain = timed(lambda: ctx.forward(views, gbuf, plain_opts, stream=sptr), max(2, steps // 2), 1)
+        # restore the persistent kernel's G-buffer for the error check
+        graph.launch(sptr)
+        stream.synchronize()
+        graph.close()
+        return views, nrays, gbuf, opts, tr, ms_p, ms_plain, st
+
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
-    ms_batched = timed(lambda: graph.launch(sptr), args.steps, args.warmup)
-    st = ctx.stats()
-    de_evals = st.de_evals
-    plain_opts = runtime.make_opts(kernel=abi.ND_KERNEL_PLAIN)
-    ms_plain = timed(lambda: ctx.forward(views, gbuf, plain_opts, stream=sptr), max(2, args.steps // 2), 1)
+    views, nrays, gbuf, opts, tune, ms_batched, ms_plain, st = run_workload(args.workload, args.steps, args.warmup)
     # end to end through the public call: host descriptors in, G-buffer to pinned host
     host = {k: torch.empty(getattr(gbuf, k).shape, dtype=getattr(gbuf, k).dtype, pin_memory=True)
             for k in ("depth", "normal", "trap", "steps")}
     d2h = sum(t.numel() * t.element_size() for t in host.values())
-    h2d = len(views) * 512
+    h2d = len(views) * 440  # the view table copied by nd_march_forward (DevView records)
 
     def e2e_step():
         ctx.forward(views, gbuf, opts, stream=sptr)
@@ -288,43 +333,60 @@ def main():
             t.copy_(getattr(gbuf, k), non_blocking=True)
 
     ms_e2e = timed(e2e_step, max(2, args.steps // 2), 1)
+    extra = None
+    if not args.no_extra and args.workload != "mandelbox_1080p":
+        v2, n2, g2, _, _, ms2, ms2_plain, st2 = run_workload("mandelbox_1080p", max(2, args.steps // 2), 2, tune=False)
+        extra = {"workload": "mandelbox_1080p (1920x1080 x 4 spp, shadow rays)", "rays_per_step": n2,
+                 "value": n2 * ws / (ms2 * 1e-3) / 1e6, "unit": "Mrays/s", "ms_per_step": ms2,
+                 "de_evals_per_s": st2.de_evals * ws / (ms2 * 1e-3),
+                 "plain": n2 * ws / (ms2_plain * 1e-3) / 1e6, "batched_over_plain": ms2_plain / ms2}
+        del g2
     clk = clocks.stop()
+    gnp = gbuf.numpy() if rank == 0 else None
 
     if ws > 1:
         t = torch.tensor([ms_batched, ms_plain, ms_e2e], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms_batched, ms_plain, ms_e2e = t.tolist()
-    graph.close()
     rays_total = nrays * ws
-    value = rays_total / (ms_batched * 1e-3) / 1e6
-    line = None
     if rank == 0:
         from numericdream_b200 import opcount
 
-        flops_per_eval, fcount = opcount.flops_per_eval_for(views)
-        flops = de_evals * flops_per_eval
-        peak = opcount.fp32_peak_tflops(clk.get("sm_max_mhz"))
+        flops_per_eval, per = opcount.flops_per_eval_for(views)
+        flops = st.de_evals * flops_per_eval
+        peak = opcount.fp32_peak_tflops(clk.get("sm_mhz") or clk.get("sm_max_mhz"))
         achieved = flops / (ms_batched * 1e-3) / 1e12
-        cpu = None
+        cpu, err = None, None
         if not args.no_cpu:
-            c = run_cpu(views, seconds_budget=15.0)
+            c = run_cpu(views, seconds_budget=15.0, with_fp64=True)
             cpu = {"value": c["rays_per_s"] / 1e6, "unit": "Mrays/s", "cores": c["cores"], "kind": "port",
-                   "sample": f"{c['rays']} rays in seeded runs of 64 spread over all views ({c['seconds']:.1f} s)"}
+                   "sample": f"{c['rays']} rays in seeded runs of 64 consecutive rays over all 64 views "
+                             f"({c['seconds']:.1f} s, FP32 oracle march)",
+                   "de_evals_per_s": c["evals_per_s"]}
+            err = error_stats(views, gnp, c)
         line = {
-            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_of(args.workload, views),
-            "de_evals_per_s": de_evals * ws / (ms_batched * 1e-3),
-            "plain": {"value": rays_total / (ms_plain * 1e-3) / 1e6, "unit": "Mrays/s", "ms_per_step": ms_plain},
+            "metric": METRIC, "value": rays_total / (ms_batched * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded views, no dataset)",
+            "config": config_of(args.workload, views, ws),
+            "de_evals_per_s": st.de_evals * ws / (ms_batched * 1e-3),
+            "plain": {"value": rays_total / (ms_plain * 1e-3) / 1e6, "unit": "Mrays/s", "ms_per_step": ms_plain,
+                      "kind": "one plain launch per view, one thread per ray"},
             "batched_over_plain": ms_plain / ms_batched,
             "e2e": {"value": rays_total / (ms_e2e * 1e-3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None, "flops_per_eval": flops_per_eval,
-                         "peak_source": "nominal SMs x 128 FP32 lanes x 2 x max SM clock"},
-            "cpu_baseline": cpu, "clocks": clk, "gpu_launches": args.steps,
+                         "frac": achieved / peak, "traffic": NCU_TRAFFIC.get(args.workload),
+                         "flops_per_eval": flops_per_eval, "sfu_per_eval": per["sfu"],
+                         "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 x sampled SM clock (not in "
+                                        "MEASURED_PEAKS.json)"},
+            "error_vs_fp64": err, "cpu_baseline": cpu, "clocks": clk,
+            "gpu_launches": 2 * args.steps,
+            "stats": {"de_evals": st.de_evals, "march": st.march_evals, "normal": st.normal_evals,
+                      "shadow": st.shadow_evals, "trap": st.trap_evals, "hits": st.hits, "refills": st.refills},
             "tune": {"kernel": tune.kernel, "blocks_per_sm": tune.blocks_per_sm,
                      "refill_threshold": tune.refill_threshold} if tune else None,
+            "second_workload": extra,
         }
         print(json.dumps(line))
     ctx.close()
