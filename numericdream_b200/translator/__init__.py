@@ -1,3 +1,3 @@
 """Build-time WGSL-subset -> C++/CUDA translator for formula plugins."""
 
-from .wgsl import TranslateError, TranslatedFormula, translate  # noqa: F401
+from .wgsl import TranslateError, TranslatedFormula, translate, translate_module  # noqa: F401

@@ -741,7 +741,8 @@ def _wrap_trunc_div(a: int, b: int) -> int:
 class FormulaCompiler:
     """Type-checks one formula module and emits its C++ namespace."""
 
-    def __init__(self, fns: list[FnDecl], consts: list[ConstDecl], ns: str):
+    def __init__(self, fns: list[FnDecl], consts: list[ConstDecl], ns: str, helper_ns: str = "ndw"):
+        self.helper_ns = helper_ns
         self.fns = {f.name: f for f in fns}
         self.fn_order = [f.name for f in fns]
         self.module_consts_src = {c.name: c for c in consts}
@@ -1164,6 +1165,8 @@ class FormulaCompiler:
                 raise TranslateError(f"{name} takes {len(ptys)} arguments", line)
             conv = [self.convert(a, t, line) for a, t in zip(args, ptys)]
             self.features.add("helper:" + name)
+            if self.helper_ns != "ndw":  # helpers translated from WGSL: <T, P> templates
+                return TE(rty, f"{self.helper_ns}::{name}<T, P>({', '.join(c.code for c in conv)})")
             return TE(rty, f"ndw::{name}<T>({', '.join(c.code for c in conv)})")
         return self.builtin(name, args, line)
 
@@ -1601,8 +1604,9 @@ class FormulaCompiler:
             if have_t != ptys or have_r != rty:
                 raise TranslateError(f"contract function {name} has the wrong signature")
 
-    def emit(self) -> str:
-        self.check_contract()
+    def emit(self, contract: bool = True) -> str:
+        if contract:
+            self.check_contract()
         lines = [f"namespace {self.ns} {{"]
         for name in self.fn_order:
             lines.append(self.fn_signature(self.fns[name]) + ";")
@@ -1648,3 +1652,14 @@ def translate(source: str, name: str) -> TranslatedFormula:
     comp = FormulaCompiler(fns, consts, ns)
     cpp = comp.emit()
     return TranslatedFormula(name, ns, cpp, parse_formula_params(source), source_hash(source), comp.features)
+
+
+def translate_module(source: str, namespace: str, helper_ns: str = "ndw", contract: bool = True) -> str:
+    """Translate a WGSL module into one C++ namespace.  With helper_ns, calls to the
+    template helper functions go to that namespace (helpers translated from WGSL)
+    instead of the hand-written library; contract=False skips the formula contract
+    check (for a module of helpers)."""
+    toks = lex(source)
+    fns, consts = Parser(toks).module()
+    comp = FormulaCompiler(fns, consts, namespace, helper_ns=helper_ns)
+    return comp.emit(contract=contract)

@@ -1,0 +1,86 @@
+"""Writes the golden fixtures of this directory from the reference's own sources.
+
+Run where a NumericDream checkout exists (default /root/reference, or ND_REFERENCE):
+
+    python tests/golden/make_golden.py
+
+* de_reference_fp64.json: FP64 distance estimates of every translatable formula of
+  the reference (its formula files and built-in Mandelbulb, with the DE helpers of
+  its shader template), evaluated by oracle/_ref (the reference WGSL translated
+  mechanically and compiled on the host, see oracle/build_ref.py) at 32 seeded points
+  in [-2, 2]^3 per parameter set: the formula's @param defaults, plus the benchmark
+  parameter sets for the Mandelbulb, Mandelbox, Menger sponge and pseudo-Kleinian.
+* template_consts.json: the values of the shader-template constants that formula
+  files may name (template.wgsl module constants).
+"""
+
+import ctypes as C
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from numericdream_b200 import workloads  # noqa: E402
+from numericdream_b200.formula import pack_params, parse_formula_params  # noqa: E402
+from numericdream_b200.translator.wgsl import TEMPLATE_CONSTS  # noqa: E402
+from oracle import build_ref  # noqa: E402
+
+EXTRA_SETS = {
+    "mandelbrot": [workloads.mandelbulb_params(8.0, 12), workloads.mandelbulb_params(5.3, 6)],
+    "amazingbox_box": [workloads.mandelbox_params(-1.5, 15), workloads.mandelbox_params(-1.7, 12),
+                       [2.0, 0.5, 1.0, 1.0, 12.0, 30.0, -20.0, 10.0, 1.0, 0.1, 0.2, 0.3]],
+    "menger3_ifs": [workloads.menger_params(3), workloads.menger_params(6)],
+    "pseudokleinian_kleinian": [workloads.pseudo_kleinian_params(0.8), workloads.pseudo_kleinian_params(1.2)],
+    "sphere_primitive": [[1.3]],
+    "cube_primitive": [[0.7]],
+}
+
+
+def main():
+    ref = build_ref.reference_root()
+    if ref is None:
+        raise SystemExit("no reference checkout")
+    lib = C.CDLL(build_ref.build())
+    lib.ref_formula_name.restype = C.c_char_p
+    lib.ref_de.argtypes = [C.c_char_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int]
+    names = [lib.ref_formula_name(i).decode() for i in range(lib.ref_formula_count())]
+    rng = np.random.default_rng(20261203)
+    out = {"points_per_set": 32, "formulas": {}}
+    for name in names:
+        path = (os.path.join(ref, "src", "gpu", "shaders", "mandelbrot.wgsl") if name == "mandelbrot"
+                else os.path.join(ref, "formulas", name + ".wgsl"))
+        with open(path, encoding="utf-8") as fh:
+            src = fh.read()
+        sets = [pack_params(parse_formula_params(src))] + [list(s) + [0.0] * (16 - len(s)) for s in EXTRA_SETS.get(name, [])]
+        entries = []
+        for prm in sets:
+            pts = rng.uniform(-2.0, 2.0, (32, 3))
+            p32 = np.asarray(prm, np.float32)
+            de = np.zeros(32)
+            assert lib.ref_de(name.encode(), p32.ctypes.data, 32, np.ascontiguousarray(pts).ctypes.data,
+                              de.ctypes.data, 64) == 0
+            entries.append({"params": [float(x) for x in p32], "points": pts.tolist(), "de": de.tolist()})
+        out["formulas"][name] = entries
+    with open(os.path.join(HERE, "de_reference_fp64.json"), "w") as fh:
+        json.dump(out, fh, separators=(",", ":"))
+    # template constants a formula may name, as the template defines them
+    with open(os.path.join(ref, "src", "gpu", "shaders", "template.wgsl"), encoding="utf-8") as fh:
+        tpl = fh.read()
+    consts = {}
+    for name in TEMPLATE_CONSTS:
+        m = re.search(r"^const\s+" + name + r"(?:\s*:\s*\w+)?\s*=\s*([^;]+);", tpl, re.M)
+        if m:
+            consts[name] = m.group(1).strip()
+    with open(os.path.join(HERE, "template_consts.json"), "w") as fh:
+        json.dump(consts, fh, indent=1, sort_keys=True)
+    print(f"{len(names)} formulas, {sum(len(v) for v in out['formulas'].values())} parameter sets")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,128 @@
+"""The CPU oracle, pinned against the reference's own formula code (golden DE values
+from oracle/_ref, committed in tests/golden) and against closed-form answers."""
+
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from numericdream_b200 import abi
+from oracle import pyoracle
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "de_reference_fp64.json")
+ORACLE_FORMULAS = ["mandelbrot", "amazingbox_box", "menger3_ifs", "pseudokleinian_kleinian", "sphere_primitive",
+                   "cube_primitive"]
+
+
+def _golden():
+    with open(GOLDEN) as fh:
+        return json.load(fh)["formulas"]
+
+
+@pytest.mark.parametrize("name", ORACLE_FORMULAS)
+def test_oracle_de_matches_reference_golden(name):
+    g = _golden()[name]
+    for entry in g:
+        pts = np.asarray(entry["points"])
+        want = np.asarray(entry["de"])
+        got, _, _ = pyoracle.de(name, entry["params"], pts, 64)
+        rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-300)
+        assert rel.max() <= 1e-12, (name, entry["params"][:6], rel.max())
+
+
+def test_golden_covers_every_formula():
+    g = _golden()
+    assert len(g) >= 54
+    for name in ORACLE_FORMULAS:
+        assert name in g
+
+
+def _view(formula_name, size, cam_z, params, **kw):
+    fid = 0  # the oracle takes the formula by name; the id is not used
+    return abi.make_view(fid, size, size, (0.0, 0.0, cam_z), fov_y_deg=60.0, params=params, **kw)
+
+
+def test_sphere_known_answer():
+    # camera on the -z axis looking at a sphere of radius R at the origin: the
+    # centre ray hits at t = |cam| - R, normal -z; every hit lies on the sphere
+    R, cz = 1.25, -3.0
+    v = _view("sphere_primitive", 65, cz, [R], eps_coef=1e-5, eps_floor=0.0, max_steps=512)
+    o = pyoracle.render(v, "sphere_primitive", 64)
+    c = 32 * 65 + 32
+    assert o["normal"][c, 3] == 1.0
+    assert abs(o["depth64"][c] - (abs(cz) - R)) <= 1e-5 * (abs(cz) - R)
+    np.testing.assert_allclose(o["normal"][c, :3], [0.0, 0.0, -1.0], atol=1e-6)
+    # all hits on the surface: |org + dir t| = R within eps(t)
+    hits = np.where(o["normal"][:, 3] > 0.5)[0]
+    assert len(hits) > 100
+    # closed-form hit count: rays whose distance to the origin is < R
+    tan30 = math.tan(math.radians(30.0))
+    n_expect = 0
+    for idx in range(65 * 65):
+        px, py = idx % 65, idx // 65
+        ux = (2.0 * (px + 0.5) / 65 - 1.0) * tan30
+        uy = (2.0 * (py + 0.5) / 65 - 1.0) * tan30
+        d = np.array([ux, uy, 1.0]) / math.sqrt(ux * ux + uy * uy + 1.0)
+        o_ = np.array([0.0, 0.0, cz])
+        b = o_ @ d
+        disc = b * b - (o_ @ o_ - R * R)
+        if disc > 1e-9:
+            n_expect += 1
+            t = -b - math.sqrt(disc)
+            if o["normal"][idx, 3] > 0.5:
+                # sphere tracing an exact SDF never overshoots: the hit is in front
+                # of the true intersection and within eps(t) of the surface
+                got = o["depth64"][idx]
+                eps = 1e-5 * got
+                assert got <= t + 1e-12
+                r = np.linalg.norm(o_ + d * got)
+                assert -1e-12 <= r - R < eps, (idx, r - R, eps)
+                # and short of it by at most eps / cos(incidence), cos = sqrt(disc) / R
+                assert got >= t - eps * R / math.sqrt(disc) - 1e-9, (idx, got, t)
+    assert abs(len(hits) - n_expect) <= 4
+
+
+def test_cube_known_answer():
+    s, cz = 0.7, -2.5
+    v = _view("cube_primitive", 33, cz, [s], eps_coef=1e-5, eps_floor=0.0, max_steps=512)
+    o = pyoracle.render(v, "cube_primitive", 64)
+    c = 16 * 33 + 16
+    assert abs(o["depth64"][c] - (abs(cz) - s)) <= 1e-5
+    np.testing.assert_allclose(o["normal"][c, :3], [0.0, 0.0, -1.0], atol=1e-5)
+
+
+def test_fp32_oracle_close_to_fp64():
+    v = _view("mandelbrot", 48, -2.5, [8.0, 12.0], eps_coef=1e-4, eps_floor=0.0)
+    a = pyoracle.render(v, "mandelbrot", 32)
+    b = pyoracle.render(v, "mandelbrot", 64)
+    ha, hb = a["normal"][:, 3] > 0.5, b["normal"][:, 3] > 0.5
+    assert (ha != hb).sum() <= 3
+    both = ha & hb
+    rel = np.abs(a["depth64"][both] - b["depth64"][both]) / b["depth64"][both]
+    assert np.percentile(rel, 99) < 1e-5
+
+
+def test_edge_cases():
+    # zero steps: march_to's loop never runs -> a miss
+    v = _view("mandelbrot", 4, -2.5, [8.0, 12.0], max_steps=0)
+    o = pyoracle.render(v, "mandelbrot", 64)
+    assert (o["normal"][:, 3] == 0).all() and (o["steps"] == 0).all()
+    # a tile of a frame gives the same rays as the same pixels of the whole frame
+    full = _view("amazingbox_box", 40, -4.0, [-1.5, 0.5, 1.0, 1.0, 10, 0, 0, 0, 1, 0, 0, 0])
+    tile = _view("amazingbox_box", 40, -4.0, [-1.5, 0.5, 1.0, 1.0, 10, 0, 0, 0, 1, 0, 0, 0],
+                 tile_x=10, tile_y=5, tile_w=7, tile_h=3)
+    of = pyoracle.render(full, "amazingbox_box", 64)
+    ot = pyoracle.render(tile, "amazingbox_box", 64)
+    idx = [(5 + y) * 40 + 10 + x for y in range(3) for x in range(7)]
+    np.testing.assert_array_equal(of["depth64"][idx], ot["depth64"])
+    # jittered samples are deterministic per seed
+    j1 = pyoracle.render(_view("mandelbrot", 8, -2.5, [8.0, 6.0], spp=4, seed=9), "mandelbrot", 64)
+    j2 = pyoracle.render(_view("mandelbrot", 8, -2.5, [8.0, 6.0], spp=4, seed=9), "mandelbrot", 64)
+    np.testing.assert_array_equal(j1["depth64"], j2["depth64"])
+
+
+def test_unknown_formula_raises():
+    with pytest.raises(ValueError):
+        pyoracle.de("no_such_formula", [0.0], np.zeros((1, 3)))
