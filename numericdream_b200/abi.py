@@ -21,6 +21,7 @@ ND_TRAP_POINT, ND_TRAP_SPHERE, ND_TRAP_BOX, ND_TRAP_CROSS, ND_TRAP_TORUS = range
 ND_TRAP_MIN, ND_TRAP_MAX, ND_TRAP_AVERAGE, ND_TRAP_LAST, ND_TRAP_ITERATION = range(5)
 ND_NORMAL_TETRA, ND_NORMAL_CENTRAL = 0, 1
 ND_KERNEL_AUTO, ND_KERNEL_PLAIN, ND_KERNEL_PERSISTENT = 0, 1, 2
+ND_VIEW_DIR64 = 1
 
 
 class nd_param_info(C.Structure):

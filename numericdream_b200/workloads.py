@@ -132,3 +132,51 @@ def mandelbulb_512(resolve, power=8.0, yaw_deg=0.0, pitch_deg=0.0, dist=2.5, siz
 
 def rays(views) -> int:
     return sum(abi.rays_of(v) for v in views)
+
+
+def find_surface_ray(ctx, fid, params, seed=5, radius=12.0, tries=64):
+    """Seeded search for a ray that hits the fractal: a camera on a sphere of the
+    given radius aimed near the origin, marched once with an FP64 DE and a 20-step
+    bisection.  Returns (origin, unit direction, hit distance)."""
+    import numpy as np
+
+    from . import runtime
+
+    rng = random.Random(seed)
+    for _ in range(tries):
+        z = rng.uniform(-1.0, 1.0)
+        phi = rng.uniform(0.0, 2.0 * math.pi)
+        s = math.sqrt(max(0.0, 1.0 - z * z))
+        org = (radius * s * math.cos(phi), radius * s * math.sin(phi), radius * z)
+        target = (rng.uniform(-0.3, 0.3), rng.uniform(-0.3, 0.3), rng.uniform(-0.3, 0.3))
+        v = abi.make_view(fid, 1, 1, org, target=target, fov_y_deg=1e-6, params=params, max_steps=4096,
+                          max_dist=4.0 * radius, eps_coef=1e-9, eps_floor=0.0, refine_budget=20)
+        g = runtime.GBuffer.allocate(1)
+        ctx.forward([v], g, runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, de_precision=64))
+        out = g.numpy()
+        if out["normal"][0, 3] > 0.5:
+            d = np.asarray(v.fwd, dtype=np.float64)
+            return org, d / np.linalg.norm(d), float(out["depth64"][0])
+    raise RuntimeError("no surface ray found")
+
+
+def deepzoom_4096(resolve, ctx, size=4096, tiles=4, standoff=1e-5, fov_deg=0.01, seed=5):
+    """Deep-zoom precision workload: Mandelbox scale -1.5, 30 iterations, a camera
+    `standoff` from the surface along a searched ray, FOV 0.01 deg, a 4096^2 frame as
+    tiles x tiles tiles; eps = 1e-8 t, FP64 ray origin/direction/t, bisection hit
+    refinement (20 steps)."""
+    fid = resolve(MANDELBOX)
+    params = mandelbox_params(-1.5, 30)
+    org, d, t = find_surface_ray(ctx, fid, params, seed=seed)
+    cam = tuple(float(org[i] + d[i] * (t - standoff)) for i in range(3))
+    target = tuple(float(cam[i] + d[i]) for i in range(3))
+    views = []
+    step = size // tiles
+    for ty in range(tiles):
+        for tx in range(tiles):
+            views.append(abi.make_view(fid, size, size, cam, target=target, fov_y_deg=fov_deg, params=params,
+                                       tile_x=tx * step, tile_y=ty * step, tile_w=step, tile_h=step,
+                                       max_steps=512, max_dist=1.0, eps_coef=1e-8, eps_floor=0.0,
+                                       refine_budget=20, normal_mode=abi.ND_NORMAL_CENTRAL, normal_h_coef=1e-8,
+                                       flags=abi.ND_VIEW_DIR64))
+    return views
