@@ -30,6 +30,10 @@
  *   nd_autotune, nd_graph_*
  *       no reference counterpart; the reference picks sub-tile sizes by a pacing
  *       heuristic (ExportPacer, fractal_renderer.zig:991) instead.
+ *   nd_orbit_view
+ *       FreeCamera's basis (src/app/camera.zig:98-112) for an orbit pose.
+ *   nd_march_backward
+ *       no reference counterpart (the reference has no gradients).
  *   nd_march_backward
  *       no reference counterpart (the reference has no gradients).
  *
@@ -100,8 +104,12 @@ typedef struct nd_trap_desc {
 enum { ND_NORMAL_TETRA = 0, ND_NORMAL_CENTRAL = 1 };
 
 /* nd_view_desc.flags: ND_VIEW_DIR64 keeps ray directions in FP64 (set
- * automatically when |right| or |up| < 1e-3, i.e. fields of view under ~0.1 deg). */
-enum { ND_VIEW_DIR64 = 1 };
+ * automatically when |right| or |up| < 1e-3, i.e. fields of view under ~0.1 deg).
+ * ND_VIEW_EXACT_HIT runs the hit bisection for its whole refine budget instead of
+ * stopping once the bracket is narrower than eps(t) (the reference's stop): the hit
+ * distance then follows the root of DE = eps(t) to bracket / 2^budget and is a
+ * smooth function of the view and the parameters, which gradients need. */
+enum { ND_VIEW_DIR64 = 1, ND_VIEW_EXACT_HIT = 2 };
 
 /* One view: a camera, a frame (or a tile of it) and one fractal instance. */
 typedef struct nd_view_desc {
@@ -215,6 +223,44 @@ nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
                            const nd_march_opts* opts, const nd_gbuffer* out, void* stream, nd_graph** graph);
 nd_status nd_graph_launch(nd_graph* graph, void* stream);
 nd_status nd_graph_destroy(nd_graph* graph);
+
+/* An orbit camera: position = target + dist * (cos(pitch) sin(yaw), sin(pitch),
+ * -cos(pitch) cos(yaw)) (angles in radians), looking at target, with FreeCamera's
+ * basis (src/app/camera.zig:98-112: right = normalize(forward x up), up = right x
+ * forward) scaled by tan(fov_y/2).  The pose the adjoint differentiates. */
+typedef struct nd_orbit_camera {
+  double target[3];
+  double yaw;
+  double pitch;
+  double dist;
+  double world_up[3];
+  double fov_y_deg;
+} nd_orbit_camera;
+
+/* Fill view->cam_pos/fwd/right/up from an orbit camera. */
+nd_status nd_orbit_view(const nd_orbit_camera* cam, nd_view_desc* view);
+
+/* Gradient of an image loss with respect to formula @params and the orbit pose.
+ * No counterpart in the reference (it has no gradients).  views/cams (HOST) are the
+ * forward call's views and their orbit cameras (view i must have been filled from
+ * cams[i]); fwd (DEVICE) the forward's G-buffer, of which depth64 and normal are
+ * read; dL_dshade (DEVICE, one float per ray) is dLoss/d(shade) for the Lambert
+ * grey level the forward wrote.  For each view the call ADDS to dL_dtheta (DEVICE,
+ * nviews x (nparams + 3) doubles) the gradient with respect to
+ * params[param_idx[0..nparams-1]] (nparams <= 4), then yaw, pitch, dist.
+ * dshade_dtheta (DEVICE, nullable) receives per G-buffer slot the nparams + 3
+ * derivatives of that ray's shade (0 for misses and back-lit rays); when it is
+ * given, dL_dtheta and dL_dshade may be NULL.
+ * Implicit differentiation at each hit: dt/dtheta = -(dDE/dtheta) / (grad DE . d - eps
+ * coef), through the central-difference normal and the Lambert term; visibility
+ * (silhouette) changes are not differentiated.  opts (nullable) selects the dual
+ * numbers' precision, de_precision 32 (default) or 64; its other fields are unused.
+ * Needs a directional light (light_dir), central-difference normals and no shadow
+ * ray; other views return ND_ERR_UNSUPPORTED.  Synchronises the stream. */
+nd_status nd_march_backward(nd_ctx* ctx, const nd_view_desc* views, const nd_orbit_camera* cams, int32_t nviews,
+                            const int32_t* param_idx, int32_t nparams, const nd_gbuffer* fwd,
+                            const float* dL_dshade, double* dL_dtheta, double* dshade_dtheta,
+                            const nd_march_opts* opts, void* stream);
 
 /* Forward march that allocates nothing: no cudaMalloc, no cudaFree, no context.
  * No counterpart in the reference.  For callers that cannot allocate device

@@ -22,6 +22,7 @@ ND_TRAP_MIN, ND_TRAP_MAX, ND_TRAP_AVERAGE, ND_TRAP_LAST, ND_TRAP_ITERATION = ran
 ND_NORMAL_TETRA, ND_NORMAL_CENTRAL = 0, 1
 ND_KERNEL_AUTO, ND_KERNEL_PLAIN, ND_KERNEL_PERSISTENT = 0, 1, 2
 ND_VIEW_DIR64 = 1
+ND_VIEW_EXACT_HIT = 2
 
 
 class nd_param_info(C.Structure):
@@ -71,6 +72,22 @@ class nd_stats(C.Structure):
 class nd_tune_result(C.Structure):
     _fields_ = [("block", C.c_int32), ("blocks_per_sm", C.c_int32), ("refill_threshold", C.c_int32),
                 ("kernel", C.c_int32), ("rays_per_s", C.c_double)]
+
+
+class nd_orbit_camera(C.Structure):
+    _fields_ = [("target", C.c_double * 3), ("yaw", C.c_double), ("pitch", C.c_double), ("dist", C.c_double),
+                ("world_up", C.c_double * 3), ("fov_y_deg", C.c_double)]
+
+
+def orbit_camera(yaw=0.0, pitch=0.0, dist=2.5, target=(0.0, 0.0, 0.0), world_up=(0.0, 1.0, 0.0),
+                 fov_y_deg=60.0) -> nd_orbit_camera:
+    """An orbit pose (angles in radians); nd_orbit_view turns it into a camera."""
+    c = nd_orbit_camera()
+    c.target[:] = [float(x) for x in target]
+    c.yaw, c.pitch, c.dist = float(yaw), float(pitch), float(dist)
+    c.world_up[:] = [float(x) for x in world_up]
+    c.fov_y_deg = float(fov_y_deg)
+    return c
 
 
 def _sub(a, b):

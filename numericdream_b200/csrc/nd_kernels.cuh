@@ -9,6 +9,7 @@
 #include <algorithm>
 
 #include "nd_rayprog.h"
+#include "nd_adjoint.cuh"
 
 namespace nd {
 
@@ -277,6 +278,7 @@ struct KernelTable {
   LaunchFn persistent_f64, persistent_f64_batched;
   LaunchFn trap_f32, trap_f32_batched, trap_f32_dir64, trap_f32_dir64_batched, trap_f64, trap_f64_batched;
   DePointsFn de_points_f32, de_points_f64;
+  AdjointFn adjoint_f32, adjoint_f32_batched, adjoint_f64, adjoint_f64_batched;
 };
 
 template <class Set> KernelTable make_kernel_table() {
@@ -298,6 +300,10 @@ template <class Set> KernelTable make_kernel_table() {
   t.trap_f64_batched = &launch_trap<Set, double, true, true>;
   t.de_points_f32 = &launch_de_points<Set, float>;
   t.de_points_f64 = &launch_de_points<Set, double>;
+  t.adjoint_f32 = &launch_adjoint<Set, float, false>;
+  t.adjoint_f32_batched = &launch_adjoint<Set, float, true>;
+  t.adjoint_f64 = &launch_adjoint<Set, double, false>;
+  t.adjoint_f64_batched = &launch_adjoint<Set, double, true>;
   return t;
 }
 

@@ -22,6 +22,7 @@
 #include <stdint.h>
 
 #include "nd_helpers.h"
+#include "nd_dual.h"
 #include "../../include/nd_march.h"
 
 #if defined(__CUDACC__)
@@ -79,6 +80,8 @@ struct DevView {
   int32_t code;         // formula index inside the kernel's formula set
   int32_t max_samples;  // max_steps * (1 + refine budget) + bisect budget
   int32_t dir64;        // ray directions need FP64 (deep-zoom cameras)
+  int32_t user_index;   // the view's index in the caller's array
+  int32_t exact_hit;    // bisect for the whole budget (ND_VIEW_EXACT_HIT)
   int32_t pad;
 };
 
@@ -182,40 +185,53 @@ template <class T> struct ParamRef {
 // distance again; average mode only counts changed iterations).  The loop stops
 // at that fixed point, e.g. as soon as a Mandelbulb point has escaped
 // (bulb_power_step returns the carry unchanged once r > 2, tpl:1019-1023).
-template <class F, class T, bool kTrap>
-ND_DEV_INLINE DEOut<T> formula_de(ndw::v3<T> pos, const float* params, const nd_trap_desc& trap, float factor) {
-  const ParamRef<T> p{params};
+//
+// PR is the parameter accessor (p[i]); the adjoint instantiates the formula code
+// with dual numbers for T and a PR whose entries carry tangents.
+template <class F, class T, bool kTrap, class PR>
+ND_DEV_INLINE DEOut<T> formula_de_p(ndw::v3<T> pos, const PR& p, const nd_trap_desc& trap, float factor) {
   ndw::IterCarry<T> c{pos, T(1)};
   TrapAcc<T> acc;
-  if (kTrap) acc = trap_begin<T>(trap);
-  int n = F::template iterations<T, ParamRef<T>>(p);
+  if constexpr (kTrap) acc = trap_begin<T>(trap);
+  int n = F::template iterations<T, PR>(p);
   n = n < kMaxIterations ? n : kMaxIterations;
   int changed = 0;
   for (int it = 0; it < n; ++it) {
     const ndw::v3<T> zp = c.z;
     const T drp = c.dr;
-    c = F::template step<T, ParamRef<T>>(c, pos, p);
+    c = F::template step<T, PR>(c, pos, p);
     const bool ch = (c.z.x != zp.x) | (c.z.y != zp.y) | (c.z.z != zp.z);
     if (!ch && !(c.dr != drp)) break;  // fixed point: nothing changes any more
-    if (kTrap) {
+    if constexpr (kTrap) {
       changed += ch ? 1 : 0;
       trap_update(acc, trap, c.z, ch, it);
     }
   }
   DEOut<T> o;
-  o.d = F::template finalize<T, ParamRef<T>>(c) * T(factor);
-  o.trap = kTrap ? trap_finish(acc, trap, n) : T(0);
+  o.d = F::template finalize<T, PR>(c) * T(factor);
+  if constexpr (kTrap) o.trap = trap_finish(acc, trap, n);
+  else o.trap = T(0);
   o.iters = changed;
   return o;
 }
 
+template <class F, class T, bool kTrap>
+ND_DEV_INLINE DEOut<T> formula_de(ndw::v3<T> pos, const float* params, const nd_trap_desc& trap, float factor) {
+  return formula_de_p<F, T, kTrap, ParamRef<T>>(pos, ParamRef<T>{params}, trap, factor);
+}
+
 // A compile-time list of formulas; code selects one (warp-uniform in practice,
-// because batched views are ordered by formula).
+// because batched views are ordered by formula).  de_with evaluates the DE alone
+// (no trap) with a caller-supplied parameter accessor.
 template <class... Fs> struct FormulaSet;
 template <class F> struct FormulaSet<F> {
   template <class T, bool kTrap = false>
   static ND_DEV_INLINE DEOut<T> de(int, ndw::v3<T> pos, const DevView& v) {
     return formula_de<F, T, kTrap>(pos, v.params, v.trap, v.factor);
+  }
+  template <class T, class PR>
+  static ND_DEV_INLINE DEOut<T> de_with(int, ndw::v3<T> pos, const PR& p, const DevView& v) {
+    return formula_de_p<F, T, false, PR>(pos, p, v.trap, v.factor);
   }
 };
 template <class F, class G, class... Rest> struct FormulaSet<F, G, Rest...> {
@@ -223,6 +239,11 @@ template <class F, class G, class... Rest> struct FormulaSet<F, G, Rest...> {
   static ND_DEV_INLINE DEOut<T> de(int code, ndw::v3<T> pos, const DevView& v) {
     if (code == 0) return formula_de<F, T, kTrap>(pos, v.params, v.trap, v.factor);
     return FormulaSet<G, Rest...>::template de<T, kTrap>(code - 1, pos, v);
+  }
+  template <class T, class PR>
+  static ND_DEV_INLINE DEOut<T> de_with(int code, ndw::v3<T> pos, const PR& p, const DevView& v) {
+    if (code == 0) return formula_de_p<F, T, false, PR>(pos, p, v.trap, v.factor);
+    return FormulaSet<G, Rest...>::template de_with<T, PR>(code - 1, pos, p, v);
   }
 };
 
@@ -267,7 +288,8 @@ template <> ND_DEV_INLINE double march_eps<double>(const DevView& v, double t) {
 
 // Primary ray of a work item: cs_wf_generate tpl:5120-5127 / fs_simple tpl:4523-4525
 // with the tile transform (fractal_renderer.zig:852-863) folded into frame pixels.
-ND_DEV_INLINE D3 ray_dir(const DevView& v, int64_t local) {
+// (ux, uy): the camera-plane coordinates of the ray, direction = fwd + ux right + uy up.
+ND_DEV_INLINE void ray_uv(const DevView& v, int64_t local, double* ux, double* uy) {
   const int64_t npix = int64_t(v.tile_w) * v.tile_h;
   const int64_t s = local / npix;
   const int64_t pix = local - s * npix;
@@ -281,7 +303,13 @@ ND_DEV_INLINE D3 ray_dir(const DevView& v, int64_t local) {
   }
   const double ndc_x = 2.0 * (double(px) + jx) / double(v.width) - 1.0;
   const double ndc_y = 1.0 - 2.0 * (double(py) + jy) / double(v.height);
-  const double ux = ndc_x * v.aspect, uy = -ndc_y;
+  *ux = ndc_x * v.aspect;
+  *uy = -ndc_y;
+}
+
+ND_DEV_INLINE D3 ray_dir(const DevView& v, int64_t local) {
+  double ux, uy;
+  ray_uv(v, local, &ux, &uy);
   double x = v.fwd[0] + v.right[0] * ux + v.up[0] * uy;
   double y = v.fwd[1] + v.right[1] * ux + v.up[1] * uy;
   double z = v.fwd[2] + v.right[2] * ux + v.up[2] * uy;
@@ -449,12 +477,12 @@ template <class T, bool kDir64> struct Lane {
           a = st;
         }
         ++k;
-        if (b - a <= e || k >= bisect_budget) begin_normal(b);
+        if ((b - a <= e && !v.exact_hit) || k >= bisect_budget) begin_normal(b);
         else if (n >= v.max_samples) finish(v, g, t_hit, 1.0f);  // march_to's loop ran out: a miss
         return;
       }
       if (d < e) {
-        if (on_hit && bisect_budget > 0 && st - a > e) {
+        if (on_hit && bisect_budget > 0 && (v.exact_hit ? st > a : st - a > e)) {
           bisecting = true;
           probing = false;
           b = st;

@@ -6,6 +6,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <complex>
 #include <map>
 #include <mutex>
 #include <string>
@@ -777,6 +778,7 @@ size_t nd_sizeof(const char* name) {
   if (n == "nd_stats") return sizeof(nd_stats);
   if (n == "nd_param_info") return sizeof(nd_param_info);
   if (n == "nd_tune_result") return sizeof(nd_tune_result);
+  if (n == "nd_orbit_camera") return sizeof(nd_orbit_camera);
   return 0;
 }
 
@@ -966,5 +968,167 @@ extern "C" nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t
     e = fn(a, host[first[l]], c, st);
     if (e != cudaSuccess) return ND_ERR_CUDA;
   }
+  return ND_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Orbit camera and the adjoint pass.
+
+namespace {
+
+// The orbit pose's camera: origin, forward and the FOV-scaled right/up, with
+// FreeCamera's basis (src/app/camera.zig:98-112).  S is double, or a complex number
+// for the complex-step derivative of the basis.
+template <class S>
+void orbit_basis(const nd_orbit_camera& c, S yaw, S pitch, S dist, S org[3], S f[3], S r[3], S u[3]) {
+  using std::cos;
+  using std::sin;
+  using std::sqrt;
+  const S cp = cos(pitch);
+  org[0] = S(c.target[0]) + dist * cp * sin(yaw);
+  org[1] = S(c.target[1]) + dist * sin(pitch);
+  org[2] = S(c.target[2]) - dist * cp * cos(yaw);
+  for (int i = 0; i < 3; ++i) f[i] = S(c.target[i]) - org[i];
+  // normalise without a modulus, so that the complex step stays analytic
+  S fn = sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+  for (int i = 0; i < 3; ++i) f[i] = f[i] / fn;
+  const double wu[3] = {c.world_up[0], c.world_up[1], c.world_up[2]};
+  r[0] = f[1] * S(wu[2]) - f[2] * S(wu[1]);
+  r[1] = f[2] * S(wu[0]) - f[0] * S(wu[2]);
+  r[2] = f[0] * S(wu[1]) - f[1] * S(wu[0]);
+  S rn = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+  for (int i = 0; i < 3; ++i) r[i] = r[i] / rn;
+  u[0] = r[1] * f[2] - r[2] * f[1];
+  u[1] = r[2] * f[0] - r[0] * f[2];
+  u[2] = r[0] * f[1] - r[1] * f[0];
+  S un = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+  const S sc = S(std::tan(c.fov_y_deg * 0.5 * 3.14159265358979323846 / 180.0));
+  for (int i = 0; i < 3; ++i) {
+    r[i] = r[i] * sc;
+    u[i] = u[i] / un * sc;
+  }
+}
+
+// d(origin, forward, right, up)/d(yaw, pitch, dist) by complex steps (exact to
+// rounding: no subtraction, step 1e-30).
+nd::PoseTangents pose_tangents(const nd_orbit_camera& c) {
+  typedef std::complex<double> Z;
+  const double h = 1e-30;
+  nd::PoseTangents T;
+  for (int j = 0; j < 3; ++j) {
+    const Z yaw(c.yaw, j == 0 ? h : 0.0), pitch(c.pitch, j == 1 ? h : 0.0), dist(c.dist, j == 2 ? h : 0.0);
+    Z o[3], f[3], r[3], u[3];
+    orbit_basis<Z>(c, yaw, pitch, dist, o, f, r, u);
+    for (int i = 0; i < 3; ++i) {
+      T.dorg[j][i] = o[i].imag() / h;
+      T.dfwd[j][i] = f[i].imag() / h;
+      T.dright[j][i] = r[i].imag() / h;
+      T.dup[j][i] = u[i].imag() / h;
+    }
+  }
+  return T;
+}
+
+}  // namespace
+
+extern "C" nd_status nd_orbit_view(const nd_orbit_camera* cam, nd_view_desc* view) {
+  if (!cam || !view) return ND_ERR_INVALID;
+  const double wl = cam->world_up[0] * cam->world_up[0] + cam->world_up[1] * cam->world_up[1] +
+                    cam->world_up[2] * cam->world_up[2];
+  if (!(cam->dist > 0.0) || !(wl > 0.0) || !(cam->fov_y_deg > 0.0) || !(cam->fov_y_deg < 180.0))
+    return ND_ERR_INVALID;
+  double o[3], f[3], r[3], u[3];
+  orbit_basis<double>(*cam, cam->yaw, cam->pitch, cam->dist, o, f, r, u);
+  for (int i = 0; i < 3; ++i) {
+    view->cam_pos[i] = o[i];
+    view->fwd[i] = f[i];
+    view->right[i] = r[i];
+    view->up[i] = u[i];
+  }
+  return ND_OK;
+}
+
+extern "C" nd_status nd_march_backward(nd_ctx* ctx, const nd_view_desc* views, const nd_orbit_camera* cams,
+                                       int32_t nviews, const int32_t* param_idx, int32_t nparams,
+                                       const nd_gbuffer* fwd, const float* dL_dshade, double* dL_dtheta,
+                                       double* dshade_dtheta, const nd_march_opts* opts, void* stream) {
+  if (!ctx) return ND_ERR_INVALID;
+  if (!cams || !fwd || !fwd->depth64 || !fwd->normal)
+    return fail(ctx, ND_ERR_INVALID, "backward needs cameras and the forward's depth64 and normal");
+  if (!dL_dtheta && !dshade_dtheta) return fail(ctx, ND_ERR_INVALID, "backward needs dL/dtheta or dshade/dtheta");
+  if (dL_dtheta && !dL_dshade) return fail(ctx, ND_ERR_INVALID, "dL/dtheta needs dL/dshade");
+  const int prec = opts ? opts->de_precision : 32;
+  if (prec != 32 && prec != 64) return fail(ctx, ND_ERR_INVALID, "de_precision must be 32 or 64");
+  if (nparams < 0 || nparams > nd::kMaxAdjParams || (nparams > 0 && !param_idx))
+    return fail(ctx, ND_ERR_INVALID, "nparams must be in [0, %d]", nd::kMaxAdjParams);
+  for (int k = 0; k < nparams; ++k)
+    if (param_idx[k] < 0 || param_idx[k] >= ND_MAX_PARAMS) return fail(ctx, ND_ERR_INVALID, "bad param index");
+  std::vector<Launch> plans;
+  int64_t total = 0;
+  nd_status s = prepare(ctx, views, nviews, fwd, &plans, &total);
+  if (s != ND_OK) return s;
+  for (int i = 0; i < nviews; ++i) {
+    const nd_view_desc& v = views[i];
+    const double l2 = double(v.light_dir[0]) * v.light_dir[0] + double(v.light_dir[1]) * v.light_dir[1] +
+                      double(v.light_dir[2]) * v.light_dir[2];
+    if (v.shadow || !(l2 > 0) || v.normal_mode != ND_NORMAL_CENTRAL)
+      return fail(ctx, ND_ERR_UNSUPPORTED, "view %d: the adjoint needs a directional light, central-difference "
+                  "normals and no shadow ray", i);
+  }
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
+  cudaStream_t st = (cudaStream_t)stream;
+  // view table and pose tangents in launch order (temporary device buffers)
+  std::vector<DevView> hv;
+  std::vector<nd::PoseTangents> ht;
+  std::vector<int64_t> out_off(nviews + 1, 0);
+  for (int i = 0; i < nviews; ++i) out_off[i + 1] = out_off[i] + int64_t(views[i].spp) * views[i].tile_w * views[i].tile_h;
+  std::vector<int> first;
+  for (const Launch& L : plans) {
+    first.push_back(int(hv.size()));
+    int64_t off = 0;
+    for (size_t k = 0; k < L.views.size(); ++k) {
+      const int vi = L.views[k];
+      DevView d = make_dev_view(views[vi], off, out_off[vi], L.codes[k]);
+      d.user_index = vi;
+      off += d.rays;
+      hv.push_back(d);
+      ht.push_back(pose_tangents(cams[vi]));
+    }
+  }
+  DevView* dv = nullptr;
+  nd::PoseTangents* dt = nullptr;
+  e = cudaMallocAsync((void**)&dv, sizeof(DevView) * hv.size(), st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&dt, sizeof(nd::PoseTangents) * ht.size(), st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dv, hv.data(), sizeof(DevView) * hv.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dt, ht.data(), sizeof(nd::PoseTangents) * ht.size(), cudaMemcpyHostToDevice, st);
+  for (size_t p = 0; p < plans.size() && e == cudaSuccess; ++p) {
+    const int nv = int(plans[p].views.size());
+    nd::AdjointArgs a;
+    memset(&a, 0, sizeof(a));
+    a.views = dv + first[p];
+    a.nviews = nv;
+    a.total_rays = 0;
+    for (int k = 0; k < nv; ++k) a.total_rays += hv[first[p] + k].rays;
+    a.tangents = dt + first[p];
+    a.depth64 = fwd->depth64;
+    a.normal4 = fwd->normal;
+    a.dL_dshade = dL_dtheta ? dL_dshade : nullptr;
+    a.grad = dL_dtheta;
+    a.dshade = dshade_dtheta;
+    a.nparam = nparams;
+    for (int k = 0; k < nparams; ++k) a.param_idx[k] = param_idx[k];
+    const KernelTable& kt = plans[p].table;
+    const nd::AdjointFn fn = prec == 64 ? (nv > 1 ? kt.adjoint_f64_batched : kt.adjoint_f64)
+                                        : (nv > 1 ? kt.adjoint_f32_batched : kt.adjoint_f32);
+    e = fn(a, hv[first[p]], st);
+  }
+  // the host staging vectors are pageable: wait for the copies before they go away
+  cudaError_t e2 = cudaStreamSynchronize(st);
+  if (dv) cudaFreeAsync(dv, st);
+  if (dt) cudaFreeAsync(dt, st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint launch");
+  if (e2 != cudaSuccess) return cuda_fail(ctx, e2, "adjoint");
   return ND_OK;
 }

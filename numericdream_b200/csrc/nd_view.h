@@ -56,6 +56,8 @@ inline DevView make_dev_view(const nd_view_desc& v, int64_t ray_offset, int64_t 
   d.normal_mode = v.normal_mode;
   d.shadow = v.shadow;
   d.code = code;
+  d.user_index = 0;
+  d.exact_hit = (v.flags & ND_VIEW_EXACT_HIT) != 0 ? 1 : 0;
   const int refine = v.march_verify ? v.refine_budget : 0;
   const int bisect = v.march_verify ? 0 : v.refine_budget;
   const int64_t ms = int64_t(v.max_steps) * (1 + refine) + bisect;

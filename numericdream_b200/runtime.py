@@ -53,6 +53,11 @@ _SIGNATURES = {
     "nd_sizeof": (C.c_size_t, [C.c_char_p]),
     "nd_de_points": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int64, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "nd_orbit_view": (C.c_int32, [C.POINTER(abi.nd_orbit_camera), C.POINTER(abi.nd_view_desc)]),
+    "nd_march_backward": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.POINTER(abi.nd_orbit_camera),
+                                      C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(abi.nd_gbuffer),
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(abi.nd_march_opts),
+                                      C.c_void_p]),
 }
 
 _lib = None
@@ -90,7 +95,7 @@ def check_layout(lib=None):
     """Compare the ctypes structure sizes with the library's own."""
     lib = lib or load_library()
     for name in ("nd_view_desc", "nd_trap_desc", "nd_gbuffer", "nd_march_opts", "nd_stats", "nd_param_info",
-                 "nd_tune_result"):
+                 "nd_tune_result", "nd_orbit_camera"):
         mine = C.sizeof(getattr(abi, name))
         theirs = lib.nd_sizeof(name.encode())
         if mine != theirs:
@@ -148,6 +153,14 @@ def view_defaults(fid: int) -> abi.nd_view_desc:
     if st != abi.ND_OK:
         raise NDError(st)
     return v
+
+
+def orbit_view(cam: abi.nd_orbit_camera, view: abi.nd_view_desc) -> abi.nd_view_desc:
+    """Set view's camera from an orbit pose (nd_orbit_view)."""
+    st = load_library().nd_orbit_view(C.byref(cam), C.byref(view))
+    if st != abi.ND_OK:
+        raise NDError(st, "nd_orbit_view")
+    return view
 
 
 def total_rays(views) -> int:
@@ -251,6 +264,31 @@ class Context:
         st = self.lib.nd_march_forward(self.handle, arr, len(views), C.byref(opts) if opts is not None else None,
                                        C.byref(g), s)
         self._check(st, "nd_march_forward")
+
+    def backward(self, views, cams, gbuf: GBuffer, dL_dshade=None, param_idx=(), de_precision=32,
+                 per_ray=False, stream=None):
+        """dLoss/dtheta (nviews x (len(param_idx) + 3): params, yaw, pitch, dist) for
+        dLoss/dshade (torch float32 on the device, one per ray).  With per_ray=True
+        returns (grad or None, dshade/dtheta per ray: rays x (len(param_idx) + 3))."""
+        import torch
+
+        k = len(param_idx) + 3
+        dev = gbuf.depth.device
+        grad = torch.zeros((len(views), k), dtype=torch.float64, device=dev) if dL_dshade is not None else None
+        per = torch.zeros((gbuf.depth.numel(), k), dtype=torch.float64, device=dev) if per_ray else None
+        arr = (abi.nd_view_desc * len(views))(*views)
+        carr = (abi.nd_orbit_camera * len(cams))(*cams)
+        pidx = (C.c_int32 * max(1, len(param_idx)))(*param_idx)
+        g = gbuf.as_abi()
+        opts = make_opts(de_precision=de_precision)
+        s = None if stream is None else C.c_void_p(stream)
+        dl = dL_dshade.contiguous() if dL_dshade is not None else None
+        st = self.lib.nd_march_backward(self.handle, arr, carr, len(views), pidx, len(param_idx), C.byref(g),
+                                        dl.data_ptr() if dl is not None else None,
+                                        grad.data_ptr() if grad is not None else None,
+                                        per.data_ptr() if per is not None else None, C.byref(opts), s)
+        self._check(st, "nd_march_backward")
+        return (grad, per) if per_ray else grad
 
     def de_points(self, view: abi.nd_view_desc, pts, de_precision: int = 32):
         """DE, trap and changed-iteration count of view's formula at points (torch, on device)."""

@@ -13,7 +13,9 @@ Five workloads, each a list of ``nd_view_desc`` (see include/nd_march.h):
                         Mandelbulb (power U[4,10]), Mandelbox (scale U[-2,-1.2]), Menger
                         (3-6 iterations), pseudo-Kleinian (box size U[0.8,1.2]); cameras
                         on spheres of radius U[1.5,4] aimed at the origin; max 384 steps.
-* ``mandelbulb_512``     the differentiation workload's forward view (Lambert, one light).
+* ``mandelbulb_512``     the differentiation workload's view: Mandelbulb with the escape
+                        radius as a parameter, Lambert shading from one light, orbit
+                        camera; ``differentiation_16`` makes its 16 problems.
 * ``deepzoom_4096``      Mandelbox scale -1.5, 30 iterations, 4096x4096 in 16 tiles of
                         1024x1024, FOV 0.01 deg, camera 1e-5 from the surface.
 
@@ -33,6 +35,7 @@ MANDELBULB = "mandelbrot"            # built-in formula (src/gpu/shaders/mandelb
 MANDELBOX = "amazingbox_box"
 MENGER = "menger3_ifs"
 PSEUDO_KLEINIAN = "pseudokleinian_kleinian"
+MANDELBULB_BAILOUT = "mandelbulb_bailout"   # this package's formulas/mandelbulb_bailout.wgsl
 
 # default light of the shadowed workloads (unit direction TO the light)
 LIGHT_DIR = (0.4, 0.8, -0.45)
@@ -119,15 +122,39 @@ def batched_64(resolve, nviews=64, seed=7, min_side=64, max_side=1024, max_steps
     return views
 
 
-def mandelbulb_512(resolve, power=8.0, yaw_deg=0.0, pitch_deg=0.0, dist=2.5, size=512):
-    """The differentiation workload's forward view: Lambert with one directional light."""
-    fid = resolve(MANDELBULB)
-    yaw, pitch = math.radians(yaw_deg), math.radians(pitch_deg)
-    pos = (dist * math.cos(pitch) * math.sin(yaw), dist * math.sin(pitch), -dist * math.cos(pitch) * math.cos(yaw))
-    v = abi.make_view(fid, size, size, pos, fov_y_deg=60.0, params=mandelbulb_params(power, 12), max_steps=256,
-                      eps_coef=1e-4, eps_floor=0.0, normal_mode=abi.ND_NORMAL_CENTRAL, normal_h_coef=1e-4,
-                      light_dir=list(LIGHT_DIR))
-    return [v]
+def mandelbulb_512(resolve, power=8.0, yaw=0.0, pitch=0.0, dist=2.5, size=512, bailout=2.0):
+    """The differentiation workload's view: Mandelbulb (12 iterations, escape radius
+    `bailout`, formulas/mandelbulb_bailout.wgsl of this package) with Lambert shading
+    from one directional light, seen by an orbit camera (angles in radians) around
+    the origin.  The hit is refined by a 40-step FP64 bisection on DE = eps(t) that
+    runs to the end of its budget (ND_VIEW_EXACT_HIT), so the hit distance is a
+    smooth function of theta.  Returns (view, orbit camera)."""
+    from . import runtime
+
+    fid = resolve(MANDELBULB_BAILOUT)
+    cam = abi.orbit_camera(yaw=yaw, pitch=pitch, dist=dist, fov_y_deg=60.0)
+    v = abi.make_view(fid, size, size, (0.0, 0.0, -dist), fov_y_deg=60.0, params=[power, 12.0, bailout],
+                      max_steps=256, eps_coef=1e-4, eps_floor=0.0, refine_budget=40,
+                      normal_mode=abi.ND_NORMAL_CENTRAL, normal_h_coef=1e-4, light_dir=list(LIGHT_DIR),
+                      flags=abi.ND_VIEW_EXACT_HIT)
+    runtime.orbit_view(cam, v)
+    return v, cam
+
+
+def differentiation_16(resolve, size=512, problems=16, seed=11):
+    """16 problems: start power U[6,10] (seeded), bailout 2, camera yaw 0, pitch 0,
+    distance 2.5; each target is rendered at power 8 with the camera yawed +2 degrees.
+    Returns (start views, start cameras, target views, target cameras)."""
+    rng = random.Random(seed)
+    sv, sc, tv, tc = [], [], [], []
+    for _ in range(problems):
+        v, c = mandelbulb_512(resolve, power=rng.uniform(6.0, 10.0), size=size)
+        sv.append(v)
+        sc.append(c)
+        v, c = mandelbulb_512(resolve, power=8.0, yaw=math.radians(2.0), size=size)
+        tv.append(v)
+        tc.append(c)
+    return sv, sc, tv, tc
 
 
 def rays(views) -> int:

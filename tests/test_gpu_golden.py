@@ -47,3 +47,19 @@ def test_gpu_de_matches_reference_golden(ctx):
     assert all(m <= 1e-9 for m, _ in worst64.values()), worst64
     # the FP32 fast-math DE stays within FP32 noise on the typical point
     assert all(m <= 1e-3 for m, _ in worst32.values()), worst32
+
+
+def test_mandelbulb_bailout_at_2_is_the_reference_mandelbulb(ctx):
+    """The package's mandelbulb_bailout formula with Bailout = 2 against the golden
+    values of the reference's built-in Mandelbulb (same power and iterations)."""
+    with open(GOLDEN) as fh:
+        entries = json.load(fh)["formulas"]["mandelbrot"]
+    fid = runtime.find_formula("mandelbulb_bailout")
+    worst = 0.0
+    for e in entries:
+        power, iters = e["params"][0], e["params"][1]
+        v = abi.make_view(fid, 1, 1, (0.0, 0.0, -3.0), params=[power, iters, 2.0])
+        d64, _, _ = ctx.de_points(v, np.asarray(e["points"]), 64)
+        worst = max(worst, float(_rel(d64, np.asarray(e["de"])).max()))
+    print("mandelbulb_bailout(2) vs reference Mandelbulb, fp64 max rel", worst)
+    assert worst <= 1e-9
