@@ -242,6 +242,41 @@ def reference_arm(args):
     return 0
 
 
+def differentiation_step(ctx, stream, sptr, timed, steps):
+    """Differentiation workload: 16 problems of a 512x512 Mandelbulb (Lambert, one
+    light, orbit camera); one step = the FP32 forward of the 16 start views, dLoss/dshade
+    of the mean-L2 loss to the targets, and the adjoint for (power, bailout, yaw, pitch,
+    dist).  The targets are rendered once, outside the timed region."""
+    import torch
+
+    from numericdream_b200 import abi, runtime, workloads
+
+    sv, sc, tv, _ = workloads.differentiation_16(runtime.find_formula)
+    n = workloads.rays(sv)
+    opts = runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT)
+    gt = runtime.GBuffer.allocate(n)
+    ctx.forward(tv, gt, opts, stream=sptr)
+    g = runtime.GBuffer.allocate(n)
+    stream.synchronize()
+    target = gt.shade.clone()
+    out = {"workload": "differentiation_16 (16 x 512x512 Mandelbulb, Lambert, orbit camera)",
+           "rays_per_step": n}
+    for prec in (32, 64):
+        def step():
+            ctx.forward(sv, g, opts, stream=sptr)
+            dl = (2.0 / n) * (g.shade - target)
+            ctx.backward(sv, sc, g, dl, param_idx=(0, 2), de_precision=prec, stream=sptr)
+
+        ms = timed(step, steps, 2)
+        out[f"ms_per_step_adjoint_fp{prec}"] = ms
+        out[f"rays_per_s_adjoint_fp{prec}"] = n / (ms * 1e-3)
+    ms_f = timed(lambda: ctx.forward(sv, g, opts, stream=sptr), steps, 2)
+    out["ms_forward"] = ms_f
+    out["note"] = ("forward + adjoint per step; the adjoint spends 3 + 6 + 7 x 5 dual-number DE evaluations "
+                   "per hit ray (gradient, normal taps, then per theta the hit and six taps)")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -341,6 +376,9 @@ def main():
                  "de_evals_per_s": st2.de_evals * ws / (ms2 * 1e-3),
                  "plain": n2 * ws / (ms2_plain * 1e-3) / 1e6, "batched_over_plain": ms2_plain / ms2}
         del g2
+    diff = None
+    if not args.no_extra and ws == 1:
+        diff = differentiation_step(ctx, stream, sptr, timed, max(2, args.steps // 2))
     clk = clocks.stop()
     gnp = gbuf.numpy() if rank == 0 else None
 
@@ -387,6 +425,7 @@ def main():
             "tune": {"kernel": tune.kernel, "blocks_per_sm": tune.blocks_per_sm,
                      "refill_threshold": tune.refill_threshold} if tune else None,
             "second_workload": extra,
+            "differentiation": diff,
         }
         print(json.dumps(line))
     ctx.close()
