@@ -182,9 +182,11 @@ template <class T> struct ParamRef {
 // no iteration index), so once one iteration returns its input carry unchanged
 // every later iteration would too, and the orbit-trap updates they would make
 // leave the accumulator as it is (min, max, last and iteration modes see the same
-// distance again; average mode only counts changed iterations).  The loop stops
-// at that fixed point, e.g. as soon as a Mandelbulb point has escaped
-// (bulb_power_step returns the carry unchanged once r > 2, tpl:1019-1023).
+// distance again; average mode only counts changed iterations).  The trap
+// evaluation stops at that fixed point.  The distance-only evaluation of the march
+// runs every iteration instead: testing the carry costs more per iteration than the
+// iterations it would skip (an escaped Mandelbulb point's step is one length and one
+// comparison), and the loop then matches march_to's evaluation exactly.
 //
 // PR is the parameter accessor (p[i]); the adjoint instantiates the formula code
 // with dual numbers for T and a PR whose entries carry tangents.
@@ -197,14 +199,16 @@ ND_DEV_INLINE DEOut<T> formula_de_p(ndw::v3<T> pos, const PR& p, const nd_trap_d
   n = n < kMaxIterations ? n : kMaxIterations;
   int changed = 0;
   for (int it = 0; it < n; ++it) {
-    const ndw::v3<T> zp = c.z;
-    const T drp = c.dr;
-    c = F::template step<T, PR>(c, pos, p);
-    const bool ch = (c.z.x != zp.x) | (c.z.y != zp.y) | (c.z.z != zp.z);
-    if (!ch && !(c.dr != drp)) break;  // fixed point: nothing changes any more
     if constexpr (kTrap) {
+      const ndw::v3<T> zp = c.z;
+      const T drp = c.dr;
+      c = F::template step<T, PR>(c, pos, p);
+      const bool ch = (c.z.x != zp.x) | (c.z.y != zp.y) | (c.z.z != zp.z);
+      if (!ch && !(c.dr != drp)) break;  // fixed point: nothing changes any more
       changed += ch ? 1 : 0;
       trap_update(acc, trap, c.z, ch, it);
+    } else {
+      c = F::template step<T, PR>(c, pos, p);
     }
   }
   DEOut<T> o;
@@ -491,6 +495,17 @@ template <class T, bool kDir64> struct Lane {
           return;
         }
         begin_normal(st);
+        return;
+      }
+      if (probing && on_hit) {
+        // a plain sphere-tracing step (no verify refinement): advance by d
+        a = t;
+        t = t + d;
+        b = t;
+        k = 0;
+        resolved = false;
+        ++i;
+        if (t > v.max_dist || i >= v.max_steps || n >= v.max_samples) finish(v, g, t_hit, 1.0f);
         return;
       }
       if (probing) {
