@@ -242,6 +242,31 @@ def reference_arm(args):
     return 0
 
 
+def small_and_deepzoom(ctx, sptr, timed, steps):
+    """The single-view Mandelbulb 256x256 (persistent and plain) and the deep-zoom frame
+    (Mandelbox, 30 iterations, 4096x4096 in 16 tiles of 1024x1024, FP64 DE)."""
+    from numericdream_b200 import abi, runtime, workloads
+
+    out = {}
+    v = workloads.mandelbulb_256(runtime.find_formula)
+    n = workloads.rays(v)
+    g = runtime.GBuffer.allocate(n)
+    for label, kern in (("persistent", abi.ND_KERNEL_PERSISTENT), ("plain", abi.ND_KERNEL_PLAIN)):
+        o = runtime.make_opts(kernel=kern)
+        ms = timed(lambda: ctx.forward(v, g, o, stream=sptr), steps, 3)
+        out[f"mandelbulb_256_{label}"] = {"ms_per_step": ms, "Mrays_per_s": n / (ms * 1e-3) / 1e6}
+    views = workloads.deepzoom_4096(runtime.find_formula, ctx)
+    n = workloads.rays(views)
+    g = runtime.GBuffer.allocate(n)
+    o = runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, de_precision=64)
+    ms = timed(lambda: ctx.forward(views, g, o, stream=sptr), 1, 1)
+    st = ctx.stats()
+    out["deepzoom_4096"] = {"ms_per_frame": ms, "Mrays_per_s": n / (ms * 1e-3) / 1e6,
+                            "de_evals_per_s": st.de_evals / (ms * 1e-3), "hits": st.hits, "rays": n,
+                            "de": "fp64 (an FP32 DE cannot resolve the 1e-12 pixel footprint: no ray hits)"}
+    return out
+
+
 def differentiation_step(ctx, stream, sptr, timed, steps):
     """Differentiation workload: 16 problems of a 512x512 Mandelbulb (Lambert, one
     light, orbit camera); one step = the FP32 forward of the 16 start views, dLoss/dshade
@@ -376,9 +401,10 @@ def main():
                  "de_evals_per_s": st2.de_evals * ws / (ms2 * 1e-3),
                  "plain": n2 * ws / (ms2_plain * 1e-3) / 1e6, "batched_over_plain": ms2_plain / ms2}
         del g2
-    diff = None
+    diff = other = None
     if not args.no_extra and ws == 1:
         diff = differentiation_step(ctx, stream, sptr, timed, max(2, args.steps // 2))
+        other = small_and_deepzoom(ctx, sptr, timed, max(2, args.steps // 2))
     clk = clocks.stop()
     gnp = gbuf.numpy() if rank == 0 else None
 
@@ -426,6 +452,7 @@ def main():
                      "refill_threshold": tune.refill_threshold} if tune else None,
             "second_workload": extra,
             "differentiation": diff,
+            "other_configs": other,
         }
         print(json.dumps(line))
     ctx.close()
