@@ -111,15 +111,28 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
   const int32_t total = int32_t(a.total_rays);
   int32_t wnext = 0, wend = 0;  // warp-uniform: taken but not yet started rays [wnext, wend)
   const int thr = a.refill_threshold;
+  const bool defer = a.hit_list != nullptr;
   while (true) {
+    int32_t hit_item = -1;
     if (L.phase == PH_DONE && L.item >= 0) {
       ++rays;
       hits += L.hit ? 1 : 0;
-      const uint32_t taps = L.hit ? normal_taps(kBatched ? a.views[L.view] : single) : 0u;
+      const uint32_t taps = (L.hit && !defer) ? normal_taps(kBatched ? a.views[L.view] : single) : 0u;
       ev_m += L.mev;
       ev_n += taps;
       ev_s += L.evals - L.mev - taps;
+      if (defer && L.hit) hit_item = L.item;
       L.item = -1;
+    }
+    if (defer) {
+      // append this pass's finished hits to the shade pass's list, one atomic per warp
+      const unsigned hm = __ballot_sync(full, hit_item >= 0);
+      if (hm) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(a.hit_count, unsigned(__popc(hm)));
+        base = __shfl_sync(full, base, 0);
+        if (hit_item >= 0) a.hit_list[base + __popc(hm & lt_mask)] = hit_item;
+      }
     }
     const unsigned idle = __ballot_sync(full, L.item < 0);
     const int nidle = __popc(idle);
@@ -167,30 +180,42 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     if (L.item >= 0) {
       const DevView& v = kBatched ? a.views[L.view] : single;
       const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(L.sample_pos(v)), v);
-      L.advance(v, de, a.out, a.t_hit);
+      L.advance(v, de, a.out, a.t_hit, defer);
     }
   }
   flush_stats(a.stats, rays, ev_m, ev_n, ev_s, hits, refills);
 }
 
-// --------------------------------------------------------------- trap pass
-// One thread per ray: the DE with the orbit trap at each hit point.  Coherent
-// (every hit costs exactly one evaluation), so it needs no refill.
+// --------------------------------------------------------------- shade pass
+// Work at the hit points, after the march: with a hit list (deferred shading) the
+// normal taps, Lambert level and, when asked, the orbit trap of every listed hit;
+// without one (inline shading, or the plain kernel) the orbit trap of every ray
+// that hit.  Every hit costs the same number of evaluations, so the pass is
+// coherent and needs no refill; it strides over its work with a resident grid.
 template <class Set, class T, bool kDir64, bool kBatched>
 __global__ void __launch_bounds__(128, MinBlocks<T>::value)
-    trap_kernel(const __grid_constant__ LaunchArgs a, const __grid_constant__ DevView single) {
-  const int64_t it = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (it >= a.total_rays) return;
-  const int vi = kBatched ? find_view(a.views, a.nviews, it) : 0;
-  const DevView& v = kBatched ? a.views[vi] : single;
-  const int64_t local = it - v.ray_offset;
-  const double t = a.t_hit[v.out_offset + local];
-  if (t < 0.0) {
-    if (a.out.trap) a.out.trap[v.out_offset + local] = 0.0f;
-    if (a.out.iters) a.out.iters[v.out_offset + local] = 0u;
-    return;
+    shade_kernel(const __grid_constant__ LaunchArgs a, const __grid_constant__ DevView single, int do_trap) {
+  const bool list = a.hit_list != nullptr;
+  const int64_t count = list ? int64_t(*a.hit_count) : a.total_rays;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  unsigned long long taps = 0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride) {
+    const int64_t it = list ? int64_t(a.hit_list[i]) : i;
+    const int vi = kBatched ? find_view(a.views, a.nviews, it) : 0;
+    const DevView& v = kBatched ? a.views[vi] : single;
+    const int64_t local = it - v.ray_offset;
+    const double t = a.t_hit[v.out_offset + local];
+    if (t < 0.0) continue;  // a miss (all-rays mode); the march wrote its outputs
+    if (list) taps += shade_at_hit<Set, T, kDir64>(v, local, t, a.out);
+    if (do_trap) trap_at_hit<Set, T, kDir64>(v, local, t, a.out);
   }
-  trap_at_hit<Set, T, kDir64>(v, local, t, a.out);
+  if (list) {
+    for (int o = 16; o > 0; o >>= 1) taps += __shfl_xor_sync(0xffffffffu, taps, o);
+    if ((threadIdx.x & 31) == 0 && taps) {
+      atomicAdd(&a.stats->normal_evals, taps);
+      atomicAdd(&a.stats->de_evals, taps);
+    }
+  }
 }
 
 // --------------------------------------------------------------- launchers
@@ -236,12 +261,20 @@ cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const 
 typedef cudaError_t (*LaunchFn)(const LaunchArgs&, const DevView&, const LaunchConfig&, cudaStream_t);
 
 template <class Set, class T, bool kDir64, bool kBatched>
-cudaError_t launch_trap(const LaunchArgs& a, const DevView& single, const LaunchConfig&, cudaStream_t s) {
-  const int64_t grid = (a.total_rays + 127) / 128;
+cudaError_t launch_shade(const LaunchArgs& a, const DevView& single, const LaunchConfig& c, int do_trap,
+                         cudaStream_t s) {
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shade_kernel<Set, T, kDir64, kBatched>, 128, 0);
+  if (e != cudaSuccess) return e;
+  int64_t grid = int64_t(std::max(per_sm, 1)) * c.num_sms;
+  const int64_t needed = (a.total_rays + 127) / 128;
+  if (grid > needed) grid = needed;
   if (grid <= 0) return cudaSuccess;
-  trap_kernel<Set, T, kDir64, kBatched><<<unsigned(grid), 128, 0, s>>>(a, single);
+  shade_kernel<Set, T, kDir64, kBatched><<<unsigned(grid), 128, 0, s>>>(a, single, do_trap);
   return cudaGetLastError();
 }
+
+typedef cudaError_t (*ShadeFn)(const LaunchArgs&, const DevView&, const LaunchConfig&, int, cudaStream_t);
 
 // DE of one formula at n points (the formula wrapper with its orbit trap), for
 // parity tests against fixed point sets.
@@ -276,7 +309,7 @@ struct KernelTable {
   LaunchFn plain_f32, plain_f32_dir64, plain_f64;
   LaunchFn persistent_f32, persistent_f32_batched, persistent_f32_dir64, persistent_f32_dir64_batched;
   LaunchFn persistent_f64, persistent_f64_batched;
-  LaunchFn trap_f32, trap_f32_batched, trap_f32_dir64, trap_f32_dir64_batched, trap_f64, trap_f64_batched;
+  ShadeFn shade_f32, shade_f32_batched, shade_f32_dir64, shade_f32_dir64_batched, shade_f64, shade_f64_batched;
   DePointsFn de_points_f32, de_points_f64;
   AdjointFn adjoint_f32, adjoint_f32_batched, adjoint_f64, adjoint_f64_batched;
 };
@@ -292,12 +325,12 @@ template <class Set> KernelTable make_kernel_table() {
   t.persistent_f32_dir64_batched = &launch_persistent<Set, float, true, true>;
   t.persistent_f64 = &launch_persistent<Set, double, true, false>;
   t.persistent_f64_batched = &launch_persistent<Set, double, true, true>;
-  t.trap_f32 = &launch_trap<Set, float, false, false>;
-  t.trap_f32_batched = &launch_trap<Set, float, false, true>;
-  t.trap_f32_dir64 = &launch_trap<Set, float, true, false>;
-  t.trap_f32_dir64_batched = &launch_trap<Set, float, true, true>;
-  t.trap_f64 = &launch_trap<Set, double, true, false>;
-  t.trap_f64_batched = &launch_trap<Set, double, true, true>;
+  t.shade_f32 = &launch_shade<Set, float, false, false>;
+  t.shade_f32_batched = &launch_shade<Set, float, false, true>;
+  t.shade_f32_dir64 = &launch_shade<Set, float, true, false>;
+  t.shade_f32_dir64_batched = &launch_shade<Set, float, true, true>;
+  t.shade_f64 = &launch_shade<Set, double, true, false>;
+  t.shade_f64_batched = &launch_shade<Set, double, true, true>;
   t.de_points_f32 = &launch_de_points<Set, float>;
   t.de_points_f64 = &launch_de_points<Set, double>;
   t.adjoint_f32 = &launch_adjoint<Set, float, false>;

@@ -101,6 +101,10 @@ struct LaunchArgs {
   int32_t refill_threshold;
   int32_t chunk;              // rays a warp takes from the work counter at a time
   int64_t deadline_ns;        // watchdog budget (globaltimer units)
+  // Deferred shading: the persistent march ends a hit ray at its hit and appends it
+  // to hit_list; the shade pass then evaluates the normal taps coherently.
+  int32_t* hit_list;          // launch-local ray indices of hits (nullptr: shading inline)
+  unsigned int* hit_count;    // entries in hit_list (zeroed before launch)
 };
 
 // --------------------------------------------------------------- orbit trap
@@ -354,6 +358,10 @@ ND_DEV_INLINE void write_result(const nd_gbuffer& g, double* t_hit, int64_t r, c
   if (g.shadow) g.shadow[r] = o.shadow;
   if (g.depth64) g.depth64[r] = o.hit ? o.t : 0.0;
   if (g.evals) g.evals[r] = o.evals;
+  if (!o.hit) {
+    if (g.trap) g.trap[r] = 0.0f;
+    if (g.iters) g.iters[r] = 0u;
+  }
 }
 
 // Lambert grey level with the camera-mounted key light of simple_geometry, or the
@@ -363,14 +371,16 @@ ND_DEV_INLINE float lambert(const DevView& v, D3 dir, double nx, double ny, doub
   if (v.use_light) {
     kx = v.light[0]; ky = v.light[1]; kz = v.light[2];
   } else {
-    kx = -dir.x + v.uup[0] * 0.45 - v.uright[0] * 0.35;
-    ky = -dir.y + v.uup[1] * 0.45 - v.uright[1] * 0.35;
-    kz = -dir.z + v.uup[2] * 0.45 - v.uright[2] * 0.35;
-    const double inv = 1.0 / sqrt(kx * kx + ky * ky + kz * kz);
+    kx = rn_add(rn_add(-dir.x, rn_mul(v.uup[0], 0.45)), -rn_mul(v.uright[0], 0.35));
+    ky = rn_add(rn_add(-dir.y, rn_mul(v.uup[1], 0.45)), -rn_mul(v.uright[1], 0.35));
+    kz = rn_add(rn_add(-dir.z, rn_mul(v.uup[2], 0.45)), -rn_mul(v.uright[2], 0.35));
+    const double inv = 1.0 / sqrt(rn_add(rn_add(rn_mul(kx, kx), rn_mul(ky, ky)), rn_mul(kz, kz)));
     kx *= inv; ky *= inv; kz *= inv;
   }
-  const double lam = fmax(nx * kx + ny * ky + nz * kz, 0.0) * double(vis);
-  return float(kSimpleAmbient + (1.0 - kSimpleAmbient) * lam);
+  // explicitly rounded (no FMA contraction), so that every kernel gives the same bits
+  const double dot = rn_add(rn_add(rn_mul(nx, kx), rn_mul(ny, ky)), rn_mul(nz, kz));
+  const double lam = rn_mul(fmax(dot, 0.0), double(vis));
+  return float(rn_add(kSimpleAmbient, rn_mul(1.0 - kSimpleAmbient, lam)));
 }
 
 ND_DEV_INLINE int find_view(const DevView* views, int nviews, int64_t item) {
@@ -382,6 +392,48 @@ ND_DEV_INLINE int find_view(const DevView* views, int nviews, int64_t item) {
   }
   return lo;
 }
+
+// --------------------------------------------------------------- normals
+// estimate_normal (tpl:1783-1804) and the 6-tap central difference, one tap at a
+// time: the position of tap k around the hit p, the accumulation of its DE value,
+// and the unit normal.  The inline (Lane) and the deferred (shade pass) paths both
+// use these, so they produce the same bits.
+template <class T> ND_DEV_INLINE D3 normal_tap_pos(const DevView& v, D3 p, double t, int k) {
+  if (v.normal_mode == ND_NORMAL_CENTRAL) {
+    const double h = v.normal_h_coef > 0.0f ? double(v.normal_h_coef) * t : march_eps<T>(v, t);
+    const double s = (k & 1) ? -h : h;
+    const int ax = k >> 1;
+    return d3(p.x + (ax == 0 ? s : 0.0), p.y + (ax == 1 ? s : 0.0), p.z + (ax == 2 ? s : 0.0));
+  }
+  return fmadd(p, tetra_k(k), march_eps<T>(v, t));
+}
+
+ND_DEV_INLINE void normal_accumulate(const DevView& v, int k, double d, float& gx, float& gy, float& gz) {
+  if (v.normal_mode == ND_NORMAL_CENTRAL) {
+    const float s = float((k & 1) ? -d : d);
+    const int ax = k >> 1;
+    if (ax == 0) gx += s;
+    else if (ax == 1) gy += s;
+    else gz += s;
+  } else {
+    const D3 kk = tetra_k(k);
+    gx += float(kk.x * d);
+    gy += float(kk.y * d);
+    gz += float(kk.z * d);
+  }
+}
+
+ND_DEV_INLINE void normal_finish(float& gx, float& gy, float& gz) {
+  // explicitly rounded, so that every kernel that inlines this rounds the same way
+  const float l = sqrtf(rn_add(rn_add(rn_mul(gx, gx), rn_mul(gy, gy)), rn_mul(gz, gz)));
+  const float inv = l > 0.0f ? 1.0f / l : 0.0f;
+  gx *= inv;
+  gy *= inv;
+  gz *= inv;
+}
+
+// Normal taps of a view (4 tetrahedral or 6 central-difference evaluations).
+ND_DEV_INLINE uint32_t normal_taps(const DevView& v) { return v.normal_mode == ND_NORMAL_CENTRAL ? 6u : 4u; }
 
 // --------------------------------------------------------------- the ray program
 enum Phase : int { PH_MARCH = 0, PH_NORMAL = 1, PH_SHADOW = 2, PH_DONE = 3 };
@@ -423,15 +475,7 @@ template <class T, bool kDir64> struct Lane {
     const D3 d = dir.get();
     if (phase == PH_MARCH) return fmadd(o, d, probing ? t : 0.5 * (a + b));
     const D3 p = fmadd(o, d, t);
-    if (phase == PH_NORMAL) {
-      if (v.normal_mode == ND_NORMAL_CENTRAL) {
-        const double h = v.normal_h_coef > 0.0f ? double(v.normal_h_coef) * t : march_eps<T>(v, t);
-        const double s = (k & 1) ? -h : h;
-        const int ax = k >> 1;
-        return d3(p.x + (ax == 0 ? s : 0.0), p.y + (ax == 1 ? s : 0.0), p.z + (ax == 2 ? s : 0.0));
-      }
-      return fmadd(p, tetra_k(k), march_eps<T>(v, t));
-    }
+    if (phase == PH_NORMAL) return normal_tap_pos<T>(v, p, t, k);
     // PH_SHADOW: origin = hit + n * bias, then along the light direction
     const D3 so = fmadd(p, d3(gx, gy, gz), kShadowBias);
     return fmadd(so, d3(v.light[0], v.light[1], v.light[2]), a);
@@ -462,8 +506,27 @@ template <class T, bool kDir64> struct Lane {
     gx = gy = gz = 0.0f;
   }
 
+  // Deferred shading: a hit ends here with the march's outputs (depth, FP64 t,
+  // steps, evaluations); the shade pass writes normal, shade and shadow.
+  ND_DEV_INLINE void finish_march(const DevView& v, const nd_gbuffer& g, double* t_hit) {
+    const int64_t r = v.out_offset + (int64_t(item) - v.ray_offset);
+    g.depth[r] = float(t);
+    if (t_hit) t_hit[r] = t;
+    if (g.steps) g.steps[r] = uint32_t(i);
+    if (g.depth64) g.depth64[r] = t;
+    if (g.evals) g.evals[r] = evals;
+    phase = PH_DONE;
+  }
+
+  ND_DEV_INLINE void hit_at(const DevView& v, double at, const nd_gbuffer& g, double* t_hit, bool defer) {
+    begin_normal(at);
+    if (defer) finish_march(v, g, t_hit);
+  }
+
   // Consume one DE result; sets phase = PH_DONE (outputs written) when finished.
-  ND_DEV_INLINE void advance(const DevView& v, const DEOut<T>& de, const nd_gbuffer& g, double* t_hit) {
+  // With defer_shade a hit ends the ray (finish_march) instead of entering PH_NORMAL.
+  ND_DEV_INLINE void advance(const DevView& v, const DEOut<T>& de, const nd_gbuffer& g, double* t_hit,
+                             bool defer_shade = false) {
     ++evals;
     const double d = double(de.d);
     if (phase == PH_MARCH) {
@@ -481,7 +544,7 @@ template <class T, bool kDir64> struct Lane {
           a = st;
         }
         ++k;
-        if ((b - a <= e && !v.exact_hit) || k >= bisect_budget) begin_normal(b);
+        if ((b - a <= e && !v.exact_hit) || k >= bisect_budget) hit_at(v, b, g, t_hit, defer_shade);
         else if (n >= v.max_samples) finish(v, g, t_hit, 1.0f);  // march_to's loop ran out: a miss
         return;
       }
@@ -494,7 +557,7 @@ template <class T, bool kDir64> struct Lane {
           if (n >= v.max_samples) finish(v, g, t_hit, 1.0f);
           return;
         }
-        begin_normal(st);
+        hit_at(v, st, g, t_hit, defer_shade);
         return;
       }
       if (probing && on_hit) {
@@ -533,25 +596,10 @@ template <class T, bool kDir64> struct Lane {
       return;
     }
     if (phase == PH_NORMAL) {
-      if (v.normal_mode == ND_NORMAL_CENTRAL) {
-        const float s = float((k & 1) ? -d : d);
-        const int ax = k >> 1;
-        if (ax == 0) gx += s;
-        else if (ax == 1) gy += s;
-        else gz += s;
-      } else {
-        const D3 kk = tetra_k(k);
-        gx += float(kk.x * d);
-        gy += float(kk.y * d);
-        gz += float(kk.z * d);
-      }
+      normal_accumulate(v, k, d, gx, gy, gz);
       ++k;
-      if (k < (v.normal_mode == ND_NORMAL_CENTRAL ? 6 : 4)) return;
-      const float l = sqrtf(gx * gx + gy * gy + gz * gz);
-      const float inv = l > 0.0f ? 1.0f / l : 0.0f;
-      gx *= inv;
-      gy *= inv;
-      gz *= inv;
+      if (k < int(normal_taps(v))) return;
+      normal_finish(gx, gy, gz);
       const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
       if (!v.shadow || steps <= 0 || kShadowBias >= 2.0 * v.max_dist) {
         finish(v, g, t_hit, 1.0f);
@@ -576,9 +624,6 @@ template <class T, bool kDir64> struct Lane {
   }
 };
 
-// Normal taps of a view (4 tetrahedral or 6 central-difference evaluations).
-ND_DEV_INLINE uint32_t normal_taps(const DevView& v) { return v.normal_mode == ND_NORMAL_CENTRAL ? 6u : 4u; }
-
 }  // namespace nd
 
 namespace nd {
@@ -594,6 +639,35 @@ ND_DEV_INLINE void trap_at_hit(const DevView& v, int64_t local, double t, const 
   const int64_t r = v.out_offset + local;
   if (g.trap) g.trap[r] = float(de.trap);
   if (g.iters) g.iters[r] = uint32_t(de.iters);
+}
+
+// The deferred part of a hit ray: its normal taps at org + dir * t (the same
+// positions, evaluation order and float accumulation as the inline PH_NORMAL phase)
+// and the Lambert level without a shadow ray.  Adds the taps to the ray's
+// evaluation count; returns them.
+template <class Set, class T, bool kDir64>
+ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, const nd_gbuffer& g) {
+  Dir<kDir64> dir;
+  dir.set(ray_dir(v, local));
+  const D3 p = fmadd(d3(v.org[0], v.org[1], v.org[2]), dir.get(), t);
+  const int taps = int(normal_taps(v));
+  float gx = 0.0f, gy = 0.0f, gz = 0.0f;
+  for (int k = 0; k < taps; ++k) {
+    const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(normal_tap_pos<T>(v, p, t, k)), v);
+    normal_accumulate(v, k, double(de.d), gx, gy, gz);
+  }
+  normal_finish(gx, gy, gz);
+  const int64_t r = v.out_offset + local;
+  if (g.normal) {
+    struct alignas(16) F4 {
+      float x, y, z, w;
+    };
+    reinterpret_cast<F4*>(g.normal)[r] = F4{gx, gy, gz, 1.0f};
+  }
+  if (g.shade) g.shade[r] = lambert(v, dir.get(), gx, gy, gz, 1.0f);
+  if (g.shadow) g.shadow[r] = 1.0f;
+  if (g.evals) g.evals[r] += uint32_t(taps);
+  return uint32_t(taps);
 }
 
 }  // namespace nd

@@ -67,7 +67,8 @@ struct nd_ctx {
   unsigned long long* d_counters = nullptr;
   int counters_cap = 0;
   Stats* d_stats = nullptr;
-  double* d_thit = nullptr;    // FP64 hit distances for the trap pass
+  double* d_thit = nullptr;    // FP64 hit distances for the shade pass
+  int32_t* d_hits = nullptr;   // hit list of the deferred shade pass
   int64_t thit_cap = 0;
   bool last_trap = false;
   DevView* h_views = nullptr;  // pinned staging
@@ -86,6 +87,7 @@ struct nd_graph {
   DevView* d_views = nullptr;
   unsigned long long* d_counters = nullptr;
   double* d_thit = nullptr;
+  int32_t* d_hits = nullptr;
   bool trap = false;
 };
 
@@ -245,13 +247,14 @@ Tuned tuned_for(const std::string& key) {
 }
 
 // Enqueue every launch of a forward call.  d_views / d_counters are device
-// buffers with room for nviews views and plans.size() counters; h_views is host
+// buffers with room for nviews views and 2 * plans.size() counters (work counters,
+// then hit counters); d_thit / d_hits hold one entry per ray; h_views is host
 // staging (pinned when owned by the context).  When views_ready is true the view
 // table is already on the device (graph replay).
 nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_march_opts* opts,
                   const nd_gbuffer* out, cudaStream_t stream, const std::vector<Launch>& plans, DevView* d_views,
-                  DevView* h_views, unsigned long long* d_counters, double* d_thit, bool copy_views,
-                  int* kernel_used) {
+                  DevView* h_views, unsigned long long* d_counters, double* d_thit, int32_t* d_hits,
+                  bool copy_views, int* kernel_used) {
   const int prec = (opts && opts->de_precision == 64) ? 64 : 32;
   // global output offsets in call order
   std::vector<int64_t> out_off(nviews + 1, 0);
@@ -273,10 +276,12 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
   }
   cudaError_t e = cudaMemsetAsync(ctx->d_stats, 0, sizeof(Stats), stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "clear stats");
-  e = cudaMemsetAsync(d_counters, 0, sizeof(unsigned long long) * plans.size(), stream);
+  e = cudaMemsetAsync(d_counters, 0, sizeof(unsigned long long) * 2 * plans.size(), stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "clear work counters");
   base = 0;
   int used = 0;
+  int64_t ray_base = 0;  // where this plan's rays start in d_hits
+  const bool want_trap = out->trap || out->iters;
   for (size_t p = 0; p < plans.size(); ++p) {
     const Launch& L = plans[p];
     const int nv = int(L.views.size());
@@ -303,8 +308,14 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       c.block = 128;
       c.blocks_per_sm = opts && opts->blocks_per_sm ? opts->blocks_per_sm : tu.blocks_per_sm;
       c.num_sms = ctx->num_sms;
-      bool dir64 = false;
-      for (int k = 0; k < nv; ++k) dir64 |= h_views[base + k].dir64 != 0;
+      bool dir64 = false, shadow = false;
+      for (int k = 0; k < nv; ++k) {
+        dir64 |= h_views[base + k].dir64 != 0;
+        shadow |= h_views[base + k].shadow != 0;
+      }
+      // the persistent march defers the normal taps to the shade pass unless a
+      // shadow ray (which starts from the normal) has to follow the hit
+      const bool defer = kernel != ND_KERNEL_PLAIN && !shadow && d_hits != nullptr && d_thit != nullptr;
       if (kernel == ND_KERNEL_PLAIN) {
         // the plain baseline: one launch per view, one thread per ray
         for (int k = 0; k < nv; ++k) {
@@ -315,22 +326,27 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       } else {
         const bool batched = nv > 1;
         LaunchFn fn = pick(L.table, kernel, prec, batched, dir64);
+        if (defer) {
+          a.hit_list = d_hits + ray_base;
+          a.hit_count = reinterpret_cast<unsigned int*>(d_counters + plans.size() + p);
+        }
         e = fn(a, h_views[base], c, stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
       }
-      if (out->trap || out->iters) {
-        // orbit trap and iteration count at every hit point
+      if (defer || want_trap) {
+        // normals of the deferred hits and/or the orbit trap at every hit point
         const bool batched = nv > 1;
         const nd::KernelTable& T = L.table;
-        LaunchFn tf = prec == 64 ? (batched ? T.trap_f64_batched : T.trap_f64)
-                                 : dir64 ? (batched ? T.trap_f32_dir64_batched : T.trap_f32_dir64)
-                                         : (batched ? T.trap_f32_batched : T.trap_f32);
-        e = tf(a, h_views[base], c, stream);
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "trap pass launch");
+        nd::ShadeFn sf = prec == 64 ? (batched ? T.shade_f64_batched : T.shade_f64)
+                                    : dir64 ? (batched ? T.shade_f32_dir64_batched : T.shade_f32_dir64)
+                                            : (batched ? T.shade_f32_batched : T.shade_f32);
+        e = sf(a, h_views[base], c, want_trap ? 1 : 0, stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "shade pass launch");
       }
       used = kernel;
     }
     base += nv;
+    ray_base += rays;
   }
   if (kernel_used) *kernel_used = used;
   return ND_OK;
@@ -504,6 +520,7 @@ nd_status nd_ctx_destroy(nd_ctx* ctx) {
   if (ctx->d_counters) cudaFree(ctx->d_counters);
   if (ctx->d_stats) cudaFree(ctx->d_stats);
   if (ctx->d_thit) cudaFree(ctx->d_thit);
+  if (ctx->d_hits) cudaFree(ctx->d_hits);
   if (ctx->h_views) cudaFreeHost(ctx->h_views);
   if (ctx->last_done) cudaEventDestroy(ctx->last_done);
   delete ctx;
@@ -541,14 +558,18 @@ nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
   // the staging buffer may still feed an earlier copy: wait for the last call
   if (ctx->have_last) cudaEventSynchronize(ctx->last_done);
   if ((s = ensure_dev(ctx, &ctx->d_views, &ctx->views_cap, nviews, "view table")) != ND_OK) return s;
-  if ((s = ensure_dev(ctx, &ctx->d_counters, &ctx->counters_cap, int(plans.size()), "work counters")) != ND_OK) return s;
+  if ((s = ensure_dev(ctx, &ctx->d_counters, &ctx->counters_cap, 2 * int(plans.size()), "work counters")) != ND_OK)
+    return s;
   const bool want_trap = out->trap || out->iters;
-  if (want_trap && ctx->thit_cap < total) {
+  if (ctx->thit_cap < total) {
     if (ctx->d_thit) cudaFree(ctx->d_thit);
+    if (ctx->d_hits) cudaFree(ctx->d_hits);
     ctx->d_thit = nullptr;
+    ctx->d_hits = nullptr;
     ctx->thit_cap = 0;
     e = cudaMalloc((void**)&ctx->d_thit, sizeof(double) * size_t(total));
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "hit-distance buffer");
+    if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_hits, sizeof(int32_t) * size_t(total));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "hit buffers");
     ctx->thit_cap = total;
   }
   if (ctx->h_views_cap < nviews) {
@@ -560,8 +581,8 @@ nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
     ctx->h_views_cap = std::max(nviews, 64);
   }
   int kernel = 0;
-  s = enqueue(ctx, views, nviews, opts, out, st, plans, ctx->d_views, ctx->h_views, ctx->d_counters,
-              want_trap ? ctx->d_thit : nullptr, true, &kernel);
+  s = enqueue(ctx, views, nviews, opts, out, st, plans, ctx->d_views, ctx->h_views, ctx->d_counters, ctx->d_thit,
+              ctx->d_hits, true, &kernel);
   if (s != ND_OK) return s;
   e = cudaEventRecord(ctx->last_done, st);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "record event");
@@ -686,8 +707,9 @@ nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
   g->ctx = ctx;
   g->trap = out->trap || out->iters;
   cudaError_t e = cudaMalloc((void**)&g->d_views, sizeof(DevView) * size_t(nviews));
-  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_counters, sizeof(unsigned long long) * plans.size());
-  if (e == cudaSuccess && g->trap) e = cudaMalloc((void**)&g->d_thit, sizeof(double) * size_t(std::max<int64_t>(total, 1)));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_counters, sizeof(unsigned long long) * 2 * plans.size());
+  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_thit, sizeof(double) * size_t(std::max<int64_t>(total, 1)));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_hits, sizeof(int32_t) * size_t(std::max<int64_t>(total, 1)));
   if (e != cudaSuccess) {
     nd_graph_destroy(g);
     return cuda_fail(ctx, e, "graph buffers");
@@ -707,8 +729,8 @@ nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
     nd_graph_destroy(g);
     return cuda_fail(ctx, e, "begin capture");
   }
-  s = enqueue(ctx, views, nviews, opts, out, cap, plans, g->d_views, hv.data(), g->d_counters, g->d_thit, false,
-              nullptr);
+  s = enqueue(ctx, views, nviews, opts, out, cap, plans, g->d_views, hv.data(), g->d_counters, g->d_thit,
+              g->d_hits, false, nullptr);
   cudaGraph_t gr = nullptr;
   e = cudaStreamEndCapture(cap, &gr);
   cudaStreamDestroy(cap);
@@ -749,6 +771,7 @@ nd_status nd_graph_destroy(nd_graph* g) {
   if (g->d_views) cudaFree(g->d_views);
   if (g->d_counters) cudaFree(g->d_counters);
   if (g->d_thit) cudaFree(g->d_thit);
+  if (g->d_hits) cudaFree(g->d_hits);
   delete g;
   return ND_OK;
 }
