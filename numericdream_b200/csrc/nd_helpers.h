@@ -21,26 +21,23 @@ template <class T> ND_HD_INLINE v3<T> box_fold(v3<T> z, T limit) {
 
 // template.wgsl:953-971: sphere inversion with a floor; radii are squared.
 template <class T> ND_HD_INLINE v4<T> sphere_fold(v3<T> z, T dr, T min_radius2, T fixed_radius2) {
+  // one scale factor instead of three branches (lanes of a warp fall in different
+  // shells); outside both radii the factor is 1, and z * 1 == z exactly
   const T r2 = dot(z, z);
-  if (r2 < min_radius2) {
-    const T t = fixed_radius2 / min_radius2;
-    return v4<T>(z * t, dr * t);
-  } else if (r2 < fixed_radius2) {
-    const T t = fixed_radius2 / r2;
-    return v4<T>(z * t, dr * t);
-  }
-  return v4<T>(z, dr);
+  const T q = fixed_radius2 / r2;
+  const T t = r2 < min_radius2 ? fixed_radius2 / min_radius2 : (r2 < fixed_radius2 ? q : T(1));
+  return v4<T>(z * t, dr * t);
 }
 
 // template.wgsl:973-985: inversion in the sphere |d|^2 < radius2 around center.
 template <class T> ND_HD_INLINE v4<T> sphere_invert_offset(v3<T> z, T dr, v3<T> center, T radius2) {
+  // both results computed and selected, so that a warp does not split on the test
   const v3<T> d = z - center;
   const T r2 = max(dot(d, d), k_epsilon_fine<T>());
-  if (r2 < radius2) {
-    const T t = radius2 / r2;
-    return v4<T>(center + d * t, dr * t);
-  }
-  return v4<T>(z, dr);
+  const T t = radius2 / r2;
+  const bool in = r2 < radius2;
+  const v3<T> zi = center + d * t;
+  return v4<T>(in ? zi.x : z.x, in ? zi.y : z.y, in ? zi.z : z.z, in ? dr * t : dr);
 }
 
 // template.wgsl:987-991: wrap into the cube of side `cell` centred at the origin.

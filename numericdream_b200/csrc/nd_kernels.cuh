@@ -41,10 +41,11 @@ __device__ __forceinline__ void flush_stats(Stats* s, unsigned long long rays, u
   }
 }
 
-// Residency the kernels are compiled for: 8 blocks of 128 threads per SM with an
-// FP32 DE (at most 64 registers per thread), 4 with an FP64 DE.
+// Residency the kernels are compiled for: 7 blocks of 128 threads per SM with an
+// FP32 DE (at most 72 registers per thread; measured 4 % faster than 8 x 64 on the
+// batched benchmark, where 64 registers spill the ray state), 4 with an FP64 DE.
 template <class T> struct MinBlocks {
-  static constexpr int value = sizeof(T) == 4 ? 8 : 4;
+  static constexpr int value = sizeof(T) == 4 ? 7 : 4;
 };
 
 // --------------------------------------------------------------- plain kernel
@@ -188,17 +189,17 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
 
 // --------------------------------------------------------------- shade pass
 // Work at the hit points, after the march: with a hit list (deferred shading) the
-// normal taps, Lambert level and, when asked, the orbit trap of every listed hit;
-// without one (inline shading, or the plain kernel) the orbit trap of every ray
-// that hit.  Every hit costs the same number of evaluations, so the pass is
-// coherent and needs no refill; it strides over its work with a resident grid.
+// normal taps, the shadow ray, the Lambert level and, when asked, the orbit trap of
+// every listed hit (the shadow rays' step counts differ, the rest is coherent);
+// without one (the plain kernel) the orbit trap of every ray that hit.  It strides
+// over its work with a resident grid.
 template <class Set, class T, bool kDir64, bool kBatched>
 __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     shade_kernel(const __grid_constant__ LaunchArgs a, const __grid_constant__ DevView single, int do_trap) {
   const bool list = a.hit_list != nullptr;
   const int64_t count = list ? int64_t(*a.hit_count) : a.total_rays;
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-  unsigned long long taps = 0;
+  unsigned long long taps = 0, shadow = 0;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride) {
     const int64_t it = list ? int64_t(a.hit_list[i]) : i;
     const int vi = kBatched ? find_view(a.views, a.nviews, it) : 0;
@@ -206,14 +207,22 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     const int64_t local = it - v.ray_offset;
     const double t = a.t_hit[v.out_offset + local];
     if (t < 0.0) continue;  // a miss (all-rays mode); the march wrote its outputs
-    if (list) taps += shade_at_hit<Set, T, kDir64>(v, local, t, a.out);
+    if (list) {
+      const uint32_t ev = shade_at_hit<Set, T, kDir64>(v, local, t, a.out);
+      taps += ev & 0xffffu;
+      shadow += ev >> 16;
+    }
     if (do_trap) trap_at_hit<Set, T, kDir64>(v, local, t, a.out);
   }
   if (list) {
-    for (int o = 16; o > 0; o >>= 1) taps += __shfl_xor_sync(0xffffffffu, taps, o);
-    if ((threadIdx.x & 31) == 0 && taps) {
+    for (int o = 16; o > 0; o >>= 1) {
+      taps += __shfl_xor_sync(0xffffffffu, taps, o);
+      shadow += __shfl_xor_sync(0xffffffffu, shadow, o);
+    }
+    if ((threadIdx.x & 31) == 0 && taps + shadow) {
       atomicAdd(&a.stats->normal_evals, taps);
-      atomicAdd(&a.stats->de_evals, taps);
+      atomicAdd(&a.stats->shadow_evals, shadow);
+      atomicAdd(&a.stats->de_evals, taps + shadow);
     }
   }
 }

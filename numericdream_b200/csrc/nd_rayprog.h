@@ -642,9 +642,10 @@ ND_DEV_INLINE void trap_at_hit(const DevView& v, int64_t local, double t, const 
 }
 
 // The deferred part of a hit ray: its normal taps at org + dir * t (the same
-// positions, evaluation order and float accumulation as the inline PH_NORMAL phase)
-// and the Lambert level without a shadow ray.  Adds the taps to the ray's
-// evaluation count; returns them.
+// positions, evaluation order and float accumulation as the inline PH_NORMAL
+// phase), the shadow ray when the view has one (the steps of PH_SHADOW), and the
+// Lambert level.  Adds the evaluations to the ray's count; returns the taps in
+// the low and the shadow steps in the high 16 bits.
 template <class Set, class T, bool kDir64>
 ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, const nd_gbuffer& g) {
   Dir<kDir64> dir;
@@ -657,6 +658,31 @@ ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, c
     normal_accumulate(v, k, double(de.d), gx, gy, gz);
   }
   normal_finish(gx, gy, gz);
+  // visibility_march (tpl:2294-2341) toward the light, opaque scene
+  float vis = 1.0f;
+  int k = 0;
+  const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
+  if (v.shadow && steps > 0 && kShadowBias < 2.0 * v.max_dist) {
+    const D3 so = fmadd(p, d3(gx, gy, gz), kShadowBias);
+    const D3 L = d3(v.light[0], v.light[1], v.light[2]);
+    double a = kShadowBias, res = 1.0;
+    while (true) {
+      const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(fmadd(so, L, a)), v);
+      const double d = double(de.d);
+      if (d < kShadowHitEps) {
+        vis = 0.0f;
+        ++k;
+        break;
+      }
+      res = fmin(res, double(v.shadow_k) * d / a);
+      a += fmax(d, kShadowMinStep);
+      ++k;
+      if (k >= steps || a >= 2.0 * v.max_dist) {
+        vis = float(fmin(fmax(res, 0.0), 1.0));
+        break;
+      }
+    }
+  }
   const int64_t r = v.out_offset + local;
   if (g.normal) {
     struct alignas(16) F4 {
@@ -664,10 +690,10 @@ ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, c
     };
     reinterpret_cast<F4*>(g.normal)[r] = F4{gx, gy, gz, 1.0f};
   }
-  if (g.shade) g.shade[r] = lambert(v, dir.get(), gx, gy, gz, 1.0f);
-  if (g.shadow) g.shadow[r] = 1.0f;
-  if (g.evals) g.evals[r] += uint32_t(taps);
-  return uint32_t(taps);
+  if (g.shade) g.shade[r] = lambert(v, dir.get(), gx, gy, gz, vis);
+  if (g.shadow) g.shadow[r] = vis;
+  if (g.evals) g.evals[r] += uint32_t(taps + k);
+  return uint32_t(taps) | (uint32_t(k) << 16);
 }
 
 }  // namespace nd

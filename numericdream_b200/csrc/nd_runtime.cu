@@ -308,14 +308,11 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       c.block = 128;
       c.blocks_per_sm = opts && opts->blocks_per_sm ? opts->blocks_per_sm : tu.blocks_per_sm;
       c.num_sms = ctx->num_sms;
-      bool dir64 = false, shadow = false;
-      for (int k = 0; k < nv; ++k) {
-        dir64 |= h_views[base + k].dir64 != 0;
-        shadow |= h_views[base + k].shadow != 0;
-      }
-      // the persistent march defers the normal taps to the shade pass unless a
-      // shadow ray (which starts from the normal) has to follow the hit
-      const bool defer = kernel != ND_KERNEL_PLAIN && !shadow && d_hits != nullptr && d_thit != nullptr;
+      bool dir64 = false;
+      for (int k = 0; k < nv; ++k) dir64 |= h_views[base + k].dir64 != 0;
+      // the persistent march leaves the normal taps and shadow rays of its hits to
+      // the shade pass
+      const bool defer = kernel != ND_KERNEL_PLAIN && d_hits != nullptr && d_thit != nullptr;
       if (kernel == ND_KERNEL_PLAIN) {
         // the plain baseline: one launch per view, one thread per ray
         for (int k = 0; k < nv; ++k) {
