@@ -37,10 +37,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # The FP32 DE is compiled with the GPU's fast division, square root and
 # transcendental approximations (--use_fast_math), which are within WGSL's own f32
 # accuracy requirements (e.g. 2.5 ulp division, 2^-11 absolute sin/cos on
-# [-pi, pi]); ND_ACCURATE_MATH=1 builds CUDA's correctly rounded / few-ulp
-# versions instead.  FP64 DEs and the FP64 march bookkeeping are unaffected, and
+# [-pi, pi]), and with the polynomial acos / atan2 of nd_wgsl.h; ND_ACCURATE_MATH=1
+# builds CUDA's correctly rounded / few-ulp versions instead.  FP64 DEs and the FP64 march bookkeeping are unaffected, and
 # eps(t) uses explicitly rounded operations either way.
-MATHFLAGS = [] if os.environ.get("ND_ACCURATE_MATH") == "1" else ["--use_fast_math"]
+MATHFLAGS = ["-DND_ACCURATE_MATH"] if os.environ.get("ND_ACCURATE_MATH") == "1" else ["--use_fast_math"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v", "--expt-relaxed-constexpr",
            "-I", CSRC, "-I", INCLUDE, "-I", GEN] + MATHFLAGS + os.environ.get("ND_NVCC_EXTRA", "").split()
 

@@ -27,6 +27,61 @@
 
 namespace ndw {
 
+// ---------------------------------------------------------------- polynomial acos / atan2
+// f32 arccosine and two-argument arctangent as short polynomials, for the fast-math
+// device build (acosf / atan2f are long range-reduced routines).  The coefficients
+// were fitted for this library (least squares on 4000 Chebyshev nodes refined by
+// Lawson's iteration toward the minimax fit):
+//   acos(a) = sqrt(1 - a) * P(a) on [0, 1], P of degree 7, |error| <= 2.2e-8;
+//   atan(a) = a * Q(a^2) on [0, 1], Q of degree 8, |error| <= 1.4e-8;
+// the other octants by acos(-x) = pi - acos(x), atan(1/a) = pi/2 - atan(a),
+// atan2(y, -x) = pi - atan2(y, x) and the sign of y.  Rounded in f32 they stay within
+// a few ulp (tests/test_wgsl_math.py), far inside WGSL's accuracy rules for acos and
+// atan2.  NaN arguments give NaN; atan2 of two infinities gives the octant angle.
+ND_HD_INLINE float nd_acos_poly(float x) {
+  const float a = fabsf(x);
+  float p = -0.0012628166408258335f;
+  p = fmaf(p, a, 0.006671243789107799f);
+  p = fmaf(p, a, -0.017089743594000825f);
+  p = fmaf(p, a, 0.030893008030167084f);
+  p = fmaf(p, a, -0.0501746996877574f);
+  p = fmaf(p, a, 0.08897904736598193f);
+  p = fmaf(p, a, -0.21459880368099798f);
+  p = fmaf(p, a, 1.5707963049937743f);
+  const float r = sqrtf(1.0f - a) * p;
+  // pi - r with pi split into an f32 head and tail
+  return x < 0.0f ? (3.14159274f - r) + -8.74227766e-8f : r;
+}
+
+ND_HD_INLINE float nd_atan2_poly(float y, float x) {
+  if (x != x || y != y) return x + y;
+  const float ax = fabsf(x), ay = fabsf(y);
+  const float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
+  const float a = mx == mn ? (mx > 0.0f ? 1.0f : 0.0f) : mn / mx;
+  const float s = a * a;
+  float q = 0.0029035175208155816f;
+  q = fmaf(q, s, -0.016282869281752363f);
+  q = fmaf(q, s, 0.04303914484614859f);
+  q = fmaf(q, s, -0.07533657424332961f);
+  q = fmaf(q, s, 0.10654668786402743f);
+  q = fmaf(q, s, -0.14207131502731904f);
+  q = fmaf(q, s, 0.19993053843505385f);
+  q = fmaf(q, s, -0.33333093945014514f);
+  q = fmaf(q, s, 0.9999999863658048f);
+  float r = a * q;
+  if (ay > ax) r = (1.57079637f - r) + -4.37113883e-8f;
+  if (copysignf(1.0f, x) < 0.0f) r = (3.14159274f - r) + -8.74227766e-8f;  // x < 0 or x = -0
+  return copysignf(r, y);
+}
+
+#if defined(__CUDA_ARCH__) && !defined(ND_ACCURATE_MATH)
+#define ND_ACOS_F(x) nd_acos_poly(x)
+#define ND_ATAN2_F(y, x) nd_atan2_poly(y, x)
+#else
+#define ND_ACOS_F(x) acosf(x)
+#define ND_ATAN2_F(y, x) atan2f(y, x)
+#endif
+
 // ---------------------------------------------------------------- scalars
 #define ND_UNARY_F(NAME, FEXPR, DEXPR)                    \
   ND_HD_INLINE float NAME(float x) { return FEXPR; }      \
@@ -36,7 +91,7 @@ ND_UNARY_F(sin, sinf(x), ::sin(x))
 ND_UNARY_F(cos, cosf(x), ::cos(x))
 ND_UNARY_F(tan, tanf(x), ::tan(x))
 ND_UNARY_F(asin, asinf(x), ::asin(x))
-ND_UNARY_F(acos, acosf(x), ::acos(x))
+ND_UNARY_F(acos, ND_ACOS_F(x), ::acos(x))
 ND_UNARY_F(atan, atanf(x), ::atan(x))
 ND_UNARY_F(sinh, sinhf(x), ::sinh(x))
 ND_UNARY_F(cosh, coshf(x), ::cosh(x))
@@ -80,7 +135,7 @@ ND_HD_INLINE uint32_t max(uint32_t a, uint32_t b) { return a > b ? a : b; }
 
 ND_HD_INLINE float pow(float x, float y) { return x < 0.0f ? __builtin_nanf("") : powf(x, y); }
 ND_HD_INLINE double pow(double x, double y) { return x < 0.0 ? __builtin_nan("") : ::pow(x, y); }
-ND_HD_INLINE float atan2(float y, float x) { return atan2f(y, x); }
+ND_HD_INLINE float atan2(float y, float x) { return ND_ATAN2_F(y, x); }
 ND_HD_INLINE double atan2(double y, double x) { return ::atan2(y, x); }
 template <class T> ND_HD_INLINE T step(T edge, T x) { return x >= edge ? T(1) : T(0); }
 template <class T> ND_HD_INLINE T clamp(T x, T lo, T hi) { return min(max(x, lo), hi); }
