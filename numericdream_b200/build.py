@@ -288,7 +288,11 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
 
 
 OPLIB = os.path.join(PKG, "libnd_opcount.so")
-CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-I", CSRC, "-I", INCLUDE, "-I", GEN]
+# ND_OPCOUNT_BUILD: the helpers take their branchy form, so that the count is of the
+# operations the reference's algorithm performs (the GPU build computes both sides of
+# some tests and selects, which gives the same values with fewer warp splits)
+CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-DND_OPCOUNT_BUILD", "-I", CSRC,
+            "-I", INCLUDE, "-I", GEN]
 
 
 def _compile_host(src, obj, headers):

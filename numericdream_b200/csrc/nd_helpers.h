@@ -21,6 +21,19 @@ template <class T> ND_HD_INLINE v3<T> box_fold(v3<T> z, T limit) {
 
 // template.wgsl:953-971: sphere inversion with a floor; radii are squared.
 template <class T> ND_HD_INLINE v4<T> sphere_fold(v3<T> z, T dr, T min_radius2, T fixed_radius2) {
+#if defined(ND_OPCOUNT_BUILD)
+  {
+    const T r2 = dot(z, z);
+    if (r2 < min_radius2) {
+      const T t = fixed_radius2 / min_radius2;
+      return v4<T>(z * t, dr * t);
+    } else if (r2 < fixed_radius2) {
+      const T t = fixed_radius2 / r2;
+      return v4<T>(z * t, dr * t);
+    }
+    return v4<T>(z, dr);
+  }
+#endif
   // one scale factor instead of three branches (lanes of a warp fall in different
   // shells); outside both radii the factor is 1, and z * 1 == z exactly
   const T r2 = dot(z, z);
@@ -31,6 +44,17 @@ template <class T> ND_HD_INLINE v4<T> sphere_fold(v3<T> z, T dr, T min_radius2, 
 
 // template.wgsl:973-985: inversion in the sphere |d|^2 < radius2 around center.
 template <class T> ND_HD_INLINE v4<T> sphere_invert_offset(v3<T> z, T dr, v3<T> center, T radius2) {
+#if defined(ND_OPCOUNT_BUILD)
+  {
+    const v3<T> d = z - center;
+    const T r2 = max(dot(d, d), k_epsilon_fine<T>());
+    if (r2 < radius2) {
+      const T t = radius2 / r2;
+      return v4<T>(center + d * t, dr * t);
+    }
+    return v4<T>(z, dr);
+  }
+#endif
   // both results computed and selected, so that a warp does not split on the test
   const v3<T> d = z - center;
   const T r2 = max(dot(d, d), k_epsilon_fine<T>());
