@@ -299,10 +299,17 @@ template <> ND_DEV_INLINE double march_eps<double>(const DevView& v, double t) {
 // (ux, uy): the camera-plane coordinates of the ray, direction = fwd + ux right + uy up.
 ND_DEV_INLINE void ray_uv(const DevView& v, int64_t local, double* ux, double* uy) {
   const int64_t npix = int64_t(v.tile_w) * v.tile_h;
-  const int64_t s = local / npix;
-  const int64_t pix = local - s * npix;
-  const int px = v.tile_x + int(pix % v.tile_w);
-  const int py = v.tile_y + int(pix / v.tile_w);
+  int px, py;
+  if (local < 0x80000000ll && npix < 0x80000000ll) {
+    // 32-bit division (a 64-bit one is a long software routine on the GPU)
+    const uint32_t pix = uint32_t(local) % uint32_t(npix);
+    px = v.tile_x + int(pix % uint32_t(v.tile_w));
+    py = v.tile_y + int(pix / uint32_t(v.tile_w));
+  } else {
+    const int64_t pix = local % npix;
+    px = v.tile_x + int(pix % v.tile_w);
+    py = v.tile_y + int(pix / v.tile_w);
+  }
   double jx = 0.5, jy = 0.5;
   if (v.spp > 1) {
     const uint64_t h = splitmix64(v.seed ^ splitmix64(uint64_t(local)));
