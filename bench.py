@@ -242,6 +242,24 @@ def reference_arm(args):
     return 0
 
 
+def profile_forward(args):
+    """One forward of the workload (persistent march + shade pass), nothing timed."""
+    import torch
+
+    from numericdream_b200 import abi, runtime, workloads
+
+    ctx = runtime.Context(0)
+    views = build_views(args.workload, runtime.find_formula)
+    g = runtime.GBuffer.allocate(workloads.rays(views))
+    ctx.forward(views, g, runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, refill_threshold=4))
+    torch.cuda.synchronize()
+    st = ctx.stats()
+    print(json.dumps({"workload": args.workload, "rays": workloads.rays(views), "de_evals": st.de_evals,
+                      "march_evals": st.march_evals, "normal_evals": st.normal_evals, "hits": st.hits}))
+    ctx.close()
+    return 0
+
+
 def small_and_deepzoom(ctx, sptr, timed, steps):
     """The single-view Mandelbulb 256x256 (persistent and plain) and the deep-zoom frame
     (Mandelbox, 30 iterations, 4096x4096 in 16 tiles of 1024x1024, FP64 DE)."""
@@ -311,9 +329,13 @@ def main():
     ap.add_argument("--workload", default="batched_64")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the second (1080p Mandelbox) workload")
+    ap.add_argument("--profile-forward", action="store_true",
+                    help="run ONE forward of the workload through the public API and exit (for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.profile_forward:
+        return profile_forward(args)
 
     import numpy as np
     import torch

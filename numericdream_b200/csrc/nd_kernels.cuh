@@ -105,6 +105,8 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
   L.phase = PH_DONE;
   L.evals = 0;
   L.hit = false;
+  L.lazy = true;
+  L.pending = 0;
   uint32_t rays = 0, hits = 0, ev_m = 0, ev_n = 0, ev_s = 0, refills = 0;
   bool exhausted = false;
   const int64_t deadline = __shfl_sync(full, globaltimer_ns(), 0) + a.deadline_ns;
@@ -113,12 +115,16 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
   int32_t wnext = 0, wend = 0;  // warp-uniform: taken but not yet started rays [wnext, wend)
   const int thr = a.refill_threshold;
   const bool defer = a.hit_list != nullptr;
-  while (true) {
+  // Finished rays keep their lane until the next refill: their outputs are written
+  // then, all together, instead of in the pass that ends each ray.
+  auto retire = [&]() {
     int32_t hit_item = -1;
-    if (L.phase == PH_DONE && L.item >= 0) {
+    if (L.item >= 0 && L.phase == PH_DONE) {
+      const DevView& v = kBatched ? a.views[L.view] : single;
+      L.flush(v, a.out, a.t_hit);
       ++rays;
       hits += L.hit ? 1 : 0;
-      const uint32_t taps = (L.hit && !defer) ? normal_taps(kBatched ? a.views[L.view] : single) : 0u;
+      const uint32_t taps = (L.hit && !defer) ? normal_taps(v) : 0u;
       ev_m += L.mev;
       ev_n += taps;
       ev_s += L.evals - L.mev - taps;
@@ -126,7 +132,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
       L.item = -1;
     }
     if (defer) {
-      // append this pass's finished hits to the shade pass's list, one atomic per warp
+      // append the retired hits to the shade pass's list, one atomic per warp
       const unsigned hm = __ballot_sync(full, hit_item >= 0);
       if (hm) {
         unsigned base = 0;
@@ -135,10 +141,20 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
         if (hit_item >= 0) a.hit_list[base + __popc(hm & lt_mask)] = hit_item;
       }
     }
-    const unsigned idle = __ballot_sync(full, L.item < 0);
-    const int nidle = __popc(idle);
+  };
+  while (true) {
+    const bool done = L.item >= 0 && L.phase == PH_DONE;
+    const unsigned free_lanes = __ballot_sync(full, L.item < 0 || done);
+    const int nfree = __popc(free_lanes);
     const bool have_work = !exhausted || wnext < wend;
-    if (have_work && nidle != 0 && (nidle >= thr || idle == full)) {
+    if (!have_work && free_lanes == full) {
+      retire();
+      break;
+    }
+    if (have_work && nfree != 0 && (nfree >= thr || free_lanes == full)) {
+      retire();
+      const unsigned idle = __ballot_sync(full, L.item < 0);
+      const int nidle = __popc(idle);
       int avail = wend - wnext;
       int32_t base = 0, nnew = 0;
       if (avail < nidle && !exhausted) {
@@ -157,7 +173,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
           const int32_t it = r < avail ? wnext + r : base + (r - avail);
           L.view = kBatched ? find_view(a.views, a.nviews, it) : 0;
           const DevView& v = kBatched ? a.views[L.view] : single;
-          L.start(v, it, L.view);
+          L.start(v, it, L.view, true);
           if (L.phase == PH_DONE) L.finish(v, a.out, a.t_hit, 1.0f);
         }
       }
@@ -169,16 +185,16 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
       }
       continue;  // lanes that finished at once go back through the bookkeeping
     }
-    if (!have_work && idle == full) break;
     if (((++tick) & 63) == 0) {
       // lane 0's clock decides for the whole warp, so the exit stays warp-uniform
       const int64_t now = __shfl_sync(full, globaltimer_ns(), 0);
       if (now > deadline) {
+        retire();
         if (lane == 0) atomicAdd(&a.stats->timeouts, 1u);
         break;
       }
     }
-    if (L.item >= 0) {
+    if (L.item >= 0 && L.phase != PH_DONE) {
       const DevView& v = kBatched ? a.views[L.view] : single;
       const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(L.sample_pos(v)), v);
       L.advance(v, de, a.out, a.t_hit, defer);

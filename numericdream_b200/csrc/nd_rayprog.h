@@ -461,8 +461,13 @@ template <class T, bool kDir64> struct Lane {
   uint32_t evals;
   uint32_t mev;   // evaluations the march used (set when the march ends)
   bool probing, bisecting, resolved, hit;
+  bool lazy;        // outputs wait for flush() (the persistent kernel writes them in batches)
+  uint8_t pending;  // outputs not yet written: 1 finish's, 2 finish_march's
+  float vis;        // shadow visibility of a pending finish
 
-  ND_DEV_INLINE void start(const DevView& v, int32_t it, int32_t vidx) {
+  ND_DEV_INLINE void start(const DevView& v, int32_t it, int32_t vidx, bool lazy_outputs = false) {
+    lazy = lazy_outputs;
+    pending = 0;
     item = it;
     view = vidx;
     dir.set(ray_dir(v, int64_t(it) - v.ray_offset));
@@ -488,8 +493,18 @@ template <class T, bool kDir64> struct Lane {
     return fmadd(so, d3(v.light[0], v.light[1], v.light[2]), a);
   }
 
-  ND_DEV_INLINE void finish(const DevView& v, const nd_gbuffer& g, double* t_hit, float vis) {
+  ND_DEV_INLINE void finish(const DevView& v, const nd_gbuffer& g, double* t_hit, float visibility) {
     if (!hit) mev = evals;
+    phase = PH_DONE;
+    if (lazy) {
+      pending = 1;
+      vis = visibility;
+      return;
+    }
+    write_finish(v, g, t_hit, visibility);
+  }
+
+  ND_DEV_INLINE void write_finish(const DevView& v, const nd_gbuffer& g, double* t_hit, float vis) const {
     RayResult r;
     r.hit = hit;
     r.t = t;
@@ -501,7 +516,13 @@ template <class T, bool kDir64> struct Lane {
     r.shadow = vis;
     r.shade = hit ? lambert(v, dir.get(), gx, gy, gz, vis) : 0.0f;
     write_result(g, t_hit, v.out_offset + (int64_t(item) - v.ray_offset), r);
-    phase = PH_DONE;
+  }
+
+  // Write the outputs a lazy lane left pending.
+  ND_DEV_INLINE void flush(const DevView& v, const nd_gbuffer& g, double* t_hit) {
+    if (pending == 1) write_finish(v, g, t_hit, vis);
+    else if (pending == 2) write_march(v, g, t_hit);
+    pending = 0;
   }
 
   ND_DEV_INLINE void begin_normal(double at) {
@@ -516,13 +537,21 @@ template <class T, bool kDir64> struct Lane {
   // Deferred shading: a hit ends here with the march's outputs (depth, FP64 t,
   // steps, evaluations); the shade pass writes normal, shade and shadow.
   ND_DEV_INLINE void finish_march(const DevView& v, const nd_gbuffer& g, double* t_hit) {
+    phase = PH_DONE;
+    if (lazy) {
+      pending = 2;
+      return;
+    }
+    write_march(v, g, t_hit);
+  }
+
+  ND_DEV_INLINE void write_march(const DevView& v, const nd_gbuffer& g, double* t_hit) const {
     const int64_t r = v.out_offset + (int64_t(item) - v.ray_offset);
     g.depth[r] = float(t);
     if (t_hit) t_hit[r] = t;
     if (g.steps) g.steps[r] = uint32_t(i);
     if (g.depth64) g.depth64[r] = t;
     if (g.evals) g.evals[r] = evals;
-    phase = PH_DONE;
   }
 
   ND_DEV_INLINE void hit_at(const DevView& v, double at, const nd_gbuffer& g, double* t_hit, bool defer) {
