@@ -185,6 +185,9 @@ typedef struct nd_stats {
   uint64_t refills;         /* persistent kernel: warp refills */
   uint32_t timeouts;        /* watchdog expiries */
   uint32_t kernel;          /* kernel that ran (ND_KERNEL_PLAIN / _PERSISTENT) */
+  double march_ms;          /* device time of the march kernels of the last nd_march_forward
+                               (CUDA events on its stream; 0 after a graph launch) */
+  double shade_ms;          /* device time of its shade passes (normals, shadows, orbit trap) */
 } nd_stats;
 
 typedef struct nd_tune_result {

@@ -66,7 +66,8 @@ class nd_stats(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("de_evals", C.c_uint64), ("march_evals", C.c_uint64),
                 ("normal_evals", C.c_uint64), ("shadow_evals", C.c_uint64), ("trap_evals", C.c_uint64),
                 ("hits", C.c_uint64),
-                ("refills", C.c_uint64), ("timeouts", C.c_uint32), ("kernel", C.c_uint32)]
+                ("refills", C.c_uint64), ("timeouts", C.c_uint32), ("kernel", C.c_uint32),
+                ("march_ms", C.c_double), ("shade_ms", C.c_double)]
 
 
 class nd_tune_result(C.Structure):

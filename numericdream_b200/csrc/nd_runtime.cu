@@ -75,6 +75,8 @@ struct nd_ctx {
   int h_views_cap = 0;
   cudaStream_t last_stream = nullptr;
   cudaEvent_t last_done = nullptr;
+  std::vector<cudaEvent_t> tev;  // timing events: per launch plan march start, march end, shade end
+  int tev_plans = 0;             // plans the last forward timed (0: none)
   bool have_last = false;
   int last_kernel = 0;
   int64_t last_rays = 0;
@@ -254,7 +256,7 @@ Tuned tuned_for(const std::string& key) {
 nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_march_opts* opts,
                   const nd_gbuffer* out, cudaStream_t stream, const std::vector<Launch>& plans, DevView* d_views,
                   DevView* h_views, unsigned long long* d_counters, double* d_thit, int32_t* d_hits,
-                  bool copy_views, int* kernel_used) {
+                  bool copy_views, int* kernel_used, cudaEvent_t* tev = nullptr) {
   const int prec = (opts && opts->de_precision == 64) ? 64 : 32;
   // global output offsets in call order
   std::vector<int64_t> out_off(nviews + 1, 0);
@@ -313,6 +315,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       // the persistent march leaves the normal taps and shadow rays of its hits to
       // the shade pass
       const bool defer = kernel != ND_KERNEL_PLAIN && d_hits != nullptr && d_thit != nullptr;
+      if (tev) cudaEventRecord(tev[3 * p], stream);
       if (kernel == ND_KERNEL_PLAIN) {
         // the plain baseline: one launch per view, one thread per ray
         for (int k = 0; k < nv; ++k) {
@@ -330,6 +333,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
         e = fn(a, h_views[base], c, stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
       }
+      if (tev) cudaEventRecord(tev[3 * p + 1], stream);
       if (defer || want_trap) {
         // normals of the deferred hits and/or the orbit trap at every hit point
         const bool batched = nv > 1;
@@ -340,6 +344,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
         e = sf(a, h_views[base], c, want_trap ? 1 : 0, stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "shade pass launch");
       }
+      if (tev) cudaEventRecord(tev[3 * p + 2], stream);
       used = kernel;
     }
     base += nv;
@@ -520,6 +525,7 @@ nd_status nd_ctx_destroy(nd_ctx* ctx) {
   if (ctx->d_hits) cudaFree(ctx->d_hits);
   if (ctx->h_views) cudaFreeHost(ctx->h_views);
   if (ctx->last_done) cudaEventDestroy(ctx->last_done);
+  for (cudaEvent_t ev : ctx->tev) cudaEventDestroy(ev);
   delete ctx;
   return ND_OK;
 }
@@ -577,9 +583,18 @@ nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
     if (e != cudaSuccess) return cuda_fail(ctx, e, "pinned view staging");
     ctx->h_views_cap = std::max(nviews, 64);
   }
+  while (ctx->tev.size() < 3 * plans.size()) {
+    cudaEvent_t ev;
+    e = cudaEventCreate(&ev);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "timing event");
+    ctx->tev.push_back(ev);
+  }
+  // a plan with no rays records no events: start from a clean slate
+  for (size_t i = 0; i < 3 * plans.size(); ++i) cudaEventRecord(ctx->tev[i], st);
   int kernel = 0;
   s = enqueue(ctx, views, nviews, opts, out, st, plans, ctx->d_views, ctx->h_views, ctx->d_counters, ctx->d_thit,
-              ctx->d_hits, true, &kernel);
+              ctx->d_hits, true, &kernel, ctx->tev.data());
+  ctx->tev_plans = s == ND_OK ? int(plans.size()) : 0;
   if (s != ND_OK) return s;
   e = cudaEventRecord(ctx->last_done, st);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "record event");
@@ -613,6 +628,11 @@ nd_status nd_last_stats(nd_ctx* ctx, nd_stats* out) {
   out->refills = h.refills;
   out->timeouts = h.timeouts;
   out->kernel = uint32_t(ctx->last_kernel);
+  for (int p = 0; p < ctx->tev_plans; ++p) {
+    float m = 0.0f, sh = 0.0f;
+    if (cudaEventElapsedTime(&m, ctx->tev[3 * p], ctx->tev[3 * p + 1]) == cudaSuccess) out->march_ms += m;
+    if (cudaEventElapsedTime(&sh, ctx->tev[3 * p + 1], ctx->tev[3 * p + 2]) == cudaSuccess) out->shade_ms += sh;
+  }
   if (h.timeouts) return fail(ctx, ND_ERR_TIMEOUT, "the device watchdog stopped %u warps", h.timeouts);
   return ND_OK;
 }
@@ -753,6 +773,7 @@ nd_status nd_graph_launch(nd_graph* g, void* stream) {
   cudaSetDevice(g->ctx->device);
   cudaError_t e = cudaGraphLaunch(g->exec, (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(g->ctx, e, "graph launch");
+  g->ctx->tev_plans = 0;
   e = cudaEventRecord(g->ctx->last_done, (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(g->ctx, e, "record event");
   g->ctx->have_last = true;
