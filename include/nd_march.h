@@ -150,6 +150,58 @@ typedef struct nd_view_desc {
  * views in call order; rays(v) = spp * tile_w * tile_h and the ray index inside a
  * view is sample * tile_w * tile_h + y * tile_w + x.  Every pointer may be NULL
  * except depth. */
+/* A scene of up to four fractal instances combined by distance (scene_de,
+ * template.wgsl:1756-1779), each with its own formula, parameters, placement
+ * (instance_local: transpose(frame) * (p - offset) / scale, tpl:1611-1615; DE factor
+ * min|scale| * clamp(step_safety), tpl:1617-1620), combine mode with the previous
+ * instances (combine_de, tpl:1708-1730) and optional hybrid mixins (eval_mixed,
+ * tpl:1321-1392: iterations cycle through hybrid_base_iters steps of the base formula,
+ * then each mixin's steps; the base formula finalises), plus up to 16 spherical carves
+ * (apply_carves, tpl:1741-1753).  Mirrors FractalInstance / MixinParams
+ * (tpl:106-141); the per-instance colours are a shading concern and not here. */
+#define ND_MAX_INSTANCES 4  /* MAX_INSTANCES tpl:22 */
+#define ND_MAX_MIXINS 3     /* MAX_MIXINS tpl:23 */
+#define ND_MAX_CARVES 16    /* MAX_CARVES tpl:32 */
+enum {
+  ND_COMBINE_UNION = 0,
+  ND_COMBINE_SMOOTH_MIN = 1,
+  ND_COMBINE_SMOOTH_MAX = 2,
+  ND_COMBINE_SMOOTH_INV_MAX = 3,
+  ND_COMBINE_SMOOTH_MIN_LIN = 4,
+  ND_COMBINE_SMOOTH_MIN_NLIN = 5,
+  ND_COMBINE_SMOOTH_MIX = 6
+};
+
+typedef struct nd_mixin_desc {
+  nd_formula_id formula;
+  int32_t iterations;              /* steps of this mixin per hybrid cycle */
+  float params[ND_MAX_PARAMS];
+} nd_mixin_desc;
+
+typedef struct nd_instance_desc {
+  nd_formula_id formula;
+  int32_t hidden;                  /* 1: skipped by scene_de */
+  float params[ND_MAX_PARAMS];
+  float offset[3];
+  float scale[3];                  /* per axis; |scale| floored at 0.001 */
+  float frame[9];                  /* rotation matrix, three columns (u.instances[i].frame) */
+  float step_safety;
+  float blend_k;                   /* combine blend radius (<= 1e-4: hard) */
+  int32_t combine_mode;            /* ND_COMBINE_*, with the instances before it */
+  int32_t mixin_count;             /* 0: the plain formula; 1..3: hybrid */
+  int32_t hybrid_base_iters;
+  int32_t hybrid_total_iters;
+  nd_mixin_desc mixins[ND_MAX_MIXINS];
+  nd_trap_desc trap;
+} nd_instance_desc;
+
+typedef struct nd_scene_desc {
+  int32_t instance_count;          /* 1..4 */
+  int32_t carve_count;             /* 0..16 */
+  nd_instance_desc instances[ND_MAX_INSTANCES];
+  float carves[ND_MAX_CARVES][4];  /* sphere centre xyz, radius w */
+} nd_scene_desc;
+
 typedef struct nd_gbuffer {
   float* depth;       /* t at the hit, 0 on a miss (R32F depth target) */
   float* normal;      /* 4 floats per ray: unit normal, w = 1 on a hit */
@@ -242,6 +294,18 @@ typedef struct nd_orbit_camera {
 
 /* Fill view->cam_pos/fwd/right/up from an orbit camera. */
 nd_status nd_orbit_view(const nd_orbit_camera* cam, nd_view_desc* view);
+
+/* nd_march_forward for scenes of several instances.  view_scene[i] >= 0 marches
+ * views[i] against scenes[view_scene[i]] (HOST array of nscenes); -1 uses the view's
+ * own single instance (formula, params, trap, step_safety).  Every formula of a call
+ * (instances, mixins and the single-instance views) must lie in one compiled formula
+ * group (ND_ERR_UNSUPPORTED otherwise; ND_GROUPS at build time adds groups); scenes run
+ * on the persistent kernel.  At a hit the G-buffer's trap and iteration count are those
+ * of the visible instance with the smallest DE there.  Replaces renderTile with a
+ * multi-instance Uniforms write (fractal_renderer.zig:3063, instances at tpl:114-141). */
+nd_status nd_march_forward_scenes(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews,
+                                  const int32_t* view_scene, const nd_scene_desc* scenes, int32_t nscenes,
+                                  const nd_march_opts* opts, const nd_gbuffer* out, void* stream);
 
 /* Gradient of an image loss with respect to formula @params and the orbit pose.
  * No counterpart in the reference (it has no gradients).  views/cams (HOST) are the

@@ -50,6 +50,94 @@ class nd_view_desc(C.Structure):
     ]
 
 
+ND_MAX_INSTANCES, ND_MAX_MIXINS, ND_MAX_CARVES = 4, 3, 16
+(ND_COMBINE_UNION, ND_COMBINE_SMOOTH_MIN, ND_COMBINE_SMOOTH_MAX, ND_COMBINE_SMOOTH_INV_MAX, ND_COMBINE_SMOOTH_MIN_LIN,
+ ND_COMBINE_SMOOTH_MIN_NLIN, ND_COMBINE_SMOOTH_MIX) = range(7)
+
+
+class nd_mixin_desc(C.Structure):
+    _fields_ = [("formula", C.c_int32), ("iterations", C.c_int32), ("params", C.c_float * ND_MAX_PARAMS)]
+
+
+class nd_instance_desc(C.Structure):
+    _fields_ = [("formula", C.c_int32), ("hidden", C.c_int32), ("params", C.c_float * ND_MAX_PARAMS),
+                ("offset", C.c_float * 3), ("scale", C.c_float * 3), ("frame", C.c_float * 9),
+                ("step_safety", C.c_float), ("blend_k", C.c_float), ("combine_mode", C.c_int32),
+                ("mixin_count", C.c_int32), ("hybrid_base_iters", C.c_int32), ("hybrid_total_iters", C.c_int32),
+                ("mixins", nd_mixin_desc * ND_MAX_MIXINS), ("trap", nd_trap_desc)]
+
+
+class nd_scene_desc(C.Structure):
+    _fields_ = [("instance_count", C.c_int32), ("carve_count", C.c_int32),
+                ("instances", nd_instance_desc * ND_MAX_INSTANCES), ("carves", (C.c_float * 4) * ND_MAX_CARVES)]
+
+
+def rotation_frame(rx_deg=0.0, ry_deg=0.0, rz_deg=0.0):
+    """The instance frame rot_z * rot_y * rot_x (template.wgsl:1392-1408; angles in
+    degrees), as three columns."""
+    def rx(a):
+        c, s = math.cos(a), math.sin(a)
+        return [[1, 0, 0], [0, c, s], [0, -s, c]]  # columns
+
+    def ry(a):
+        c, s = math.cos(a), math.sin(a)
+        return [[c, 0, -s], [0, 1, 0], [s, 0, c]]
+
+    def rz(a):
+        c, s = math.cos(a), math.sin(a)
+        return [[c, s, 0], [-s, c, 0], [0, 0, 1]]
+
+    def mul(a, b):  # column-major 3x3: column j of a * b is a * (column j of b)
+        return [[sum(a[k][i] * b[j][k] for k in range(3)) for i in range(3)] for j in range(3)]
+
+    m = mul(rz(math.radians(rz_deg)), mul(ry(math.radians(ry_deg)), rx(math.radians(rx_deg))))
+    return [m[c][r] for c in range(3) for r in range(3)]
+
+
+def make_instance(formula: int, params=None, offset=(0.0, 0.0, 0.0), scale=(1.0, 1.0, 1.0), rotation_deg=(0.0, 0.0, 0.0),
+                  step_safety=1.0, blend_k=0.0, combine_mode=ND_COMBINE_UNION, hidden=False, mixins=(),
+                  hybrid_base_iters=0, hybrid_total_iters=0, trap=None) -> nd_instance_desc:
+    """One scene instance; mixins: [(formula, iterations, params), ...]."""
+    d = nd_instance_desc()
+    d.formula = formula
+    d.hidden = 1 if hidden else 0
+    for i, p in enumerate((params or [])[:ND_MAX_PARAMS]):
+        d.params[i] = p
+    d.offset[:] = [float(x) for x in offset]
+    d.scale[:] = [float(x) for x in scale]
+    d.frame[:] = rotation_frame(*rotation_deg)
+    d.step_safety, d.blend_k, d.combine_mode = step_safety, blend_k, combine_mode
+    d.mixin_count = len(mixins)
+    for j, (f, n, prm) in enumerate(mixins):
+        d.mixins[j].formula = f
+        d.mixins[j].iterations = n
+        for i, p in enumerate(prm[:ND_MAX_PARAMS]):
+            d.mixins[j].params[i] = p
+    d.hybrid_base_iters, d.hybrid_total_iters = hybrid_base_iters, hybrid_total_iters
+    d.trap.shape = ND_TRAP_POINT
+    d.trap.radius = 1.0
+    d.trap.box[:] = [1.0, 1.0, 1.0]
+    d.trap.span = 1.5
+    for k, v in (trap or {}).items():
+        if k in ("center", "box"):
+            getattr(d.trap, k)[:] = v
+        else:
+            setattr(d.trap, k, v)
+    return d
+
+
+def make_scene(instances, carves=()) -> nd_scene_desc:
+    """A scene of 1..4 instances and up to 16 carves (x, y, z, radius)."""
+    s = nd_scene_desc()
+    s.instance_count = len(instances)
+    for i, inst in enumerate(instances):
+        s.instances[i] = inst
+    s.carve_count = len(carves)
+    for i, c in enumerate(carves):
+        s.carves[i][:] = [float(x) for x in c]
+    return s
+
+
 class nd_gbuffer(C.Structure):
     _fields_ = [("depth", C.c_void_p), ("normal", C.c_void_p), ("trap", C.c_void_p), ("steps", C.c_void_p),
                 ("iters", C.c_void_p), ("shade", C.c_void_p), ("shadow", C.c_void_p), ("depth64", C.c_void_p),

@@ -48,6 +48,12 @@ NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "
 # batch belongs to a compiled group.  The default group holds the four formulas
 # of the batched benchmark (Mandelbulb, Mandelbox, Menger sponge, pseudo-Kleinian).
 DEFAULT_GROUPS = {"mixed4": ["mandelbrot", "amazingbox_box", "menger3_ifs", "pseudokleinian_kleinian"]}
+# Groups also carry the multi-instance scene kernels: a scene's formulas (instances
+# and mixins) must all lie in one group.  ND_GROUPS adds groups:
+# "name=f1,f2,...;name2=..." (formula file stems).
+for _spec in filter(None, os.environ.get("ND_GROUPS", "").split(";")):
+    _name, _, _members = _spec.partition("=")
+    DEFAULT_GROUPS[_name.strip()] = [m.strip() for m in _members.split(",") if m.strip()]
 
 
 def reference_root():
@@ -154,7 +160,7 @@ nd::KernelTable nd_kernels_{tf.namespace}() {{ return nd::make_kernel_table<nd::
 #include "nd_kernels.cuh"
 {incs}
 {traits}
-nd::KernelTable nd_group_{gname}() {{ return nd::make_kernel_table<nd::FormulaSet<{setargs}>>(); }}
+nd::KernelTable nd_group_{gname}() {{ return nd::make_kernel_table<nd::FormulaSet<{setargs}>, true>(); }}
 """)
         units.append(unit)
         groups.append((gname, [index[m] for m in members]))

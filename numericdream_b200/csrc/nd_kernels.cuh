@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value) plain_kernel(const _
 // tpl:5083-5105), and a warp keeps marching neighbouring pixels.  Whatever phase
 // a lane is in, each pass of the loop is one DE evaluation for every busy lane.
 
-template <class Set, class T, bool kDir64, bool kBatched>
+template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false>
 __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     persistent_kernel(const __grid_constant__ LaunchArgs a, const __grid_constant__ DevView single) {
   const unsigned full = 0xffffffffu;
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     }
     if (L.item >= 0 && L.phase != PH_DONE) {
       const DevView& v = kBatched ? a.views[L.view] : single;
-      const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(L.sample_pos(v)), v);
+      const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(L.sample_pos(v)), a.scenes);
       L.advance(v, de, a.out, a.t_hit, defer);
     }
   }
@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
 // every listed hit (the shadow rays' step counts differ, the rest is coherent);
 // without one (the plain kernel) the orbit trap of every ray that hit.  It strides
 // over its work with a resident grid.
-template <class Set, class T, bool kDir64, bool kBatched>
+template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false>
 __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     shade_kernel(const __grid_constant__ LaunchArgs a, const __grid_constant__ DevView single, int do_trap) {
   const bool list = a.hit_list != nullptr;
@@ -224,11 +224,11 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     const double t = a.t_hit[v.out_offset + local];
     if (t < 0.0) continue;  // a miss (all-rays mode); the march wrote its outputs
     if (list) {
-      const uint32_t ev = shade_at_hit<Set, T, kDir64>(v, local, t, a.out);
+      const uint32_t ev = shade_at_hit<Set, T, kDir64, kScenes>(v, local, t, a.out, a.scenes);
       taps += ev & 0xffffu;
       shadow += ev >> 16;
     }
-    if (do_trap) trap_at_hit<Set, T, kDir64>(v, local, t, a.out);
+    if (do_trap) trap_at_hit<Set, T, kDir64, kScenes>(v, local, t, a.out, a.scenes);
   }
   if (list) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -260,13 +260,13 @@ cudaError_t launch_plain(const LaunchArgs& a, const DevView& single, const Launc
   return cudaGetLastError();
 }
 
-template <class Set, class T, bool kDir64, bool kBatched>
+template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false>
 cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const LaunchConfig& c, cudaStream_t s) {
   const int block = 128;
   int per_sm = c.blocks_per_sm;
   if (per_sm <= 0) {
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, persistent_kernel<Set, T, kDir64, kBatched>, block, 0);
+        &per_sm, persistent_kernel<Set, T, kDir64, kBatched, kScenes>, block, 0);
     if (e != cudaSuccess) return e;
     if (per_sm <= 0) per_sm = 1;
   }
@@ -279,23 +279,24 @@ cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const 
   LaunchArgs b = a;
   const int64_t warps = grid * (block / 32);
   b.chunk = int32_t(std::max<int64_t>(1, std::min<int64_t>(64, a.total_rays / (warps * 4))));
-  persistent_kernel<Set, T, kDir64, kBatched><<<unsigned(grid), block, 0, s>>>(b, single);
+  persistent_kernel<Set, T, kDir64, kBatched, kScenes><<<unsigned(grid), block, 0, s>>>(b, single);
   return cudaGetLastError();
 }
 
 typedef cudaError_t (*LaunchFn)(const LaunchArgs&, const DevView&, const LaunchConfig&, cudaStream_t);
 
-template <class Set, class T, bool kDir64, bool kBatched>
+template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false>
 cudaError_t launch_shade(const LaunchArgs& a, const DevView& single, const LaunchConfig& c, int do_trap,
                          cudaStream_t s) {
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shade_kernel<Set, T, kDir64, kBatched>, 128, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shade_kernel<Set, T, kDir64, kBatched, kScenes>,
+                                                                128, 0);
   if (e != cudaSuccess) return e;
   int64_t grid = int64_t(std::max(per_sm, 1)) * c.num_sms;
   const int64_t needed = (a.total_rays + 127) / 128;
   if (grid > needed) grid = needed;
   if (grid <= 0) return cudaSuccess;
-  shade_kernel<Set, T, kDir64, kBatched><<<unsigned(grid), 128, 0, s>>>(a, single, do_trap);
+  shade_kernel<Set, T, kDir64, kBatched, kScenes><<<unsigned(grid), 128, 0, s>>>(a, single, do_trap);
   return cudaGetLastError();
 }
 
@@ -337,10 +338,24 @@ struct KernelTable {
   ShadeFn shade_f32, shade_f32_batched, shade_f32_dir64, shade_f32_dir64_batched, shade_f64, shade_f64_batched;
   DePointsFn de_points_f32, de_points_f64;
   AdjointFn adjoint_f32, adjoint_f32_batched, adjoint_f64, adjoint_f64_batched;
+  // multi-instance scenes (formula groups only; null in single-formula tables)
+  LaunchFn scene_persistent_f32, scene_persistent_f32_dir64, scene_persistent_f64;
+  ShadeFn scene_shade_f32, scene_shade_f32_dir64, scene_shade_f64;
 };
 
-template <class Set> KernelTable make_kernel_table() {
+template <class Set, bool kWithScenes = false> KernelTable make_kernel_table() {
   KernelTable t;
+  if constexpr (kWithScenes) {
+    t.scene_persistent_f32 = &launch_persistent<Set, float, false, true, true>;
+    t.scene_persistent_f32_dir64 = &launch_persistent<Set, float, true, true, true>;
+    t.scene_persistent_f64 = &launch_persistent<Set, double, true, true, true>;
+    t.scene_shade_f32 = &launch_shade<Set, float, false, true, true>;
+    t.scene_shade_f32_dir64 = &launch_shade<Set, float, true, true, true>;
+    t.scene_shade_f64 = &launch_shade<Set, double, true, true, true>;
+  } else {
+    t.scene_persistent_f32 = t.scene_persistent_f32_dir64 = t.scene_persistent_f64 = nullptr;
+    t.scene_shade_f32 = t.scene_shade_f32_dir64 = t.scene_shade_f64 = nullptr;
+  }
   t.plain_f32 = &launch_plain<Set, float, false>;
   t.plain_f32_dir64 = &launch_plain<Set, float, true>;
   t.plain_f64 = &launch_plain<Set, double, true>;

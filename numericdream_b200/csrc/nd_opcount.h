@@ -103,7 +103,7 @@ inline void count_ray(const DevView& view, int64_t ray, ndw::OpCounts* out, uint
   if (L.hit) {  // the trap pass: one DE with the orbit trap at the hit point
     ++*evals;
     g.trap = &depth;
-    trap_at_hit<Set, ndw::CF, false>(v, ray - v.ray_offset, L.t, g);
+    trap_at_hit<Set, ndw::CF, false>(v, ray - v.ray_offset, L.t, g, nullptr);
   }
   out->add += c.add - before.add;
   out->mul += c.mul - before.mul;

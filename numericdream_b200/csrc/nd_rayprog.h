@@ -82,6 +82,7 @@ struct DevView {
   int32_t dir64;        // ray directions need FP64 (deep-zoom cameras)
   int32_t user_index;   // the view's index in the caller's array
   int32_t exact_hit;    // bisect for the whole budget (ND_VIEW_EXACT_HIT)
+  int32_t scene;        // index into the launch's scene table, -1: the single instance above
   int32_t pad;
 };
 
@@ -105,6 +106,7 @@ struct LaunchArgs {
   // to hit_list; the shade pass then evaluates the normal taps coherently.
   int32_t* hit_list;          // launch-local ray indices of hits (nullptr: shading inline)
   unsigned int* hit_count;    // entries in hit_list (zeroed before launch)
+  const struct DevScene* scenes;  // multi-instance scenes of the launch's views (may be null)
 };
 
 // --------------------------------------------------------------- orbit trap
@@ -231,6 +233,9 @@ ND_DEV_INLINE DEOut<T> formula_de(ndw::v3<T> pos, const float* params, const nd_
 // A compile-time list of formulas; code selects one (warp-uniform in practice,
 // because batched views are ordered by formula).  de_with evaluates the DE alone
 // (no trap) with a caller-supplied parameter accessor.
+// eval / step / finalize dispatch on a code like the reference's eval_formula /
+// eval_step / eval_finalize (fractal_renderer.zig:529-534); a code outside the set
+// gives NO_SURFACE_DE (1e6) / the carry unchanged.
 template <class... Fs> struct FormulaSet;
 template <class F> struct FormulaSet<F> {
   template <class T, bool kTrap = false>
@@ -240,6 +245,20 @@ template <class F> struct FormulaSet<F> {
   template <class T, class PR>
   static ND_DEV_INLINE DEOut<T> de_with(int, ndw::v3<T> pos, const PR& p, const DevView& v) {
     return formula_de_p<F, T, false, PR>(pos, p, v.trap, v.factor);
+  }
+  template <class T, bool kTrap>
+  static ND_DEV_INLINE DEOut<T> eval(int code, ndw::v3<T> pos, const float* params, const nd_trap_desc& trap) {
+    if (code != 0) return DEOut<T>{T(1e6), T(0), 0};
+    return formula_de<F, T, kTrap>(pos, params, trap, 1.0f);
+  }
+  template <class T>
+  static ND_DEV_INLINE ndw::IterCarry<T> step(int code, ndw::IterCarry<T> c, ndw::v3<T> pos, const float* params) {
+    if (code != 0) return c;
+    return F::template step<T, ParamRef<T>>(c, pos, ParamRef<T>{params});
+  }
+  template <class T> static ND_DEV_INLINE T finalize(int code, ndw::IterCarry<T> c) {
+    if (code != 0) return T(1e6);
+    return F::template finalize<T, ParamRef<T>>(c);
   }
 };
 template <class F, class G, class... Rest> struct FormulaSet<F, G, Rest...> {
@@ -253,7 +272,169 @@ template <class F, class G, class... Rest> struct FormulaSet<F, G, Rest...> {
     if (code == 0) return formula_de_p<F, T, false, PR>(pos, p, v.trap, v.factor);
     return FormulaSet<G, Rest...>::template de_with<T, PR>(code - 1, pos, p, v);
   }
+  template <class T, bool kTrap>
+  static ND_DEV_INLINE DEOut<T> eval(int code, ndw::v3<T> pos, const float* params, const nd_trap_desc& trap) {
+    if (code == 0) return formula_de<F, T, kTrap>(pos, params, trap, 1.0f);
+    return FormulaSet<G, Rest...>::template eval<T, kTrap>(code - 1, pos, params, trap);
+  }
+  template <class T>
+  static ND_DEV_INLINE ndw::IterCarry<T> step(int code, ndw::IterCarry<T> c, ndw::v3<T> pos, const float* params) {
+    if (code == 0) return F::template step<T, ParamRef<T>>(c, pos, ParamRef<T>{params});
+    return FormulaSet<G, Rest...>::template step<T>(code - 1, c, pos, params);
+  }
+  template <class T> static ND_DEV_INLINE T finalize(int code, ndw::IterCarry<T> c) {
+    if (code == 0) return F::template finalize<T, ParamRef<T>>(c);
+    return FormulaSet<G, Rest...>::template finalize<T>(code - 1, c);
+  }
 };
+
+// --------------------------------------------------------------- scenes
+// A multi-instance scene as the kernels read it (built on the host from
+// nd_scene_desc): per instance the inverse placement and DE factor precomputed.
+struct DevInstance {
+  float params[ND_MAX_PARAMS];
+  float mparams[ND_MAX_MIXINS][ND_MAX_PARAMS];
+  float col[3][3];     // rotation frame columns: local_i = (col_i . (p - off)) / s_i
+  float off[3];
+  float s[3];          // signed scale, |s| >= 0.001 (instance_scale_magnitude)
+  float factor;        // min |s| * clamp(step_safety, 0.001, 1)
+  float blend_k;
+  nd_trap_desc trap;
+  int32_t code, hidden, combine, mixin_count, base_n, total_n;
+  int32_t mcode[ND_MAX_MIXINS], miters[ND_MAX_MIXINS];
+};
+struct DevScene {
+  int32_t count, carve_count;
+  DevInstance inst[ND_MAX_INSTANCES];
+  float carves[ND_MAX_CARVES][4];
+};
+
+// combine_de (tpl:1708-1730), the distance only.
+template <class T> ND_DEV_INLINE T combine_de(int mode, T d, T di, T k) {
+  if (mode == ND_COMBINE_UNION) return ndw::min(d, di);
+  if (mode == ND_COMBINE_SMOOTH_MIN) return ndw::smin(d, di, k);
+  if (mode == ND_COMBINE_SMOOTH_MIX) return ndw::smix(d, di, k);
+  if (mode == ND_COMBINE_SMOOTH_MAX) return ndw::smax(d, di, k);
+  if (mode == ND_COMBINE_SMOOTH_INV_MAX) return ndw::ssub(di, d, k);
+  if (mode == ND_COMBINE_SMOOTH_MIN_LIN) return ndw::smin_lin(d, di, k);
+  return ndw::smin_nlin(d, di, k);
+}
+
+// eval_mixed (tpl:1361-1392) with hybrid_cycle_len / hybrid_step (tpl:1335-1359),
+// distance before the instance factor; the trap follows every step.
+template <class Set, class T, bool kTrap>
+ND_DEV_INLINE DEOut<T> eval_mixed(const DevInstance& in, ndw::v3<T> pos) {
+  ndw::IterCarry<T> c{pos, T(1)};
+  TrapAcc<T> acc;
+  if constexpr (kTrap) acc = trap_begin<T>(in.trap);
+  const int base_n = in.base_n > 0 ? in.base_n : 0;
+  const int mixins = in.mixin_count < ND_MAX_MIXINS ? in.mixin_count : ND_MAX_MIXINS;
+  int cycle = base_n;
+  for (int j = 0; j < mixins; ++j) cycle += in.miters[j] > 0 ? in.miters[j] : 0;
+  if (cycle < 1) cycle = 1;
+  int total = in.total_n > 0 ? in.total_n : 0;
+  total = total < kMaxIterations ? total : kMaxIterations;
+  int changed = 0;
+  for (int it = 0; it < total; ++it) {
+    int pos_in = it % cycle;
+    int code = in.code;
+    const float* p = in.params;
+    bool have = true;
+    if (pos_in >= base_n) {
+      pos_in -= base_n;
+      have = false;
+      for (int j = 0; j < mixins; ++j) {
+        const int nj = in.miters[j] > 0 ? in.miters[j] : 0;
+        if (pos_in < nj) {
+          code = in.mcode[j];
+          p = in.mparams[j];
+          have = true;
+          break;
+        }
+        pos_in -= nj;
+      }
+    }
+    const ndw::v3<T> zp = c.z;
+    if (have) c = Set::template step<T>(code, c, pos, p);
+    if constexpr (kTrap) {
+      const bool ch = (c.z.x != zp.x) | (c.z.y != zp.y) | (c.z.z != zp.z);
+      changed += ch ? 1 : 0;
+      trap_update(acc, in.trap, c.z, ch, it);
+    }
+  }
+  DEOut<T> o;
+  o.d = Set::template finalize<T>(in.code, c);
+  if constexpr (kTrap) o.trap = trap_finish(acc, in.trap, total);
+  else o.trap = T(0);
+  o.iters = changed;
+  return o;
+}
+
+// instance_de_trap (tpl:1626-1630): the instance's local DE times its factor.
+template <class Set, class T, bool kTrap>
+ND_DEV_INLINE DEOut<T> instance_de(const DevInstance& in, ndw::v3<T> pos) {
+  const T dx = pos.x - T(in.off[0]), dy = pos.y - T(in.off[1]), dz = pos.z - T(in.off[2]);
+  const ndw::v3<T> local = ndw::v3<T>(
+      (T(in.col[0][0]) * dx + T(in.col[0][1]) * dy + T(in.col[0][2]) * dz) / T(in.s[0]),
+      (T(in.col[1][0]) * dx + T(in.col[1][1]) * dy + T(in.col[1][2]) * dz) / T(in.s[1]),
+      (T(in.col[2][0]) * dx + T(in.col[2][1]) * dy + T(in.col[2][2]) * dz) / T(in.s[2]));
+  DEOut<T> o = in.mixin_count > 0 ? eval_mixed<Set, T, kTrap>(in, local)
+                                  : Set::template eval<T, kTrap>(in.code, local, in.params, in.trap);
+  o.d = o.d * T(in.factor);
+  return o;
+}
+
+// scene_de (tpl:1756-1779) and apply_carves (tpl:1741-1753); no domain warps or
+// particles (stubs in the reference's default variant).  With kTrap, the trap and
+// iteration count of the visible instance with the smallest DE.
+template <class Set, class T, bool kTrap>
+ND_DEV_INLINE DEOut<T> scene_de(const DevScene& S, ndw::v3<T> pos, double max_dist) {
+  const T empty = T(float(max_dist) * 2.0f + 1.0f);  // empty_scene_de
+  T d = empty, best = T(0);
+  bool first = true;
+  DEOut<T> o;
+  o.trap = T(0);
+  o.iters = 0;
+  const int count = S.count > 1 ? (S.count < ND_MAX_INSTANCES ? S.count : ND_MAX_INSTANCES) : 1;
+  for (int i = 0; i < count; ++i) {
+    const DevInstance& in = S.inst[i];
+    if (in.hidden) continue;
+    const DEOut<T> di = instance_de<Set, T, kTrap>(in, pos);
+    if constexpr (kTrap) {
+      if (first || di.d < best) {
+        best = di.d;
+        o.trap = di.trap;
+        o.iters = di.iters;
+      }
+    }
+    d = first ? di.d : combine_de<T>(in.combine, d, di.d, T(in.blend_k));
+    first = false;
+  }
+  if (first) {
+    o.d = empty;
+    return o;
+  }
+  const int carves = S.carve_count < ND_MAX_CARVES ? S.carve_count : ND_MAX_CARVES;
+  for (int i = 0; i < carves; ++i) {
+    const float* c = S.carves[i];
+    const T r = T(c[3]);
+    const T len = ndw::length(pos - ndw::v3<T>(T(c[0]), T(c[1]), T(c[2])));
+    d = ndw::ssub(len - r, d, T(0.2) * r);  // CARVE_BLEND = 0.2
+  }
+  o.d = d;
+  return o;
+}
+
+// The DE a view's rays see: its single instance, or (kernels compiled with kScenes)
+// its scene.  Only the scene kernels carry the scene code, so that it costs the
+// single-instance march no registers.
+template <class Set, class T, bool kTrap = false, bool kScenes = false>
+ND_DEV_INLINE DEOut<T> view_de(const DevView& v, ndw::v3<T> pos, const DevScene* scenes) {
+  if constexpr (kScenes) {
+    if (v.scene >= 0) return scene_de<Set, T, kTrap>(scenes[v.scene], pos, v.max_dist);
+  }
+  return Set::template de<T, kTrap>(v.code, pos, v);
+}
 
 // --------------------------------------------------------------- helpers
 ND_DEV_INLINE uint64_t splitmix64(uint64_t x) {
@@ -666,12 +847,13 @@ namespace nd {
 
 // The orbit trap and changed-iteration count at a ray's hit point: the formula
 // wrapper with its trap (formula_N) evaluated once at org + dir * t_hit.
-template <class Set, class T, bool kDir64>
-ND_DEV_INLINE void trap_at_hit(const DevView& v, int64_t local, double t, const nd_gbuffer& g) {
+template <class Set, class T, bool kDir64, bool kScenes = false>
+ND_DEV_INLINE void trap_at_hit(const DevView& v, int64_t local, double t, const nd_gbuffer& g,
+                               const DevScene* scenes) {
   Dir<kDir64> dir;
   dir.set(ray_dir(v, local));
   const D3 p = fmadd(d3(v.org[0], v.org[1], v.org[2]), dir.get(), t);
-  const DEOut<T> de = Set::template de<T, true>(v.code, to_t<T>(p), v);
+  const DEOut<T> de = view_de<Set, T, true, kScenes>(v, to_t<T>(p), scenes);
   const int64_t r = v.out_offset + local;
   if (g.trap) g.trap[r] = float(de.trap);
   if (g.iters) g.iters[r] = uint32_t(de.iters);
@@ -682,15 +864,16 @@ ND_DEV_INLINE void trap_at_hit(const DevView& v, int64_t local, double t, const 
 // phase), the shadow ray when the view has one (the steps of PH_SHADOW), and the
 // Lambert level.  Adds the evaluations to the ray's count; returns the taps in
 // the low and the shadow steps in the high 16 bits.
-template <class Set, class T, bool kDir64>
-ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, const nd_gbuffer& g) {
+template <class Set, class T, bool kDir64, bool kScenes = false>
+ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, const nd_gbuffer& g,
+                                    const DevScene* scenes) {
   Dir<kDir64> dir;
   dir.set(ray_dir(v, local));
   const D3 p = fmadd(d3(v.org[0], v.org[1], v.org[2]), dir.get(), t);
   const int taps = int(normal_taps(v));
   float gx = 0.0f, gy = 0.0f, gz = 0.0f;
   for (int k = 0; k < taps; ++k) {
-    const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(normal_tap_pos<T>(v, p, t, k)), v);
+    const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(normal_tap_pos<T>(v, p, t, k)), scenes);
     normal_accumulate(v, k, double(de.d), gx, gy, gz);
   }
   normal_finish(gx, gy, gz);
@@ -703,7 +886,7 @@ ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, c
     const D3 L = d3(v.light[0], v.light[1], v.light[2]);
     double a = kShadowBias, res = 1.0;
     while (true) {
-      const DEOut<T> de = Set::template de<T>(v.code, to_t<T>(fmadd(so, L, a)), v);
+      const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(fmadd(so, L, a)), scenes);
       const double d = double(de.d);
       if (d < kShadowHitEps) {
         vis = 0.0f;

@@ -70,6 +70,8 @@ struct nd_ctx {
   double* d_thit = nullptr;    // FP64 hit distances for the shade pass
   int32_t* d_hits = nullptr;   // hit list of the deferred shade pass
   int64_t thit_cap = 0;
+  nd::DevScene* d_scenes = nullptr;  // multi-instance scene table
+  int scenes_cap = 0;
   bool last_trap = false;
   DevView* h_views = nullptr;  // pinned staging
   int h_views_cap = 0;
@@ -159,6 +161,7 @@ template <class T> nd_status ensure_dev(nd_ctx* ctx, T** p, int* cap, int need, 
 // kernel table.
 struct Launch {
   KernelTable table;
+  std::vector<int> members; // formula ids of the table's set, in code order
   std::vector<int> views;  // indices into the caller's array
   std::vector<int> codes;  // formula code of each view inside the table's set
   int64_t rays = 0;
@@ -174,15 +177,39 @@ std::string set_key(const std::vector<int>& formulas) {
   return k;
 }
 
-nd_status plan(nd_ctx* ctx, const nd_view_desc* views, int nviews, std::vector<Launch>* out) {
+// The multi-instance scenes of a forward call (nd_march_forward_scenes).
+struct SceneInput {
+  const int32_t* view_scene = nullptr;  // per view: scene index or -1
+  const nd_scene_desc* scenes = nullptr;
+  int nscenes = 0;
+  int scene_of(int view) const { return view_scene ? view_scene[view] : -1; }
+};
+
+// Every formula a view's rays evaluate: its own, or its scene's instances and mixins.
+std::vector<int> view_formulas(const nd_view_desc& v, int scene, const SceneInput& sc) {
+  if (scene < 0) return {v.formula};
+  std::vector<int> f;
+  const nd_scene_desc& S = sc.scenes[scene];
+  for (int i = 0; i < S.instance_count; ++i) {
+    const nd_instance_desc& in = S.instances[i];
+    f.push_back(in.formula);
+    for (int j = 0; j < in.mixin_count; ++j) f.push_back(in.mixins[j].formula);
+  }
+  return f;
+}
+
+nd_status plan(nd_ctx* ctx, const nd_view_desc* views, int nviews, std::vector<Launch>* out,
+               const SceneInput& sc = SceneInput()) {
   std::vector<int> distinct;
+  const bool any_scene = sc.nscenes > 0;
   for (int i = 0; i < nviews; ++i)
-    if (std::find(distinct.begin(), distinct.end(), views[i].formula) == distinct.end())
-      distinct.push_back(views[i].formula);
+    for (int f : view_formulas(views[i], sc.scene_of(i), sc))
+      if (std::find(distinct.begin(), distinct.end(), f) == distinct.end()) distinct.push_back(f);
   out->clear();
-  if (distinct.size() == 1) {
+  if (distinct.size() == 1 && !any_scene) {
     Launch L;
     L.table = nd_formula_entries[distinct[0]].kernels();
+    L.members = distinct;
     for (int i = 0; i < nviews; ++i) {
       L.views.push_back(i);
       L.codes.push_back(0);
@@ -203,12 +230,14 @@ nd_status plan(nd_ctx* ctx, const nd_view_desc* views, int nviews, std::vector<L
     if (!covers) continue;
     Launch L;
     L.table = G.kernels();
+    L.members.assign(G.members, G.members + G.count);
     // order the views by formula code so that warps stay formula-uniform
     std::vector<int> order(nviews);
     for (int i = 0; i < nviews; ++i) order[i] = i;
     auto code_of = [&](int vi) {
+      const int f = view_formulas(views[vi], sc.scene_of(vi), sc)[0];
       for (int m = 0; m < G.count; ++m)
-        if (G.members[m] == views[vi].formula) return m;
+        if (G.members[m] == f) return m;
       return 0;
     };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return code_of(a) < code_of(b); });
@@ -220,10 +249,17 @@ nd_status plan(nd_ctx* ctx, const nd_view_desc* views, int nviews, std::vector<L
     out->push_back(L);
     return ND_OK;
   }
+  if (any_scene) {
+    std::string names;
+    for (int f : distinct) names += std::string(names.empty() ? "" : ", ") + nd_formula_entries[f].name;
+    return fail(ctx, ND_ERR_UNSUPPORTED, "the call's formulas (%s) are not in one compiled formula group "
+                "(build with ND_GROUPS)", names.c_str());
+  }
   // otherwise one launch per formula
   for (int f : distinct) {
     Launch L;
     L.table = nd_formula_entries[f].kernels();
+    L.members = {f};
     for (int i = 0; i < nviews; ++i)
       if (views[i].formula == f) {
         L.views.push_back(i);
@@ -256,7 +292,8 @@ Tuned tuned_for(const std::string& key) {
 nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_march_opts* opts,
                   const nd_gbuffer* out, cudaStream_t stream, const std::vector<Launch>& plans, DevView* d_views,
                   DevView* h_views, unsigned long long* d_counters, double* d_thit, int32_t* d_hits,
-                  bool copy_views, int* kernel_used, cudaEvent_t* tev = nullptr) {
+                  bool copy_views, int* kernel_used, cudaEvent_t* tev = nullptr,
+                  const SceneInput& sc = SceneInput(), nd::DevScene* d_scenes = nullptr) {
   const int prec = (opts && opts->de_precision == 64) ? 64 : 32;
   // global output offsets in call order
   std::vector<int64_t> out_off(nviews + 1, 0);
@@ -268,9 +305,39 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
     for (size_t k = 0; k < L.views.size(); ++k) {
       const int vi = L.views[k];
       h_views[base + k] = make_dev_view(views[vi], off, out_off[vi], L.codes[k]);
+      h_views[base + k].scene = sc.scene_of(vi);
       off += h_views[base + k].rays;
     }
     base += int(L.views.size());
+  }
+  if (sc.nscenes > 0 && d_scenes) {
+    // scenes are only accepted when one formula group covers the call: one plan
+    const std::vector<int>& members = plans[0].members;
+    auto code_of = [&](int f) {
+      for (size_t m = 0; m < members.size(); ++m)
+        if (members[m] == f) return int(m);
+      return -1;
+    };
+    std::vector<nd::DevScene> hs(sc.nscenes);
+    for (int k = 0; k < sc.nscenes; ++k) {
+      const nd_scene_desc& S = sc.scenes[k];
+      nd::DevScene& D = hs[k];
+      memset(&D, 0, sizeof(D));
+      D.count = S.instance_count;
+      D.carve_count = S.carve_count;
+      for (int i = 0; i < ND_MAX_INSTANCES && i < S.instance_count; ++i) {
+        int mcode[ND_MAX_MIXINS] = {0, 0, 0};
+        for (int j = 0; j < S.instances[i].mixin_count && j < ND_MAX_MIXINS; ++j)
+          mcode[j] = code_of(S.instances[i].mixins[j].formula);
+        D.inst[i] = nd::make_dev_instance(S.instances[i], code_of(S.instances[i].formula), mcode);
+      }
+      for (int c = 0; c < ND_MAX_CARVES; ++c)
+        for (int q = 0; q < 4; ++q) D.carves[c][q] = S.carves[c][q];
+    }
+    // from pageable memory: returns once the table is staged, so hs may go
+    cudaError_t e = cudaMemcpyAsync(d_scenes, hs.data(), sizeof(nd::DevScene) * hs.size(), cudaMemcpyHostToDevice,
+                                    stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy scenes");
   }
   if (copy_views && base > 0) {
     cudaError_t e = cudaMemcpyAsync(d_views, h_views, sizeof(DevView) * size_t(base), cudaMemcpyHostToDevice, stream);
@@ -301,6 +368,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       a.out = *out;
       a.t_hit = d_thit;
       a.counter = d_counters + p;
+      a.scenes = d_scenes;
       a.stats = ctx->d_stats;
       a.refill_threshold = std::max(1, std::min(32, opts && opts->refill_threshold ? opts->refill_threshold : tu.refill_threshold));
       const int wd = opts && opts->watchdog_ms > 0 ? opts->watchdog_ms : 10000;
@@ -316,6 +384,8 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       // the shade pass
       const bool defer = kernel != ND_KERNEL_PLAIN && d_hits != nullptr && d_thit != nullptr;
       if (tev) cudaEventRecord(tev[3 * p], stream);
+      if (sc.nscenes > 0 && kernel == ND_KERNEL_PLAIN)
+        return fail(ctx, ND_ERR_UNSUPPORTED, "scenes run on the persistent kernel only");
       if (kernel == ND_KERNEL_PLAIN) {
         // the plain baseline: one launch per view, one thread per ray
         for (int k = 0; k < nv; ++k) {
@@ -326,6 +396,11 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       } else {
         const bool batched = nv > 1;
         LaunchFn fn = pick(L.table, kernel, prec, batched, dir64);
+        if (sc.nscenes > 0) {
+          fn = prec == 64 ? L.table.scene_persistent_f64
+                          : (dir64 ? L.table.scene_persistent_f32_dir64 : L.table.scene_persistent_f32);
+          if (!fn) return fail(ctx, ND_ERR_UNSUPPORTED, "no scene kernels in this formula set");
+        }
         if (defer) {
           a.hit_list = d_hits + ray_base;
           a.hit_count = reinterpret_cast<unsigned int*>(d_counters + plans.size() + p);
@@ -341,6 +416,8 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
         nd::ShadeFn sf = prec == 64 ? (batched ? T.shade_f64_batched : T.shade_f64)
                                     : dir64 ? (batched ? T.shade_f32_dir64_batched : T.shade_f32_dir64)
                                             : (batched ? T.shade_f32_batched : T.shade_f32);
+        if (sc.nscenes > 0)
+          sf = prec == 64 ? T.scene_shade_f64 : (dir64 ? T.scene_shade_f32_dir64 : T.scene_shade_f32);
         e = sf(a, h_views[base], c, want_trap ? 1 : 0, stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "shade pass launch");
       }
@@ -355,7 +432,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
 }
 
 nd_status prepare(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_gbuffer* out,
-                  std::vector<Launch>* plans, int64_t* total) {
+                  std::vector<Launch>* plans, int64_t* total, const SceneInput& sc = SceneInput()) {
   if (!ctx) return ND_ERR_INVALID;
   if (!views || nviews <= 0 || nviews > kMaxViews) return fail(ctx, ND_ERR_INVALID, "nviews %d out of range", nviews);
   if (!out || !out->depth) return fail(ctx, ND_ERR_INVALID, "the G-buffer needs at least a depth pointer");
@@ -370,7 +447,26 @@ nd_status prepare(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const 
     if (t > kMaxRays) return fail(ctx, ND_ERR_INVALID, "too many rays in one call");
   }
   *total = t;
-  return plan(ctx, views, nviews, plans);
+  for (int i = 0; i < nviews; ++i) {
+    const int k = sc.scene_of(i);
+    if (k < -1 || k >= sc.nscenes) return fail(ctx, ND_ERR_INVALID, "view %d: scene index %d out of range", i, k);
+    if (k < 0) continue;
+    const nd_scene_desc& S = sc.scenes[k];
+    if (S.instance_count < 1 || S.instance_count > ND_MAX_INSTANCES || S.carve_count < 0 ||
+        S.carve_count > ND_MAX_CARVES)
+      return fail(ctx, ND_ERR_INVALID, "scene %d: instance_count 1..%d, carve_count 0..%d", k, ND_MAX_INSTANCES,
+                  ND_MAX_CARVES);
+    for (int j = 0; j < S.instance_count; ++j) {
+      const nd_instance_desc& in = S.instances[j];
+      if (in.formula < 0 || in.formula >= nd_formula_entry_count || in.mixin_count < 0 ||
+          in.mixin_count > ND_MAX_MIXINS || in.combine_mode < ND_COMBINE_UNION || in.combine_mode > ND_COMBINE_SMOOTH_MIX)
+        return fail(ctx, ND_ERR_INVALID, "scene %d instance %d: bad formula, mixin count or combine mode", k, j);
+      for (int m = 0; m < in.mixin_count; ++m)
+        if (in.mixins[m].formula < 0 || in.mixins[m].formula >= nd_formula_entry_count)
+          return fail(ctx, ND_ERR_INVALID, "scene %d instance %d mixin %d: bad formula", k, j, m);
+    }
+  }
+  return plan(ctx, views, nviews, plans, sc);
 }
 
 }  // namespace
@@ -523,6 +619,7 @@ nd_status nd_ctx_destroy(nd_ctx* ctx) {
   if (ctx->d_stats) cudaFree(ctx->d_stats);
   if (ctx->d_thit) cudaFree(ctx->d_thit);
   if (ctx->d_hits) cudaFree(ctx->d_hits);
+  if (ctx->d_scenes) cudaFree(ctx->d_scenes);
   if (ctx->h_views) cudaFreeHost(ctx->h_views);
   if (ctx->last_done) cudaEventDestroy(ctx->last_done);
   for (cudaEvent_t ev : ctx->tev) cudaEventDestroy(ev);
@@ -547,11 +644,14 @@ nd_status nd_count_rays(const nd_view_desc* views, int32_t nviews, int64_t* tota
   return ND_OK;
 }
 
-nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_march_opts* opts,
-                           const nd_gbuffer* out, void* stream) {
+}  // extern "C"
+
+namespace {
+nd_status forward_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_march_opts* opts,
+                       const nd_gbuffer* out, void* stream, const SceneInput& sc) {
   std::vector<Launch> plans;
   int64_t total = 0;
-  nd_status s = prepare(ctx, views, nviews, out, &plans, &total);
+  nd_status s = prepare(ctx, views, nviews, out, &plans, &total, sc);
   if (s != ND_OK) return s;
   if (opts && opts->de_precision != 0 && opts->de_precision != 32 && opts->de_precision != 64)
     return fail(ctx, ND_ERR_INVALID, "de_precision must be 32 or 64");
@@ -592,8 +692,10 @@ nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
   // a plan with no rays records no events: start from a clean slate
   for (size_t i = 0; i < 3 * plans.size(); ++i) cudaEventRecord(ctx->tev[i], st);
   int kernel = 0;
+  if (sc.nscenes > 0 && (s = ensure_dev(ctx, &ctx->d_scenes, &ctx->scenes_cap, sc.nscenes, "scene table")) != ND_OK)
+    return s;
   s = enqueue(ctx, views, nviews, opts, out, st, plans, ctx->d_views, ctx->h_views, ctx->d_counters, ctx->d_thit,
-              ctx->d_hits, true, &kernel, ctx->tev.data());
+              ctx->d_hits, true, &kernel, ctx->tev.data(), sc, sc.nscenes > 0 ? ctx->d_scenes : nullptr);
   ctx->tev_plans = s == ND_OK ? int(plans.size()) : 0;
   if (s != ND_OK) return s;
   e = cudaEventRecord(ctx->last_done, st);
@@ -604,6 +706,27 @@ nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
   ctx->last_rays = total;
   ctx->last_trap = want_trap;
   return ND_OK;
+}
+}  // namespace
+
+extern "C" {
+
+nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_march_opts* opts,
+                           const nd_gbuffer* out, void* stream) {
+  return forward_impl(ctx, views, nviews, opts, out, stream, SceneInput());
+}
+
+nd_status nd_march_forward_scenes(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const int32_t* view_scene,
+                                  const nd_scene_desc* scenes, int32_t nscenes, const nd_march_opts* opts,
+                                  const nd_gbuffer* out, void* stream) {
+  if (!ctx) return ND_ERR_INVALID;
+  if (nscenes < 0 || (nscenes > 0 && (!scenes || !view_scene)))
+    return fail(ctx, ND_ERR_INVALID, "scenes need a view_scene array and a scene array");
+  SceneInput sc;
+  sc.view_scene = view_scene;
+  sc.scenes = scenes;
+  sc.nscenes = nscenes;
+  return forward_impl(ctx, views, nviews, opts, out, stream, sc);
 }
 
 nd_status nd_last_stats(nd_ctx* ctx, nd_stats* out) {
@@ -820,6 +943,9 @@ size_t nd_sizeof(const char* name) {
   if (n == "nd_param_info") return sizeof(nd_param_info);
   if (n == "nd_tune_result") return sizeof(nd_tune_result);
   if (n == "nd_orbit_camera") return sizeof(nd_orbit_camera);
+  if (n == "nd_scene_desc") return sizeof(nd_scene_desc);
+  if (n == "nd_instance_desc") return sizeof(nd_instance_desc);
+  if (n == "nd_mixin_desc") return sizeof(nd_mixin_desc);
   return 0;
 }
 

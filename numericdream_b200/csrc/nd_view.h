@@ -58,6 +58,7 @@ inline DevView make_dev_view(const nd_view_desc& v, int64_t ray_offset, int64_t 
   d.code = code;
   d.user_index = 0;
   d.exact_hit = (v.flags & ND_VIEW_EXACT_HIT) != 0 ? 1 : 0;
+  d.scene = -1;
   const int refine = v.march_verify ? v.refine_budget : 0;
   const int bisect = v.march_verify ? 0 : v.refine_budget;
   const int64_t ms = int64_t(v.max_steps) * (1 + refine) + bisect;
@@ -67,6 +68,38 @@ inline DevView make_dev_view(const nd_view_desc& v, int64_t ray_offset, int64_t 
   const double rn = sqrt(v.right[0] * v.right[0] + v.right[1] * v.right[1] + v.right[2] * v.right[2]);
   const double un = sqrt(v.up[0] * v.up[0] + v.up[1] * v.up[1] + v.up[2] * v.up[2]);
   d.dir64 = ((v.flags & ND_VIEW_DIR64) != 0 || std::max(rn, un) < 1e-3) ? 1 : 0;
+  return d;
+}
+
+// One scene instance as the kernels read it.  code / mcode: the instance's and its
+// mixins' formula indices inside the launch's formula set.
+inline DevInstance make_dev_instance(const nd_instance_desc& in, int code, const int* mcode) {
+  DevInstance d;
+  memset(&d, 0, sizeof(d));
+  for (int k = 0; k < ND_MAX_PARAMS; ++k) d.params[k] = in.params[k];
+  for (int j = 0; j < ND_MAX_MIXINS; ++j) {
+    for (int k = 0; k < ND_MAX_PARAMS; ++k) d.mparams[j][k] = in.mixins[j].params[k];
+    d.mcode[j] = mcode[j];
+    d.miters[j] = in.mixins[j].iterations;
+  }
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) d.col[c][r] = in.frame[3 * c + r];
+  float mag_min = 1e30f;
+  for (int i = 0; i < 3; ++i) {
+    d.off[i] = in.offset[i];
+    const float mag = std::max(fabsf(in.scale[i]), 0.001f);  // MIN_INSTANCE_SCALE
+    d.s[i] = in.scale[i] < 0.0f ? -mag : mag;
+    mag_min = std::min(mag_min, mag);
+  }
+  d.factor = mag_min * std::min(std::max(in.step_safety, 0.001f), 1.0f);
+  d.blend_k = in.blend_k;
+  d.trap = in.trap;
+  d.code = code;
+  d.hidden = in.hidden ? 1 : 0;
+  d.combine = in.combine_mode;
+  d.mixin_count = std::min(std::max(in.mixin_count, 0), ND_MAX_MIXINS);
+  d.base_n = in.hybrid_base_iters;
+  d.total_n = in.hybrid_total_iters;
   return d;
 }
 

@@ -54,6 +54,9 @@ _SIGNATURES = {
     "nd_de_points": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int64, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "nd_orbit_view": (C.c_int32, [C.POINTER(abi.nd_orbit_camera), C.POINTER(abi.nd_view_desc)]),
+    "nd_march_forward_scenes": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(C.c_int32),
+                                            C.POINTER(abi.nd_scene_desc), C.c_int32, C.POINTER(abi.nd_march_opts),
+                                            C.POINTER(abi.nd_gbuffer), C.c_void_p]),
     "nd_march_backward": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.POINTER(abi.nd_orbit_camera),
                                       C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(abi.nd_gbuffer),
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(abi.nd_march_opts),
@@ -95,7 +98,7 @@ def check_layout(lib=None):
     """Compare the ctypes structure sizes with the library's own."""
     lib = lib or load_library()
     for name in ("nd_view_desc", "nd_trap_desc", "nd_gbuffer", "nd_march_opts", "nd_stats", "nd_param_info",
-                 "nd_tune_result", "nd_orbit_camera"):
+                 "nd_tune_result", "nd_orbit_camera", "nd_scene_desc", "nd_instance_desc", "nd_mixin_desc"):
         mine = C.sizeof(getattr(abi, name))
         theirs = lib.nd_sizeof(name.encode())
         if mine != theirs:
@@ -264,6 +267,18 @@ class Context:
         st = self.lib.nd_march_forward(self.handle, arr, len(views), C.byref(opts) if opts is not None else None,
                                        C.byref(g), s)
         self._check(st, "nd_march_forward")
+
+    def forward_scenes(self, views, view_scene, scenes, gbuf: GBuffer, opts: abi.nd_march_opts | None = None,
+                       stream=None):
+        """nd_march_forward_scenes: view i uses scenes[view_scene[i]] (-1: its own instance)."""
+        arr = (abi.nd_view_desc * len(views))(*views)
+        vs = (C.c_int32 * len(views))(*view_scene)
+        sarr = (abi.nd_scene_desc * max(1, len(scenes)))(*scenes)
+        g = gbuf.as_abi()
+        s = None if stream is None else C.c_void_p(stream)
+        st = self.lib.nd_march_forward_scenes(self.handle, arr, len(views), vs, sarr, len(scenes),
+                                              C.byref(opts) if opts is not None else None, C.byref(g), s)
+        self._check(st, "nd_march_forward_scenes")
 
     def backward(self, views, cams, gbuf: GBuffer, dL_dshade=None, param_idx=(), de_precision=32,
                  per_ray=False, stream=None):
