@@ -307,6 +307,188 @@ template <class R> DE<R> eval_de(int kind, V3<R> pos, const R* p, const nd_trap_
   }
 }
 
+// eval_step / eval_finalize dispatch (fractal_renderer.zig:529-534).
+template <class R> Carry<R> step_kind(int kind, Carry<R> c, V3<R> pos, const R* p) {
+  switch (kind) {
+    case F_MANDELBULB: return Mandelbulb<R>::step(c, pos, p);
+    case F_MANDELBOX: return Mandelbox<R>::step(c, pos, p);
+    case F_MENGER3: return Menger3<R>::step(c, pos, p);
+    case F_PSEUDOKLEINIAN: return PseudoKleinian<R>::step(c, pos, p);
+    case F_SPHERE: return SpherePrim<R>::step(c, pos, p);
+    default: return CubePrim<R>::step(c, pos, p);
+  }
+}
+template <class R> R finalize_kind(int kind, Carry<R> c) {
+  switch (kind) {
+    case F_MANDELBULB: return Mandelbulb<R>::finalize(c);
+    case F_MANDELBOX: return Mandelbox<R>::finalize(c);
+    case F_MENGER3: return Menger3<R>::finalize(c);
+    case F_PSEUDOKLEINIAN: return PseudoKleinian<R>::finalize(c);
+    case F_SPHERE: return SpherePrim<R>::finalize(c);
+    default: return CubePrim<R>::finalize(c);
+  }
+}
+
+// ------------------------------------------------------------------ scenes
+// Smooth combine family (tpl:1648-1706): k <= 1e-4 is the hard operation.
+template <class R> R mixr(R a, R b, R h) { return a * (R(1) - h) + b * h; }
+template <class R> R s_min(R a, R b, R k) {
+  if (k <= R(0.0001)) return std::fmin(a, b);
+  const R h = clampv(R(0.5) + R(0.5) * (b - a) / k, R(0), R(1));
+  return mixr(b, a, h) - k * h * (R(1) - h);
+}
+template <class R> R s_max(R a, R b, R k) {
+  if (k <= R(0.0001)) return std::fmax(a, b);
+  const R h = clampv(R(0.5) - R(0.5) * (b - a) / k, R(0), R(1));
+  return mixr(b, a, h) + k * h * (R(1) - h);
+}
+template <class R> R s_sub(R cut, R base, R k) {
+  if (k <= R(0.0001)) return std::fmax(-cut, base);
+  const R h = clampv(R(0.5) - R(0.5) * (base + cut) / k, R(0), R(1));
+  return mixr(base, -cut, h) + k * h * (R(1) - h);
+}
+template <class R> R s_min_lin(R a, R b, R k) {
+  if (k <= R(0.0001)) return std::fmin(a, b);
+  return std::fmin(b - std::fmax(k - a, R(0)), a - std::fmax(k - b, R(0)));
+}
+template <class R> R s_min_nlin(R a, R b, R k) {
+  if (k <= R(0.0001)) return std::fmin(a, b);
+  const R ra = std::fmax(k - a, R(0)), rb = std::fmax(k - b, R(0));
+  return std::fmin(b - ra * (k - rb) / k, a - rb * (k - ra) / k);
+}
+template <class R> R s_mix(R a, R b, R k) {
+  if (k <= R(0.0001)) return std::fmin(a, b);
+  const R h = clampv(R(0.5) + R(0.5) * (b - a) / k, R(0), R(1));
+  return mixr(b, a, h);
+}
+// combine_de (tpl:1708-1730): d is the scene so far, di the next instance.
+template <class R> R combine(int mode, R d, R di, R k) {
+  switch (mode) {
+    case ND_COMBINE_UNION: return std::fmin(d, di);
+    case ND_COMBINE_SMOOTH_MIN: return s_min(d, di, k);
+    case ND_COMBINE_SMOOTH_MAX: return s_max(d, di, k);
+    case ND_COMBINE_SMOOTH_INV_MAX: return s_sub(di, d, k);
+    case ND_COMBINE_SMOOTH_MIN_LIN: return s_min_lin(d, di, k);
+    case ND_COMBINE_SMOOTH_MIN_NLIN: return s_min_nlin(d, di, k);
+    default: return s_mix(d, di, k);
+  }
+}
+
+// scene_de (tpl:1756-1779) over an nd_scene_desc: per instance the inverse placement
+// (instance_local tpl:1597-1609: rotation frame, then per-axis signed scale with
+// |s| >= 0.001), the DE factor min|s| * clamp(step_safety, 0.001, 1)
+// (tpl:1611-1620), hybrid mixins (eval_mixed tpl:1335-1392), then the carves
+// (apply_carves tpl:1741-1753, blend 0.2 r).  The trap and iteration count are those
+// of the visible instance with the smallest DE.  kind / mkind hold oracle formula
+// kinds for the instances' and mixins' formula ids.
+template <class R> struct SceneEval {
+  const nd_scene_desc* scene = nullptr;
+  int kind[ND_MAX_INSTANCES] = {0, 0, 0, 0};
+  int mkind[ND_MAX_INSTANCES][ND_MAX_MIXINS] = {};
+  double max_dist = 0;
+
+  DE<R> mixed(const nd_instance_desc& in, int slot, V3<R> pos) const {
+    R p[ND_MAX_PARAMS], mp[ND_MAX_MIXINS][ND_MAX_PARAMS];
+    for (int k = 0; k < ND_MAX_PARAMS; ++k) p[k] = R(in.params[k]);
+    for (int j = 0; j < ND_MAX_MIXINS; ++j)
+      for (int k = 0; k < ND_MAX_PARAMS; ++k) mp[j][k] = R(in.mixins[j].params[k]);
+    const int base_n = std::max(in.hybrid_base_iters, 0);
+    const int mixins = std::min(std::max(in.mixin_count, 0), ND_MAX_MIXINS);
+    int cycle = base_n;
+    for (int j = 0; j < mixins; ++j) cycle += std::max(in.mixins[j].iterations, 0);
+    cycle = std::max(cycle, 1);
+    const int total = std::min(std::max(in.hybrid_total_iters, 0), 4096);
+    Carry<R> c{pos, R(1)};
+    TrapAcc<R> acc = trap_begin<R>(in.trap);
+    int changed = 0;
+    for (int it = 0; it < total; ++it) {
+      int at = it % cycle;
+      int k = kind[slot];
+      const R* pp = p;
+      bool have = true;
+      if (at >= base_n) {  // hybrid_step: which mixin owns this iteration
+        at -= base_n;
+        have = false;
+        for (int j = 0; j < mixins; ++j) {
+          const int nj = std::max(in.mixins[j].iterations, 0);
+          if (at < nj) {
+            k = mkind[slot][j];
+            pp = mp[j];
+            have = true;
+            break;
+          }
+          at -= nj;
+        }
+      }
+      const V3<R> zp = c.z;
+      if (have) c = step_kind(k, c, pos, pp);
+      if (c.z.x != zp.x || c.z.y != zp.y || c.z.z != zp.z) ++changed;
+      trap_update(acc, in.trap, c.z, zp, it);
+    }
+    DE<R> o;
+    o.d = finalize_kind(kind[slot], c);
+    o.trap = trap_finish(acc, in.trap, total);
+    o.iters = changed;
+    return o;
+  }
+
+  DE<R> instance(int slot, V3<R> pos) const {
+    const nd_instance_desc& in = scene->instances[slot];
+    R s[3], mag_min = R(1e30);
+    for (int i = 0; i < 3; ++i) {
+      const R mag = std::fmax(std::fabs(R(in.scale[i])), R(0.001));
+      s[i] = in.scale[i] < 0.0f ? -mag : mag;
+      mag_min = std::fmin(mag_min, mag);
+    }
+    const R factor = mag_min * clampv(R(in.step_safety), R(0.001), R(1));
+    const V3<R> d = pos - V3<R>(R(in.offset[0]), R(in.offset[1]), R(in.offset[2]));
+    R f[9];  // frame columns: local_i = (column_i . d) / s_i
+    for (int i = 0; i < 9; ++i) f[i] = R(in.frame[i]);
+    const V3<R> local((f[0] * d.x + f[1] * d.y + f[2] * d.z) / s[0], (f[3] * d.x + f[4] * d.y + f[5] * d.z) / s[1],
+                      (f[6] * d.x + f[7] * d.y + f[8] * d.z) / s[2]);
+    DE<R> o;
+    if (in.mixin_count > 0) {
+      o = mixed(in, slot, local);
+    } else {
+      R p[ND_MAX_PARAMS];
+      for (int k = 0; k < ND_MAX_PARAMS; ++k) p[k] = R(in.params[k]);
+      o = eval_de<R>(kind[slot], local, p, in.trap, R(1));
+    }
+    o.d = o.d * factor;
+    return o;
+  }
+
+  DE<R> de(V3<R> pos) const {
+    const R empty = R(float(max_dist) * 2.0f + 1.0f);  // empty_scene_de
+    DE<R> o{empty, R(0), 0};
+    R d = empty, best = R(0);
+    bool first = true;
+    const int count = std::min(std::max(scene->instance_count, 1), ND_MAX_INSTANCES);
+    for (int i = 0; i < count; ++i) {
+      const nd_instance_desc& in = scene->instances[i];
+      if (in.hidden) continue;
+      const DE<R> di = instance(i, pos);
+      if (first || di.d < best) {
+        best = di.d;
+        o.trap = di.trap;
+        o.iters = di.iters;
+      }
+      d = first ? di.d : combine<R>(in.combine_mode, d, di.d, R(in.blend_k));
+      first = false;
+    }
+    if (first) return DE<R>{empty, R(0), 0};
+    const int carves = std::min(std::max(scene->carve_count, 0), ND_MAX_CARVES);
+    for (int i = 0; i < carves; ++i) {
+      const float* c = scene->carves[i];
+      const R r = R(c[3]);
+      const R l = len(pos - V3<R>(R(c[0]), R(c[1]), R(c[2])));
+      d = s_sub(l - r, d, R(0.2) * r);
+    }
+    o.d = d;
+    return o;
+  }
+};
+
 // ------------------------------------------------------------------ per-ray result
 struct RayOut {
   double depth;       // t at the hit, 0 on a miss
@@ -343,6 +525,7 @@ template <class R> struct Tracer {
   V3<double> org;
   uint32_t evals = 0;
   double de_scale = 1.0;  // every DE value is multiplied by this (stability probes)
+  const SceneEval<R>* scene = nullptr;  // a multi-instance scene instead of the view's formula
 
   Tracer(const nd_view_desc& view, int k) : v(view), kind(k) {
     for (int i = 0; i < ND_MAX_PARAMS; ++i) p[i] = R(view.params[i]);
@@ -352,7 +535,8 @@ template <class R> struct Tracer {
 
   DE<R> de_at(V3<double> pos) {
     ++evals;
-    DE<R> o = eval_de<R>(kind, V3<R>(R(pos.x), R(pos.y), R(pos.z)), p, v.trap, factor);
+    const V3<R> q(R(pos.x), R(pos.y), R(pos.z));
+    DE<R> o = scene ? scene->de(q) : eval_de<R>(kind, q, p, v.trap, factor);
     if (de_scale != 1.0) o.d = R(double(o.d) * de_scale);
     return o;
   }

@@ -8,6 +8,25 @@
 
 using namespace oracle;
 
+static void write_ray(const RayOut& o, int64_t i, float* depth, float* normal4, float* trap, uint32_t* steps,
+                      uint32_t* iters, float* shade, float* shadow, double* depth64, uint32_t* evals, double* margin) {
+  if (depth) depth[i] = float(o.depth);
+  if (depth64) depth64[i] = o.depth;
+  if (normal4) {
+    normal4[4 * i] = float(o.normal[0]);
+    normal4[4 * i + 1] = float(o.normal[1]);
+    normal4[4 * i + 2] = float(o.normal[2]);
+    normal4[4 * i + 3] = o.hit ? 1.0f : 0.0f;
+  }
+  if (trap) trap[i] = float(o.trap);
+  if (steps) steps[i] = o.steps;
+  if (iters) iters[i] = o.iters;
+  if (shade) shade[i] = float(o.shade);
+  if (shadow) shadow[i] = float(o.shadow);
+  if (evals) evals[i] = o.evals;
+  if (margin) margin[i] = o.margin;
+}
+
 extern "C" {
 
 int oracle_formula_index(const char* name) { return formula_index(name); }
@@ -61,21 +80,75 @@ int oracle_render(const nd_view_desc* view, const char* formula_name, int precis
 #pragma omp for schedule(dynamic, 64)
     for (int64_t i = 0; i < n; ++i) {
       const RayOut o = precision == 32 ? tf.trace(first + i) : td.trace(first + i);
-      if (depth) depth[i] = float(o.depth);
-      if (depth64) depth64[i] = o.depth;
-      if (normal4) {
-        normal4[4 * i] = float(o.normal[0]);
-        normal4[4 * i + 1] = float(o.normal[1]);
-        normal4[4 * i + 2] = float(o.normal[2]);
-        normal4[4 * i + 3] = o.hit ? 1.0f : 0.0f;
-      }
-      if (trap) trap[i] = float(o.trap);
-      if (steps) steps[i] = o.steps;
-      if (iters) iters[i] = o.iters;
-      if (shade) shade[i] = float(o.shade);
-      if (shadow) shadow[i] = float(o.shadow);
-      if (evals) evals[i] = o.evals;
-      if (margin) margin[i] = o.margin;
+      write_ray(o, i, depth, normal4, trap, steps, iters, shade, shadow, depth64, evals, margin);
+    }
+  }
+  return 0;
+}
+
+static int scene_kinds(const int32_t* kinds, const int32_t* mixin_kinds, SceneEval<float>& sf, SceneEval<double>& sd) {
+  for (int i = 0; i < ND_MAX_INSTANCES; ++i) {
+    if (kinds[i] < 0 || kinds[i] >= F_COUNT) return -1;
+    sf.kind[i] = sd.kind[i] = kinds[i];
+    for (int j = 0; j < ND_MAX_MIXINS; ++j) {
+      const int k = mixin_kinds[i * ND_MAX_MIXINS + j];
+      if (k < 0 || k >= F_COUNT) return -1;
+      sf.mkind[i][j] = sd.mkind[i][j] = k;
+    }
+  }
+  return 0;
+}
+
+// The scene DE (and nearest instance's trap and changed-iteration count) at n points.
+int oracle_scene_de(const nd_scene_desc* scene, const int32_t* kinds, const int32_t* mixin_kinds, double max_dist,
+                    int precision, int64_t n, const double* pts, double* de, double* trap_out, int32_t* iters) {
+  SceneEval<float> sf;
+  SceneEval<double> sd;
+  sf.scene = sd.scene = scene;
+  sf.max_dist = sd.max_dist = max_dist;
+  if (scene_kinds(kinds, mixin_kinds, sf, sd) != 0) return -1;
+  for (int64_t i = 0; i < n; ++i) {
+    double d, t;
+    int it;
+    if (precision == 32) {
+      const DE<float> r = sf.de(V3<float>(float(pts[3 * i]), float(pts[3 * i + 1]), float(pts[3 * i + 2])));
+      d = r.d; t = r.trap; it = r.iters;
+    } else {
+      const DE<double> r = sd.de(V3<double>(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]));
+      d = r.d; t = r.trap; it = r.iters;
+    }
+    de[i] = d;
+    if (trap_out) trap_out[i] = t;
+    if (iters) iters[i] = it;
+  }
+  return 0;
+}
+
+// Trace rays [first, first + n) of one view against a multi-instance scene.  kinds
+// holds the oracle formula kind of each instance, mixin_kinds those of each
+// instance's mixins (row-major [instance][mixin]).  Outputs as oracle_render.
+int oracle_render_scene(const nd_view_desc* view, const nd_scene_desc* scene, const int32_t* kinds,
+                        const int32_t* mixin_kinds, int precision, int nthreads, int64_t first, int64_t n,
+                        float* depth, float* normal4, float* trap, uint32_t* steps, uint32_t* iters, float* shade,
+                        float* shadow, double* depth64, uint32_t* evals, double* margin, double de_scale) {
+  SceneEval<float> sf;
+  SceneEval<double> sd;
+  sf.scene = sd.scene = scene;
+  sf.max_dist = sd.max_dist = view->max_dist;
+  if (scene_kinds(kinds, mixin_kinds, sf, sd) != 0) return -1;
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel num_threads(nthreads)
+  {
+    Tracer<float> tf(*view, kinds[0]);
+    Tracer<double> td(*view, kinds[0]);
+    tf.de_scale = de_scale;
+    td.de_scale = de_scale;
+    tf.scene = &sf;
+    td.scene = &sd;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i) {
+      const RayOut o = precision == 32 ? tf.trace(first + i) : td.trace(first + i);
+      write_ray(o, i, depth, normal4, trap, steps, iters, shade, shadow, depth64, evals, margin);
     }
   }
   return 0;

@@ -16,15 +16,16 @@ _LIB = None
 def lib():
     global _LIB
     if _LIB is None:
-        path = os.path.join(HERE, "_build", "liboracle.so")
-        if not os.path.exists(path):
-            from . import build_oracle
-            build_oracle.build()
+        from . import build_oracle
+        path = build_oracle.build()  # rebuilt only when a source is newer than the library
         _LIB = C.CDLL(path)
         _LIB.oracle_formula_index.argtypes = [C.c_char_p]
         _LIB.oracle_de.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p]
         _LIB.oracle_render.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_int64, C.c_int64] + [C.c_void_p] * 10 + [C.c_double]
+        _LIB.oracle_render_scene.argtypes = ([C.c_void_p] * 4 + [C.c_int, C.c_int, C.c_int64, C.c_int64]
+                                             + [C.c_void_p] * 10 + [C.c_double])
+        _LIB.oracle_scene_de.argtypes = ([C.c_void_p] * 3 + [C.c_double, C.c_int, C.c_int64] + [C.c_void_p] * 4)
         _LIB.oracle_max_threads.restype = C.c_int
     return _LIB
 
@@ -52,26 +53,32 @@ def de(name: str, params, pts, precision=64, trap: abi.nd_trap_desc | None = Non
     return out, tr, it
 
 
-def render(view: abi.nd_view_desc, formula_name: str, precision=64, nthreads=0, first=0, n=None, de_scale=1.0):
-    """Trace rays [first, first+n) of one view; returns a dict of numpy arrays."""
-    total = abi.rays_of(view)
-    if n is None:
-        n = total - first
-    out = {
+STABILITY_DELTA = 1e-4
+_KEYS = ["depth", "normal", "trap", "steps", "iters", "shade", "shadow", "depth64", "evals", "margin"]
+
+
+def _outputs(n):
+    return {
         "depth": np.zeros(n, np.float32), "normal": np.zeros((n, 4), np.float32), "trap": np.zeros(n, np.float32),
         "steps": np.zeros(n, np.uint32), "iters": np.zeros(n, np.uint32), "shade": np.zeros(n, np.float32),
         "shadow": np.zeros(n, np.float32), "depth64": np.zeros(n, np.float64), "evals": np.zeros(n, np.uint32),
         "margin": np.zeros(n, np.float64),
     }
-    keys = ["depth", "normal", "trap", "steps", "iters", "shade", "shadow", "depth64", "evals", "margin"]
+
+
+def render(view: abi.nd_view_desc, formula_name: str, precision=64, nthreads=0, first=0, n=None, de_scale=1.0):
+    """Trace rays [first, first+n) of one view; returns a dict of numpy arrays."""
+    total = abi.rays_of(view)
+    if n is None:
+        n = total - first
+    out = _outputs(n)
     rc = lib().oracle_render(C.addressof(view), formula_name.encode(), precision, nthreads, first, n,
-                             *[out[k].ctypes.data for k in keys], de_scale)
+                             *[out[k].ctypes.data for k in _KEYS], de_scale)
     if rc != 0:
         raise ValueError(f"oracle has no formula {formula_name!r}")
     return out
 
 
-STABILITY_DELTA = 1e-4
 
 
 def unstable_rays(view: abi.nd_view_desc, formula_name: str, delta: float = STABILITY_DELTA, nthreads=0):
@@ -81,6 +88,66 @@ def unstable_rays(view: abi.nd_view_desc, formula_name: str, delta: float = STAB
     base = render(view, formula_name, 64, nthreads)
     lo = render(view, formula_name, 64, nthreads, de_scale=1.0 - delta)
     hi = render(view, formula_name, 64, nthreads, de_scale=1.0 + delta)
+    h = [o["normal"][:, 3] > 0.5 for o in (base, lo, hi)]
+    unstable = (h[0] != h[1]) | (h[0] != h[2])
+    unstable |= (base["steps"] != lo["steps"]) | (base["steps"] != hi["steps"])
+    return unstable, base
+
+
+def _scene_kinds(scene: abi.nd_scene_desc, names):
+    """Oracle formula kinds of a scene's instances and mixins; names maps a formula
+    id to its formula name."""
+    def kind(fid):
+        k = lib().oracle_formula_index(names(fid).encode())
+        if k < 0:
+            raise ValueError(f"oracle has no formula {names(fid)!r}")
+        return k
+
+    kinds = np.zeros(abi.ND_MAX_INSTANCES, np.int32)
+    mk = np.zeros((abi.ND_MAX_INSTANCES, abi.ND_MAX_MIXINS), np.int32)
+    for i in range(scene.instance_count):
+        inst = scene.instances[i]
+        kinds[i] = kind(inst.formula)
+        for j in range(inst.mixin_count):
+            mk[i, j] = kind(inst.mixins[j].formula)
+    return kinds, mk
+
+
+def scene_de(scene: abi.nd_scene_desc, names, pts, max_dist=24.0, precision=64):
+    """The scene DE, nearest instance's trap and changed-iteration count at points."""
+    kinds, mk = _scene_kinds(scene, names)
+    pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    n = pts.shape[0]
+    out, tr, it = np.zeros(n, np.float64), np.zeros(n, np.float64), np.zeros(n, np.int32)
+    rc = lib().oracle_scene_de(C.addressof(scene), kinds.ctypes.data, mk.ctypes.data, max_dist, precision, n,
+                               pts.ctypes.data, out.ctypes.data, tr.ctypes.data, it.ctypes.data)
+    if rc != 0:
+        raise ValueError("oracle_scene_de refused the scene")
+    return out, tr, it
+
+
+def render_scene(view: abi.nd_view_desc, scene: abi.nd_scene_desc, names, precision=64, nthreads=0, first=0, n=None,
+                 de_scale=1.0):
+    """Trace rays of one view against a multi-instance scene; names maps a formula id
+    to its formula name (the ids the instances and mixins use)."""
+    kinds, mk = _scene_kinds(scene, names)
+    total = abi.rays_of(view)
+    if n is None:
+        n = total - first
+    out = _outputs(n)
+    rc = lib().oracle_render_scene(C.addressof(view), C.addressof(scene), kinds.ctypes.data, mk.ctypes.data,
+                                   precision, nthreads, first, n, *[out[k].ctypes.data for k in _KEYS], de_scale)
+    if rc != 0:
+        raise ValueError("oracle_render_scene refused the scene")
+    return out
+
+
+def unstable_scene_rays(view: abi.nd_view_desc, scene: abi.nd_scene_desc, names, delta: float = STABILITY_DELTA,
+                        nthreads=0):
+    """unstable_rays for a view rendered against a multi-instance scene."""
+    base = render_scene(view, scene, names, 64, nthreads)
+    lo = render_scene(view, scene, names, 64, nthreads, de_scale=1.0 - delta)
+    hi = render_scene(view, scene, names, 64, nthreads, de_scale=1.0 + delta)
     h = [o["normal"][:, 3] > 0.5 for o in (base, lo, hi)]
     unstable = (h[0] != h[1]) | (h[0] != h[2])
     unstable |= (base["steps"] != lo["steps"]) | (base["steps"] != hi["steps"])
