@@ -54,7 +54,7 @@
 extern "C" {
 #endif
 
-#define ND_ABI_VERSION 1
+#define ND_ABI_VERSION 2
 #define ND_MAX_PARAMS 16          /* fractal_renderer.zig:47 */
 #define ND_PARAM_NAME_LEN 24      /* CustomParam.name [24:0]u8, formula.zig:7 */
 
@@ -143,13 +143,16 @@ typedef struct nd_view_desc {
   float shadow_k;         /* soft-shadow sharpness k */
   float step_safety;      /* instance step safety, clamped to [0.001, 1] */
   int32_t flags;          /* ND_VIEW_* bits */
-  int32_t reserved[3];
+  /* Empty-space accelerator (cs_build_accel template.wgsl:5412-5431, accel_skip
+   * :428-447, cascade placement src/gpu/accel.zig:32-56): a camera-centred cascade of
+   * accel_levels grids of accel_res^3 safe skip distances, built by the library for
+   * this view before its march.  accel_res 0 = off; otherwise clamped to 16..160 and
+   * rounded down to a multiple of 4, levels to 1..8 (reference defaults 64, 6, 0.92). */
+  int32_t accel_res;
+  int32_t accel_levels;
+  float accel_safety;     /* every recorded skip is multiplied by this */
 } nd_view_desc;
 
-/* G-buffer of one forward call.  Rays of view v occupy [ray_offset(v), +rays(v)),
- * views in call order; rays(v) = spp * tile_w * tile_h and the ray index inside a
- * view is sample * tile_w * tile_h + y * tile_w + x.  Every pointer may be NULL
- * except depth. */
 /* A scene of up to four fractal instances combined by distance (scene_de,
  * template.wgsl:1756-1779), each with its own formula, parameters, placement
  * (instance_local: transpose(frame) * (p - offset) / scale, tpl:1611-1615; DE factor
@@ -202,6 +205,10 @@ typedef struct nd_scene_desc {
   float carves[ND_MAX_CARVES][4];  /* sphere centre xyz, radius w */
 } nd_scene_desc;
 
+/* G-buffer of one forward call.  Rays of view v occupy [ray_offset(v), +rays(v)),
+ * views in call order; rays(v) = spp * tile_w * tile_h and the ray index inside a
+ * view is sample * tile_w * tile_h + y * tile_w + x.  Every pointer may be NULL
+ * except depth. */
 typedef struct nd_gbuffer {
   float* depth;       /* t at the hit, 0 on a miss (R32F depth target) */
   float* normal;      /* 4 floats per ray: unit normal, w = 1 on a hit */
@@ -240,6 +247,8 @@ typedef struct nd_stats {
   double march_ms;          /* device time of the march kernels of the last nd_march_forward
                                (CUDA events on its stream; 0 after a graph launch) */
   double shade_ms;          /* device time of its shade passes (normals, shadows, orbit trap) */
+  uint64_t accel_voxels;    /* accelerator grid cells built (one DE evaluation each, not in de_evals) */
+  double accel_ms;          /* device time of the accelerator grid builds */
 } nd_stats;
 
 typedef struct nd_tune_result {
@@ -352,6 +361,15 @@ nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t nviews, co
  * fractal_renderer.zig:490-512) in FP32 (de_precision 32) or FP64 (64). */
 nd_status nd_de_points(nd_ctx* ctx, const nd_view_desc* view, int64_t n, const double* pts, double* de,
                        double* trap, uint32_t* iters, int32_t de_precision, void* stream);
+
+/* The empty-space accelerator grid of one view (its own formula; accel_res > 0),
+ * as nd_march_forward builds it before the view's march (cs_build_accel,
+ * template.wgsl:5412-5431): grid is a DEVICE array of capacity floats that receives
+ * levels * res^3 safe skip distances ([level][z][y][x]); prm (HOST, 32 floats)
+ * receives the cascade placement (corner xyz, cell size per cascade, zeros past the
+ * last); *count the number of floats.  Synchronous. */
+nd_status nd_accel_grid(nd_ctx* ctx, const nd_view_desc* view, int32_t de_precision, float* grid, int64_t capacity,
+                        float* prm, int64_t* count);
 
 /* Size of a public struct by name ("nd_view_desc", ...), for binding layout checks. */
 size_t nd_sizeof(const char* name);

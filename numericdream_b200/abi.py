@@ -46,7 +46,7 @@ class nd_view_desc(C.Structure):
         ("refine_budget", C.c_int32), ("march_verify", C.c_int32), ("high_quality", C.c_int32),
         ("hq_footprint_px", C.c_float), ("normal_mode", C.c_int32), ("normal_h_coef", C.c_float),
         ("shadow", C.c_int32), ("light_dir", C.c_float * 3), ("shadow_k", C.c_float), ("step_safety", C.c_float),
-        ("flags", C.c_int32), ("reserved", C.c_int32 * 3),
+        ("flags", C.c_int32), ("accel_res", C.c_int32), ("accel_levels", C.c_int32), ("accel_safety", C.c_float),
     ]
 
 
@@ -155,7 +155,8 @@ class nd_stats(C.Structure):
                 ("normal_evals", C.c_uint64), ("shadow_evals", C.c_uint64), ("trap_evals", C.c_uint64),
                 ("hits", C.c_uint64),
                 ("refills", C.c_uint64), ("timeouts", C.c_uint32), ("kernel", C.c_uint32),
-                ("march_ms", C.c_double), ("shade_ms", C.c_double)]
+                ("march_ms", C.c_double), ("shade_ms", C.c_double), ("accel_voxels", C.c_uint64),
+                ("accel_ms", C.c_double)]
 
 
 class nd_tune_result(C.Structure):
@@ -241,6 +242,9 @@ def make_view(formula: int, width: int, height: int, cam_pos, target=(0.0, 0.0, 
     v.shadow = 0
     v.shadow_k = 16.0
     v.step_safety = 1.0
+    v.accel_res = 0          # empty-space accelerator off; the reference's defaults otherwise
+    v.accel_levels = 6
+    v.accel_safety = 0.92
     for k, val in kw.items():
         if k == "trap":
             for tk, tv in val.items():

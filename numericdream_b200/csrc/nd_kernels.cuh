@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value) plain_kernel(const _
 // tpl:5083-5105), and a warp keeps marching neighbouring pixels.  Whatever phase
 // a lane is in, each pass of the loop is one DE evaluation for every busy lane.
 
-template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false>
+template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, bool kAccel = false>
 __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     persistent_kernel(const __grid_constant__ LaunchArgs a, const __grid_constant__ DevView single) {
   const unsigned full = 0xffffffffu;
@@ -196,8 +196,15 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     }
     if (L.item >= 0 && L.phase != PH_DONE) {
       const DevView& v = kBatched ? a.views[L.view] : single;
-      const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(L.sample_pos(v)), a.scenes);
-      L.advance(v, de, a.out, a.t_hit, defer);
+      if constexpr (kAccel) {
+        // the accelerator's jumps come before the probe, so that every pass of this
+        // loop still ends in one DE evaluation per busy lane
+        if (L.phase == PH_MARCH && L.probing && v.accel_levels > 0) L.accel_skips(v, a.out, a.t_hit);
+      }
+      if (L.phase != PH_DONE) {
+        const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(L.sample_pos(v)), a.scenes);
+        L.advance(v, de, a.out, a.t_hit, defer);
+      }
     }
   }
   flush_stats(a.stats, rays, ev_m, ev_n, ev_s, hits, refills);
@@ -209,7 +216,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
 // every listed hit (the shadow rays' step counts differ, the rest is coherent);
 // without one (the plain kernel) the orbit trap of every ray that hit.  It strides
 // over its work with a resident grid.
-template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false>
+template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, bool kAccel = false>
 __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     shade_kernel(const __grid_constant__ LaunchArgs a, const __grid_constant__ DevView single, int do_trap) {
   const bool list = a.hit_list != nullptr;
@@ -224,7 +231,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     const double t = a.t_hit[v.out_offset + local];
     if (t < 0.0) continue;  // a miss (all-rays mode); the march wrote its outputs
     if (list) {
-      const uint32_t ev = shade_at_hit<Set, T, kDir64, kScenes>(v, local, t, a.out, a.scenes);
+      const uint32_t ev = shade_at_hit<Set, T, kDir64, kScenes, kAccel>(v, local, t, a.out, a.scenes);
       taps += ev & 0xffffu;
       shadow += ev >> 16;
     }
@@ -260,13 +267,13 @@ cudaError_t launch_plain(const LaunchArgs& a, const DevView& single, const Launc
   return cudaGetLastError();
 }
 
-template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false>
+template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, bool kAccel = false>
 cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const LaunchConfig& c, cudaStream_t s) {
   const int block = 128;
   int per_sm = c.blocks_per_sm;
   if (per_sm <= 0) {
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, persistent_kernel<Set, T, kDir64, kBatched, kScenes>, block, 0);
+        &per_sm, persistent_kernel<Set, T, kDir64, kBatched, kScenes, kAccel>, block, 0);
     if (e != cudaSuccess) return e;
     if (per_sm <= 0) per_sm = 1;
   }
@@ -279,28 +286,81 @@ cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const 
   LaunchArgs b = a;
   const int64_t warps = grid * (block / 32);
   b.chunk = int32_t(std::max<int64_t>(1, std::min<int64_t>(64, a.total_rays / (warps * 4))));
-  persistent_kernel<Set, T, kDir64, kBatched, kScenes><<<unsigned(grid), block, 0, s>>>(b, single);
+  persistent_kernel<Set, T, kDir64, kBatched, kScenes, kAccel><<<unsigned(grid), block, 0, s>>>(b, single);
   return cudaGetLastError();
 }
 
 typedef cudaError_t (*LaunchFn)(const LaunchArgs&, const DevView&, const LaunchConfig&, cudaStream_t);
 
-template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false>
+template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, bool kAccel = false>
 cudaError_t launch_shade(const LaunchArgs& a, const DevView& single, const LaunchConfig& c, int do_trap,
                          cudaStream_t s) {
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shade_kernel<Set, T, kDir64, kBatched, kScenes>,
-                                                                128, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, shade_kernel<Set, T, kDir64, kBatched, kScenes, kAccel>, 128, 0);
   if (e != cudaSuccess) return e;
   int64_t grid = int64_t(std::max(per_sm, 1)) * c.num_sms;
   const int64_t needed = (a.total_rays + 127) / 128;
   if (grid > needed) grid = needed;
   if (grid <= 0) return cudaSuccess;
-  shade_kernel<Set, T, kDir64, kBatched, kScenes><<<unsigned(grid), 128, 0, s>>>(a, single, do_trap);
+  shade_kernel<Set, T, kDir64, kBatched, kScenes, kAccel><<<unsigned(grid), 128, 0, s>>>(a, single, do_trap);
   return cudaGetLastError();
 }
 
 typedef cudaError_t (*ShadeFn)(const LaunchArgs&, const DevView&, const LaunchConfig&, int, cudaStream_t);
+
+// --------------------------------------------------------------- accelerator build
+// cs_build_accel (tpl:5412-5431): one thread per voxel of every accelerated view of
+// a launch; the DE the view's rays see at the voxel centre, less the half diagonal of
+// the cell, times the safety factor, floored at 0.  jobs[j] = (view index, first
+// voxel) in voxel order; a view's voxels are [level][z][y][x] of its grid.  The
+// centre and the skip are rounded step by step (no contraction), like the CPU
+// restatement.
+struct AccelJob {
+  int32_t view;
+  int32_t pad;
+  int64_t begin;
+};
+
+template <class Set, class T, bool kScenes>
+__global__ void __launch_bounds__(128) accel_build_kernel(const DevView* __restrict__ views,
+                                                          const AccelJob* __restrict__ jobs, int njobs, int64_t total,
+                                                          const DevScene* scenes) {
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += stride) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].begin <= i) lo = mid;
+      else hi = mid - 1;
+    }
+    const DevView& v = views[jobs[lo].view];
+    const uint32_t local = uint32_t(i - jobs[lo].begin);  // < 8 * 160^3
+    const uint32_t r = uint32_t(v.accel_res);
+    const uint32_t x = local % r, y = (local / r) % r, gz = local / (r * r);
+    const uint32_t l = gz / r, z = gz % r;
+    const float cell = v.accel_prm[l][3];
+    const float cx = __fadd_rn(v.accel_prm[l][0], __fmul_rn(__fadd_rn(float(x), 0.5f), cell));
+    const float cy = __fadd_rn(v.accel_prm[l][1], __fmul_rn(__fadd_rn(float(y), 0.5f), cell));
+    const float cz = __fadd_rn(v.accel_prm[l][2], __fmul_rn(__fadd_rn(float(z), 0.5f), cell));
+    const DEOut<T> de = view_de<Set, T, false, kScenes>(v, ndw::v3<T>(T(cx), T(cy), T(cz)), scenes);
+    const float d = float(de.d);
+    const float safe = fmaxf(__fsub_rn(d, __fmul_rn(0.8660254f, cell)), 0.0f);  // HALF_SQRT3 tpl:62
+    v.accel_grid[local] = __fmul_rn(safe, v.accel_safety);
+  }
+}
+
+template <class Set, class T, bool kScenes>
+cudaError_t launch_accel_build(const DevView* views, const AccelJob* jobs, int njobs, int64_t total,
+                               const DevScene* scenes, int num_sms, cudaStream_t s) {
+  if (total <= 0 || njobs <= 0) return cudaSuccess;
+  int64_t grid = (total + 127) / 128;
+  grid = std::min<int64_t>(grid, int64_t(num_sms) * 16);
+  accel_build_kernel<Set, T, kScenes><<<unsigned(grid), 128, 0, s>>>(views, jobs, njobs, total, scenes);
+  return cudaGetLastError();
+}
+
+typedef cudaError_t (*AccelBuildFn)(const DevView*, const AccelJob*, int, int64_t, const DevScene*, int, cudaStream_t);
 
 // DE of one formula at n points (the formula wrapper with its orbit trap), for
 // parity tests against fixed point sets.
@@ -341,6 +401,14 @@ struct KernelTable {
   // multi-instance scenes (formula groups only; null in single-formula tables)
   LaunchFn scene_persistent_f32, scene_persistent_f32_dir64, scene_persistent_f64;
   ShadeFn scene_shade_f32, scene_shade_f32_dir64, scene_shade_f64;
+  // empty-space accelerator: its grid build and the batched march / shade pass that
+  // read it (FP32 directions or FP64 DE), without and with scenes
+  AccelBuildFn accel_build_f32, accel_build_f64;
+  LaunchFn persistent_f32_accel, persistent_f64_accel;
+  ShadeFn shade_f32_accel, shade_f64_accel;
+  AccelBuildFn scene_accel_build_f32, scene_accel_build_f64;
+  LaunchFn scene_persistent_f32_accel, scene_persistent_f64_accel;
+  ShadeFn scene_shade_f32_accel, scene_shade_f64_accel;
 };
 
 template <class Set, bool kWithScenes = false> KernelTable make_kernel_table() {
@@ -352,10 +420,25 @@ template <class Set, bool kWithScenes = false> KernelTable make_kernel_table() {
     t.scene_shade_f32 = &launch_shade<Set, float, false, true, true>;
     t.scene_shade_f32_dir64 = &launch_shade<Set, float, true, true, true>;
     t.scene_shade_f64 = &launch_shade<Set, double, true, true, true>;
+    t.scene_accel_build_f32 = &launch_accel_build<Set, float, true>;
+    t.scene_accel_build_f64 = &launch_accel_build<Set, double, true>;
+    t.scene_persistent_f32_accel = &launch_persistent<Set, float, false, true, true, true>;
+    t.scene_persistent_f64_accel = &launch_persistent<Set, double, true, true, true, true>;
+    t.scene_shade_f32_accel = &launch_shade<Set, float, false, true, true, true>;
+    t.scene_shade_f64_accel = &launch_shade<Set, double, true, true, true, true>;
   } else {
     t.scene_persistent_f32 = t.scene_persistent_f32_dir64 = t.scene_persistent_f64 = nullptr;
     t.scene_shade_f32 = t.scene_shade_f32_dir64 = t.scene_shade_f64 = nullptr;
+    t.scene_accel_build_f32 = t.scene_accel_build_f64 = nullptr;
+    t.scene_persistent_f32_accel = t.scene_persistent_f64_accel = nullptr;
+    t.scene_shade_f32_accel = t.scene_shade_f64_accel = nullptr;
   }
+  t.accel_build_f32 = &launch_accel_build<Set, float, false>;
+  t.accel_build_f64 = &launch_accel_build<Set, double, false>;
+  t.persistent_f32_accel = &launch_persistent<Set, float, false, true, false, true>;
+  t.persistent_f64_accel = &launch_persistent<Set, double, true, true, false, true>;
+  t.shade_f32_accel = &launch_shade<Set, float, false, true, false, true>;
+  t.shade_f64_accel = &launch_shade<Set, double, true, true, false, true>;
   t.plain_f32 = &launch_plain<Set, float, false>;
   t.plain_f32_dir64 = &launch_plain<Set, float, true>;
   t.plain_f64 = &launch_plain<Set, double, true>;

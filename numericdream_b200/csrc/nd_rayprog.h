@@ -40,6 +40,8 @@ ND_DEV_INLINE float rn_add(float a, float b) { return __fadd_rn(a, b); }
 ND_DEV_INLINE double rn_mul(double a, double b) { return __dmul_rn(a, b); }
 ND_DEV_INLINE double rn_add(double a, double b) { return __dadd_rn(a, b); }
 ND_DEV_INLINE double fma_d(double a, double b, double c) { return __fma_rn(a, b, c); }
+ND_DEV_INLINE float rn_div(float a, float b) { return __fdiv_rn(a, b); }
+ND_DEV_INLINE float load_ro(const float* p) { return __ldg(p); }
 #else
 // host builds of this header are compiled with -ffp-contract=off
 ND_DEV_INLINE float rn_mul(float a, float b) { return a * b; }
@@ -47,6 +49,8 @@ ND_DEV_INLINE float rn_add(float a, float b) { return a + b; }
 ND_DEV_INLINE double rn_mul(double a, double b) { return a * b; }
 ND_DEV_INLINE double rn_add(double a, double b) { return a + b; }
 ND_DEV_INLINE double fma_d(double a, double b, double c) { return ::fma(a, b, c); }
+ND_DEV_INLINE float rn_div(float a, float b) { return a / b; }
+ND_DEV_INLINE float load_ro(const float* p) { return *p; }
 #endif
 
 constexpr int kMaxIterations = 4096;   // watchdog cap on de_iterations()
@@ -57,6 +61,8 @@ constexpr double kShadowMinStep = 0.001;
 constexpr double kSimpleAmbient = 0.18;  // SIMPLE_AMBIENT tpl:4418
 
 // Per-view record the kernels read (built on the host from nd_view_desc).
+constexpr int kAccelMaxCascades = 8;  // MAX_CASCADES tpl:31, accel.zig:8
+
 struct DevView {
   double org[3];
   double fwd[3];
@@ -83,7 +89,13 @@ struct DevView {
   int32_t user_index;   // the view's index in the caller's array
   int32_t exact_hit;    // bisect for the whole budget (ND_VIEW_EXACT_HIT)
   int32_t scene;        // index into the launch's scene table, -1: the single instance above
-  int32_t pad;
+  // empty-space accelerator of this view (accel_levels 0: none): cascade l covers
+  // accel_res^3 cells of size accel_prm[l][3] from corner accel_prm[l][0..2]
+  int32_t accel_levels;
+  int32_t accel_res;
+  float accel_safety;
+  float* accel_grid;    // [level][z][y][x] safe skip distances
+  float accel_prm[kAccelMaxCascades][4];
 };
 
 struct Stats {
@@ -475,6 +487,24 @@ template <> ND_DEV_INLINE double march_eps<double>(const DevView& v, double t) {
   return rn_add(rn_mul(double(v.eps_coef), t), double(v.eps_floor));
 }
 
+// accel_skip (tpl:428-447): the safe skip recorded for the finest cascade cell that
+// holds p, 0 outside every cascade.  The cell index uses IEEE division, as the
+// reference's f32 `/` and the CPU restatement do.
+ND_DEV_INLINE float accel_skip(const DevView& v, float px, float py, float pz) {
+  const float rf = float(v.accel_res);
+  for (int l = 0; l < v.accel_levels; ++l) {
+    const float cell = v.accel_prm[l][3];
+    if (!(cell > 0.0f)) continue;
+    const float fx = floorf(rn_div(px - v.accel_prm[l][0], cell));
+    const float fy = floorf(rn_div(py - v.accel_prm[l][1], cell));
+    const float fz = floorf(rn_div(pz - v.accel_prm[l][2], cell));
+    if (!(fx >= 0.0f && fy >= 0.0f && fz >= 0.0f && fx < rf && fy < rf && fz < rf)) continue;
+    const int r = v.accel_res;
+    return load_ro(v.accel_grid + ((int64_t(l) * r + int(fz)) * r + int(fy)) * r + int(fx));
+  }
+  return 0.0f;
+}
+
 // Primary ray of a work item: cs_wf_generate tpl:5120-5127 / fs_simple tpl:4523-4525
 // with the tile transform (fractal_renderer.zig:852-863) folded into frame pixels.
 // (ux, uy): the camera-plane coordinates of the ray, direction = fwd + ux right + uy up.
@@ -674,6 +704,27 @@ template <class T, bool kDir64> struct Lane {
     return fmadd(so, d3(v.light[0], v.light[1], v.light[2]), a);
   }
 
+  // The accelerator's jumps before a probe (march_to tpl:1890-1900): while the
+  // recorded skip at the probe position exceeds eps(t), advance without a DE
+  // evaluation; each jump is a step and a sample of march_to's loop.  May end the
+  // ray (a miss).
+  ND_DEV_INLINE void accel_skips(const DevView& v, const nd_gbuffer& g, double* t_hit) {
+    const D3 o = d3(v.org[0], v.org[1], v.org[2]);
+    while (true) {
+      const D3 p = fmadd(o, dir.get(), t);
+      const double skip = double(accel_skip(v, float(p.x), float(p.y), float(p.z)));
+      if (!(skip > march_eps<T>(v, t))) return;
+      a = t;
+      t = t + skip;
+      ++i;
+      ++n;
+      if (t > v.max_dist || i >= v.max_steps || n >= v.max_samples) {
+        finish(v, g, t_hit, 1.0f);
+        return;
+      }
+    }
+  }
+
   ND_DEV_INLINE void finish(const DevView& v, const nd_gbuffer& g, double* t_hit, float visibility) {
     if (!hit) mev = evals;
     phase = PH_DONE;
@@ -864,7 +915,7 @@ ND_DEV_INLINE void trap_at_hit(const DevView& v, int64_t local, double t, const 
 // phase), the shadow ray when the view has one (the steps of PH_SHADOW), and the
 // Lambert level.  Adds the evaluations to the ray's count; returns the taps in
 // the low and the shadow steps in the high 16 bits.
-template <class Set, class T, bool kDir64, bool kScenes = false>
+template <class Set, class T, bool kDir64, bool kScenes = false, bool kAccel = false>
 ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, const nd_gbuffer& g,
                                     const DevScene* scenes) {
   Dir<kDir64> dir;
@@ -879,14 +930,29 @@ ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, c
   normal_finish(gx, gy, gz);
   // visibility_march (tpl:2294-2341) toward the light, opaque scene
   float vis = 1.0f;
-  int k = 0;
+  int k = 0, sev = 0;  // shadow steps, shadow DE evaluations
   const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
   if (v.shadow && steps > 0 && kShadowBias < 2.0 * v.max_dist) {
     const D3 so = fmadd(p, d3(gx, gy, gz), kShadowBias);
     const D3 L = d3(v.light[0], v.light[1], v.light[2]);
     double a = kShadowBias, res = 1.0;
     while (true) {
-      const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(fmadd(so, L, a)), scenes);
+      const D3 q = fmadd(so, L, a);
+      if constexpr (kAccel) {
+        // visibility_march tpl:2297-2303: a recorded safe jump instead of an evaluation
+        const double skip = double(accel_skip(v, float(q.x), float(q.y), float(q.z)));
+        if (skip > kShadowMinStep && double(v.shadow_k) * skip >= res * a) {
+          a += skip;
+          ++k;
+          if (k >= steps || a >= 2.0 * v.max_dist) {
+            vis = float(fmin(fmax(res, 0.0), 1.0));
+            break;
+          }
+          continue;
+        }
+      }
+      const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(q), scenes);
+      ++sev;
       const double d = double(de.d);
       if (d < kShadowHitEps) {
         vis = 0.0f;
@@ -911,8 +977,8 @@ ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, c
   }
   if (g.shade) g.shade[r] = lambert(v, dir.get(), gx, gy, gz, vis);
   if (g.shadow) g.shadow[r] = vis;
-  if (g.evals) g.evals[r] += uint32_t(taps + k);
-  return uint32_t(taps) | (uint32_t(k) << 16);
+  if (g.evals) g.evals[r] += uint32_t(taps + sev);
+  return uint32_t(taps) | (uint32_t(sev) << 16);
 }
 
 }  // namespace nd

@@ -72,12 +72,18 @@ struct nd_ctx {
   int64_t thit_cap = 0;
   nd::DevScene* d_scenes = nullptr;  // multi-instance scene table
   int scenes_cap = 0;
+  float* d_accel = nullptr;          // accelerator grids of the views that have one
+  int64_t accel_cap = 0;             // floats
+  nd::AccelJob* d_accel_jobs = nullptr;
+  int accel_jobs_cap = 0;
+  uint64_t last_accel_voxels = 0;
   bool last_trap = false;
   DevView* h_views = nullptr;  // pinned staging
   int h_views_cap = 0;
   cudaStream_t last_stream = nullptr;
   cudaEvent_t last_done = nullptr;
-  std::vector<cudaEvent_t> tev;  // timing events: per launch plan march start, march end, shade end
+  std::vector<cudaEvent_t> tev;  // timing events per launch plan: accelerator build start, march start,
+                                 // march end, shade end
   int tev_plans = 0;             // plans the last forward timed (0: none)
   bool have_last = false;
   int last_kernel = 0;
@@ -92,6 +98,8 @@ struct nd_graph {
   unsigned long long* d_counters = nullptr;
   double* d_thit = nullptr;
   int32_t* d_hits = nullptr;
+  float* d_accel = nullptr;
+  nd::AccelJob* d_accel_jobs = nullptr;
   bool trap = false;
 };
 
@@ -137,6 +145,9 @@ nd_status validate_view(nd_ctx* ctx, const nd_view_desc& v, int idx) {
     return fail(ctx, ND_ERR_INVALID, "view %d: bad max_dist/epsilon", idx);
   if (v.normal_mode != ND_NORMAL_TETRA && v.normal_mode != ND_NORMAL_CENTRAL)
     return fail(ctx, ND_ERR_INVALID, "view %d: bad normal_mode %d", idx, v.normal_mode);
+  if (v.accel_res < 0) return fail(ctx, ND_ERR_INVALID, "view %d: accel_res %d < 0", idx, v.accel_res);
+  if (v.accel_res > 0 && !(v.accel_safety > 0.0f && v.accel_safety <= 1.0f))
+    return fail(ctx, ND_ERR_INVALID, "view %d: accel_safety %g out of (0, 1]", idx, double(v.accel_safety));
   if (v.shadow) {
     const double l2 = double(v.light_dir[0]) * v.light_dir[0] + double(v.light_dir[1]) * v.light_dir[1] +
                       double(v.light_dir[2]) * v.light_dir[2];
@@ -293,22 +304,50 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
                   const nd_gbuffer* out, cudaStream_t stream, const std::vector<Launch>& plans, DevView* d_views,
                   DevView* h_views, unsigned long long* d_counters, double* d_thit, int32_t* d_hits,
                   bool copy_views, int* kernel_used, cudaEvent_t* tev = nullptr,
-                  const SceneInput& sc = SceneInput(), nd::DevScene* d_scenes = nullptr) {
+                  const SceneInput& sc = SceneInput(), nd::DevScene* d_scenes = nullptr, float* d_accel = nullptr,
+                  nd::AccelJob* d_jobs = nullptr, std::vector<nd::AccelJob>* jobs_out = nullptr) {
   const int prec = (opts && opts->de_precision == 64) ? 64 : 32;
   // global output offsets in call order
   std::vector<int64_t> out_off(nviews + 1, 0);
   for (int i = 0; i < nviews; ++i) out_off[i + 1] = out_off[i] + int64_t(views[i].spp) * views[i].tile_w * views[i].tile_h;
+  // accelerator grids: one region of d_accel per view that has one, and per plan
+  // the build jobs (plan-local view index, first voxel in the plan's voxel order)
+  std::vector<nd::AccelJob> jobs;
+  std::vector<int> job_begin(plans.size() + 1, 0);
+  std::vector<int64_t> plan_voxels(plans.size(), 0);
+  int64_t voxel_off = 0;
   int base = 0;
   for (size_t p = 0; p < plans.size(); ++p) {
     const Launch& L = plans[p];
     int64_t off = 0;
+    job_begin[p] = int(jobs.size());
     for (size_t k = 0; k < L.views.size(); ++k) {
       const int vi = L.views[k];
       h_views[base + k] = make_dev_view(views[vi], off, out_off[vi], L.codes[k]);
       h_views[base + k].scene = sc.scene_of(vi);
       off += h_views[base + k].rays;
+      const int64_t nvox = nd::accel_voxels_of(views[vi]);
+      if (nvox > 0) {
+        if (!d_accel || !d_jobs) return fail(ctx, ND_ERR_UNSUPPORTED, "view %d: no accelerator memory on this path", vi);
+        nd::place_accel(h_views[base + k], views[vi], d_accel + voxel_off);
+        nd::AccelJob j;
+        j.view = int32_t(k);
+        j.pad = 0;
+        j.begin = plan_voxels[p];
+        jobs.push_back(j);
+        plan_voxels[p] += nvox;
+        voxel_off += nvox;
+      }
     }
     base += int(L.views.size());
+  }
+  job_begin[plans.size()] = int(jobs.size());
+  if (jobs_out) *jobs_out = jobs;
+  if (copy_views && !jobs.empty()) {
+    // from pageable memory: returns once the jobs are staged
+    cudaError_t e = cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(nd::AccelJob) * jobs.size(), cudaMemcpyHostToDevice,
+                                    stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy accelerator jobs");
   }
   if (sc.nscenes > 0 && d_scenes) {
     // scenes are only accepted when one formula group covers the call: one plan
@@ -359,6 +398,12 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
     if (rays > 0) {
       const Tuned tu = tuned_for(L.key);
       int kernel = opts && opts->kernel ? opts->kernel : tu.kernel;
+      const bool accel = plan_voxels[p] > 0;
+      if (accel && kernel == ND_KERNEL_PLAIN) {
+        if (opts && opts->kernel == ND_KERNEL_PLAIN)
+          return fail(ctx, ND_ERR_UNSUPPORTED, "the empty-space accelerator runs on the persistent kernel only");
+        kernel = ND_KERNEL_PERSISTENT;
+      }
       LaunchArgs a;
       memset(&a, 0, sizeof(a));
       a.views = d_views + base;
@@ -383,9 +428,24 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       // the persistent march leaves the normal taps and shadow rays of its hits to
       // the shade pass
       const bool defer = kernel != ND_KERNEL_PLAIN && d_hits != nullptr && d_thit != nullptr;
-      if (tev) cudaEventRecord(tev[3 * p], stream);
+      if (tev) cudaEventRecord(tev[4 * p], stream);
       if (sc.nscenes > 0 && kernel == ND_KERNEL_PLAIN)
         return fail(ctx, ND_ERR_UNSUPPORTED, "scenes run on the persistent kernel only");
+      const nd::KernelTable& T = L.table;
+      const bool scn = sc.nscenes > 0;
+      if (accel) {
+        if (prec == 32 && dir64)
+          return fail(ctx, ND_ERR_UNSUPPORTED,
+                      "the empty-space accelerator needs FP32 ray directions or an FP64 DE (deep-zoom view)");
+        if (!defer) return fail(ctx, ND_ERR_UNSUPPORTED, "the empty-space accelerator needs the deferred shade pass");
+        nd::AccelBuildFn bf = scn ? (prec == 64 ? T.scene_accel_build_f64 : T.scene_accel_build_f32)
+                                  : (prec == 64 ? T.accel_build_f64 : T.accel_build_f32);
+        if (!bf) return fail(ctx, ND_ERR_UNSUPPORTED, "no accelerator kernels in this formula set");
+        e = bf(d_views + base, d_jobs + job_begin[p], job_begin[p + 1] - job_begin[p], plan_voxels[p],
+               scn ? d_scenes : nullptr, ctx->num_sms, stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "accelerator build launch");
+      }
+      if (tev) cudaEventRecord(tev[4 * p + 1], stream);
       if (kernel == ND_KERNEL_PLAIN) {
         // the plain baseline: one launch per view, one thread per ray
         for (int k = 0; k < nv; ++k) {
@@ -396,10 +456,14 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       } else {
         const bool batched = nv > 1;
         LaunchFn fn = pick(L.table, kernel, prec, batched, dir64);
-        if (sc.nscenes > 0) {
-          fn = prec == 64 ? L.table.scene_persistent_f64
-                          : (dir64 ? L.table.scene_persistent_f32_dir64 : L.table.scene_persistent_f32);
+        if (scn) {
+          fn = prec == 64 ? T.scene_persistent_f64 : (dir64 ? T.scene_persistent_f32_dir64 : T.scene_persistent_f32);
           if (!fn) return fail(ctx, ND_ERR_UNSUPPORTED, "no scene kernels in this formula set");
+        }
+        if (accel) {
+          fn = scn ? (prec == 64 ? T.scene_persistent_f64_accel : T.scene_persistent_f32_accel)
+                   : (prec == 64 ? T.persistent_f64_accel : T.persistent_f32_accel);
+          if (!fn) return fail(ctx, ND_ERR_UNSUPPORTED, "no accelerator kernels in this formula set");
         }
         if (defer) {
           a.hit_list = d_hits + ray_base;
@@ -408,20 +472,21 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
         e = fn(a, h_views[base], c, stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
       }
-      if (tev) cudaEventRecord(tev[3 * p + 1], stream);
+      if (tev) cudaEventRecord(tev[4 * p + 2], stream);
       if (defer || want_trap) {
         // normals of the deferred hits and/or the orbit trap at every hit point
         const bool batched = nv > 1;
-        const nd::KernelTable& T = L.table;
         nd::ShadeFn sf = prec == 64 ? (batched ? T.shade_f64_batched : T.shade_f64)
                                     : dir64 ? (batched ? T.shade_f32_dir64_batched : T.shade_f32_dir64)
                                             : (batched ? T.shade_f32_batched : T.shade_f32);
-        if (sc.nscenes > 0)
-          sf = prec == 64 ? T.scene_shade_f64 : (dir64 ? T.scene_shade_f32_dir64 : T.scene_shade_f32);
+        if (scn) sf = prec == 64 ? T.scene_shade_f64 : (dir64 ? T.scene_shade_f32_dir64 : T.scene_shade_f32);
+        if (accel)
+          sf = scn ? (prec == 64 ? T.scene_shade_f64_accel : T.scene_shade_f32_accel)
+                   : (prec == 64 ? T.shade_f64_accel : T.shade_f32_accel);
         e = sf(a, h_views[base], c, want_trap ? 1 : 0, stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "shade pass launch");
       }
-      if (tev) cudaEventRecord(tev[3 * p + 2], stream);
+      if (tev) cudaEventRecord(tev[4 * p + 3], stream);
       used = kernel;
     }
     base += nv;
@@ -620,6 +685,8 @@ nd_status nd_ctx_destroy(nd_ctx* ctx) {
   if (ctx->d_thit) cudaFree(ctx->d_thit);
   if (ctx->d_hits) cudaFree(ctx->d_hits);
   if (ctx->d_scenes) cudaFree(ctx->d_scenes);
+  if (ctx->d_accel) cudaFree(ctx->d_accel);
+  if (ctx->d_accel_jobs) cudaFree(ctx->d_accel_jobs);
   if (ctx->h_views) cudaFreeHost(ctx->h_views);
   if (ctx->last_done) cudaEventDestroy(ctx->last_done);
   for (cudaEvent_t ev : ctx->tev) cudaEventDestroy(ev);
@@ -683,19 +750,38 @@ nd_status forward_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, c
     if (e != cudaSuccess) return cuda_fail(ctx, e, "pinned view staging");
     ctx->h_views_cap = std::max(nviews, 64);
   }
-  while (ctx->tev.size() < 3 * plans.size()) {
+  int64_t voxels = 0;
+  int accel_views = 0;
+  for (int i = 0; i < nviews; ++i) {
+    const int64_t nv = nd::accel_voxels_of(views[i]);
+    voxels += nv;
+    accel_views += nv > 0 ? 1 : 0;
+  }
+  if (voxels > 0 && ctx->accel_cap < voxels) {
+    if (ctx->d_accel) cudaFree(ctx->d_accel);
+    ctx->d_accel = nullptr;
+    ctx->accel_cap = 0;
+    e = cudaMalloc((void**)&ctx->d_accel, sizeof(float) * size_t(voxels));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "accelerator grids");
+    ctx->accel_cap = voxels;
+  }
+  if (accel_views > 0 &&
+      (s = ensure_dev(ctx, &ctx->d_accel_jobs, &ctx->accel_jobs_cap, accel_views, "accelerator jobs")) != ND_OK)
+    return s;
+  while (ctx->tev.size() < 4 * plans.size()) {
     cudaEvent_t ev;
     e = cudaEventCreate(&ev);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "timing event");
     ctx->tev.push_back(ev);
   }
   // a plan with no rays records no events: start from a clean slate
-  for (size_t i = 0; i < 3 * plans.size(); ++i) cudaEventRecord(ctx->tev[i], st);
+  for (size_t i = 0; i < 4 * plans.size(); ++i) cudaEventRecord(ctx->tev[i], st);
   int kernel = 0;
   if (sc.nscenes > 0 && (s = ensure_dev(ctx, &ctx->d_scenes, &ctx->scenes_cap, sc.nscenes, "scene table")) != ND_OK)
     return s;
   s = enqueue(ctx, views, nviews, opts, out, st, plans, ctx->d_views, ctx->h_views, ctx->d_counters, ctx->d_thit,
-              ctx->d_hits, true, &kernel, ctx->tev.data(), sc, sc.nscenes > 0 ? ctx->d_scenes : nullptr);
+              ctx->d_hits, true, &kernel, ctx->tev.data(), sc, sc.nscenes > 0 ? ctx->d_scenes : nullptr,
+              ctx->d_accel, ctx->d_accel_jobs);
   ctx->tev_plans = s == ND_OK ? int(plans.size()) : 0;
   if (s != ND_OK) return s;
   e = cudaEventRecord(ctx->last_done, st);
@@ -705,6 +791,7 @@ nd_status forward_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, c
   ctx->last_kernel = kernel;
   ctx->last_rays = total;
   ctx->last_trap = want_trap;
+  ctx->last_accel_voxels = uint64_t(voxels);
   return ND_OK;
 }
 }  // namespace
@@ -751,10 +838,12 @@ nd_status nd_last_stats(nd_ctx* ctx, nd_stats* out) {
   out->refills = h.refills;
   out->timeouts = h.timeouts;
   out->kernel = uint32_t(ctx->last_kernel);
+  out->accel_voxels = ctx->last_accel_voxels;
   for (int p = 0; p < ctx->tev_plans; ++p) {
-    float m = 0.0f, sh = 0.0f;
-    if (cudaEventElapsedTime(&m, ctx->tev[3 * p], ctx->tev[3 * p + 1]) == cudaSuccess) out->march_ms += m;
-    if (cudaEventElapsedTime(&sh, ctx->tev[3 * p + 1], ctx->tev[3 * p + 2]) == cudaSuccess) out->shade_ms += sh;
+    float b = 0.0f, m = 0.0f, sh = 0.0f;
+    if (cudaEventElapsedTime(&b, ctx->tev[4 * p], ctx->tev[4 * p + 1]) == cudaSuccess) out->accel_ms += b;
+    if (cudaEventElapsedTime(&m, ctx->tev[4 * p + 1], ctx->tev[4 * p + 2]) == cudaSuccess) out->march_ms += m;
+    if (cudaEventElapsedTime(&sh, ctx->tev[4 * p + 2], ctx->tev[4 * p + 3]) == cudaSuccess) out->shade_ms += sh;
   }
   if (h.timeouts) return fail(ctx, ND_ERR_TIMEOUT, "the device watchdog stopped %u warps", h.timeouts);
   return ND_OK;
@@ -779,12 +868,14 @@ nd_status nd_autotune(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, co
     int kernel, per_sm, thr;
   };
   std::vector<Cand> cands;
-  cands.push_back({ND_KERNEL_PLAIN, 0, 1});
+  bool any_accel = false;
+  for (int i = 0; i < nviews; ++i) any_accel |= nd::accel_voxels_of(views[i]) > 0;
+  if (!any_accel) cands.push_back({ND_KERNEL_PLAIN, 0, 1});  // the accelerator runs on the persistent kernel
   for (int per_sm : {0, 4, 8})
     for (int thr : {1, 4, 8, 16, 24})
       cands.push_back({ND_KERNEL_PERSISTENT, per_sm, thr});
   double best = 1e30;
-  Cand bc = cands[1];
+  Cand bc = cands[any_accel ? 0 : 1];
   for (const Cand& c : cands) {
     nd_march_opts o;
     memset(&o, 0, sizeof(o));
@@ -850,10 +941,20 @@ nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
   if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_counters, sizeof(unsigned long long) * 2 * plans.size());
   if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_thit, sizeof(double) * size_t(std::max<int64_t>(total, 1)));
   if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_hits, sizeof(int32_t) * size_t(std::max<int64_t>(total, 1)));
+  int64_t voxels = 0;
+  int accel_views = 0;
+  for (int i = 0; i < nviews; ++i) {
+    voxels += nd::accel_voxels_of(views[i]);
+    accel_views += nd::accel_voxels_of(views[i]) > 0 ? 1 : 0;
+  }
+  if (e == cudaSuccess && voxels > 0) e = cudaMalloc((void**)&g->d_accel, sizeof(float) * size_t(voxels));
+  if (e == cudaSuccess && accel_views > 0)
+    e = cudaMalloc((void**)&g->d_accel_jobs, sizeof(nd::AccelJob) * size_t(accel_views));
   if (e != cudaSuccess) {
     nd_graph_destroy(g);
     return cuda_fail(ctx, e, "graph buffers");
   }
+  std::vector<nd::AccelJob> jobs;
   std::vector<DevView> hv(nviews);
   // fill the host table (enqueue builds it) without launching: capture does both
   cudaStream_t st = (cudaStream_t)stream;
@@ -870,7 +971,7 @@ nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
     return cuda_fail(ctx, e, "begin capture");
   }
   s = enqueue(ctx, views, nviews, opts, out, cap, plans, g->d_views, hv.data(), g->d_counters, g->d_thit,
-              g->d_hits, false, nullptr);
+              g->d_hits, false, nullptr, nullptr, SceneInput(), nullptr, g->d_accel, g->d_accel_jobs, &jobs);
   cudaGraph_t gr = nullptr;
   e = cudaStreamEndCapture(cap, &gr);
   cudaStreamDestroy(cap);
@@ -881,6 +982,8 @@ nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
   }
   g->graph = gr;
   e = cudaMemcpy(g->d_views, hv.data(), sizeof(DevView) * size_t(nviews), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !jobs.empty())
+    e = cudaMemcpy(g->d_accel_jobs, jobs.data(), sizeof(nd::AccelJob) * jobs.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, gr, 0);
   if (e != cudaSuccess) {
     nd_graph_destroy(g);
@@ -913,6 +1016,8 @@ nd_status nd_graph_destroy(nd_graph* g) {
   if (g->d_counters) cudaFree(g->d_counters);
   if (g->d_thit) cudaFree(g->d_thit);
   if (g->d_hits) cudaFree(g->d_hits);
+  if (g->d_accel) cudaFree(g->d_accel);
+  if (g->d_accel_jobs) cudaFree(g->d_accel_jobs);
   delete g;
   return ND_OK;
 }
@@ -928,6 +1033,40 @@ nd_status nd_de_points(nd_ctx* ctx, const nd_view_desc* view, int64_t n, const d
   const nd::DePointsFn fn = de_precision == 64 ? t.de_points_f64 : t.de_points_f32;
   cudaError_t e = fn(v, n, pts, de, trap, iters, (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "nd_de_points launch");
+  return ND_OK;
+}
+
+nd_status nd_accel_grid(nd_ctx* ctx, const nd_view_desc* view, int32_t de_precision, float* grid, int64_t capacity,
+                        float* prm, int64_t* count) {
+  if (!ctx || !view || !grid || !prm || !count) return fail(ctx, ND_ERR_INVALID, "bad nd_accel_grid arguments");
+  nd_status s = validate_view(ctx, *view, 0);
+  if (s != ND_OK) return s;
+  const int64_t n = nd::accel_voxels_of(*view);
+  if (n <= 0) return fail(ctx, ND_ERR_INVALID, "the view has no accelerator (accel_res 0)");
+  if (n > capacity) return fail(ctx, ND_ERR_INVALID, "grid capacity %lld < %lld", (long long)capacity, (long long)n);
+  cudaSetDevice(ctx->device);
+  DevView v = make_dev_view(*view, 0, 0, 0);
+  nd::place_accel(v, *view, grid);
+  for (int l = 0; l < nd::kAccelMaxCascades; ++l)
+    for (int a = 0; a < 4; ++a) prm[4 * l + a] = l < v.accel_levels ? v.accel_prm[l][a] : 0.0f;
+  const KernelTable t = nd_formula_entries[view->formula].kernels();
+  const nd::AccelBuildFn fn = de_precision == 64 ? t.accel_build_f64 : t.accel_build_f32;
+  DevView* dv = nullptr;
+  nd::AccelJob* dj = nullptr;
+  nd::AccelJob job;
+  job.view = 0;
+  job.pad = 0;
+  job.begin = 0;
+  cudaError_t e = cudaMalloc((void**)&dv, sizeof(DevView));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&dj, sizeof(job));
+  if (e == cudaSuccess) e = cudaMemcpy(dv, &v, sizeof(DevView), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = fn(dv, dj, 1, n, nullptr, ctx->num_sms, nullptr);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (dv) cudaFree(dv);
+  if (dj) cudaFree(dj);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "nd_accel_grid");
+  *count = n;
   return ND_OK;
 }
 
@@ -1021,6 +1160,7 @@ extern "C" nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t
   for (int i = 0; i < nviews; ++i) {
     const nd_status s = validate_view(nullptr, views[i], i);
     if (s != ND_OK) return s;
+    if (views[i].accel_res > 0) return ND_ERR_UNSUPPORTED;  // the accelerator grid needs device memory
     total += int64_t(views[i].spp) * views[i].tile_w * views[i].tile_h;
     if (total > int64_t(0x7fffffff)) return ND_ERR_INVALID;
   }

@@ -71,6 +71,39 @@ inline DevView make_dev_view(const nd_view_desc& v, int64_t ray_offset, int64_t 
   return d;
 }
 
+// Accelerator geometry of a view: resolution clamped to 16..160 and rounded down to a
+// multiple of 4 (clampResolution, src/gpu/accel.zig:28-31), 1..8 cascades; 0 = off.
+inline int accel_res_of(const nd_view_desc& v) {
+  return v.accel_res <= 0 ? 0 : std::min(std::max(v.accel_res, 16), 160) / 4 * 4;
+}
+inline int accel_levels_of(const nd_view_desc& v) {
+  return std::min(std::max(v.accel_levels, 1), kAccelMaxCascades);
+}
+inline int64_t accel_voxels_of(const nd_view_desc& v) {
+  const int64_t r = accel_res_of(v);
+  return r ? int64_t(accel_levels_of(v)) * r * r * r : 0;
+}
+
+// Cascades centred on the camera (placeCascades, src/gpu/accel.zig:32-56, f32 like
+// the reference): the coarsest cell spans 2 max_dist / res, each finer cascade halves
+// it, corners snapped to the cascade's cell grid.  grid: levels * res^3 floats.
+inline void place_accel(DevView& d, const nd_view_desc& v, float* grid) {
+  const int res = accel_res_of(v), levels = accel_levels_of(v);
+  d.accel_res = res;
+  d.accel_levels = res ? levels : 0;
+  d.accel_safety = v.accel_safety;
+  d.accel_grid = grid;
+  if (!res) return;
+  const float res_f = float(res);
+  const float coarsest = std::max(2.0f * v.max_dist / res_f, 1e-6f);
+  for (int l = 0; l < levels; ++l) {
+    const float cell = coarsest / float(1u << (levels - 1 - l));
+    const float half = 0.5f * res_f * cell;
+    for (int a = 0; a < 3; ++a) d.accel_prm[l][a] = std::floor((float(v.cam_pos[a]) - half) / cell) * cell;
+    d.accel_prm[l][3] = cell;
+  }
+}
+
 // One scene instance as the kernels read it.  code / mcode: the instance's and its
 // mixins' formula indices inside the launch's formula set.
 inline DevInstance make_dev_instance(const nd_instance_desc& in, int code, const int* mcode) {

@@ -54,6 +54,8 @@ _SIGNATURES = {
     "nd_de_points": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int64, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "nd_orbit_view": (C.c_int32, [C.POINTER(abi.nd_orbit_camera), C.POINTER(abi.nd_view_desc)]),
+    "nd_accel_grid": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.c_void_p, C.c_int64,
+                                  C.c_void_p, C.POINTER(C.c_int64)]),
     "nd_march_forward_scenes": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(C.c_int32),
                                             C.POINTER(abi.nd_scene_desc), C.c_int32, C.POINTER(abi.nd_march_opts),
                                             C.POINTER(abi.nd_gbuffer), C.c_void_p]),
@@ -319,6 +321,22 @@ class Context:
         self._check(st, "nd_de_points")
         torch.cuda.synchronize(pts.device)
         return de.cpu().numpy(), tr.cpu().numpy(), it.cpu().numpy()
+
+    def accel_grid(self, view: abi.nd_view_desc, de_precision: int = 32):
+        """nd_accel_grid: the view's accelerator grid ([level][z][y][x], numpy) and its
+        cascade placement (8 x (corner xyz, cell))."""
+        import numpy as np
+        import torch
+
+        res = min(max(view.accel_res, 16), 160) // 4 * 4
+        levels = min(max(view.accel_levels, 1), 8)
+        grid = torch.empty(levels * res ** 3, dtype=torch.float32, device=f"cuda:{self.device}")
+        prm = np.zeros((8, 4), np.float32)
+        n = C.c_int64()
+        st = self.lib.nd_accel_grid(self.handle, C.byref(view), de_precision, grid.data_ptr(), grid.numel(),
+                                    prm.ctypes.data, C.byref(n))
+        self._check(st, "nd_accel_grid")
+        return grid.cpu().numpy().reshape(levels, res, res, res), prm
 
     def stats(self) -> abi.nd_stats:
         out = abi.nd_stats()

@@ -23,6 +23,7 @@
 #include <string.h>
 #include <algorithm>
 #include <string>
+#include <vector>
 
 #include "../include/nd_march.h"
 
@@ -489,6 +490,64 @@ template <class R> struct SceneEval {
   }
 };
 
+// ------------------------------------------------------------------ empty-space accelerator
+// Cascade placement (placeCascades, src/gpu/accel.zig:32-56, clampResolution :28-31),
+// the grid build (cs_build_accel tpl:5412-5431) and the lookup (accel_skip
+// tpl:428-447), in f32 like the reference; grid layout [level][z][y][x].
+constexpr int kAccelMaxCascades = 8;  // MAX_CASCADES tpl:31
+inline int accel_clamp_res(int res) { return std::min(std::max(res, 16), 160) / 4 * 4; }
+inline int accel_clamp_levels(int levels) { return std::min(std::max(levels, 1), kAccelMaxCascades); }
+
+struct AccelGrid {
+  int res = 0, levels = 0;
+  float prm[kAccelMaxCascades][4] = {};  // corner xyz, cell size
+  std::vector<float> v;
+
+  void place(const double cam[3], float max_dist, int nlevels, int nres) {
+    res = nres;
+    levels = nlevels;
+    const float res_f = float(std::max(res, 1));
+    const float coarsest = std::fmax(2.0f * max_dist / res_f, 1e-6f);
+    for (int l = 0; l < levels; ++l) {
+      const float cell = coarsest / float(1u << (levels - 1 - l));
+      const float half = 0.5f * res_f * cell;
+      for (int a = 0; a < 3; ++a) prm[l][a] = std::floor((float(cam[a]) - half) / cell) * cell;
+      prm[l][3] = cell;
+    }
+  }
+
+  // de(V3<float> centre) -> distance (any float type); safe skip per voxel centre
+  template <class F> void build(float safety, int nthreads, F&& de) {
+    const int64_t r = res, total = int64_t(levels) * r * r * r;
+    v.assign(size_t(total), 0.0f);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 256)
+    for (int64_t idx = 0; idx < total; ++idx) {
+      const int64_t x = idx % r, y = (idx / r) % r, gz = idx / (r * r);
+      const int l = int(gz / r);
+      const int64_t z = gz % r;
+      const float cell = prm[l][3];
+      const V3<float> c(prm[l][0] + (float(x) + 0.5f) * cell, prm[l][1] + (float(y) + 0.5f) * cell,
+                        prm[l][2] + (float(z) + 0.5f) * cell);
+      const float d = float(de(c));
+      v[size_t(idx)] = std::fmax(d - 0.8660254f * cell, 0.0f) * safety;  // HALF_SQRT3 tpl:62
+    }
+  }
+
+  float skip(float px, float py, float pz) const {
+    for (int l = 0; l < levels; ++l) {
+      const float cell = prm[l][3];
+      if (!(cell > 0.0f)) continue;
+      const float fx = std::floor((px - prm[l][0]) / cell);
+      const float fy = std::floor((py - prm[l][1]) / cell);
+      const float fz = std::floor((pz - prm[l][2]) / cell);
+      const float rf = float(res);
+      if (!(fx >= 0.0f && fy >= 0.0f && fz >= 0.0f && fx < rf && fy < rf && fz < rf)) continue;
+      return v[((size_t(l) * res + size_t(fz)) * res + size_t(fy)) * res + size_t(fx)];
+    }
+    return 0.0f;
+  }
+};
+
 // ------------------------------------------------------------------ per-ray result
 struct RayOut {
   double depth;       // t at the hit, 0 on a miss
@@ -526,6 +585,7 @@ template <class R> struct Tracer {
   uint32_t evals = 0;
   double de_scale = 1.0;  // every DE value is multiplied by this (stability probes)
   const SceneEval<R>* scene = nullptr;  // a multi-instance scene instead of the view's formula
+  const AccelGrid* accel = nullptr;     // the view's empty-space accelerator, when it has one
 
   Tracer(const nd_view_desc& view, int k) : v(view), kind(k) {
     for (int i = 0; i < ND_MAX_PARAMS; ++i) p[i] = R(view.params[i]);
@@ -564,6 +624,18 @@ template <class R> struct Tracer {
       const double st = probing ? t : 0.5 * (lo + hi);
       const double e = eps(st);
       const V3<double> pos = org + dir * st;
+      if (probing && accel) {
+        // accel_skip before the DE (march_to tpl:1890-1900): a safe jump costs no evaluation
+        const double skip = double(accel->skip(float(pos.x), float(pos.y), float(pos.z)));
+        if (skip > e) {
+          lo = st;
+          t = st + skip;
+          ++i;
+          o.margin = std::min(o.margin, std::fabs(t - max_t) / max_t);
+          if (t > max_t || i >= max_steps) break;
+          continue;
+        }
+      }
       const DE<R> de = de_at(pos);
       const double d = double(de.d);
       o.margin = std::min(o.margin, std::fabs(d - e) / std::max(e, 1e-30));
@@ -650,7 +722,15 @@ template <class R> struct Tracer {
     double t = 0.004, res = 1.0;
     for (int i = 0; i < steps; ++i) {
       if (t >= light_dist) break;
-      const double d = double(de_at(o + l * t).d);
+      const V3<double> p = o + l * t;
+      if (accel) {  // visibility_march tpl:2297-2303
+        const double skip = double(accel->skip(float(p.x), float(p.y), float(p.z)));
+        if (skip > 0.001 && double(v.shadow_k) * skip >= res * t) {
+          t += skip;
+          continue;
+        }
+      }
+      const double d = double(de_at(p).d);
       if (d < 0.0005) return 0.0;
       res = std::min(res, double(v.shadow_k) * d / t);
       t += std::max(d, 0.001);

@@ -27,7 +27,45 @@ static void write_ray(const RayOut& o, int64_t i, float* depth, float* normal4, 
   if (margin) margin[i] = o.margin;
 }
 
+// The view's empty-space accelerator grid (when accel_res > 0), built from the DE the
+// view's rays see (its formula, or its scene), scaled by de_scale like every DE value.
+template <class R>
+static bool build_view_accel(AccelGrid& g, const nd_view_desc& v, int kind, const SceneEval<R>* sc, double de_scale,
+                             int nthreads) {
+  if (v.accel_res <= 0) return false;
+  g.place(v.cam_pos, v.max_dist, accel_clamp_levels(v.accel_levels), accel_clamp_res(v.accel_res));
+  R p[ND_MAX_PARAMS];
+  for (int k = 0; k < ND_MAX_PARAMS; ++k) p[k] = R(v.params[k]);
+  const R factor = R(std::min(std::max(double(v.step_safety), 0.001), 1.0));
+  g.build(v.accel_safety, nthreads, [&](V3<float> c) {
+    const V3<R> q(R(c.x), R(c.y), R(c.z));
+    R d = sc ? sc->de(q).d : eval_de<R>(kind, q, p, v.trap, factor).d;
+    if (de_scale != 1.0) d = R(double(d) * de_scale);
+    return d;
+  });
+  return true;
+}
+
 extern "C" {
+
+// The accelerator grid of one view (its own formula): levels * res^3 floats into
+// grid (capacity in floats) and the cascade placement (corner xyz, cell) into prm;
+// returns the number of floats, or -1.
+int64_t oracle_accel_grid(const nd_view_desc* view, const char* formula_name, int precision, int nthreads,
+                          float* grid, int64_t capacity, float* prm) {
+  const int kind = formula_index(formula_name);
+  if (kind < 0 || view->accel_res <= 0) return -1;
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  AccelGrid g;
+  if (precision == 32) build_view_accel<float>(g, *view, kind, nullptr, 1.0, nthreads);
+  else build_view_accel<double>(g, *view, kind, nullptr, 1.0, nthreads);
+  const int64_t n = int64_t(g.v.size());
+  if (n > capacity) return -1;
+  memcpy(grid, g.v.data(), sizeof(float) * size_t(n));
+  for (int l = 0; l < kAccelMaxCascades; ++l)
+    for (int a = 0; a < 4; ++a) prm[4 * l + a] = g.prm[l][a];
+  return n;
+}
 
 int oracle_formula_index(const char* name) { return formula_index(name); }
 
@@ -71,12 +109,16 @@ int oracle_render(const nd_view_desc* view, const char* formula_name, int precis
   const int kind = formula_index(formula_name);
   if (kind < 0) return -1;
   if (nthreads <= 0) nthreads = omp_get_max_threads();
+  AccelGrid grid;
+  const bool accel = precision == 32 ? build_view_accel<float>(grid, *view, kind, nullptr, de_scale, nthreads)
+                                     : build_view_accel<double>(grid, *view, kind, nullptr, de_scale, nthreads);
 #pragma omp parallel num_threads(nthreads)
   {
     Tracer<float> tf(*view, kind);
     Tracer<double> td(*view, kind);
     tf.de_scale = de_scale;
     td.de_scale = de_scale;
+    tf.accel = td.accel = accel ? &grid : nullptr;
 #pragma omp for schedule(dynamic, 64)
     for (int64_t i = 0; i < n; ++i) {
       const RayOut o = precision == 32 ? tf.trace(first + i) : td.trace(first + i);
@@ -137,12 +179,16 @@ int oracle_render_scene(const nd_view_desc* view, const nd_scene_desc* scene, co
   sf.max_dist = sd.max_dist = view->max_dist;
   if (scene_kinds(kinds, mixin_kinds, sf, sd) != 0) return -1;
   if (nthreads <= 0) nthreads = omp_get_max_threads();
+  AccelGrid grid;
+  const bool accel = precision == 32 ? build_view_accel<float>(grid, *view, kinds[0], &sf, de_scale, nthreads)
+                                     : build_view_accel<double>(grid, *view, kinds[0], &sd, de_scale, nthreads);
 #pragma omp parallel num_threads(nthreads)
   {
     Tracer<float> tf(*view, kinds[0]);
     Tracer<double> td(*view, kinds[0]);
     tf.de_scale = de_scale;
     td.de_scale = de_scale;
+    tf.accel = td.accel = accel ? &grid : nullptr;
     tf.scene = &sf;
     td.scene = &sd;
 #pragma omp for schedule(dynamic, 64)

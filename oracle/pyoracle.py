@@ -26,6 +26,9 @@ def lib():
         _LIB.oracle_render_scene.argtypes = ([C.c_void_p] * 4 + [C.c_int, C.c_int, C.c_int64, C.c_int64]
                                              + [C.c_void_p] * 10 + [C.c_double])
         _LIB.oracle_scene_de.argtypes = ([C.c_void_p] * 3 + [C.c_double, C.c_int, C.c_int64] + [C.c_void_p] * 4)
+        _LIB.oracle_accel_grid.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_void_p, C.c_int64,
+                                           C.c_void_p]
+        _LIB.oracle_accel_grid.restype = C.c_int64
         _LIB.oracle_max_threads.restype = C.c_int
     return _LIB
 
@@ -152,3 +155,17 @@ def unstable_scene_rays(view: abi.nd_view_desc, scene: abi.nd_scene_desc, names,
     unstable = (h[0] != h[1]) | (h[0] != h[2])
     unstable |= (base["steps"] != lo["steps"]) | (base["steps"] != hi["steps"])
     return unstable, base
+
+
+def accel_grid(view: abi.nd_view_desc, formula_name: str, precision=64, nthreads=0):
+    """The view's empty-space accelerator grid ([level][z][y][x] safe skips) and its
+    cascade placement (8 x (corner xyz, cell))."""
+    res = min(max(view.accel_res, 16), 160) // 4 * 4
+    levels = min(max(view.accel_levels, 1), 8)
+    grid = np.zeros(levels * res ** 3, np.float32)
+    prm = np.zeros((8, 4), np.float32)
+    n = lib().oracle_accel_grid(C.addressof(view), formula_name.encode(), precision, nthreads, grid.ctypes.data,
+                                grid.size, prm.ctypes.data)
+    if n < 0:
+        raise ValueError("oracle_accel_grid refused the view")
+    return grid.reshape(levels, res, res, res), prm
