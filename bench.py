@@ -282,6 +282,24 @@ def small_and_deepzoom(ctx, sptr, timed, steps):
     out["deepzoom_4096"] = {"ms_per_frame": ms, "Mrays_per_s": n / (ms * 1e-3) / 1e6,
                             "de_evals_per_s": st.de_evals / (ms * 1e-3), "hits": st.hits, "rays": n,
                             "de": "fp64 (an FP32 DE cannot resolve the 1e-12 pixel footprint: no ray hits)"}
+    # batched_64 with the empty-space accelerator on: the reference's default grid
+    # (64^3 x 6 cascades, safety 0.92) and a coarse one; grids built inside every step
+    views = workloads.batched_64(runtime.find_formula)
+    n = workloads.rays(views)
+    g = runtime.GBuffer.allocate(n)
+    o = runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT)
+    for res in (64, 16):
+        av = []
+        for v in views:
+            w = abi.nd_view_desc.from_buffer_copy(v)
+            w.accel_res, w.accel_levels, w.accel_safety = res, 6, 0.92
+            av.append(w)
+        ms = timed(lambda: ctx.forward(av, g, o, stream=sptr), steps, 3)
+        st = ctx.stats()
+        out[f"batched_64_accel_{res}"] = {"ms_per_step": ms, "Mrays_per_s": n / (ms * 1e-3) / 1e6,
+                                          "march_evals": st.march_evals, "grid_cells": st.accel_voxels,
+                                          "grid_build_ms": st.accel_ms, "march_ms": st.march_ms,
+                                          "hits": st.hits}
     return out
 
 
@@ -419,7 +437,7 @@ def main():
     host = {k: torch.empty(getattr(gbuf, k).shape, dtype=getattr(gbuf, k).dtype, pin_memory=True)
             for k in ("depth", "normal", "trap", "steps")}
     d2h = sum(t.numel() * t.element_size() for t in host.values())
-    h2d = len(views) * 440  # the view table copied by nd_march_forward (DevView records)
+    h2d = len(views) * runtime.load_library().nd_sizeof(b"DevView")  # the view table nd_march_forward copies
 
     def e2e_step():
         ctx.forward(views, gbuf, opts, stream=sptr)

@@ -230,7 +230,10 @@ typedef struct nd_march_opts {
   int32_t refill_threshold;  /* persistent: refill a warp once this many lanes idle (0 = default) */
   int32_t de_precision;      /* 32 (default) or 64: float type of the DE itself */
   int32_t watchdog_ms;       /* device watchdog per launch (0 = 10000 ms) */
-  int32_t reserved[2];
+  int32_t accel_chain;       /* accelerator jumps a ray takes per pass of the persistent
+                                march before it waits for the next pass (0 = 4, < 0 = no
+                                limit); the march itself is unchanged */
+  int32_t reserved;
 } nd_march_opts;
 
 typedef struct nd_stats {

@@ -147,7 +147,7 @@ class nd_gbuffer(C.Structure):
 class nd_march_opts(C.Structure):
     _fields_ = [("kernel", C.c_int32), ("block", C.c_int32), ("blocks_per_sm", C.c_int32),
                 ("refill_threshold", C.c_int32), ("de_precision", C.c_int32), ("watchdog_ms", C.c_int32),
-                ("reserved", C.c_int32 * 2)]
+                ("accel_chain", C.c_int32), ("reserved", C.c_int32)]
 
 
 class nd_stats(C.Structure):

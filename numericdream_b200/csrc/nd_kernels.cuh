@@ -196,12 +196,14 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     }
     if (L.item >= 0 && L.phase != PH_DONE) {
       const DevView& v = kBatched ? a.views[L.view] : single;
+      bool probe = true;
       if constexpr (kAccel) {
-        // the accelerator's jumps come before the probe, so that every pass of this
-        // loop still ends in one DE evaluation per busy lane
-        if (L.phase == PH_MARCH && L.probing && v.accel_levels > 0) L.accel_skips(v, a.out, a.t_hit);
+        // the accelerator's jumps come before the probe; a ray with more jumps to take
+        // than the per-pass limit takes the rest in later passes
+        if (L.phase == PH_MARCH && L.probing && v.accel_levels > 0)
+          probe = L.accel_skips(v, a.out, a.t_hit, a.accel_chain);
       }
-      if (L.phase != PH_DONE) {
+      if (probe && L.phase != PH_DONE) {
         const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(L.sample_pos(v)), a.scenes);
         L.advance(v, de, a.out, a.t_hit, defer);
       }

@@ -120,6 +120,7 @@ struct LaunchArgs {
   Stats* stats;
   int32_t refill_threshold;
   int32_t chunk;              // rays a warp takes from the work counter at a time
+  int32_t accel_chain;        // accelerator jumps per lane and pass (0: no limit)
   int64_t deadline_ns;        // watchdog budget (globaltimer units)
   // Deferred shading: the persistent march ends a hit ray at its hit and appends it
   // to hit_list; the shade pass then evaluates the normal taps coherently.
@@ -728,19 +729,22 @@ template <class T, bool kDir64> struct Lane {
   // recorded skip at the probe position exceeds eps(t), advance without a DE
   // evaluation; each jump is a step and a sample of march_to's loop.  May end the
   // ray (a miss).
-  ND_DEV_INLINE void accel_skips(const DevView& v, const nd_gbuffer& g, double* t_hit) {
+  // At most `chain` jumps (0: no limit); returns true when the ray may probe now,
+  // false when it ended or has more jumps to take (in a later pass).
+  ND_DEV_INLINE bool accel_skips(const DevView& v, const nd_gbuffer& g, double* t_hit, int chain) {
     const D3 o = d3(v.org[0], v.org[1], v.org[2]);
-    while (true) {
+    for (int jumps = 0;; ++jumps) {
       const D3 p = fmadd(o, dir.get(), t);
       const double skip = double(accel_skip(v, float(p.x), float(p.y), float(p.z)));
-      if (!(skip > march_eps<T>(v, t))) return;
+      if (!(skip > march_eps<T>(v, t))) return true;
+      if (chain > 0 && jumps >= chain) return false;
       a = t;
       t = t + skip;
       ++i;
       ++n;
       if (t > v.max_dist || i >= v.max_steps || n >= v.max_samples) {
         finish(v, g, t_hit, 1.0f);
-        return;
+        return false;
       }
     }
   }

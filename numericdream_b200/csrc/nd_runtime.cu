@@ -416,6 +416,9 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       a.scenes = d_scenes;
       a.stats = ctx->d_stats;
       a.refill_threshold = std::max(1, std::min(32, opts && opts->refill_threshold ? opts->refill_threshold : tu.refill_threshold));
+      // 4 jumps per pass measured fastest on batched views (1, 2, 4 and no limit tried)
+      const int chain = opts ? opts->accel_chain : 0;
+      a.accel_chain = chain > 0 ? chain : (chain < 0 ? 0 : 4);
       const int wd = opts && opts->watchdog_ms > 0 ? opts->watchdog_ms : 10000;
       a.deadline_ns = int64_t(wd) * 1000000;
       LaunchConfig c;
@@ -1085,6 +1088,7 @@ size_t nd_sizeof(const char* name) {
   if (n == "nd_scene_desc") return sizeof(nd_scene_desc);
   if (n == "nd_instance_desc") return sizeof(nd_instance_desc);
   if (n == "nd_mixin_desc") return sizeof(nd_mixin_desc);
+  if (n == "DevView") return sizeof(DevView);  // the per-view record a forward call copies to the device
   return 0;
 }
 

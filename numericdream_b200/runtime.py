@@ -223,10 +223,11 @@ class GBuffer:
         return out
 
 
-def make_opts(kernel=abi.ND_KERNEL_AUTO, blocks_per_sm=0, refill_threshold=0, de_precision=32, watchdog_ms=0):
+def make_opts(kernel=abi.ND_KERNEL_AUTO, blocks_per_sm=0, refill_threshold=0, de_precision=32, watchdog_ms=0,
+              accel_chain=0):
     o = abi.nd_march_opts()
     o.kernel, o.blocks_per_sm, o.refill_threshold = kernel, blocks_per_sm, refill_threshold
-    o.de_precision, o.watchdog_ms = de_precision, watchdog_ms
+    o.de_precision, o.watchdog_ms, o.accel_chain = de_precision, watchdog_ms, accel_chain
     return o
 
 
