@@ -374,6 +374,21 @@ nd_status nd_de_points(nd_ctx* ctx, const nd_view_desc* view, int64_t n, const d
 nd_status nd_accel_grid(nd_ctx* ctx, const nd_view_desc* view, int32_t de_precision, float* grid, int64_t capacity,
                         float* prm, int64_t* count);
 
+/* A scene file (.dream JSON, version <= 12; src/app/scene_file.zig) as one view and
+ * one scene: the camera (FreeCamera position / forward / up; right = forward x up,
+ * 90 degree vertical field of view), the march settings of the bench export
+ * (render_settings: max_steps, max_dist and MarchPrecision, high quality on), and up
+ * to four instances with their formulas (by file stem; an empty path is the built-in
+ * Mandelbulb), @param values (by name, over the formula's defaults), placement,
+ * combine mode, mixins and orbit trap.  width / height <= 0 take the file's
+ * export size.  *needs_scene = 0 when the view alone describes the scene (one
+ * visible instance at the identity placement, no mixins): render it with
+ * nd_march_forward; otherwise with nd_march_forward_scenes (view_scene = {0}).
+ * Lights, fog, sky, materials, warps and particles are not read.  The message of a
+ * failure goes to err. */
+nd_status nd_scene_file_load(const char* json, size_t len, int32_t width, int32_t height, nd_view_desc* view,
+                             nd_scene_desc* scene, int32_t* needs_scene, char* err, size_t err_len);
+
 /* Size of a public struct by name ("nd_view_desc", ...), for binding layout checks. */
 size_t nd_sizeof(const char* name);
 

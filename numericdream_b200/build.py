@@ -47,7 +47,12 @@ NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "
 # Mixed-formula batches run in ONE persistent launch when every formula of the
 # batch belongs to a compiled group.  The default group holds the four formulas
 # of the batched benchmark (Mandelbulb, Mandelbox, Menger sponge, pseudo-Kleinian).
-DEFAULT_GROUPS = {"mixed4": ["mandelbrot", "amazingbox_box", "menger3_ifs", "pseudokleinian_kleinian"]}
+DEFAULT_GROUPS = {"mixed4": ["mandelbrot", "amazingbox_box", "menger3_ifs", "pseudokleinian_kleinian"],
+                  # scenes of fractals standing on / beside primitives, as the
+                  # reference's bench scenes are built (a call takes the first group
+                  # that covers it, so the benchmark batches still use mixed4)
+                  "scenes6": ["mandelbrot", "amazingbox_box", "menger3_ifs", "pseudokleinian_kleinian",
+                              "sphere_primitive", "cube_primitive"]}
 # Groups also carry the multi-instance scene kernels: a scene's formulas (instances
 # and mixins) must all lie in one group.  ND_GROUPS adds groups:
 # "name=f1,f2,...;name2=..." (formula file stems).
@@ -261,9 +266,11 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
                 if f"formulas/{n}.inc" in open(u).read()]
         fheaders[u] = headers + incs
     runtime = os.path.join(CSRC, "nd_runtime.cu")
-    all_units = units + [reg, runtime]
+    scene_file = os.path.join(CSRC, "nd_scene_file.cu")
+    all_units = units + [reg, runtime, scene_file]
     fheaders[reg] = headers
     fheaders[runtime] = headers
+    fheaders[scene_file] = headers
     jobs = jobs or max(1, os.cpu_count() or 1)
     objs = []
     errors = []

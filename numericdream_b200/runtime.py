@@ -56,6 +56,8 @@ _SIGNATURES = {
     "nd_orbit_view": (C.c_int32, [C.POINTER(abi.nd_orbit_camera), C.POINTER(abi.nd_view_desc)]),
     "nd_accel_grid": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.c_void_p, C.c_int64,
                                   C.c_void_p, C.POINTER(C.c_int64)]),
+    "nd_scene_file_load": (C.c_int32, [C.c_char_p, C.c_size_t, C.c_int32, C.c_int32, C.POINTER(abi.nd_view_desc),
+                                       C.POINTER(abi.nd_scene_desc), C.POINTER(C.c_int32), C.c_char_p, C.c_size_t]),
     "nd_march_forward_scenes": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(C.c_int32),
                                             C.POINTER(abi.nd_scene_desc), C.c_int32, C.POINTER(abi.nd_march_opts),
                                             C.POINTER(abi.nd_gbuffer), C.c_void_p]),
@@ -150,6 +152,26 @@ def formula_params(fid: int) -> list:
     if st != abi.ND_OK:
         raise NDError(st, f"formula id {fid}")
     return [buf[i] for i in range(n.value)]
+
+
+def load_scene_file(source, width: int = 0, height: int = 0):
+    """nd_scene_file_load: a .dream scene (a path or the JSON text) as (view, scene);
+    scene is None when the view alone describes it (render with Context.forward),
+    else render with Context.forward_scenes([view], [0], [scene], ...)."""
+    if isinstance(source, (bytes, bytearray)):
+        data = bytes(source)
+    elif isinstance(source, str) and source.lstrip().startswith("{"):
+        data = source.encode("utf-8")
+    else:
+        with open(source, "rb") as fh:
+            data = fh.read()
+    view, scene, needs = abi.nd_view_desc(), abi.nd_scene_desc(), C.c_int32()
+    err = C.create_string_buffer(512)
+    st = load_library().nd_scene_file_load(data, len(data), width, height, C.byref(view), C.byref(scene),
+                                           C.byref(needs), err, 512)
+    if st != abi.ND_OK:
+        raise NDError(st, err.value.decode())
+    return view, (scene if needs.value else None)
 
 
 def view_defaults(fid: int) -> abi.nd_view_desc:
