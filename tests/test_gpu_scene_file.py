@@ -68,7 +68,7 @@ def test_fractal_on_primitives(ctx):
            "instances": [inst("", (0, 0, 0), (1, 1, 1), rotation={"x": 20, "y": 30, "z": 0}),
                          inst("formulas/cube_primitive.wgsl", (0, -1.35, 0), (6, 0.1, 6)),
                          inst("formulas/menger3_ifs.wgsl", (2.1, -0.45, -1.2), (0.75, 0.75, 0.75)),
-                         inst("formulas/sphere_primitive.wgsl", (-1.75, -0.8, 0.7), (1, 1, 1), [("Size", 0.45)])],
+                         inst("formulas/sphere_primitive.wgsl", (-1.75, -0.8, 0.7), (1, 1, 1), [("Radius", 0.45)])],
            "lights": [], "fog_emitters": []}
     view, scene = runtime.load_scene_file(json.dumps(doc))
     assert scene is not None and scene.instance_count == 4
