@@ -71,6 +71,109 @@ def helper_module(template: str, names) -> str:
     return "\n".join(parts) + "\n"
 
 
+# The march of the path, from the shader template: march_epsilon (tpl:1813-1815),
+# march_to (tpl:1859-1963) and tetra_gradient (tpl:1790-1804).  The text is rewritten
+# only where the template reaches state outside the function, so that the functions
+# translate on their own: uniform fields become entries of a settings array m
+# (MARCH_SETTINGS), the coarse-march and overstep-watch switches (module-scope
+# private variables, false for this pass) become false, warp_step_limit and
+# accel_skip (warps off, accelerator off) become their off values, scene_de(pos)
+# gains the parameter arrays, and MarchResult(hit, dist, steps, evals) is returned
+# as a vec4f.
+MARCH_FUNCS = ["march_epsilon", "march_to", "tetra_gradient"]
+MARCH_SETTINGS = {"u.resolution.y": 8, "u.epsilon_coefficient": 0, "u.epsilon_floor": 1, "u.max_steps": 2,
+                  "u.refine_fast": 3, "u.refine_hq": 4, "u.high_quality": 5, "u.march_verify": 6,
+                  "u.hq_footprint_budget_px": 7}
+# m[9]: the instance DE factor clamp(step_safety, 0.001, 1) (instance_de_factor
+# tpl:1617-1620 with scale 1)
+MARCH_FORMULAS = ["mandelbrot", "amazingbox_box", "menger3_ifs", "pseudokleinian_kleinian", "sphere_primitive",
+                  "cube_primitive"]
+MARCH_PRELUDE = """
+fn march_result(h: bool, d: f32, s: f32, e: f32) -> vec4f { return vec4f(select(0.0, 1.0, h), d, s, e); }
+fn scene_de(pos: vec3f, p: Params, m: Params) -> f32 {
+    var c = IterCarry(pos, 1.0);
+    let n = de_iterations(p);
+    for (var i = 0; i < n; i++) { c = de_step(c, pos, p); }
+    return de_finalize(c) * m[9];
+}
+"""
+
+
+def march_module(template: str) -> str:
+    """march_epsilon, march_to and tetra_gradient of the template, rewritten as above."""
+    sigs = {"march_epsilon": ("(t: f32)", "(t: f32, m: Params)"),
+            "march_to": ("(origin: vec3f, dir: vec3f, max_t: f32)",
+                         "(origin: vec3f, dir: vec3f, max_t: f32, p: Params, m: Params)"),
+            "tetra_gradient": ("(pos: vec3f, e: f32)", "(pos: vec3f, e: f32, p: Params, m: Params)")}
+    out = []
+    for name in MARCH_FUNCS:
+        fn = _extract_fn(template, name)
+        old, new = sigs[name]
+        if old not in fn:
+            raise ValueError(f"{name}: unexpected signature")
+        fn = fn.replace(old, new)
+        for field, k in MARCH_SETTINGS.items():
+            fn = fn.replace(field, f"m[{k}]")
+        fn = fn.replace("g_coarse_march", "false").replace("g_overstep_watch", "false")
+        fn = re.sub(r"^\s*g_overstep_(worst|count)\s*\+?=.*;\s*$", "", fn, flags=re.M)
+        fn = re.sub(r"warp_step_limit\([^()]*\)", "INFINITE_DISTANCE", fn)
+        fn = re.sub(r"accel_skip\([^()]*\)", "0.0", fn)
+        fn = re.sub(r"(?<!fn )\bscene_de\(([^()]*(?:\([^()]*\)[^()]*)*)\)", r"scene_de(\1, p, m)", fn)
+        fn = re.sub(r"(?<!fn )\bmarch_epsilon\(([^()]*)\)", r"march_epsilon(\1, m)", fn)
+        fn = fn.replace("-> MarchResult", "-> vec4f").replace("MarchResult(", "march_result(")
+        if re.search(r"\bu\.[a-z]", fn):
+            raise ValueError(f"{name}: a uniform field is not mapped")
+        out.append(fn)
+    consts = [l for l in template.split("\n")
+              if re.match(r"^const (INFINITE_DISTANCE|COARSE_[A-Z_]+|OVERSTEP_TOLERANCE|TETRAHEDRAL_TAPS)\b", l)]
+    return "\n".join(consts) + "\n" + MARCH_PRELUDE + "\n".join(out) + "\n"
+
+
+MARCH_DRIVER = """
+template <class T> struct RefMarchParams {
+  const float* v;
+  T operator[](int i) const { return T(v[i]); }
+};
+// One primary ray of the fs_simple pass (tpl:4522-4538): pixel centre, tile
+// transform, dir = normalize(forward + uv.x right + uv.y up), march_to to max_dist,
+// and at a hit normalize(tetra_gradient(p, march_epsilon(t))).  out[8]: hit, t,
+// steps, evals (march), normal xyz, normal evals.
+template <class T, class F>
+static void ref_trace_ray(const nd_view_desc& v, const float* prm, const float* m, int64_t local, F&& fns,
+                          double* out) {
+  using V = ndw::v3<T>;
+  const int64_t npix = int64_t(v.tile_w) * v.tile_h;
+  const int64_t pix = local % npix;
+  const T px = T(v.tile_x + int(pix % v.tile_w)) + T(0.5), py = T(v.tile_y + int(pix / v.tile_w)) + T(0.5);
+  const T ndc_x = px / T(v.width) * T(2) - T(1), ndc_y = T(1) - py / T(v.height) * T(2);
+  const T aspect = T(v.width) / T(v.height);
+  const T ux = ndc_x * aspect, uy = -ndc_y;
+  const V fwd(T(v.fwd[0]), T(v.fwd[1]), T(v.fwd[2])), right(T(v.right[0]), T(v.right[1]), T(v.right[2])),
+      up(T(v.up[0]), T(v.up[1]), T(v.up[2]));
+  const V dir = ndw::normalize(fwd + right * ux + up * uy);
+  const V org(T(v.cam_pos[0]), T(v.cam_pos[1]), T(v.cam_pos[2]));
+  RefMarchParams<T> P{prm}, M{m};
+  const ndw::v4<T> r = fns.march(org, dir, T(v.max_dist), P, M);
+  out[0] = double(r.x); out[1] = double(r.y); out[2] = double(r.z); out[3] = double(r.w);
+  out[4] = out[5] = out[6] = out[7] = 0.0;
+  if (r.x > T(0.5)) {
+    const V pos = org + dir * r.y;
+    const V n = ndw::normalize(fns.gradient(pos, fns.eps(r.y, M), P, M));
+    out[4] = double(n.x); out[5] = double(n.y); out[6] = double(n.z); out[7] = 4.0;
+  }
+}
+static void ref_march_settings(const nd_view_desc& v, float* m) {
+  for (int i = 0; i < 16; ++i) m[i] = 0.0f;
+  m[0] = v.eps_coef; m[1] = v.eps_floor; m[2] = float(v.max_steps);
+  m[3] = v.high_quality ? 0.0f : float(v.refine_budget);  // refine_fast
+  m[4] = v.high_quality ? float(v.refine_budget) : 0.0f;  // refine_hq
+  m[5] = float(v.high_quality); m[6] = float(v.march_verify); m[7] = v.hq_footprint_px;
+  m[8] = float(v.height);
+  m[9] = v.step_safety < 0.001f ? 0.001f : (v.step_safety > 1.0f ? 1.0f : v.step_safety);
+}
+"""
+
+
 def build(force: bool = False):
     ref = reference_root()
     if ref is None:
@@ -106,8 +209,17 @@ def build(force: bool = False):
         except TranslateError:
             continue
         names.append((name, ns))
+    march_src = march_module(template)
+    march_units, march_names = [], []
+    for name in MARCH_FORMULAS:
+        with open(files[name], encoding="utf-8") as fh:
+            src = fh.read()
+        ns = "ndrefm_" + name
+        march_units.append(translate_module(src + "\n" + march_src, ns, helper_ns="ndref_tpl"))
+        march_names.append((name, ns))
     lines = ['// reference formula code, mechanically translated (generated; do not edit)',
-             '#include <stdint.h>', '#include <string.h>', '#include "nd_wgsl.h"', helpers] + units
+             '#include <stdint.h>', '#include <string.h>', '#include "nd_wgsl.h"',
+             '#include "../../include/nd_march.h"', helpers] + units + march_units + [MARCH_DRIVER]
     lines.append("""
 template <class T> struct RefParams {
   const float* v;
@@ -151,10 +263,42 @@ extern "C" int ref_de(const char* name, const float* params, int64_t n, const do
   return -1;
 }}
 """)
+    cases = []
+    for k, (name, ns) in enumerate(march_names):
+        lines.append(f"""struct RefMarchFns{k} {{
+  template <class T, class P> ndw::v4<T> march(ndw::v3<T> o, ndw::v3<T> d, T max_t, const P& p, const P& m) const {{
+    return {ns}::march_to<T, P>(o, d, max_t, p, m);
+  }}
+  template <class T, class P> ndw::v3<T> gradient(ndw::v3<T> pos, T e, const P& p, const P& m) const {{
+    return {ns}::tetra_gradient<T, P>(pos, e, p, m);
+  }}
+  template <class T, class P> T eps(T t, const P& m) const {{ return {ns}::march_epsilon<T, P>(t, m); }}
+}};""")
+        cases.append(f'    if (strcmp(name, "{name}") == 0) {{ RefMarchFns{k} f; if (precision == 32) '
+                     f'ref_trace_ray<float>(*v, v->params, m, i, f, o); else ref_trace_ray<double>(*v, v->params, m, i, f, o); continue; }}')
+    lines.append("""
+// The reference's fs_simple primary pass for rays [first, first + n) of a view (tile
+// and spp 1 only): out[8 i ..] as ref_trace_ray.  -1 for a formula without a march.
+extern "C" int ref_trace(const nd_view_desc* v, const char* name, int precision, int64_t first, int64_t n,
+                         double* out) {
+  float m[16];
+  ref_march_settings(*v, m);
+  int found = 0;
+""" + "\n".join(f'  found |= strcmp(name, "{n}") == 0;' for n, _ in march_names) + """
+  if (!found) return -1;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t j = 0; j < n; ++j) {
+    const int64_t i = first + j;
+    double* o = out + 8 * j;
+""" + "\n".join(cases) + """
+  }
+  return 0;
+}
+""")
     src = os.path.join(OUT, "ref_formulas.cpp")
     with open(src, "w", encoding="utf-8") as fh:
         fh.write("\n".join(lines))
-    cmd = ["g++", "-std=c++17", "-O1", "-fPIC", "-shared", "-ffp-contract=off",
+    cmd = ["g++", "-std=c++17", "-O1", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
            "-I", os.path.join(ROOT, "numericdream_b200", "csrc"), src, "-o", LIB + ".tmp"]
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)

@@ -200,6 +200,41 @@ int oracle_render_scene(const nd_view_desc* view, const nd_scene_desc* scene, co
   return 0;
 }
 
+// The primary march alone along given unit directions from the view's camera:
+// out4[4 i ..] = hit, t, probe steps, DE evaluations (march_to's MarchResult).
+int oracle_march_dirs(const nd_view_desc* view, const char* formula_name, int precision, int64_t n,
+                      const double* dirs, double* out4) {
+  const int kind = formula_index(formula_name);
+  if (kind < 0) return -1;
+#pragma omp parallel
+  {
+    Tracer<float> tf(*view, kind);
+    Tracer<double> td(*view, kind);
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i) {
+      RayOut o;
+      memset(&o, 0, sizeof(o));
+      const V3<double> d(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]);
+      if (precision == 32) {
+        DE<float> h{0.0f, 0.0f, 0};
+        tf.evals = 0;
+        tf.march(d, o, h);
+        o.evals = tf.evals;
+      } else {
+        DE<double> h{0.0, 0.0, 0};
+        td.evals = 0;
+        td.march(d, o, h);
+        o.evals = td.evals;
+      }
+      out4[4 * i] = o.hit;
+      out4[4 * i + 1] = o.depth;
+      out4[4 * i + 2] = o.steps;
+      out4[4 * i + 3] = o.evals;
+    }
+  }
+  return 0;
+}
+
 int oracle_max_threads(void) { return omp_get_max_threads(); }
 
 }  // extern "C"

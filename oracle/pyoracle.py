@@ -29,6 +29,7 @@ def lib():
         _LIB.oracle_accel_grid.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_void_p, C.c_int64,
                                            C.c_void_p]
         _LIB.oracle_accel_grid.restype = C.c_int64
+        _LIB.oracle_march_dirs.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p]
         _LIB.oracle_max_threads.restype = C.c_int
     return _LIB
 
@@ -169,3 +170,15 @@ def accel_grid(view: abi.nd_view_desc, formula_name: str, precision=64, nthreads
     if n < 0:
         raise ValueError("oracle_accel_grid refused the view")
     return grid.reshape(levels, res, res, res), prm
+
+
+def march_dirs(view: abi.nd_view_desc, formula_name: str, dirs, precision=64):
+    """The oracle's primary march from the view's camera along given unit directions:
+    (n, 4) array of hit, t, probe steps, DE evaluations."""
+    dirs = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros((dirs.shape[0], 4), np.float64)
+    rc = lib().oracle_march_dirs(C.addressof(view), formula_name.encode(), precision, dirs.shape[0],
+                                 dirs.ctypes.data, out.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"oracle has no formula {formula_name!r}")
+    return out

@@ -12,6 +12,11 @@ Run where a NumericDream checkout exists (default /root/reference, or ND_REFEREN
   parameter sets for the Mandelbulb, Mandelbox, Menger sponge and pseudo-Kleinian.
 * template_consts.json: the values of the shader-template constants that formula
   files may name (template.wgsl module constants).
+* march_reference_fp64.json: the reference's own fs_simple primary pass (march_to,
+  march_epsilon and tetra_gradient of its shader template, run by oracle/_ref in FP64)
+  on 16x16 rays of one view per formula of the benchmarks and per march mode (sphere
+  tracing with bisection; high quality with 20 refinements; verify each step): per
+  ray hit, t, probe steps, march evaluations and the tetrahedral normal.
 """
 
 import ctypes as C
@@ -40,6 +45,38 @@ EXTRA_SETS = {
     "sphere_primitive": [[1.3]],
     "cube_primitive": [[0.7]],
 }
+
+
+MARCH_CASES = [("mandelbrot", workloads.mandelbulb_params(8.0, 12), (0.3, 0.8, -2.4)),
+               ("amazingbox_box", workloads.mandelbox_params(-1.5, 15), (0.5, 0.9, -4.0)),
+               ("menger3_ifs", workloads.menger_params(4), (0.6, 0.9, -2.7)),
+               ("pseudokleinian_kleinian", workloads.pseudo_kleinian_params(1.0), (0.2, 0.3, -2.0)),
+               ("sphere_primitive", [1.0], (0.2, 0.3, -3.0)),
+               ("cube_primitive", [0.7], (0.6, 0.9, -3.0))]
+MARCH_MODES = [{}, {"high_quality": 1, "refine_budget": 20}, {"march_verify": 1, "refine_budget": 3}]
+
+
+def march_view(params, cam, mode):
+    from numericdream_b200 import abi
+
+    return abi.make_view(0, 16, 16, cam, fov_y_deg=60.0, params=params, max_steps=256, **mode)
+
+
+def write_march(lib):
+    lib.ref_trace.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int64, C.c_int64, C.c_void_p]
+    cases = []
+    for name, params, cam in MARCH_CASES:
+        for mode in MARCH_MODES:
+            v = march_view(params, cam, mode)
+            out = np.zeros((256, 8))
+            assert lib.ref_trace(C.addressof(v), name.encode(), 64, 0, 256, out.ctypes.data) == 0
+            cases.append({"formula": name, "params": [float(x) for x in params], "camera": list(cam), "mode": mode,
+                          "hit": [int(x) for x in out[:, 0]], "t": out[:, 1].tolist(),
+                          "steps": [int(x) for x in out[:, 2]], "evals": [int(x) for x in out[:, 3]],
+                          "normal": np.round(out[:, 4:7], 8).tolist()})
+    with open(os.path.join(HERE, "march_reference_fp64.json"), "w") as fh:
+        json.dump({"view": "16x16, fov 60, max_steps 256, make_view defaults otherwise", "cases": cases}, fh,
+                  separators=(",", ":"))
 
 
 def main():
@@ -79,7 +116,9 @@ def main():
             consts[name] = m.group(1).strip()
     with open(os.path.join(HERE, "template_consts.json"), "w") as fh:
         json.dump(consts, fh, indent=1, sort_keys=True)
-    print(f"{len(names)} formulas, {sum(len(v) for v in out['formulas'].values())} parameter sets")
+    write_march(lib)
+    print(f"{len(names)} formulas, {sum(len(v) for v in out['formulas'].values())} parameter sets, "
+          f"{len(MARCH_CASES) * len(MARCH_MODES)} march cases")
 
 
 if __name__ == "__main__":

@@ -63,3 +63,35 @@ def test_mandelbulb_bailout_at_2_is_the_reference_mandelbulb(ctx):
         worst = max(worst, float(_rel(d64, np.asarray(e["de"])).max()))
     print("mandelbulb_bailout(2) vs reference Mandelbulb, fp64 max rel", worst)
     assert worst <= 1e-9
+
+
+MARCH_GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "march_reference_fp64.json")
+
+
+@pytest.mark.parametrize("kernel", [abi.ND_KERNEL_PERSISTENT, abi.ND_KERNEL_PLAIN])
+def test_gpu_march_matches_the_reference_march(ctx, kernel):
+    """The CUDA march with an FP64 DE against the reference's own march code run in
+    FP64 (tests/golden/march_reference_fp64.json: march_to, bisection, verify and
+    high-quality modes, tetrahedral normals): the hit decisions and probe steps agree
+    but for rays the last bits of the DE decide (the GPU's FP64 DE contracts into
+    FMAs), the hit distance to 1e-9."""
+    with open(MARCH_GOLDEN) as fh:
+        cases = json.load(fh)["cases"]
+    for c in cases:
+        v = abi.make_view(runtime.find_formula(c["formula"]), 16, 16, tuple(c["camera"]), fov_y_deg=60.0,
+                          params=c["params"], max_steps=256, **c["mode"])
+        g = runtime.GBuffer.allocate(256)
+        ctx.forward([v], g, runtime.make_opts(kernel=kernel, de_precision=64))
+        o = g.numpy()
+        hit = np.array(c["hit"]) == 1
+        gh = o["normal"][:, 3] > 0.5
+        what = f"{c['formula']} {c['mode']}"
+        assert (gh != hit).sum() <= 1, what
+        assert (o["steps"] != np.array(c["steps"])).sum() <= 2, what
+        both = gh & hit
+        t = np.array(c["t"])
+        if both.any():
+            rel = np.abs(o["depth64"][both] - t[both]) / t[both]
+            assert np.percentile(rel, 99) <= 1e-9, (what, rel.max())
+            ang = np.degrees(np.arccos(np.clip((o["normal"][both, :3] * np.array(c["normal"])[both]).sum(1), -1, 1)))
+            assert np.percentile(ang, 99) <= 0.01, what

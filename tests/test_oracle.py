@@ -126,3 +126,29 @@ def test_edge_cases():
 def test_unknown_formula_raises():
     with pytest.raises(ValueError):
         pyoracle.de("no_such_formula", [0.0], np.zeros((1, 3)))
+
+
+MARCH_GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "march_reference_fp64.json")
+
+
+def test_oracle_march_matches_the_reference_march():
+    """The hand-written march (march_to, bisection, verify and high-quality modes) and
+    tetrahedral normal against the reference's own march code run in FP64
+    (tests/golden/march_reference_fp64.json, written by oracle/_ref)."""
+    with open(MARCH_GOLDEN) as fh:
+        cases = json.load(fh)["cases"]
+    assert len(cases) == 18
+    for c in cases:
+        v = abi.make_view(0, 16, 16, tuple(c["camera"]), fov_y_deg=60.0, params=c["params"], max_steps=256,
+                          **c["mode"])
+        o = pyoracle.render(v, c["formula"], 64)
+        hit = np.array(c["hit"]) == 1
+        what = f"{c['formula']} {c['mode']}"
+        np.testing.assert_array_equal(o["normal"][:, 3] > 0.5, hit, err_msg=what)
+        np.testing.assert_array_equal(o["steps"], c["steps"], err_msg=what)
+        np.testing.assert_array_equal(o["evals"], np.array(c["evals"]) + 4 * hit, err_msg=what)
+        t = np.array(c["t"])
+        rel = np.abs(o["depth64"][hit] - t[hit]) / t[hit]
+        assert rel.max(initial=0.0) <= 1e-13, what
+        np.testing.assert_allclose(o["normal"][hit, :3], np.array(c["normal"])[hit], atol=1e-6, err_msg=what)
+        assert hit.sum() > 0 or c["formula"] == "pseudokleinian_kleinian"
