@@ -24,7 +24,9 @@ cpu_baseline  the oracle's FP32 march (same formulas, same march) on every host 
 
 --impl reference times the CPU implementation of the path on the host cores: the
 reference app itself only runs through WebGPU, which this machine cannot run, so its
-march is timed as the oracle's FP32 restatement with every host thread.
+own march code (march_to and estimate_normal of its shader template, translated
+mechanically and compiled for the host into oracle/_ref) is timed in FP32 with every
+host thread; where that library was not built, the oracle's FP32 restatement.
 """
 
 from __future__ import annotations
@@ -177,6 +179,56 @@ def run_cpu(views, seconds_budget=15.0, with_fp64=False):
     return res
 
 
+def reference_lib():
+    """oracle/_ref's library (the reference's own march, compiled for the host), or None
+    where it was not built (it needs the reference's sources at build time)."""
+    import ctypes as C
+
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_formulas.so")
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    if not hasattr(lib, "ref_trace"):
+        return None
+    lib.ref_trace.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int64, C.c_int64, C.c_void_p]
+    lib.ref_trace.restype = C.c_int
+    return lib
+
+
+def run_cpu_reference(lib, views, seconds_budget=15.0):
+    """The reference's own fs_simple primary pass (march_to and estimate_normal of its
+    shader template, translated mechanically and compiled for the host; FP32 like the
+    reference) on all host cores over a bounded, seeded sample of the views' rays."""
+    import ctypes as C
+
+    import numpy as np
+
+    from numericdream_b200 import runtime
+    from oracle import pyoracle
+
+    cores = pyoracle.max_threads()
+    names = [runtime.formula_name(v.formula).encode() for v in views]
+
+    def run(chunks):
+        rays = evals = 0
+        for vi, first, n in chunks:
+            out = np.zeros((n, 8))
+            if lib.ref_trace(C.addressof(views[vi]), names[vi], 32, first, n, out.ctypes.data) != 0:
+                raise RuntimeError(f"no reference march for {names[vi]!r}")
+            rays += n
+            evals += int(out[:, 3].sum() + out[:, 7].sum())
+        return rays, evals
+
+    t0 = time.perf_counter()
+    r0, _ = run(cpu_sample(views, 2048, seed=1))
+    rate = r0 / max(time.perf_counter() - t0, 1e-6)
+    chunks = cpu_sample(views, max(int(rate * seconds_budget), 4096), seed=2)
+    t0 = time.perf_counter()
+    rays, evals = run(chunks)
+    dt = time.perf_counter() - t0
+    return {"rays_per_s": rays / dt, "evals_per_s": evals / dt, "rays": rays, "seconds": dt, "cores": cores}
+
+
 def error_stats(views, gbuf_np, cpu):
     """GPU output against the FP64 oracle on the sampled rays (hits of both)."""
     import numpy as np
@@ -223,21 +275,31 @@ def reference_arm(args):
     views = build_views(args.workload, runtime.find_formula)
     per, res = [], None
     budget = max(2.0, 60.0 / max(args.steps + args.warmup, 1))
+    ref = reference_lib()
     for i in range(args.warmup + args.steps):
-        res = run_cpu(views, seconds_budget=budget)
+        res = run_cpu_reference(ref, views, seconds_budget=budget) if ref else run_cpu(views, seconds_budget=budget)
         if i >= args.warmup:
             per.append(res)
     v = sum(r["rays_per_s"] for r in per) / len(per) / 1e6
+    if ref:
+        kind = "reference"
+        note = ("the reference's own fs_simple pass (march_to and estimate_normal of its shader template, "
+                "translated mechanically and compiled for the host by oracle/build_ref.py), FP32 as in the "
+                "reference, all host threads; the reference app itself runs only through WebGPU, unavailable "
+                "on this box")
+    else:
+        kind = "port"
+        note = ("the reference's march restated on the CPU (FP32, all host threads); the reference app itself "
+                "runs only through WebGPU, unavailable on this box")
     line = {"metric": METRIC, "value": v, "unit": "Mrays/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config_of(args.workload, views, 1),
             "de_evals_per_s": sum(r["evals_per_s"] for r in per) / len(per),
-            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": res["cores"], "kind": "port",
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": res["cores"], "kind": kind,
                              "sample": f"{res['rays']} rays per step in seeded runs of 64 over all views"},
             "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference's march restated on the CPU (FP32, all host threads); "
-                    "the reference app itself runs only through WebGPU, unavailable on this box"}
+            "note": note}
     print(json.dumps(line))
     return 0
 
@@ -475,12 +537,23 @@ def main():
         achieved = flops / (kms[0] * 1e-3) / 1e12
         cpu, err = None, None
         if not args.no_cpu:
-            c = run_cpu(views, seconds_budget=15.0, with_fp64=True)
-            cpu = {"value": c["rays_per_s"] / 1e6, "unit": "Mrays/s", "cores": c["cores"], "kind": "port",
-                   "sample": f"{c['rays']} rays in seeded runs of 64 consecutive rays over all 64 views "
-                             f"({c['seconds']:.1f} s, FP32 oracle march)",
-                   "de_evals_per_s": c["evals_per_s"]}
+            c = run_cpu(views, seconds_budget=10.0, with_fp64=True)
             err = error_stats(views, gnp, c)
+            ref = reference_lib()
+            if ref:
+                r = run_cpu_reference(ref, views, seconds_budget=10.0)
+                cpu = {"value": r["rays_per_s"] / 1e6, "unit": "Mrays/s", "cores": r["cores"], "kind": "reference",
+                       "sample": f"{r['rays']} rays in seeded runs of 64 consecutive rays over all 64 views "
+                                 f"({r['seconds']:.1f} s, the reference's own march_to + estimate_normal "
+                                 f"compiled for the host, FP32)",
+                       "de_evals_per_s": r["evals_per_s"],
+                       "port": {"value": c["rays_per_s"] / 1e6, "de_evals_per_s": c["evals_per_s"],
+                                "kind": "the oracle's FP32 march"}}
+            else:
+                cpu = {"value": c["rays_per_s"] / 1e6, "unit": "Mrays/s", "cores": c["cores"], "kind": "port",
+                       "sample": f"{c['rays']} rays in seeded runs of 64 consecutive rays over all 64 views "
+                                 f"({c['seconds']:.1f} s, FP32 oracle march)",
+                       "de_evals_per_s": c["evals_per_s"]}
         line = {
             "metric": METRIC, "value": rays_total / (ms_batched * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True,

@@ -298,7 +298,7 @@ extern "C" int ref_trace(const nd_view_desc* v, const char* name, int precision,
     src = os.path.join(OUT, "ref_formulas.cpp")
     with open(src, "w", encoding="utf-8") as fh:
         fh.write("\n".join(lines))
-    cmd = ["g++", "-std=c++17", "-O1", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
+    cmd = ["g++", "-std=c++17", "-O3", "-march=x86-64-v3", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
            "-I", os.path.join(ROOT, "numericdream_b200", "csrc"), src, "-o", LIB + ".tmp"]
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)
