@@ -14,8 +14,13 @@
 // reference's own formula sources, mechanically translated and compiled under
 // oracle/_ref (see build_ref.py), on fixed point sets committed as tests/golden
 // fixtures, and (b) against closed-form answers for the sphere and cube
-// primitives.  The march, normals and shadow logic are pinned only by (b) and by
-// reading: for those, parity with the reference is otherwise unpinned.
+// primitives.  The march (march_to with its bisection, verify and high-quality
+// modes, march_epsilon) and the tetrahedral normal are pinned the same way as (a):
+// the reference's own functions of the shader template, translated mechanically and
+// compiled under oracle/_ref, traced the same rays in FP64, and this restatement
+// matches the committed results bit for bit (hit, t, steps, evaluations).  The
+// shadow ray, the central-difference normal, the Lambert level and the scene,
+// accelerator and trap code are pinned by closed forms and reading only.
 #pragma once
 
 #include <stdint.h>
