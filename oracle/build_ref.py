@@ -196,7 +196,8 @@ def build(force: bool = False):
     os.makedirs(OUT, exist_ok=True)
     with open(tpl_path, encoding="utf-8") as fh:
         template = fh.read()
-    helpers = translate_module(helper_module(template, list(TEMPLATE_FUNCS)), "ndref_tpl", contract=False)
+    helpers = translate_module(helper_module(template, list(TEMPLATE_FUNCS) + ["combine_de"]), "ndref_tpl",
+                               contract=False)
     units, names = [], []
     for name, path in files.items():
         with open(path, encoding="utf-8") as fh:
@@ -293,6 +294,18 @@ extern "C" int ref_trace(const nd_view_desc* v, const char* name, int precision,
 """ + "\n".join(cases) + """
   }
   return 0;
+}
+""")
+    lines.append("""
+// combine_de (tpl:1708-1730) of the template: (distance, material weight) of an
+// instance combined into the scene so far, at n inputs (mode, d, di, k).
+extern "C" void ref_combine(int64_t n, const int32_t* mode, const float* d, const float* di, const float* k,
+                            float* out2) {
+  for (int64_t i = 0; i < n; ++i) {
+    const ndw::v2<float> r = ndref_tpl::combine_de<float, RefMarchParams<float>>(mode[i], d[i], di[i], k[i]);
+    out2[2 * i] = r.x;
+    out2[2 * i + 1] = r.y;
+  }
 }
 """)
     src = os.path.join(OUT, "ref_formulas.cpp")

@@ -235,6 +235,11 @@ int oracle_march_dirs(const nd_view_desc* view, const char* formula_name, int pr
   return 0;
 }
 
+// The oracle's combine (combine_de distance, f32) at n inputs.
+void oracle_combine(int64_t n, const int32_t* mode, const float* d, const float* di, const float* k, float* out) {
+  for (int64_t i = 0; i < n; ++i) out[i] = combine<float>(mode[i], d[i], di[i], k[i]);
+}
+
 int oracle_max_threads(void) { return omp_get_max_threads(); }
 
 }  // extern "C"

@@ -30,6 +30,7 @@ def lib():
                                            C.c_void_p]
         _LIB.oracle_accel_grid.restype = C.c_int64
         _LIB.oracle_march_dirs.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p]
+        _LIB.oracle_combine.argtypes = [C.c_int64] + [C.c_void_p] * 5
         _LIB.oracle_max_threads.restype = C.c_int
     return _LIB
 
@@ -181,4 +182,14 @@ def march_dirs(view: abi.nd_view_desc, formula_name: str, dirs, precision=64):
                                  dirs.ctypes.data, out.ctypes.data)
     if rc != 0:
         raise ValueError(f"oracle has no formula {formula_name!r}")
+    return out
+
+
+def combine(mode, d, di, k):
+    """The oracle's combine_de distance (f32) elementwise."""
+    mode = np.ascontiguousarray(mode, np.int32)
+    d, di, k = (np.ascontiguousarray(x, np.float32) for x in (d, di, k))
+    out = np.zeros(mode.size, np.float32)
+    lib().oracle_combine(mode.size, mode.ctypes.data, d.ctypes.data, di.ctypes.data, k.ctypes.data,
+                         out.ctypes.data)
     return out

@@ -17,6 +17,8 @@ Run where a NumericDream checkout exists (default /root/reference, or ND_REFEREN
   on 16x16 rays of one view per formula of the benchmarks and per march mode (sphere
   tracing with bisection; high quality with 20 refinements; verify each step): per
   ray hit, t, probe steps, march evaluations and the tetrahedral normal.
+* combine_reference_f32.json: the reference's combine_de (instance combine modes,
+  template.wgsl:1708-1730, with smin ... smix) in f32 at 2,800 seeded inputs.
 """
 
 import ctypes as C
@@ -79,6 +81,24 @@ def write_march(lib):
                   separators=(",", ":"))
 
 
+def write_combine(lib):
+    lib.ref_combine.argtypes = [C.c_int64] + [C.c_void_p] * 5
+    rng = np.random.default_rng(5)
+    n = 7 * 400
+    mode = np.repeat(np.arange(7, dtype=np.int32), 400)
+    d = rng.uniform(-1.0, 1.0, n).astype(np.float32)
+    di = rng.uniform(-1.0, 1.0, n).astype(np.float32)
+    k = rng.uniform(0.0, 0.6, n).astype(np.float32)
+    k[::10] = 0.0        # the hard operations
+    k[5::10] = 1e-4      # SMOOTH_K_MIN itself
+    out = np.zeros(2 * n, np.float32)
+    lib.ref_combine(n, mode.ctypes.data, d.ctypes.data, di.ctypes.data, k.ctypes.data, out.ctypes.data)
+    rec = {"mode": mode.tolist(), "d": d.tolist(), "di": di.tolist(), "k": k.tolist(),
+           "de": out[0::2].tolist(), "weight": out[1::2].tolist()}
+    with open(os.path.join(HERE, "combine_reference_f32.json"), "w") as fh:
+        json.dump(rec, fh, separators=(",", ":"))
+
+
 def main():
     ref = build_ref.reference_root()
     if ref is None:
@@ -117,6 +137,7 @@ def main():
     with open(os.path.join(HERE, "template_consts.json"), "w") as fh:
         json.dump(consts, fh, indent=1, sort_keys=True)
     write_march(lib)
+    write_combine(lib)
     print(f"{len(names)} formulas, {sum(len(v) for v in out['formulas'].values())} parameter sets, "
           f"{len(MARCH_CASES) * len(MARCH_MODES)} march cases")
 
