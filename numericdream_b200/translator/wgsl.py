@@ -173,6 +173,12 @@ class If(Stmt):
 
 
 @dataclasses.dataclass
+class Switch(Stmt):
+    sel: Expr
+    clauses: list   # [(case expressions, has default, body)]
+
+
+@dataclasses.dataclass
 class For(Stmt):
     init: Optional[Stmt]
     cond: Optional[Expr]
@@ -394,7 +400,9 @@ class Parser:
             self.i += 1
             self.expect(";")
             return Continue(tok.line)
-        if t in ("loop", "switch", "discard"):
+        if t == "switch":
+            return self.switch_stmt()
+        if t in ("loop", "discard"):
             raise TranslateError(f"'{t}' is not in the supported subset", tok.line)
         s = self.simple_stmt()
         self.expect(";")
@@ -429,6 +437,31 @@ class Parser:
             self.i += 1
             return IncDec(tok.line, e, nt)
         return ExprStmt(tok.line, e)
+
+    def switch_stmt(self):
+        # switch sel { case a, b: { ... } case c, default: { ... } default: { ... } }
+        line = self.expect("switch").line
+        sel = self.expr()
+        self.expect("{")
+        clauses = []
+        while not self.eat("}"):
+            cases, dflt = [], False
+            if self.eat("default"):
+                dflt = True
+            else:
+                self.expect("case")
+                while True:
+                    if self.eat("default"):
+                        dflt = True
+                    else:
+                        cases.append(self.expr())
+                    if not self.eat(","):
+                        break
+                    if self.at(":") or self.at("{"):
+                        break
+            self.eat(":")
+            clauses.append((cases, dflt, self.block()))
+        return Switch(line, sel, clauses)
 
     def if_stmt(self):
         line = self.expect("if").line
@@ -1552,6 +1585,57 @@ class FormulaCompiler:
                 raise TranslateError("while condition must be bool", s.line)
             self.features.add("loop")
             return [pad + f"while ({c.code}) {{"] + self.block(s.body, ind + 1) + [pad + "}"]
+        if isinstance(s, Switch):
+            # an if / else-if chain on the selector: WGSL clauses do not fall through;
+            # a `break` inside a clause (leave the switch) is outside the subset
+            sel = self.expr(s.sel)
+            if sel.ty.kind != "s" or sel.ty.scalar not in ("i32", "u32"):
+                sel = self.convert(sel, I32, s.line) if is_abstract(sel.ty) else sel
+            if sel.ty.kind != "s" or sel.ty.scalar not in ("i32", "u32"):
+                raise TranslateError("switch selector must be an integer", s.line)
+
+            def has_break(body):
+                for st in body:
+                    if isinstance(st, Break):
+                        return True
+                    if isinstance(st, If) and (has_break(st.then) or (st.els and has_break(st.els))):
+                        return True
+                    if isinstance(st, Block) and has_break(st.body):
+                        return True
+                return False
+
+            var = f"sw_{s.line}_{len(self.features)}"
+            out = [pad + "{", pad + f"    const {cpp_type(sel.ty)} {var} = {sel.code};"]
+            default_body = None
+            first = True
+            for cases, dflt, body in s.clauses:
+                if has_break(body):
+                    raise TranslateError("break inside a switch clause is outside the subset", s.line)
+                if dflt:
+                    default_body = body
+                    if not cases:
+                        continue
+                conds = []
+                for c in cases:
+                    ce = self.expr(c)
+                    ce = self.convert(ce, sel.ty, s.line) if (is_abstract(ce.ty) or ce.ty != sel.ty) else ce
+                    conds.append(f"{var} == {ce.code}")
+                if dflt:
+                    continue  # `case x, default` is the default clause
+                out.append(pad + f"    {'if' if first else '} else if'} ({' || '.join(conds)}) {{")
+                out += self.block(body, ind + 2)
+                first = False
+            if default_body is not None:
+                if first:
+                    out.append(pad + "    {")
+                else:
+                    out.append(pad + "    } else {")
+                out += self.block(default_body, ind + 2)
+                out.append(pad + "    }")
+            elif not first:
+                out.append(pad + "    }")
+            out.append(pad + "}")
+            return out
         if isinstance(s, Break):
             return [pad + "break;"]
         if isinstance(s, Continue):

@@ -129,6 +129,40 @@ def march_module(template: str) -> str:
     return "\n".join(consts) + "\n" + MARCH_PRELUDE + "\n".join(out) + "\n"
 
 
+# The orbit trap of the formula wrapper: orbit_trap_distance / _begin / _update /
+# _finish (tpl:1227-1289) with the OrbitTrap record passed as an array t (center xyz,
+# shape, box xyz, mode, radius, tube: TRAP_FIELDS), and the per-formula wrapper that
+# the reference generates (appendFormulaWrapper, fractal_renderer.zig:490-512), read
+# from the Zig source, with the distance LOD off (lod_iterations(n) = (n, 1), so
+# lod_blend gives the full-iteration carry) and the trap record as a parameter.
+TRAP_FUNCS = ["orbit_trap_distance", "orbit_trap_begin", "orbit_trap_update", "orbit_trap_finish"]
+TRAP_FIELDS = {"t.center": "vec3f(t[0], t[1], t[2])", "t.shape": "i32(t[3])", "t.box": "vec3f(t[4], t[5], t[6])",
+               "t.mode": "i32(t[7])", "t.radius": "t[8]", "t.tube": "t[9]"}
+
+
+def trap_module(template: str, renderer_zig: str) -> str:
+    out = [l for l in template.split("\n") if re.match(r"^const TRAP_[A-Z_]+ = ", l)]
+    for name in TRAP_FUNCS:
+        fn = _extract_fn(template, name).replace("t: OrbitTrap", "t: Params")
+        for field, expr in TRAP_FIELDS.items():
+            fn = fn.replace(field, expr)
+        out.append(fn)
+    m = re.search(r"fn appendFormulaWrapper\(.*?\n(.*?)\n\s*, \.\{code\}\);", renderer_zig, re.S)
+    if not m:
+        raise ValueError("appendFormulaWrapper not found")
+    body = "\n".join(l.split("\\\\", 1)[1] for l in m.group(1).split("\n") if "\\\\" in l)
+    body = body.replace("{{", "{").replace("}}", "}").replace("_{0}", "")
+    body = body.replace("fn formula(pos: vec3f, p: Params, slot: i32)", "fn formula_trap(pos: vec3f, p: Params, t: Params)")
+    body = re.sub(r"^\s*g_image_slot = .*;\s*$", "", body, flags=re.M)
+    body = re.sub(r"^\s*let trap_spec = orbit_trap\(slot\);\s*$", "", body, flags=re.M).replace("trap_spec", "t")
+    body = re.sub(r"lod_iterations\(([^()]*\([^()]*\))\)", r"vec2f(f32(\1), 1.0)", body)
+    body = body.replace("lod_blend(carry_lo, carry, lod.y)", "carry")
+    if "slot" in body or "lod_" in body or "formula_trap" not in body:
+        raise ValueError("unexpected formula wrapper text")
+    out.append(body)
+    return "\n".join(out) + "\n"
+
+
 MARCH_DRIVER = """
 template <class T> struct RefMarchParams {
   const float* v;
@@ -211,12 +245,14 @@ def build(force: bool = False):
             continue
         names.append((name, ns))
     march_src = march_module(template)
+    with open(os.path.join(ref, "src", "gpu", "fractal_renderer.zig"), encoding="utf-8") as fh:
+        trap_src = trap_module(template, fh.read())
     march_units, march_names = [], []
     for name in MARCH_FORMULAS:
         with open(files[name], encoding="utf-8") as fh:
             src = fh.read()
         ns = "ndrefm_" + name
-        march_units.append(translate_module(src + "\n" + march_src, ns, helper_ns="ndref_tpl"))
+        march_units.append(translate_module(src + "\n" + march_src + "\n" + trap_src, ns, helper_ns="ndref_tpl"))
         march_names.append((name, ns))
     lines = ['// reference formula code, mechanically translated (generated; do not edit)',
              '#include <stdint.h>', '#include <string.h>', '#include "nd_wgsl.h"',
@@ -264,7 +300,7 @@ extern "C" int ref_de(const char* name, const float* params, int64_t n, const do
   return -1;
 }}
 """)
-    cases = []
+    cases, trap_cases = [], []
     for k, (name, ns) in enumerate(march_names):
         lines.append(f"""struct RefMarchFns{k} {{
   template <class T, class P> ndw::v4<T> march(ndw::v3<T> o, ndw::v3<T> d, T max_t, const P& p, const P& m) const {{
@@ -274,9 +310,24 @@ extern "C" int ref_de(const char* name, const float* params, int64_t n, const do
     return {ns}::tetra_gradient<T, P>(pos, e, p, m);
   }}
   template <class T, class P> T eps(T t, const P& m) const {{ return {ns}::march_epsilon<T, P>(t, m); }}
+  template <class T, class P> ndw::v2<T> de_trap(ndw::v3<T> pos, const P& p, const P& t) const {{
+    return {ns}::formula_trap<T, P>(pos, p, t);
+  }}
 }};""")
+        trap_cases.append(f'  if (strcmp(name, "{name}") == 0) {{ RefMarchFns{k} f; for (int64_t i = 0; i < n; ++i) {{ '
+                          f'if (precision == 32) {{ const auto r = f.de_trap<float>(ndw::v3<float>(float(pts[3*i]), float(pts[3*i+1]), float(pts[3*i+2])), RefMarchParams<float>{{params}}, RefMarchParams<float>{{trap}}); out2[2*i] = r.x; out2[2*i+1] = r.y; }} '
+                          f'else {{ const auto r = f.de_trap<double>(ndw::v3<double>(pts[3*i], pts[3*i+1], pts[3*i+2]), RefMarchParams<double>{{params}}, RefMarchParams<double>{{trap}}); out2[2*i] = r.x; out2[2*i+1] = r.y; }} }} return 0; }}')
         cases.append(f'    if (strcmp(name, "{name}") == 0) {{ RefMarchFns{k} f; if (precision == 32) '
                      f'ref_trace_ray<float>(*v, v->params, m, i, f, o); else ref_trace_ray<double>(*v, v->params, m, i, f, o); continue; }}')
+    lines.append("""
+// The reference's generated formula wrapper (DE and orbit trap) at n points; trap:
+// center xyz, shape, box xyz, mode, radius, tube.  -1 for a formula without one.
+extern "C" int ref_de_trap(const char* name, const float* params, const float* trap, int precision, int64_t n,
+                           const double* pts, double* out2) {
+""" + "\n".join(trap_cases) + """
+  return -1;
+}
+""")
     lines.append("""
 // The reference's fs_simple primary pass for rays [first, first + n) of a view (tile
 // and spp 1 only): out[8 i ..] as ref_trace_ray.  -1 for a formula without a march.

@@ -17,6 +17,10 @@ Run where a NumericDream checkout exists (default /root/reference, or ND_REFEREN
   on 16x16 rays of one view per formula of the benchmarks and per march mode (sphere
   tracing with bisection; high quality with 20 refinements; verify each step): per
   ray hit, t, probe steps, march evaluations and the tetrahedral normal.
+* trap_reference_fp64.json: the reference's generated formula wrapper (formula_N,
+  fractal_renderer.zig:490-512, distance LOD off) with its orbit-trap functions
+  (template.wgsl:1227-1289), FP64, at 32 seeded points per formula of the benchmarks
+  for every trap shape (closest approach) and every trap mode (box shell).
 * combine_reference_f32.json: the reference's combine_de (instance combine modes,
   template.wgsl:1708-1730, with smin ... smix) in f32 at 2,800 seeded inputs.
 """
@@ -81,6 +85,29 @@ def write_march(lib):
                   separators=(",", ":"))
 
 
+TRAP_SPECS = [dict(shape=sh, mode=0) for sh in range(5)] + [dict(shape=2, mode=md) for md in range(1, 5)]
+
+
+def write_trap(lib):
+    lib.ref_de_trap.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p]
+    rng = np.random.default_rng(7)
+    cases = []
+    for name, params, _ in MARCH_CASES:
+        for spec in TRAP_SPECS:
+            trap = np.array([0.1, -0.2, 0.15, spec["shape"], 0.6, 0.5, 0.7, spec["mode"], 0.9, 0.25], np.float32)
+            pts = rng.uniform(-1.5, 1.5, (32, 3))
+            prm = np.zeros(16, np.float32)
+            prm[:len(params)] = params
+            out = np.zeros((32, 2))
+            assert lib.ref_de_trap(name.encode(), prm.ctypes.data, trap.ctypes.data, 64, 32,
+                                   np.ascontiguousarray(pts).ctypes.data, out.ctypes.data) == 0
+            cases.append({"formula": name, "params": [float(x) for x in prm], "trap": [float(x) for x in trap],
+                          "points": pts.tolist(), "de": out[:, 0].tolist(), "trap_value": out[:, 1].tolist()})
+    with open(os.path.join(HERE, "trap_reference_fp64.json"), "w") as fh:
+        json.dump({"trap_fields": "center xyz, shape, box xyz, mode, radius, tube", "cases": cases}, fh,
+                  separators=(",", ":"))
+
+
 def write_combine(lib):
     lib.ref_combine.argtypes = [C.c_int64] + [C.c_void_p] * 5
     rng = np.random.default_rng(5)
@@ -138,6 +165,7 @@ def main():
         json.dump(consts, fh, indent=1, sort_keys=True)
     write_march(lib)
     write_combine(lib)
+    write_trap(lib)
     print(f"{len(names)} formulas, {sum(len(v) for v in out['formulas'].values())} parameter sets, "
           f"{len(MARCH_CASES) * len(MARCH_MODES)} march cases")
 

@@ -95,3 +95,29 @@ def test_gpu_march_matches_the_reference_march(ctx, kernel):
             assert np.percentile(rel, 99) <= 1e-9, (what, rel.max())
             ang = np.degrees(np.arccos(np.clip((o["normal"][both, :3] * np.array(c["normal"])[both]).sum(1), -1, 1)))
             assert np.percentile(ang, 99) <= 0.01, what
+
+
+TRAP_GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "trap_reference_fp64.json")
+
+
+def test_gpu_trap_matches_the_reference_wrapper(ctx):
+    """The CUDA formula wrapper's DE and orbit trap (nd_de_points, FP64 and FP32) against
+    the reference's generated wrapper with its trap functions run in FP64."""
+    from tests.test_oracle import trap_desc
+
+    with open(TRAP_GOLDEN) as fh:
+        cases = json.load(fh)["cases"]
+    worst64 = worst32 = 0.0
+    for c in cases:
+        v = abi.make_view(runtime.find_formula(c["formula"]), 1, 1, (0.0, 0.0, -3.0), params=c["params"])
+        v.trap = trap_desc(c["trap"])
+        pts = np.asarray(c["points"])
+        d64, t64, _ = ctx.de_points(v, pts, 64)
+        d32, t32, _ = ctx.de_points(v, pts, 32)
+        want = np.asarray(c["trap_value"])
+        worst64 = max(worst64, float(np.max(_rel(t64, want))))
+        worst32 = max(worst32, float(np.median(_rel(t32, want))))
+        np.testing.assert_allclose(d64, c["de"], rtol=1e-9, atol=1e-12)
+    print("trap: fp64 max rel", worst64, "fp32 worst median rel", worst32)
+    assert worst64 <= 1e-9
+    assert worst32 <= 1e-3

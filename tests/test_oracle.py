@@ -152,3 +152,30 @@ def test_oracle_march_matches_the_reference_march():
         assert rel.max(initial=0.0) <= 1e-13, what
         np.testing.assert_allclose(o["normal"][hit, :3], np.array(c["normal"])[hit], atol=1e-6, err_msg=what)
         assert hit.sum() > 0 or c["formula"] == "pseudokleinian_kleinian"
+
+
+TRAP_GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "trap_reference_fp64.json")
+
+
+def trap_desc(t):
+    """nd_trap_desc from a fixture's trap record (center xyz, shape, box xyz, mode, radius, tube)."""
+    d = abi.nd_trap_desc()
+    d.center[:] = t[0:3]
+    d.shape = int(t[3])
+    d.box[:] = t[4:7]
+    d.mode = int(t[7])
+    d.radius, d.tube, d.span = t[8], t[9], 1.5
+    return d
+
+
+def test_oracle_trap_matches_the_reference_wrapper():
+    """DE and orbit trap of the oracle's formula wrapper against the reference's
+    generated wrapper with its trap functions, FP64 (tests/golden/trap_reference_fp64.json)."""
+    with open(TRAP_GOLDEN) as fh:
+        cases = json.load(fh)["cases"]
+    assert len(cases) == 6 * 9
+    for c in cases:
+        de, tr, _ = pyoracle.de(c["formula"], c["params"], np.array(c["points"]), 64, trap=trap_desc(c["trap"]))
+        what = f"{c['formula']} trap {c['trap'][3]:.0f}/{c['trap'][7]:.0f}"
+        np.testing.assert_allclose(de, c["de"], rtol=1e-13, atol=1e-15, err_msg=what)
+        np.testing.assert_allclose(tr, c["trap_value"], rtol=1e-13, atol=1e-15, err_msg=what)
