@@ -18,9 +18,11 @@
 // modes, march_epsilon) and the tetrahedral normal are pinned the same way as (a):
 // the reference's own functions of the shader template, translated mechanically and
 // compiled under oracle/_ref, traced the same rays in FP64, and this restatement
-// matches the committed results bit for bit (hit, t, steps, evaluations).  The
-// shadow ray, the central-difference normal, the Lambert level and the scene,
-// accelerator and trap code are pinned by closed forms and reading only.
+// matches the committed results bit for bit (hit, t, steps, evaluations); so are
+// the orbit trap (the reference's generated formula wrapper and trap functions) and
+// the combine modes (its combine_de).  The shadow ray, the central-difference
+// normal, the Lambert level, the scene assembly and the accelerator are pinned by
+// closed forms and reading only.
 #pragma once
 
 #include <stdint.h>

@@ -46,6 +46,17 @@ fn r_var_default() -> f32 { var x: vec3f; return x.x + x.y + x.z; }
 fn r_abstract_mix(x: f32) -> f32 { return 2 * x + 1; }
 fn r_step(e: f32, x: f32) -> f32 { return step(e, x); }
 fn r_mix(a: f32, b: f32, t: f32) -> f32 { return mix(a, b, t); }
+const TWO = 2;
+fn r_switch(x: i32) -> f32 {
+    var d: f32 = 0.5;
+    switch x {
+        case 1: { d = 10.0; }
+        case TWO, 3: { d = 20.0; }
+        case 4, default: { d = -1.0; }
+    }
+    switch x { case 7: { d += 100.0; } }
+    return d;
+}
 fn r_loop(n: i32) -> i32 {
     var s = 0;
     for (var i = 0; i < n; i++) {
@@ -68,6 +79,8 @@ CALLS = [
     ("r_matvec(ndw::v3<float>(0, 1, 0))", 4.0 + 10 * 2.0),
     ("r_arr(3)", 6.0), ("r_arr(9)", 6.0), ("r_arr(-1)", 0.0), ("r_var_default()", 0.0), ("r_abstract_mix(1.5f)", 4.0),
     ("r_step(1.0f, 1.0f)", 1.0), ("r_step(1.0f, 0.5f)", 0.0), ("r_mix(2.0f, 4.0f, 0.25f)", 2.5), ("r_loop(10)", 8),
+    ("r_switch(1)", 10.0), ("r_switch(2)", 20.0), ("r_switch(3)", 20.0), ("r_switch(4)", -1.0), ("r_switch(9)", -1.0),
+    ("r_switch(7)", 99.0),
 ]
 
 
@@ -96,7 +109,8 @@ def test_wgsl_semantics_on_the_host():
 
 @pytest.mark.parametrize("src, msg", [
     ("fn f() -> i32 { loop { break; } return 0; }", "loop"),
-    ("fn f(x: i32) -> i32 { switch x { default: {} } return 0; }", "switch"),
+    ("fn f(x: i32) -> i32 { for (var i = 0; i < 2; i++) { switch x { default: { break; } } } return 0; }",
+     "break inside a switch"),
     ("var<private> g: f32;", "module-scope"),
     ("struct S { a: f32 }", "struct"),
     ("fn f(x: f32) -> f32 { return nosuch(x); }", "unknown function"),
