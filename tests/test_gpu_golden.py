@@ -93,10 +93,9 @@ def test_gpu_march_matches_the_reference_march(ctx, kernel):
         if both.any():
             rel = np.abs(o["depth64"][both] - t[both]) / t[both]
             # a ray whose last DE bits flip a probe or bisection decision ends within
-            # eps(t) of the reference's hit; every other ray to the FP64 DE's rounding
-            same = (o["steps"][both] == np.array(c["steps"])[both])
+            # eps(t) of the reference's hit; the others agree to the FP64 DE's rounding
             assert rel.max() <= 1e-4, (what, rel.max())
-            assert np.percentile(rel[same], 99) <= 1e-9, (what, rel[same].max())
+            assert (rel <= 1e-9).mean() >= 0.95, (what, np.sort(rel)[-5:])
             ang = np.degrees(np.arccos(np.clip((o["normal"][both, :3] * np.array(c["normal"])[both]).sum(1), -1, 1)))
             # the normal sums its taps in f32 (as the reference does), so it carries
             # f32 cancellation even with an FP64 DE: a few hundredths of a degree
