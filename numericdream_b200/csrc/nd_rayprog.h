@@ -209,7 +209,8 @@ template <class T> struct ParamRef {
 // every later iteration would too, and the orbit-trap updates they would make
 // leave the accumulator as it is (min, max, last and iteration modes see the same
 // distance again; average mode only counts changed iterations).  The trap
-// evaluation stops at that fixed point.  The distance-only evaluation of the march
+// evaluation stops right after recording that fixed point (the first unchanged
+// carry is still recorded: on the first iteration it is the only record).  The distance-only evaluation of the march
 // runs every iteration instead: testing the carry costs more per iteration than the
 // iterations it would skip (an escaped Mandelbulb point's step is one length and one
 // comparison), and the loop then matches march_to's evaluation exactly.
@@ -230,9 +231,11 @@ ND_DEV_INLINE DEOut<T> formula_de_p(ndw::v3<T> pos, const PR& p, const nd_trap_d
       const T drp = c.dr;
       c = F::template step<T, PR>(c, pos, p);
       const bool ch = (c.z.x != zp.x) | (c.z.y != zp.y) | (c.z.z != zp.z);
-      if (!ch && !(c.dr != drp)) break;  // fixed point: nothing changes any more
       changed += ch ? 1 : 0;
       trap_update(acc, trap, c.z, ch, it);
+      // fixed point: every later update would see this same carry (the one just
+      // recorded), so nothing changes any more
+      if (!ch && !(c.dr != drp)) break;
     } else {
       c = F::template step<T, PR>(c, pos, p);
     }
