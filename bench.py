@@ -212,7 +212,7 @@ def run_cpu_reference(lib, views, seconds_budget=15.0):
     def run(chunks):
         rays = evals = 0
         for vi, first, n in chunks:
-            out = np.zeros((n, 8))
+            out = np.zeros((n, 12))
             if lib.ref_trace(C.addressof(views[vi]), names[vi], 32, first, n, out.ctypes.data) != 0:
                 raise RuntimeError(f"no reference march for {names[vi]!r}")
             rays += n

@@ -163,6 +163,58 @@ def trap_module(template: str, renderer_zig: str) -> str:
     return "\n".join(out) + "\n"
 
 
+# The shadow ray: visibility_march (tpl:2282-2342) for an opaque scene (the
+# reference's scene_has_transparency false, photons and fake caustics off: the
+# transparent-hit branch is cut, and the spectral tint, which stays 1 then, becomes
+# an f32), its VisParams record passed as an array (VIS_FIELDS), built by the driver
+# from the template's SHADOW_* constants in shadow_factor's order (tpl:2365-2375,
+# checked against the template text).  And the Lambert level of simple_geometry
+# (tpl:4492-4507): its key_dir / lambert / shade statements.
+VIS_FIELDS = ["k", "t0", "hit_eps", "exit_slope", "exit_bias", "step_floor", "floor_growth", "min_step", "tint_cut"]
+SHADOW_ARGS = ["mix(light.shadow_softness, SHADOW_HARD_K, light.hard_shadows)", "bias", "SHADOW_HIT_EPS",
+               "SHADOW_EXIT_SLOPE", "SHADOW_EXIT_BIAS", "SHADOW_STEP_FLOOR", "SHADOW_FLOOR_GROWTH", "SHADOW_MIN_STEP",
+               "SHADOW_TINT_CUT", "min(i32(u.max_steps), SHADOW_MAX_STEPS)", "true"]
+
+
+def shadow_module(template: str):
+    """visibility_march and the simple shade as WGSL, and the SHADOW_* constants."""
+    sf = _extract_fn(template, "shadow_factor")
+    m = re.search(r"VisParams\((.*)\);", sf)
+    args = [a.strip() for a in re.split(r",(?![^()]*\))", m.group(1))] if m else []
+    if args != SHADOW_ARGS or "let bias = SHADOW_BIAS;" not in sf:
+        raise ValueError("shadow_factor builds VisParams differently than expected")
+    consts = {}
+    for name in ("SHADOW_BIAS", "SHADOW_HIT_EPS", "SHADOW_EXIT_SLOPE", "SHADOW_EXIT_BIAS", "SHADOW_STEP_FLOOR",
+                 "SHADOW_FLOOR_GROWTH", "SHADOW_MIN_STEP", "SHADOW_TINT_CUT", "SHADOW_MAX_STEPS"):
+        c = re.search(r"^const " + name + r"\s*=\s*([0-9.eE+-]+);", template, re.M)
+        consts[name] = c.group(1)
+    fn = _extract_fn(template, "visibility_march")
+    old_sig = "(origin: vec3f, light_dir: vec3f, light_dist: f32, vp: VisParams) -> Spec"
+    if old_sig not in fn:
+        raise ValueError("visibility_march: unexpected signature")
+    fn = fn.replace(old_sig, "(origin: vec3f, light_dir: vec3f, light_dist: f32, vp: Params, fp: Params, m: Params) -> f32")
+    for i, f in enumerate(VIS_FIELDS):
+        fn = re.sub(r"\bvp\." + f + r"\b", f"vp[{i}]", fn)
+    fn = fn.replace("vp.steps", "i32(vp[9])").replace("vp.caustics", "(vp[10] > 0.5)")
+    fn = fn.replace("approx_on(APPROX_FAKE_CAUSTICS)", "false").replace("photons_on()", "false")
+    fn = fn.replace("!scene_has_transparency", "true")
+    fn = re.sub(r"let mat = hit_material\(p\)\.mat;.*?(?=\n\s*in_solid = true;)", "", fn, flags=re.S)
+    fn = fn.replace("spec_splat(", "(").replace("spec_scale(tint, ", "tint * (")
+    fn = re.sub(r"accel_skip\([^()]*\)", "0.0", fn)
+    fn = re.sub(r"(?<!fn )\bscene_de\(([^()]*)\)", r"scene_de(\1, fp, m)", fn)
+    if re.search(r"\bspec_\w+\(|\bhit_material\(|\bfake_caustic\(|\bu\.[a-z]|VisParams|\bSpec\b", fn):
+        raise ValueError("visibility_march: unexpected reach outside the function")
+    sg = _extract_fn(template, "simple_geometry")
+    stmts = [re.search(r"^\s*let " + v + r" = .*;$", sg, re.M) for v in ("key_dir", "lambert", "shade")]
+    if not all(stmts):
+        raise ValueError("simple_geometry: unexpected text")
+    body = "\n".join(x.group(0) for x in stmts).replace("u.camera_up", "cam_up").replace("u.camera_right", "cam_right")
+    shade = ("fn simple_shade(dir: vec3f, normal: vec3f, cam_up: vec3f, cam_right: vec3f) -> f32 {\n" + body +
+             "\n    return shade;\n}\n")
+    simple_consts = [l for l in template.split("\n") if re.match(r"^const SIMPLE_(AMBIENT|KEY_UP|KEY_LEFT) = ", l)]
+    return "\n".join(simple_consts) + "\n" + fn + "\n" + shade, consts
+
+
 MARCH_DRIVER = """
 template <class T> struct RefMarchParams {
   const float* v;
@@ -170,11 +222,14 @@ template <class T> struct RefMarchParams {
 };
 // One primary ray of the fs_simple pass (tpl:4522-4538): pixel centre, tile
 // transform, dir = normalize(forward + uv.x right + uv.y up), march_to to max_dist,
-// and at a hit normalize(tetra_gradient(p, march_epsilon(t))).  out[8]: hit, t,
-// steps, evals (march), normal xyz, normal evals.
+// and at a hit normalize(tetra_gradient(p, march_epsilon(t))), simple_geometry's
+// Lambert level with the camera key light and, when the view has a shadow ray, the
+// visibility toward its LIGHT_GLOBAL light (light_sample_ex: distance 2 max_dist)
+// from p + n SHADOW_BIAS.  out[12]: hit, t, steps, evals (march), normal xyz, normal
+// evals, shade, shadow visibility (1 without a shadow ray), 0, 0.
 template <class T, class F>
-static void ref_trace_ray(const nd_view_desc& v, const float* prm, const float* m, int64_t local, F&& fns,
-                          double* out) {
+static void ref_trace_ray(const nd_view_desc& v, const float* prm, const float* m, const float* vis, int64_t local,
+                          F&& fns, double* out) {
   using V = ndw::v3<T>;
   const int64_t npix = int64_t(v.tile_w) * v.tile_h;
   const int64_t pix = local % npix;
@@ -189,12 +244,32 @@ static void ref_trace_ray(const nd_view_desc& v, const float* prm, const float* 
   RefMarchParams<T> P{prm}, M{m};
   const ndw::v4<T> r = fns.march(org, dir, T(v.max_dist), P, M);
   out[0] = double(r.x); out[1] = double(r.y); out[2] = double(r.z); out[3] = double(r.w);
-  out[4] = out[5] = out[6] = out[7] = 0.0;
+  for (int k = 4; k < 12; ++k) out[k] = 0.0;
+  out[9] = 1.0;
   if (r.x > T(0.5)) {
     const V pos = org + dir * r.y;
     const V n = ndw::normalize(fns.gradient(pos, fns.eps(r.y, M), P, M));
     out[4] = double(n.x); out[5] = double(n.y); out[6] = double(n.z); out[7] = 4.0;
+    out[8] = double(fns.shade(dir, n, up, right));
+    if (v.shadow) {
+      const V ld = ndw::normalize(V(T(v.light_dir[0]), T(v.light_dir[1]), T(v.light_dir[2])));
+      RefMarchParams<T> VP{vis};
+      const ndw::v2<T> s = fns.visibility(pos + n * T(vis[1]), ld, T(v.max_dist) * T(2), VP, P, M);
+      out[9] = double(s.x);
+      out[10] = double(s.y);
+    }
   }
+}
+// VisParams of shadow_factor (tpl:2370): k = mix(softness, SHADOW_HARD_K, hard) with
+// the soft light of the view (k = shadow_k), then the SHADOW_* constants.
+static void ref_shadow_settings(const nd_view_desc& v, float* vis) {
+  for (int i = 0; i < 16; ++i) vis[i] = 0.0f;
+  vis[0] = v.shadow_k;
+  vis[1] = REF_SHADOW_BIAS; vis[2] = REF_SHADOW_HIT_EPS; vis[3] = REF_SHADOW_EXIT_SLOPE;
+  vis[4] = REF_SHADOW_EXIT_BIAS; vis[5] = REF_SHADOW_STEP_FLOOR; vis[6] = REF_SHADOW_FLOOR_GROWTH;
+  vis[7] = REF_SHADOW_MIN_STEP; vis[8] = REF_SHADOW_TINT_CUT;
+  vis[9] = float(v.max_steps < REF_SHADOW_MAX_STEPS ? v.max_steps : REF_SHADOW_MAX_STEPS);
+  vis[10] = 1.0f;
 }
 static void ref_march_settings(const nd_view_desc& v, float* m) {
   for (int i = 0; i < 16; ++i) m[i] = 0.0f;
@@ -245,6 +320,8 @@ def build(force: bool = False):
             continue
         names.append((name, ns))
     march_src = march_module(template)
+    shadow_src, shadow_consts = shadow_module(template)
+    march_src += "\n" + shadow_src
     with open(os.path.join(ref, "src", "gpu", "fractal_renderer.zig"), encoding="utf-8") as fh:
         trap_src = trap_module(template, fh.read())
     march_units, march_names = [], []
@@ -256,7 +333,9 @@ def build(force: bool = False):
         march_names.append((name, ns))
     lines = ['// reference formula code, mechanically translated (generated; do not edit)',
              '#include <stdint.h>', '#include <string.h>', '#include "nd_wgsl.h"',
-             '#include "../../include/nd_march.h"', helpers] + units + march_units + [MARCH_DRIVER]
+             '#include "../../include/nd_march.h"', helpers] + units + march_units + \
+            [f"static const float REF_{k} = float({v});" for k, v in shadow_consts.items() if k != "SHADOW_MAX_STEPS"] + \
+            [f"static const int REF_SHADOW_MAX_STEPS = {shadow_consts['SHADOW_MAX_STEPS']};", MARCH_DRIVER]
     lines.append("""
 template <class T> struct RefParams {
   const float* v;
@@ -313,12 +392,20 @@ extern "C" int ref_de(const char* name, const float* params, int64_t n, const do
   template <class T, class P> ndw::v2<T> de_trap(ndw::v3<T> pos, const P& p, const P& t) const {{
     return {ns}::formula_trap<T, P>(pos, p, t);
   }}
+  template <class T> T shade(ndw::v3<T> dir, ndw::v3<T> n, ndw::v3<T> up, ndw::v3<T> right) const {{
+    return {ns}::simple_shade<T, RefMarchParams<T>>(dir, n, up, right);
+  }}
+  // visibility (its DE evaluations are not counted: 0)
+  template <class T, class P> ndw::v2<T> visibility(ndw::v3<T> o, ndw::v3<T> l, T dist, const P& vp, const P& p,
+                                                    const P& m) const {{
+    return ndw::v2<T>({ns}::visibility_march<T, P>(o, l, dist, vp, p, m), T(0));
+  }}
 }};""")
         trap_cases.append(f'  if (strcmp(name, "{name}") == 0) {{ RefMarchFns{k} f; for (int64_t i = 0; i < n; ++i) {{ '
                           f'if (precision == 32) {{ const auto r = f.de_trap<float>(ndw::v3<float>(float(pts[3*i]), float(pts[3*i+1]), float(pts[3*i+2])), RefMarchParams<float>{{params}}, RefMarchParams<float>{{trap}}); out2[2*i] = r.x; out2[2*i+1] = r.y; }} '
                           f'else {{ const auto r = f.de_trap<double>(ndw::v3<double>(pts[3*i], pts[3*i+1], pts[3*i+2]), RefMarchParams<double>{{params}}, RefMarchParams<double>{{trap}}); out2[2*i] = r.x; out2[2*i+1] = r.y; }} }} return 0; }}')
         cases.append(f'    if (strcmp(name, "{name}") == 0) {{ RefMarchFns{k} f; if (precision == 32) '
-                     f'ref_trace_ray<float>(*v, v->params, m, i, f, o); else ref_trace_ray<double>(*v, v->params, m, i, f, o); continue; }}')
+                     f'ref_trace_ray<float>(*v, v->params, m, vis, i, f, o); else ref_trace_ray<double>(*v, v->params, m, vis, i, f, o); continue; }}')
     lines.append("""
 // The reference's generated formula wrapper (DE and orbit trap) at n points; trap:
 // center xyz, shape, box xyz, mode, radius, tube.  -1 for a formula without one.
@@ -330,18 +417,19 @@ extern "C" int ref_de_trap(const char* name, const float* params, const float* t
 """)
     lines.append("""
 // The reference's fs_simple primary pass for rays [first, first + n) of a view (tile
-// and spp 1 only): out[8 i ..] as ref_trace_ray.  -1 for a formula without a march.
+// and spp 1 only): out[12 i ..] as ref_trace_ray.  -1 for a formula without a march.
 extern "C" int ref_trace(const nd_view_desc* v, const char* name, int precision, int64_t first, int64_t n,
                          double* out) {
-  float m[16];
+  float m[16], vis[16];
   ref_march_settings(*v, m);
+  ref_shadow_settings(*v, vis);
   int found = 0;
 """ + "\n".join(f'  found |= strcmp(name, "{n}") == 0;' for n, _ in march_names) + """
   if (!found) return -1;
 #pragma omp parallel for schedule(dynamic, 64)
   for (int64_t j = 0; j < n; ++j) {
     const int64_t i = first + j;
-    double* o = out + 8 * j;
+    double* o = out + 12 * j;
 """ + "\n".join(cases) + """
   }
   return 0;

@@ -17,6 +17,9 @@ Run where a NumericDream checkout exists (default /root/reference, or ND_REFEREN
   on 16x16 rays of one view per formula of the benchmarks and per march mode (sphere
   tracing with bisection; high quality with 20 refinements; verify each step): per
   ray hit, t, probe steps, march evaluations and the tetrahedral normal.
+* shade_reference_fp64.json: simple_geometry's Lambert level (camera key light) and
+  the opaque shadow ray (visibility_march with shadow_factor's parameters) of the
+  reference, FP64, on 16x16 rays of four benchmark formulas, with and without a light.
 * trap_reference_fp64.json: the reference's generated formula wrapper (formula_N,
   fractal_renderer.zig:490-512, distance LOD off) with its orbit-trap functions
   (template.wgsl:1227-1289), FP64, at 32 seeded points per formula of the benchmarks
@@ -74,7 +77,7 @@ def write_march(lib):
     for name, params, cam in MARCH_CASES:
         for mode in MARCH_MODES:
             v = march_view(params, cam, mode)
-            out = np.zeros((256, 8))
+            out = np.zeros((256, 12))
             assert lib.ref_trace(C.addressof(v), name.encode(), 64, 0, 256, out.ctypes.data) == 0
             cases.append({"formula": name, "params": [float(x) for x in params], "camera": list(cam), "mode": mode,
                           "hit": [int(x) for x in out[:, 0]], "t": out[:, 1].tolist(),
@@ -83,6 +86,24 @@ def write_march(lib):
     with open(os.path.join(HERE, "march_reference_fp64.json"), "w") as fh:
         json.dump({"view": "16x16, fov 60, max_steps 256, make_view defaults otherwise", "cases": cases}, fh,
                   separators=(",", ":"))
+    # the Lambert level (simple_geometry's camera key light, which takes the camera's
+    # up and right as they are: a 90 degree field of view keeps them unit) and the
+    # shadow ray toward a directional light
+    from numericdream_b200 import abi
+
+    shade_cases = []
+    for name, params, cam in MARCH_CASES[:4]:
+        for shadow in (0, 1):
+            v = abi.make_view(0, 16, 16, cam, fov_y_deg=90.0, params=params, max_steps=256, shadow=shadow,
+                              light_dir=(0.4, 0.8, -0.45) if shadow else (0.0, 0.0, 0.0))
+            out = np.zeros((256, 12))
+            assert lib.ref_trace(C.addressof(v), name.encode(), 64, 0, 256, out.ctypes.data) == 0
+            shade_cases.append({"formula": name, "params": [float(x) for x in params], "camera": list(cam),
+                                "shadow": shadow, "hit": [int(x) for x in out[:, 0]],
+                                "shade": out[:, 8].tolist(), "visibility": out[:, 9].tolist()})
+    with open(os.path.join(HERE, "shade_reference_fp64.json"), "w") as fh:
+        json.dump({"view": "16x16, fov 90, max_steps 256; light_dir (0.4, 0.8, -0.45) with a shadow ray",
+                   "cases": shade_cases}, fh, separators=(",", ":"))
 
 
 TRAP_SPECS = [dict(shape=sh, mode=0) for sh in range(5)] + [dict(shape=2, mode=md) for md in range(1, 5)]
