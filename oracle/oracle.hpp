@@ -20,9 +20,9 @@
 // compiled under oracle/_ref, traced the same rays in FP64, and this restatement
 // matches the committed results bit for bit (hit, t, steps, evaluations); so are
 // the orbit trap (the reference's generated formula wrapper and trap functions) and
-// the combine modes (its combine_de).  The shadow ray, the central-difference
-// normal, the Lambert level, the scene assembly and the accelerator are pinned by
-// closed forms and reading only.
+// the combine modes (its combine_de), the opaque shadow ray (visibility_march) and
+// the Lambert level (simple_geometry).  The central-difference normal, the scene
+// assembly and the accelerator are pinned by closed forms and reading only.
 #pragma once
 
 #include <stdint.h>

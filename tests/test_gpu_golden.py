@@ -127,3 +127,28 @@ def test_gpu_trap_matches_the_reference_wrapper(ctx):
     # FP64 to rounding (the GPU contracts into FMAs along the iterations)
     assert worst64 <= 1e-8
     assert worst32 <= 1e-3
+
+
+SHADE_GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "shade_reference_fp64.json")
+
+
+def test_gpu_shade_and_shadow_match_the_reference(ctx):
+    """The CUDA Lambert level and shadow visibility (FP64 DE) against the reference's
+    simple_geometry and visibility_march run in FP64."""
+    with open(SHADE_GOLDEN) as fh:
+        cases = json.load(fh)["cases"]
+    for c in cases:
+        kw = dict(shadow=1, light_dir=(0.4, 0.8, -0.45)) if c["shadow"] else {}
+        v = abi.make_view(runtime.find_formula(c["formula"]), 16, 16, tuple(c["camera"]), fov_y_deg=90.0,
+                          params=c["params"], max_steps=256, **kw)
+        g = runtime.GBuffer.allocate(256)
+        ctx.forward([v], g, runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, de_precision=64))
+        o = g.numpy()
+        hit = (np.array(c["hit"]) == 1) & (o["normal"][:, 3] > 0.5)
+        if c["shadow"]:
+            dv = np.abs(o["shadow"][hit] - np.array(c["visibility"])[hit])
+            share = 0.8 if c["formula"] == "pseudokleinian_kleinian" else 0.97
+            assert (dv <= 1e-4).mean() >= share, (c["formula"], (dv <= 1e-4).mean())
+        else:
+            ds = np.abs(o["shade"][hit] - np.array(c["shade"])[hit])
+            assert np.percentile(ds, 99) <= 1e-4, (c["formula"], ds.max())
