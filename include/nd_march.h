@@ -365,6 +365,49 @@ nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t nviews, co
 nd_status nd_de_points(nd_ctx* ctx, const nd_view_desc* view, int64_t n, const double* pts, double* de,
                        double* trap, uint32_t* iters, int32_t de_precision, void* stream);
 
+/* Lite shading of a forward call's hits (shade_lite, template.wgsl:4424-4444, as
+ * render_lite draws a hit :4446-4458): the material from the view's colour strip
+ * (sample_gradient :2003-2023 at orbit_trap_to_strip :2025-2035 of the ray's orbit
+ * trap), ambient occlusion (calc_ao :1825-1840), and every light's Lambert and
+ * Blinn-Phong terms (light_sample_ex :2178-2190 for point and global lights),
+ * times 1 - Fresnel (fresnel_schlick :3424-3430).  No shadows, as in the reference's
+ * lite pass.  Misses take the background colour (the reference's sky is out of
+ * this pass's scope).  Colour stops are sorted by position, as the reference's
+ * host does (sortedColorOrder, scene_state.zig:98-108). */
+#define ND_MAX_COLOR_STOPS 16  /* MAX_COLOR_STOPS tpl:24 */
+#define ND_MAX_LIGHTS 8        /* MAX_LIGHTS tpl:27 */
+enum { ND_LIGHT_POINT = 0, ND_LIGHT_GLOBAL = 1 };
+typedef struct nd_color_stop {
+  float color[3];
+  float position;    /* along the strip, 0..1 */
+  float glossiness;  /* 0..1: specular weight and power mix(4, 128, g) */
+  float ior;         /* Fresnel index (>= 1 used) */
+  float reserved[2];
+} nd_color_stop;
+typedef struct nd_light {
+  float color[3];
+  float brightness;
+  float position_or_direction[3]; /* point: position; global: direction to the light */
+  int32_t type;                   /* ND_LIGHT_POINT / ND_LIGHT_GLOBAL */
+} nd_light;
+typedef struct nd_lite_desc {
+  int32_t color_count;            /* 0: the default material */
+  int32_t light_count;
+  int32_t ambient_occlusion;      /* 1: calc_ao (5 DE evaluations per hit); 0: none */
+  int32_t specular;               /* 1: Blinn-Phong term on */
+  float background[3];
+  int32_t reserved;
+  nd_color_stop colors[ND_MAX_COLOR_STOPS];
+  nd_light lights[ND_MAX_LIGHTS];
+} nd_lite_desc;
+
+/* Lite shading of the views of an earlier nd_march_forward with the same views:
+ * in holds its depth64, normal and trap (device); lite one descriptor per view
+ * (host); rgba (device, 4 floats per ray in G-buffer order) receives the colour
+ * and w = 1 on a hit, 0 on a miss.  Single-instance views (no scenes). */
+nd_status nd_shade_lite(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_lite_desc* lite,
+                        const nd_gbuffer* in, float* rgba, void* stream);
+
 /* The empty-space accelerator grid of one view (its own formula; accel_res > 0),
  * as nd_march_forward builds it before the view's march (cs_build_accel,
  * template.wgsl:5412-5431): grid is a DEVICE array of capacity floats that receives

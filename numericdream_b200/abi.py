@@ -138,6 +138,46 @@ def make_scene(instances, carves=()) -> nd_scene_desc:
     return s
 
 
+ND_MAX_COLOR_STOPS, ND_MAX_LIGHTS = 16, 8
+ND_LIGHT_POINT, ND_LIGHT_GLOBAL = 0, 1
+
+
+class nd_color_stop(C.Structure):
+    _fields_ = [("color", C.c_float * 3), ("position", C.c_float), ("glossiness", C.c_float), ("ior", C.c_float),
+                ("reserved", C.c_float * 2)]
+
+
+class nd_light(C.Structure):
+    _fields_ = [("color", C.c_float * 3), ("brightness", C.c_float), ("position_or_direction", C.c_float * 3),
+                ("type", C.c_int32)]
+
+
+class nd_lite_desc(C.Structure):
+    _fields_ = [("color_count", C.c_int32), ("light_count", C.c_int32), ("ambient_occlusion", C.c_int32),
+                ("specular", C.c_int32), ("background", C.c_float * 3), ("reserved", C.c_int32),
+                ("colors", nd_color_stop * ND_MAX_COLOR_STOPS), ("lights", nd_light * ND_MAX_LIGHTS)]
+
+
+def make_lite(colors=(), lights=(), ambient_occlusion=True, specular=True, background=(0.1, 0.11, 0.13)):
+    """Lite shading descriptor.  colors: [(rgb, position, glossiness, ior)];
+    lights: [(type, position_or_direction, rgb, brightness)]."""
+    d = nd_lite_desc()
+    d.color_count, d.light_count = len(colors), len(lights)
+    d.ambient_occlusion, d.specular = int(bool(ambient_occlusion)), int(bool(specular))
+    d.background[:] = [float(x) for x in background]
+    for i, (rgb, pos, gloss, ior) in enumerate(colors):
+        c = d.colors[i]
+        c.color[:] = [float(x) for x in rgb]
+        c.position, c.glossiness, c.ior = pos, gloss, ior
+    for i, (kind, p, rgb, bright) in enumerate(lights):
+        l = d.lights[i]
+        l.type = kind
+        l.position_or_direction[:] = [float(x) for x in p]
+        l.color[:] = [float(x) for x in rgb]
+        l.brightness = bright
+    return d
+
+
 class nd_gbuffer(C.Structure):
     _fields_ = [("depth", C.c_void_p), ("normal", C.c_void_p), ("trap", C.c_void_p), ("steps", C.c_void_p),
                 ("iters", C.c_void_p), ("shade", C.c_void_p), ("shadow", C.c_void_p), ("depth64", C.c_void_p),

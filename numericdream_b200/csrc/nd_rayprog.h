@@ -1008,4 +1008,119 @@ ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, c
   return uint32_t(taps) | (uint32_t(sev) << 16);
 }
 
+// --------------------------------------------------------------- lite shading
+// orbit_trap_to_strip (tpl:2025-2035): the trap value as a position on the colour
+// strip (TRAP_MIN_SPAN 1e-4; repeat 1 = fract, 2 = mirror, else clamp).
+ND_DEV_INLINE float trap_strip(const nd_trap_desc& t, float v) {
+  const float x = v / fmaxf(t.span, 1e-4f) + t.offset;
+  if (t.repeat == 1) return x - floorf(x);
+  if (t.repeat == 2) {
+    const float h = x * 0.5f;
+    return 1.0f - fabsf((h - floorf(h)) * 2.0f - 1.0f);
+  }
+  return fminf(fmaxf(x, 0.0f), 1.0f);
+}
+
+struct LiteMaterial {
+  float r, g, b, gloss, ior;
+};
+
+// sample_gradient (tpl:2003-2023) over stops sorted by position, with mix_material's
+// blend of the two neighbours (tpl:1980-2001) for the fields shade_lite reads; no
+// stops: default_material (DEFAULT_ALBEDO, DEFAULT_GLOSSINESS, DEFAULT_IOR,
+// tpl:1965-1977).
+ND_DEV_INLINE LiteMaterial lite_material(const nd_lite_desc& L, float t) {
+  const int count = L.color_count < ND_MAX_COLOR_STOPS ? L.color_count : ND_MAX_COLOR_STOPS;
+  auto of = [](const nd_color_stop& c) { return LiteMaterial{c.color[0], c.color[1], c.color[2], c.glossiness, c.ior}; };
+  if (count <= 0) return LiteMaterial{0.8f, 0.8f, 0.85f, 0.3f, 1.5f};
+  if (count == 1 || t <= L.colors[0].position) return of(L.colors[0]);
+  if (t >= L.colors[count - 1].position) return of(L.colors[count - 1]);
+  for (int i = 0; i < count - 1; ++i) {
+    const nd_color_stop& a = L.colors[i];
+    const nd_color_stop& b = L.colors[i + 1];
+    if (t >= a.position && t <= b.position) {
+      const float f = (t - a.position) / fmaxf(b.position - a.position, 1e-4f);  // GRADIENT_MIN_SPAN
+      const float h = 1.0f - f;
+      auto mx = [h](float x, float y) { return x * (1.0f - h) + y * h; };  // mix(b, a, h)
+      return LiteMaterial{mx(b.color[0], a.color[0]), mx(b.color[1], a.color[1]), mx(b.color[2], a.color[2]),
+                          mx(b.glossiness, a.glossiness), mx(b.ior, a.ior)};
+    }
+  }
+  return of(L.colors[count - 1]);
+}
+
+// fresnel_schlick (tpl:3424-3430)
+ND_DEV_INLINE float fresnel_schlick(float cos_theta, float ior) {
+  const float r0root = (1.0f - ior) / (1.0f + ior);
+  const float r0 = r0root * r0root;
+  const float c = fminf(fmaxf(1.0f - fabsf(cos_theta), 0.0f), 1.0f);
+  const float c2 = c * c;
+  return r0 + (1.0f - r0) * c2 * c2 * c;
+}
+
+// calc_ao (tpl:1817-1840): 5 DE samples along the normal, radius clamp(0.04 t,
+// 0.003, 0.25), steps (0.2 + 0.2 i) radius, weights 0.6^i, strength 2.
+template <class Set, class T>
+ND_DEV_INLINE float calc_ao(const DevView& v, D3 pos, float nx, float ny, float nz, double t) {
+  const float radius = fminf(fmaxf(float(t) * 0.04f, 0.003f), 0.25f);
+  float occlusion = 0.0f, weight = 1.0f;
+  for (int i = 0; i < 5; ++i) {
+    const float step = radius * (0.2f + 0.2f * float(i));
+    const D3 q = d3(pos.x + double(nx * step), pos.y + double(ny * step), pos.z + double(nz * step));
+    const float d = float(Set::template de<T>(v.code, to_t<T>(q), v).d);
+    occlusion += fmaxf(step - d, 0.0f) * weight;
+    weight *= 0.6f;
+  }
+  return fminf(fmaxf(1.0f - 2.0f * occlusion / radius, 0.0f), 1.0f);
+}
+
+// shade_lite (tpl:4424-4444) at a hit at distance t along the ray with normal n and
+// orbit-trap value trap: (1 - F) (albedo (0.15 AO + sum ndotl c) + sum specular).
+template <class Set, class T, bool kDir64>
+ND_DEV_INLINE void lite_at_hit(const DevView& v, const nd_lite_desc& L, int64_t local, double t, float nx, float ny,
+                               float nz, float trap, float* rgb) {
+  Dir<kDir64> dir;
+  dir.set(ray_dir(v, local));
+  const D3 dd = dir.get();
+  const D3 pos = fmadd(d3(v.org[0], v.org[1], v.org[2]), dd, t);
+  const LiteMaterial m = lite_material(L, trap_strip(v.trap, trap));
+  const float spec_power = 4.0f + (128.0f - 4.0f) * fminf(fmaxf(m.gloss, 0.0f), 1.0f);  // SPEC_POWER_MIN/MAX
+  const float dx = float(dd.x), dy = float(dd.y), dz = float(dd.z);
+  const float fresnel = fresnel_schlick(dx * nx + dy * ny + dz * nz, fmaxf(m.ior, 1.0f));
+  const float amb = 0.15f * (L.ambient_occlusion ? calc_ao<Set, T>(v, pos, nx, ny, nz, t) : 1.0f);  // AMBIENT_INTENSITY
+  float dr = amb, dg = amb, db = amb, sr = 0.0f, sg = 0.0f, sb = 0.0f;
+  const int lights = L.light_count < ND_MAX_LIGHTS ? L.light_count : ND_MAX_LIGHTS;
+  for (int i = 0; i < lights; ++i) {
+    const nd_light& l = L.lights[i];
+    float lx, ly, lz, cr = l.color[0] * l.brightness, cg = l.color[1] * l.brightness, cb = l.color[2] * l.brightness;
+    if (l.type == ND_LIGHT_POINT) {  // light_sample_ex tpl:2180-2185
+      const float tx = l.position_or_direction[0] - float(pos.x), ty = l.position_or_direction[1] - float(pos.y),
+                  tz = l.position_or_direction[2] - float(pos.z);
+      const float dist = sqrtf(tx * tx + ty * ty + tz * tz);
+      const float inv = 1.0f / fmaxf(dist, 1e-4f);  // EPSILON
+      lx = tx * inv; ly = ty * inv; lz = tz * inv;
+      const float fall = 1.0f / fmaxf(dist * dist, 0.01f);  // LIGHT_MIN_DIST_SQ
+      cr *= fall; cg *= fall; cb *= fall;
+    } else {  // LIGHT_GLOBAL tpl:2186-2189
+      const float px = l.position_or_direction[0], py = l.position_or_direction[1], pz = l.position_or_direction[2];
+      const float inv = 1.0f / sqrtf(px * px + py * py + pz * pz);
+      lx = px * inv; ly = py * inv; lz = pz * inv;
+    }
+    const float ndotl = fmaxf(nx * lx + ny * ly + nz * lz, 0.0f);
+    if (ndotl <= 0.0f) continue;
+    dr += cr * ndotl; dg += cg * ndotl; db += cb * ndotl;
+    if (L.specular) {
+      float hx = lx - dx, hy = ly - dy, hz = lz - dz;
+      const float hl = 1.0f / sqrtf(hx * hx + hy * hy + hz * hz);
+      hx *= hl; hy *= hl; hz *= hl;
+      const float sp = powf(fmaxf(nx * hx + ny * hy + nz * hz, 0.0f), spec_power) * m.gloss;
+      sr += cr * sp; sg += cg * sp; sb += cb * sp;
+    }
+  }
+  const float k = 1.0f - fresnel;
+  rgb[0] = k * (m.r * dr + sr);
+  rgb[1] = k * (m.g * dg + sg);
+  rgb[2] = k * (m.b * db + sb);
+}
+
 }  // namespace nd

@@ -77,6 +77,8 @@ struct nd_ctx {
   nd::AccelJob* d_accel_jobs = nullptr;
   int accel_jobs_cap = 0;
   uint64_t last_accel_voxels = 0;
+  nd_lite_desc* d_lite = nullptr;    // lite-shading descriptors, in plan order
+  int lite_cap = 0;
   bool last_trap = false;
   DevView* h_views = nullptr;  // pinned staging
   int h_views_cap = 0;
@@ -690,6 +692,7 @@ nd_status nd_ctx_destroy(nd_ctx* ctx) {
   if (ctx->d_scenes) cudaFree(ctx->d_scenes);
   if (ctx->d_accel) cudaFree(ctx->d_accel);
   if (ctx->d_accel_jobs) cudaFree(ctx->d_accel_jobs);
+  if (ctx->d_lite) cudaFree(ctx->d_lite);
   if (ctx->h_views) cudaFreeHost(ctx->h_views);
   if (ctx->last_done) cudaEventDestroy(ctx->last_done);
   for (cudaEvent_t ev : ctx->tev) cudaEventDestroy(ev);
@@ -1039,6 +1042,89 @@ nd_status nd_de_points(nd_ctx* ctx, const nd_view_desc* view, int64_t n, const d
   return ND_OK;
 }
 
+nd_status nd_shade_lite(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_lite_desc* lite,
+                        const nd_gbuffer* in, float* rgba, void* stream) {
+  if (!ctx) return ND_ERR_INVALID;
+  if (!lite || !rgba || (uintptr_t(rgba) & 15)) return fail(ctx, ND_ERR_INVALID, "lite descriptors and a 16-byte aligned rgba");
+  if (!in || !in->depth64 || !in->normal || !in->trap)
+    return fail(ctx, ND_ERR_INVALID, "lite shading reads the forward's depth64, normal and trap");
+  std::vector<Launch> plans;
+  int64_t total = 0;
+  nd_status s = prepare(ctx, views, nviews, in, &plans, &total);
+  if (s != ND_OK) return s;
+  for (int i = 0; i < nviews; ++i) {
+    const nd_lite_desc& L = lite[i];
+    if (L.color_count < 0 || L.color_count > ND_MAX_COLOR_STOPS || L.light_count < 0 || L.light_count > ND_MAX_LIGHTS)
+      return fail(ctx, ND_ERR_INVALID, "view %d: color_count 0..%d, light_count 0..%d", i, ND_MAX_COLOR_STOPS,
+                  ND_MAX_LIGHTS);
+    for (int k = 0; k < L.light_count; ++k)
+      if (L.lights[k].type != ND_LIGHT_POINT && L.lights[k].type != ND_LIGHT_GLOBAL)
+        return fail(ctx, ND_ERR_UNSUPPORTED, "view %d light %d: only point and global lights", i, k);
+  }
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ctx->have_last) cudaEventSynchronize(ctx->last_done);  // the staging buffer may feed an earlier copy
+  if ((s = ensure_dev(ctx, &ctx->d_views, &ctx->views_cap, nviews, "view table")) != ND_OK) return s;
+  if ((s = ensure_dev(ctx, &ctx->d_lite, &ctx->lite_cap, nviews, "lite descriptors")) != ND_OK) return s;
+  if (ctx->h_views_cap < nviews) {
+    if (ctx->h_views) cudaFreeHost(ctx->h_views);
+    ctx->h_views = nullptr;
+    ctx->h_views_cap = 0;
+    e = cudaMallocHost((void**)&ctx->h_views, sizeof(DevView) * size_t(std::max(nviews, 64)));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "pinned view staging");
+    ctx->h_views_cap = std::max(nviews, 64);
+  }
+  // views and descriptors in plan order; colour stops sorted by position
+  std::vector<int64_t> out_off(nviews + 1, 0);
+  for (int i = 0; i < nviews; ++i) out_off[i + 1] = out_off[i] + int64_t(views[i].spp) * views[i].tile_w * views[i].tile_h;
+  std::vector<nd_lite_desc> hl(nviews);
+  int base = 0;
+  for (const Launch& L : plans) {
+    int64_t off = 0;
+    for (size_t k = 0; k < L.views.size(); ++k) {
+      const int vi = L.views[k];
+      ctx->h_views[base + k] = make_dev_view(views[vi], off, out_off[vi], L.codes[k]);
+      off += ctx->h_views[base + k].rays;
+      nd_lite_desc d = lite[vi];
+      for (int a = 1; a < d.color_count; ++a)
+        for (int b = a; b > 0 && d.colors[b - 1].position > d.colors[b].position; --b)
+          std::swap(d.colors[b - 1], d.colors[b]);
+      hl[base + k] = d;
+    }
+    base += int(L.views.size());
+  }
+  e = cudaMemcpyAsync(ctx->d_views, ctx->h_views, sizeof(DevView) * size_t(nviews), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->d_lite, hl.data(), sizeof(nd_lite_desc) * size_t(nviews), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "copy lite tables");
+  base = 0;
+  for (const Launch& L : plans) {
+    const int nv = int(L.views.size());
+    int64_t rays = 0;
+    bool dir64 = false;
+    for (int k = 0; k < nv; ++k) {
+      rays += ctx->h_views[base + k].rays;
+      dir64 |= ctx->h_views[base + k].dir64 != 0;
+    }
+    LaunchArgs a;
+    memset(&a, 0, sizeof(a));
+    a.views = ctx->d_views + base;
+    a.nviews = nv;
+    a.total_rays = rays;
+    a.out = *in;
+    // the shading arithmetic is f32 like the reference's; so is the DE of its AO taps
+    const nd::LiteFn fn = dir64 ? L.table.lite_f32_dir64 : L.table.lite_f32;
+    e = fn(a, ctx->d_lite + base, rgba, ctx->num_sms, st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "lite shading launch");
+    base += nv;
+  }
+  e = cudaEventRecord(ctx->last_done, st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "record event");
+  ctx->have_last = true;
+  return ND_OK;
+}
+
 nd_status nd_accel_grid(nd_ctx* ctx, const nd_view_desc* view, int32_t de_precision, float* grid, int64_t capacity,
                         float* prm, int64_t* count) {
   if (!ctx || !view || !grid || !prm || !count) return fail(ctx, ND_ERR_INVALID, "bad nd_accel_grid arguments");
@@ -1088,6 +1174,9 @@ size_t nd_sizeof(const char* name) {
   if (n == "nd_scene_desc") return sizeof(nd_scene_desc);
   if (n == "nd_instance_desc") return sizeof(nd_instance_desc);
   if (n == "nd_mixin_desc") return sizeof(nd_mixin_desc);
+  if (n == "nd_lite_desc") return sizeof(nd_lite_desc);
+  if (n == "nd_color_stop") return sizeof(nd_color_stop);
+  if (n == "nd_light") return sizeof(nd_light);
   if (n == "DevView") return sizeof(DevView);  // the per-view record a forward call copies to the device
   return 0;
 }

@@ -58,6 +58,8 @@ _SIGNATURES = {
                                   C.c_void_p, C.POINTER(C.c_int64)]),
     "nd_scene_file_load": (C.c_int32, [C.c_char_p, C.c_size_t, C.c_int32, C.c_int32, C.POINTER(abi.nd_view_desc),
                                        C.POINTER(abi.nd_scene_desc), C.POINTER(C.c_int32), C.c_char_p, C.c_size_t]),
+    "nd_shade_lite": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(abi.nd_lite_desc),
+                                  C.POINTER(abi.nd_gbuffer), C.c_void_p, C.c_void_p]),
     "nd_march_forward_scenes": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(C.c_int32),
                                             C.POINTER(abi.nd_scene_desc), C.c_int32, C.POINTER(abi.nd_march_opts),
                                             C.POINTER(abi.nd_gbuffer), C.c_void_p]),
@@ -102,7 +104,8 @@ def check_layout(lib=None):
     """Compare the ctypes structure sizes with the library's own."""
     lib = lib or load_library()
     for name in ("nd_view_desc", "nd_trap_desc", "nd_gbuffer", "nd_march_opts", "nd_stats", "nd_param_info",
-                 "nd_tune_result", "nd_orbit_camera", "nd_scene_desc", "nd_instance_desc", "nd_mixin_desc"):
+                 "nd_tune_result", "nd_orbit_camera", "nd_scene_desc", "nd_instance_desc", "nd_mixin_desc",
+                 "nd_lite_desc", "nd_color_stop", "nd_light"):
         mine = C.sizeof(getattr(abi, name))
         theirs = lib.nd_sizeof(name.encode())
         if mine != theirs:
@@ -344,6 +347,21 @@ class Context:
         self._check(st, "nd_de_points")
         torch.cuda.synchronize(pts.device)
         return de.cpu().numpy(), tr.cpu().numpy(), it.cpu().numpy()
+
+    def shade_lite(self, views, lites, gbuf: GBuffer, stream=None):
+        """nd_shade_lite over the G-buffer of a forward of the same views: an (n, 4)
+        float32 device tensor, rgb and w = 1 on a hit."""
+        import torch
+
+        n = gbuf.depth.shape[0]
+        rgba = torch.empty((n, 4), dtype=torch.float32, device=gbuf.depth.device)
+        arr = (abi.nd_view_desc * len(views))(*views)
+        la = (abi.nd_lite_desc * len(views))(*lites)
+        g = gbuf.as_abi()
+        s = None if stream is None else C.c_void_p(stream)
+        st = self.lib.nd_shade_lite(self.handle, arr, len(views), la, C.byref(g), rgba.data_ptr(), s)
+        self._check(st, "nd_shade_lite")
+        return rgba
 
     def accel_grid(self, view: abi.nd_view_desc, de_precision: int = 32):
         """nd_accel_grid: the view's accelerator grid ([level][z][y][x], numpy) and its

@@ -215,6 +215,27 @@ def shadow_module(template: str):
     return "\n".join(simple_consts) + "\n" + fn + "\n" + shade, consts
 
 
+# Pieces of the lite shading: calc_ao (tpl:1825-1840, the ambient-occlusion part
+# switched on, its hotspot bookkeeping dropped), fresnel_schlick (tpl:3424-3430) and
+# orbit_trap_to_strip (tpl:2025-2035, the instance's span / offset / repeat passed as
+# an array s).
+def lite_module(template: str) -> str:
+    ao = _extract_fn(template, "calc_ao").replace("(pos: vec3f, normal: vec3f, t: f32)",
+                                                  "(pos: vec3f, normal: vec3f, t: f32, p: Params, m: Params)")
+    ao = ao.replace("!part_on(PART_AMBIENT_OCCLUSION)", "false")
+    ao = re.sub(r"^\s*(let hot_prev = hot_enter\(.*\);|g_hot_src = hot_prev;)\s*$", "", ao, flags=re.M)
+    ao = re.sub(r"(?<!fn )\bscene_de\(([^()]*)\)", r"scene_de(\1, p, m)", ao)
+    st = _extract_fn(template, "orbit_trap_to_strip").replace("(slot: i32, v: f32)", "(s: Params, v: f32)")
+    for field, k in (("trap_span", 0), ("trap_offset", 1), ("trap_repeat", 2)):
+        st = st.replace(f"u.instances[slot].{field}", f"s[{k}]")
+    fr = _extract_fn(template, "fresnel_schlick")
+    for name, fn in (("calc_ao", ao), ("orbit_trap_to_strip", st)):
+        if re.search(r"\bu\.|hot_|part_on|slot", fn):
+            raise ValueError(f"{name}: unexpected reach outside the function")
+    consts = [l for l in template.split("\n") if re.match(r"^const (AO_[A-Z_]+|TRAP_MIN_SPAN|TRAP_STRIP_[A-Z]+) = ", l)]
+    return "\n".join(consts) + "\n" + ao + "\n" + st + "\n" + fr + "\n"
+
+
 MARCH_DRIVER = """
 template <class T> struct RefMarchParams {
   const float* v;
@@ -321,7 +342,7 @@ def build(force: bool = False):
         names.append((name, ns))
     march_src = march_module(template)
     shadow_src, shadow_consts = shadow_module(template)
-    march_src += "\n" + shadow_src
+    march_src += "\n" + shadow_src + "\n" + lite_module(template)
     with open(os.path.join(ref, "src", "gpu", "fractal_renderer.zig"), encoding="utf-8") as fh:
         trap_src = trap_module(template, fh.read())
     march_units, march_names = [], []
@@ -395,6 +416,11 @@ extern "C" int ref_de(const char* name, const float* params, int64_t n, const do
   template <class T> T shade(ndw::v3<T> dir, ndw::v3<T> n, ndw::v3<T> up, ndw::v3<T> right) const {{
     return {ns}::simple_shade<T, RefMarchParams<T>>(dir, n, up, right);
   }}
+  template <class T, class P> T ao(ndw::v3<T> pos, ndw::v3<T> n, T t, const P& p, const P& m) const {{
+    return {ns}::calc_ao<T, P>(pos, n, t, p, m);
+  }}
+  template <class T, class P> T strip(const P& s, T v) const {{ return {ns}::orbit_trap_to_strip<T, P>(s, v); }}
+  template <class T> T fresnel(T c, T ior) const {{ return {ns}::fresnel_schlick<T, RefMarchParams<T>>(c, ior); }}
   // visibility (its DE evaluations are not counted: 0)
   template <class T, class P> ndw::v2<T> visibility(ndw::v3<T> o, ndw::v3<T> l, T dist, const P& vp, const P& p,
                                                     const P& m) const {{
@@ -406,6 +432,31 @@ extern "C" int ref_de(const char* name, const float* params, int64_t n, const do
                           f'else {{ const auto r = f.de_trap<double>(ndw::v3<double>(pts[3*i], pts[3*i+1], pts[3*i+2]), RefMarchParams<double>{{params}}, RefMarchParams<double>{{trap}}); out2[2*i] = r.x; out2[2*i+1] = r.y; }} }} return 0; }}')
         cases.append(f'    if (strcmp(name, "{name}") == 0) {{ RefMarchFns{k} f; if (precision == 32) '
                      f'ref_trace_ray<float>(*v, v->params, m, vis, i, f, o); else ref_trace_ray<double>(*v, v->params, m, vis, i, f, o); continue; }}')
+    ao_cases = "\n".join(f'  if (strcmp(name, "{n}") == 0) {{ RefMarchFns{k} f; for (int64_t i = 0; i < n; ++i) '
+                          f'out[i] = double(f.ao<double>(ndw::v3<double>(pos[3*i], pos[3*i+1], pos[3*i+2]), '
+                          f'ndw::v3<double>(nrm[3*i], nrm[3*i+1], nrm[3*i+2]), t[i], P, M)); return 0; }}'
+                          for k, (n, _) in enumerate(march_names))
+    lines.append("""
+// calc_ao of the reference at n hit points (FP64; the view's formula and settings).
+extern "C" int ref_ao(const nd_view_desc* v, const char* name, int64_t n, const double* pos, const double* nrm,
+                      const double* t, double* out) {
+  float m[16];
+  ref_march_settings(*v, m);
+  RefMarchParams<double> P{v->params}, M{m};
+""" + ao_cases + """
+  return -1;
+}
+// orbit_trap_to_strip and fresnel_schlick of the reference (f32) at n inputs.
+extern "C" void ref_strip_fresnel(int64_t n, const float* span_offset_repeat, const float* v, const float* cosv,
+                                  const float* ior, float* strip, float* fresnel) {
+  RefMarchFns0 f;
+  for (int64_t i = 0; i < n; ++i) {
+    RefMarchParams<float> s{span_offset_repeat + 3 * i};
+    strip[i] = f.strip<float>(s, v[i]);
+    fresnel[i] = f.fresnel<float>(cosv[i], ior[i]);
+  }
+}
+""")
     lines.append("""
 // The reference's generated formula wrapper (DE and orbit trap) at n points; trap:
 // center xyz, shape, box xyz, mode, radius, tube.  -1 for a formula without one.

@@ -555,6 +555,23 @@ struct AccelGrid {
   }
 };
 
+// orbit_trap_to_strip (tpl:2025-2035): TRAP_MIN_SPAN 1e-4; repeat 1 fract, 2 mirror.
+template <class R> R trap_strip(R span, R offset, int repeat, R v) {
+  const R x = v / std::fmax(span, R(1e-4)) + offset;
+  if (repeat == 1) return x - std::floor(x);
+  if (repeat == 2) return R(1) - std::fabs((x * R(0.5) - std::floor(x * R(0.5))) * R(2) - R(1));
+  return clampv(x, R(0), R(1));
+}
+
+// fresnel_schlick (tpl:3424-3430)
+template <class R> R fresnel_schlick(R cos_theta, R ior) {
+  const R r0root = (R(1) - ior) / (R(1) + ior);
+  const R r0 = r0root * r0root;
+  const R c = clampv(R(1) - std::fabs(cos_theta), R(0), R(1));
+  const R c2 = c * c;
+  return r0 + (R(1) - r0) * c2 * c2 * c;
+}
+
 // ------------------------------------------------------------------ per-ray result
 struct RayOut {
   double depth;       // t at the hit, 0 on a miss
@@ -743,6 +760,101 @@ template <class R> struct Tracer {
       t += std::max(d, 0.001);
     }
     return clampv(res, 0.0, 1.0);
+  }
+
+  // Primary ray direction of a work item (camera ray, see trace()).
+  V3<double> ray_dir(int64_t ray) const {
+    const int64_t npix = int64_t(v.tile_w) * v.tile_h;
+    const int64_t s = ray / npix, pix = ray % npix;
+    const int px = v.tile_x + int(pix % v.tile_w), py = v.tile_y + int(pix / v.tile_w);
+    double jx = 0.5, jy = 0.5;
+    if (v.spp > 1) jitter2(v.seed, uint64_t(s * npix + pix), &jx, &jy);
+    const double ndc_x = 2.0 * (px + jx) / v.width - 1.0;
+    const double ndc_y = 1.0 - 2.0 * (py + jy) / v.height;
+    const double ux = ndc_x * double(v.width) / double(v.height), uy = -ndc_y;
+    const V3<double> f(v.fwd[0], v.fwd[1], v.fwd[2]), r(v.right[0], v.right[1], v.right[2]),
+        u(v.up[0], v.up[1], v.up[2]);
+    return norm(f + r * ux + u * uy);
+  }
+
+  // Lite shading of a hit (shade_lite tpl:4424-4444): material from the colour strip
+  // (orbit_trap_to_strip tpl:2025-2035, sample_gradient tpl:2003-2023 with
+  // mix_material tpl:1980-2001, default_material tpl:1965-1977), ambient occlusion
+  // (calc_ao tpl:1817-1840), point / global lights (light_sample_ex tpl:2178-2189),
+  // Blinn-Phong with power mix(4, 128, glossiness) (tpl:3071-3072), times
+  // 1 - fresnel_schlick (tpl:3424-3430).
+  // calc_ao (tpl:1817-1840)
+  double ao(V3<double> pos, V3<double> n, double t) {
+    const double radius = clampv(t * 0.04, 0.003, 0.25);
+    double occ = 0.0, w = 1.0;
+    for (int i = 0; i < 5; ++i) {
+      const double step = radius * (0.2 + 0.2 * i);
+      const double d = double(de_at(pos + n * step).d);
+      occ += std::max(step - d, 0.0) * w;
+      w *= 0.6;
+    }
+    return clampv(1.0 - 2.0 * occ / radius, 0.0, 1.0);
+  }
+
+  void lite(const nd_lite_desc& L, int64_t ray, double t, V3<double> n, double trap, double* rgb) {
+    const V3<double> dir = ray_dir(ray);
+    const V3<double> pos = org + dir * t;
+    const double strip = trap_strip<double>(v.trap.span, v.trap.offset, v.trap.repeat, trap);
+    double col[3] = {0.8, 0.8, 0.85}, gloss = 0.3, ior = 1.5;
+    const int count = std::min(L.color_count, ND_MAX_COLOR_STOPS);
+    auto take = [&](const nd_color_stop& c) {
+      for (int k = 0; k < 3; ++k) col[k] = c.color[k];
+      gloss = c.glossiness;
+      ior = c.ior;
+    };
+    if (count > 0) {
+      if (count == 1 || strip <= L.colors[0].position) {
+        take(L.colors[0]);
+      } else if (strip >= L.colors[count - 1].position) {
+        take(L.colors[count - 1]);
+      } else {
+        take(L.colors[count - 1]);
+        for (int i = 0; i < count - 1; ++i) {
+          const nd_color_stop& a = L.colors[i];
+          const nd_color_stop& b = L.colors[i + 1];
+          if (strip >= a.position && strip <= b.position) {
+            const double f = (strip - a.position) / std::max(double(b.position) - a.position, 1e-4);
+            for (int k = 0; k < 3; ++k) col[k] = b.color[k] + (a.color[k] - b.color[k]) * (1.0 - f);
+            gloss = b.glossiness + (a.glossiness - b.glossiness) * (1.0 - f);
+            ior = b.ior + (a.ior - b.ior) * (1.0 - f);
+            break;
+          }
+        }
+      }
+    }
+    const double spec_power = 4.0 + (128.0 - 4.0) * clampv(gloss, 0.0, 1.0);
+    const double fresnel = fresnel_schlick(dot(dir, n), std::max(ior, 1.0));
+    const double occl = L.ambient_occlusion ? ao(pos, n, t) : 1.0;
+    double diff[3] = {0.15 * occl, 0.15 * occl, 0.15 * occl}, spec[3] = {0, 0, 0};
+    for (int i = 0; i < std::min(L.light_count, ND_MAX_LIGHTS); ++i) {
+      const nd_light& l = L.lights[i];
+      const V3<double> p(l.position_or_direction[0], l.position_or_direction[1], l.position_or_direction[2]);
+      double lc[3] = {double(l.color[0]) * l.brightness, double(l.color[1]) * l.brightness,
+                      double(l.color[2]) * l.brightness};
+      V3<double> ld;
+      if (l.type == ND_LIGHT_POINT) {
+        const V3<double> tl = p - pos;
+        const double dist = len(tl);
+        ld = tl / std::max(dist, 1e-4);
+        for (double& x2 : lc) x2 /= std::max(dist * dist, 0.01);
+      } else {
+        ld = norm(p);
+      }
+      const double ndotl = std::max(dot(n, ld), 0.0);
+      if (ndotl <= 0.0) continue;
+      for (int k = 0; k < 3; ++k) diff[k] += lc[k] * ndotl;
+      if (L.specular) {
+        const V3<double> h = norm(ld - dir);
+        const double sp = std::pow(std::max(dot(n, h), 0.0), spec_power) * gloss;
+        for (int k = 0; k < 3; ++k) spec[k] += lc[k] * sp;
+      }
+    }
+    for (int k = 0; k < 3; ++k) rgb[k] = (1.0 - fresnel) * (col[k] * diff[k] + spec[k]);
   }
 
   RayOut trace(int64_t ray) {

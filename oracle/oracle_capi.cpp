@@ -235,6 +235,59 @@ int oracle_march_dirs(const nd_view_desc* view, const char* formula_name, int pr
   return 0;
 }
 
+// Lite shading of rays [first, first + n) of one view from given forward outputs
+// (depth64, normal4, trap, indexed 0..n-1): rgba[4 i ..] = rgb, w = hit.
+int oracle_shade_lite(const nd_view_desc* view, const char* formula_name, const nd_lite_desc* lite, int precision,
+                      int64_t first, int64_t n, const double* depth64, const float* normal4, const float* trap,
+                      float* rgba) {
+  const int kind = formula_index(formula_name);
+  if (kind < 0) return -1;
+#pragma omp parallel
+  {
+    Tracer<float> tf(*view, kind);
+    Tracer<double> td(*view, kind);
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i) {
+      if (!(normal4[4 * i + 3] > 0.5f)) {
+        for (int k = 0; k < 3; ++k) rgba[4 * i + k] = lite->background[k];
+        rgba[4 * i + 3] = 0.0f;
+        continue;
+      }
+      const V3<double> nn(normal4[4 * i], normal4[4 * i + 1], normal4[4 * i + 2]);
+      double rgb[3];
+      if (precision == 32) tf.lite(*lite, first + i, depth64[i], nn, trap[i], rgb);
+      else td.lite(*lite, first + i, depth64[i], nn, trap[i], rgb);
+      for (int k = 0; k < 3; ++k) rgba[4 * i + k] = float(rgb[k]);
+      rgba[4 * i + 3] = 1.0f;
+    }
+  }
+  return 0;
+}
+
+// The oracle's calc_ao at n hit points (positions, normals, t).
+int oracle_ao(const nd_view_desc* view, const char* formula_name, int precision, int64_t n, const double* pos,
+              const double* nrm, const double* t, double* out) {
+  const int kind = formula_index(formula_name);
+  if (kind < 0) return -1;
+  Tracer<float> tf(*view, kind);
+  Tracer<double> td(*view, kind);
+  for (int64_t i = 0; i < n; ++i) {
+    const V3<double> p(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]), q(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]);
+    out[i] = precision == 32 ? tf.ao(p, q, t[i]) : td.ao(p, q, t[i]);
+  }
+  return 0;
+}
+
+// The oracle's orbit_trap_to_strip and fresnel_schlick (f32) at n inputs.
+void oracle_strip_fresnel(int64_t n, const float* span_offset_repeat, const float* v, const float* cosv,
+                          const float* ior, float* strip, float* fresnel) {
+  for (int64_t i = 0; i < n; ++i) {
+    const float* s = span_offset_repeat + 3 * i;
+    strip[i] = trap_strip<float>(s[0], s[1], int(s[2] + 0.5f), v[i]);
+    fresnel[i] = fresnel_schlick<float>(cosv[i], ior[i]);
+  }
+}
+
 // The oracle's combine (combine_de distance, f32) at n inputs.
 void oracle_combine(int64_t n, const int32_t* mode, const float* d, const float* di, const float* k, float* out) {
   for (int64_t i = 0; i < n; ++i) out[i] = combine<float>(mode[i], d[i], di[i], k[i]);

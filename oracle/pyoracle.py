@@ -31,6 +31,10 @@ def lib():
         _LIB.oracle_accel_grid.restype = C.c_int64
         _LIB.oracle_march_dirs.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p]
         _LIB.oracle_combine.argtypes = [C.c_int64] + [C.c_void_p] * 5
+        _LIB.oracle_shade_lite.argtypes = ([C.c_void_p, C.c_char_p, C.c_void_p, C.c_int, C.c_int64, C.c_int64]
+                                           + [C.c_void_p] * 4)
+        _LIB.oracle_ao.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int64] + [C.c_void_p] * 4
+        _LIB.oracle_strip_fresnel.argtypes = [C.c_int64] + [C.c_void_p] * 6
         _LIB.oracle_max_threads.restype = C.c_int
     return _LIB
 
@@ -193,3 +197,38 @@ def combine(mode, d, di, k):
     lib().oracle_combine(mode.size, mode.ctypes.data, d.ctypes.data, di.ctypes.data, k.ctypes.data,
                          out.ctypes.data)
     return out
+
+
+def shade_lite(view: abi.nd_view_desc, formula_name: str, lite: abi.nd_lite_desc, gbuf: dict, precision=64, first=0):
+    """The oracle's lite shading from forward outputs (depth64, normal, trap arrays)."""
+    depth64 = np.ascontiguousarray(gbuf["depth64"], np.float64)
+    normal = np.ascontiguousarray(gbuf["normal"], np.float32)
+    trap = np.ascontiguousarray(gbuf["trap"], np.float32)
+    n = depth64.shape[0]
+    out = np.zeros((n, 4), np.float32)
+    rc = lib().oracle_shade_lite(C.addressof(view), formula_name.encode(), C.addressof(lite), precision, first, n,
+                                 depth64.ctypes.data, normal.ctypes.data, trap.ctypes.data, out.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"oracle has no formula {formula_name!r}")
+    return out
+
+
+def ao(view: abi.nd_view_desc, formula_name: str, pos, nrm, t, precision=64):
+    """The oracle's calc_ao at hit points."""
+    pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+    nrm = np.ascontiguousarray(nrm, np.float64).reshape(-1, 3)
+    t = np.ascontiguousarray(t, np.float64)
+    out = np.zeros(t.size, np.float64)
+    lib().oracle_ao(C.addressof(view), formula_name.encode(), precision, t.size, pos.ctypes.data, nrm.ctypes.data,
+                    t.ctypes.data, out.ctypes.data)
+    return out
+
+
+def strip_fresnel(sor, v, cosv, ior):
+    """The oracle's orbit_trap_to_strip (sor: (n, 3) span, offset, repeat) and fresnel_schlick, f32."""
+    sor = np.ascontiguousarray(sor, np.float32).reshape(-1, 3)
+    v, cosv, ior = (np.ascontiguousarray(x, np.float32) for x in (v, cosv, ior))
+    st, fr = np.zeros(v.size, np.float32), np.zeros(v.size, np.float32)
+    lib().oracle_strip_fresnel(v.size, sor.ctypes.data, v.ctypes.data, cosv.ctypes.data, ior.ctypes.data,
+                               st.ctypes.data, fr.ctypes.data)
+    return st, fr

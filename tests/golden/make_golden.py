@@ -24,6 +24,9 @@ Run where a NumericDream checkout exists (default /root/reference, or ND_REFEREN
   fractal_renderer.zig:490-512, distance LOD off) with its orbit-trap functions
   (template.wgsl:1227-1289), FP64, at 32 seeded points per formula of the benchmarks
   for every trap shape (closest approach) and every trap mode (box shell).
+* lite_reference.json: pieces of the reference's lite shading: calc_ao (FP64) at the
+  hits of the march fixture's sphere-tracing cases, orbit_trap_to_strip and
+  fresnel_schlick (f32) at 600 seeded inputs.
 * combine_reference_f32.json: the reference's combine_de (instance combine modes,
   template.wgsl:1708-1730, with smin ... smix) in f32 at 2,800 seeded inputs.
 """
@@ -129,6 +132,53 @@ def write_trap(lib):
                   separators=(",", ":"))
 
 
+def write_lite(lib):
+    """calc_ao at the hits of the march fixture's default-mode cases; strip and Fresnel
+    at seeded inputs."""
+    from numericdream_b200 import abi
+
+    lib.ref_ao.argtypes = [C.c_void_p, C.c_char_p, C.c_int64] + [C.c_void_p] * 4
+    lib.ref_strip_fresnel.argtypes = [C.c_int64] + [C.c_void_p] * 6
+    with open(os.path.join(HERE, "march_reference_fp64.json")) as fh:
+        march = json.load(fh)["cases"]
+    ao_cases = []
+    for c in march:
+        if c["mode"]:
+            continue
+        v = march_view(c["params"], c["camera"], c["mode"])
+        hit = np.where(np.array(c["hit"]) == 1)[0][:64]
+        idx = np.arange(256)
+        px, py = idx % 16, idx // 16
+        ux = (2.0 * (px + 0.5) / 16 - 1.0) * 1.0
+        uy = -(1.0 - 2.0 * (py + 0.5) / 16)
+        d = np.array(v.fwd[:])[None] + np.array(v.right[:])[None] * ux[:, None] + np.array(v.up[:])[None] * uy[:, None]
+        d /= np.linalg.norm(d, axis=1)[:, None]
+        t = np.array(c["t"])[hit]
+        pos = np.array(v.cam_pos[:])[None] + d[hit] * t[:, None]
+        nrm = np.array(c["normal"])[hit]
+        nrm /= np.linalg.norm(nrm, axis=1)[:, None]
+        out = np.zeros(len(hit))
+        assert lib.ref_ao(C.addressof(v), c["formula"].encode(), len(hit), np.ascontiguousarray(pos).ctypes.data,
+                          np.ascontiguousarray(nrm).ctypes.data, np.ascontiguousarray(t).ctypes.data,
+                          out.ctypes.data) == 0
+        ao_cases.append({"formula": c["formula"], "params": c["params"], "camera": c["camera"],
+                         "pos": pos.tolist(), "normal": nrm.tolist(), "t": t.tolist(), "ao": out.tolist()})
+    rng = np.random.default_rng(9)
+    n = 600
+    sor = np.stack([rng.uniform(0.0, 3.0, n), rng.uniform(-1.0, 1.0, n), rng.integers(0, 3, n)], 1).astype(np.float32)
+    sor[::25, 0] = 0.0  # spans below TRAP_MIN_SPAN
+    val = rng.uniform(-3.0, 5.0, n).astype(np.float32)
+    cosv = rng.uniform(-1.0, 1.0, n).astype(np.float32)
+    ior = rng.uniform(1.0, 2.5, n).astype(np.float32)
+    st, fr = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    lib.ref_strip_fresnel(n, sor.ctypes.data, val.ctypes.data, cosv.ctypes.data, ior.ctypes.data, st.ctypes.data,
+                          fr.ctypes.data)
+    with open(os.path.join(HERE, "lite_reference.json"), "w") as fh:
+        json.dump({"ao": ao_cases, "strip_fresnel": {"span_offset_repeat": sor.tolist(), "v": val.tolist(),
+                                                    "cos": cosv.tolist(), "ior": ior.tolist(), "strip": st.tolist(),
+                                                    "fresnel": fr.tolist()}}, fh, separators=(",", ":"))
+
+
 def write_combine(lib):
     lib.ref_combine.argtypes = [C.c_int64] + [C.c_void_p] * 5
     rng = np.random.default_rng(5)
@@ -187,6 +237,7 @@ def main():
     write_march(lib)
     write_combine(lib)
     write_trap(lib)
+    write_lite(lib)
     print(f"{len(names)} formulas, {sum(len(v) for v in out['formulas'].values())} parameter sets, "
           f"{len(MARCH_CASES) * len(MARCH_MODES)} march cases")
 
