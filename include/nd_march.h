@@ -432,6 +432,12 @@ nd_status nd_accel_grid(nd_ctx* ctx, const nd_view_desc* view, int32_t de_precis
 nd_status nd_scene_file_load(const char* json, size_t len, int32_t width, int32_t height, nd_view_desc* view,
                              nd_scene_desc* scene, int32_t* needs_scene, char* err, size_t err_len);
 
+/* The lite-shading descriptor of a scene file: the first instance's colour stops
+ * (position, color, glossiness, ior), its visible point and global lights (a global
+ * light's direction, a point light's position; ray lights are left out), ambient
+ * occlusion and specular on, the simple pass's background colour. */
+nd_status nd_scene_file_lite(const char* json, size_t len, nd_lite_desc* lite, char* err, size_t err_len);
+
 /* Size of a public struct by name ("nd_view_desc", ...), for binding layout checks. */
 size_t nd_sizeof(const char* name);
 

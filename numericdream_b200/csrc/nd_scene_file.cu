@@ -455,7 +455,77 @@ struct Loader {
   }
 };
 
+// The lite-shading descriptor of a scene file: the first instance's colour stops
+// (ColorStopState: position, color, glossiness, ior) and the visible point and global
+// lights (LightState.toGpu, scene_state.zig:594-612: a global light's direction, a
+// point light's position; ray lights are not part of the lite pass and are left out).
+bool load_lite(const JVal& root, nd_lite_desc* out, std::string* err) {
+  memset(out, 0, sizeof(*out));
+  out->ambient_occlusion = 1;
+  out->specular = 1;
+  out->background[0] = 0.10f;  // SIMPLE_BACKGROUND (tpl:4419); the sky is not part of this pass
+  out->background[1] = 0.11f;
+  out->background[2] = 0.13f;
+  const JVal* ins = root.kind == JVal::OBJ ? root.get("instances") : nullptr;
+  if (!ins || ins->kind != JVal::ARR || ins->arr.empty()) {
+    *err = "the scene has no instances";
+    return false;
+  }
+  const JVal* colors = ins->arr[0].get("colors");
+  if (colors && colors->kind == JVal::ARR)
+    for (const JVal& c : colors->arr) {
+      if (out->color_count >= ND_MAX_COLOR_STOPS) break;
+      nd_color_stop& d = out->colors[out->color_count++];
+      const JVal* rgb = c.get("color");
+      for (int k = 0; k < 3; ++k)
+        d.color[k] = rgb && rgb->kind == JVal::ARR && rgb->arr.size() > size_t(k) ? float(Loader::num(&rgb->arr[k], 0.5)) : 0.5f;
+      d.position = float(Loader::num(c.get("position"), 0.0));
+      d.glossiness = float(Loader::num(c.get("glossiness"), 0.0));
+      d.ior = float(Loader::num(c.get("ior"), 1.5));
+    }
+  const JVal* lights = root.get("lights");
+  if (lights && lights->kind == JVal::ARR)
+    for (const JVal& l : lights->arr) {
+      if (out->light_count >= ND_MAX_LIGHTS) break;
+      if (!Loader::boolean(l.get("visible"), true)) continue;
+      const JVal* kind = l.get("kind");
+      const std::string k = kind && kind->kind == JVal::STR ? kind->str : "global";
+      if (k != "point" && k != "global") continue;
+      nd_light& d = out->lights[out->light_count++];
+      d.type = k == "point" ? ND_LIGHT_POINT : ND_LIGHT_GLOBAL;
+      const JVal* rgb = l.get("color");
+      for (int q = 0; q < 3; ++q)
+        d.color[q] = rgb && rgb->kind == JVal::ARR && rgb->arr.size() > size_t(q) ? float(Loader::num(&rgb->arr[q], 1.0)) : 1.0f;
+      d.brightness = float(Loader::num(l.get("brightness"), 1.0));
+      const double zero[3] = {0, 0, 0};
+      Loader::vec3_or(l.get(d.type == ND_LIGHT_POINT ? "position" : "direction"), zero, d.position_or_direction);
+    }
+  return true;
+}
+
 }  // namespace
+
+extern "C" nd_status nd_scene_file_lite(const char* json, size_t len, nd_lite_desc* lite, char* err, size_t err_len) {
+  std::string msg;
+  JVal root;
+  JsonParser p(json ? json : "", json ? len : 0);
+  nd_status st = ND_OK;
+  if (!json || !lite) {
+    msg = "bad arguments";
+    st = ND_ERR_INVALID;
+  } else if (!p.parse(&root)) {
+    msg = p.error();
+    st = ND_ERR_INVALID;
+  } else if (!load_lite(root, lite, &msg)) {
+    st = ND_ERR_INVALID;
+  }
+  if (err && err_len) {
+    const size_t n = std::min(err_len - 1, msg.size());
+    memcpy(err, msg.data(), n);
+    err[n] = 0;
+  }
+  return st;
+}
 
 extern "C" nd_status nd_scene_file_load(const char* json, size_t len, int32_t width, int32_t height,
                                         nd_view_desc* view, nd_scene_desc* scene, int32_t* needs_scene, char* err,

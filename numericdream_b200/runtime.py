@@ -60,6 +60,7 @@ _SIGNATURES = {
                                        C.POINTER(abi.nd_scene_desc), C.POINTER(C.c_int32), C.c_char_p, C.c_size_t]),
     "nd_shade_lite": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(abi.nd_lite_desc),
                                   C.POINTER(abi.nd_gbuffer), C.c_void_p, C.c_void_p]),
+    "nd_scene_file_lite": (C.c_int32, [C.c_char_p, C.c_size_t, C.POINTER(abi.nd_lite_desc), C.c_char_p, C.c_size_t]),
     "nd_march_forward_scenes": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(C.c_int32),
                                             C.POINTER(abi.nd_scene_desc), C.c_int32, C.POINTER(abi.nd_march_opts),
                                             C.POINTER(abi.nd_gbuffer), C.c_void_p]),
@@ -175,6 +176,24 @@ def load_scene_file(source, width: int = 0, height: int = 0):
     if st != abi.ND_OK:
         raise NDError(st, err.value.decode())
     return view, (scene if needs.value else None)
+
+
+def load_scene_file_lite(source) -> abi.nd_lite_desc:
+    """nd_scene_file_lite: the lite-shading descriptor (colour stops of the first
+    instance, point and global lights) of a .dream scene (a path or the JSON text)."""
+    if isinstance(source, (bytes, bytearray)):
+        data = bytes(source)
+    elif isinstance(source, str) and source.lstrip().startswith("{"):
+        data = source.encode("utf-8")
+    else:
+        with open(source, "rb") as fh:
+            data = fh.read()
+    lite = abi.nd_lite_desc()
+    err = C.create_string_buffer(256)
+    st = load_library().nd_scene_file_lite(data, len(data), C.byref(lite), err, 256)
+    if st != abi.ND_OK:
+        raise NDError(st, err.value.decode())
+    return lite
 
 
 def view_defaults(fid: int) -> abi.nd_view_desc:

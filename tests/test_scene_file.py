@@ -118,3 +118,23 @@ def test_scene_file_refusals(ndlib):
     d = json.loads(_minimal())
     d["note"] = "café \"quoted\" \\ 😀"
     runtime.load_scene_file(json.dumps(d))
+
+
+def test_scene_file_lite(ndlib):
+    lite = runtime.load_scene_file_lite(SCENE)
+    assert (lite.color_count, lite.light_count, lite.ambient_occlusion, lite.specular) == (2, 2, 1, 1)
+    # stops as saved (the shading call sorts them by position)
+    assert lite.colors[0].position == 1.0 and lite.colors[1].position == 0.0
+    np.testing.assert_allclose(lite.colors[1].color[:], [0.1, 0.2, 0.5], atol=1e-7)
+    assert abs(lite.colors[0].glossiness - 0.7) < 1e-7 and abs(lite.colors[0].ior - 1.6) < 1e-7
+    # the global light's direction, the point light's position; the ray light and the
+    # hidden light are left out
+    a, b = lite.lights[0], lite.lights[1]
+    assert a.type == abi.ND_LIGHT_GLOBAL and b.type == abi.ND_LIGHT_POINT
+    np.testing.assert_allclose(a.position_or_direction[:], [-0.4, 0.8, 0.3], atol=1e-7)
+    np.testing.assert_allclose(b.position_or_direction[:], [1.5, 2.0, 2.5], atol=1e-7)
+    assert (a.brightness, b.brightness) == (1.5, 4.0)
+    np.testing.assert_allclose(lite.background[:], [0.10, 0.11, 0.13], atol=1e-7)
+    # a scene without stops or lights: the default material, no lights
+    bare = runtime.load_scene_file_lite(_minimal())
+    assert (bare.color_count, bare.light_count) == (0, 0)
