@@ -312,8 +312,15 @@ def profile_forward(args):
 
     ctx = runtime.Context(0)
     views = build_views(args.workload, runtime.find_formula)
+    for v in views:
+        if args.accel_res:
+            v.accel_res, v.accel_levels, v.accel_safety = args.accel_res, 6, 0.92
     g = runtime.GBuffer.allocate(workloads.rays(views))
     ctx.forward(views, g, runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, refill_threshold=4))
+    if args.with_lite:
+        lite = abi.make_lite([((0.05, 0.05, 0.22), 0.0, 0.2, 1.3), ((1.0, 0.95, 0.82), 1.0, 0.8, 1.7)],
+                             [(abi.ND_LIGHT_GLOBAL, (0.4, 0.8, -0.45), (1.0, 0.95, 0.9), 1.2)])
+        ctx.shade_lite(views, [lite] * len(views), g)
     torch.cuda.synchronize()
     st = ctx.stats()
     print(json.dumps({"workload": args.workload, "rays": workloads.rays(views), "de_evals": st.de_evals,
@@ -344,12 +351,24 @@ def small_and_deepzoom(ctx, sptr, timed, steps):
     out["deepzoom_4096"] = {"ms_per_frame": ms, "Mrays_per_s": n / (ms * 1e-3) / 1e6,
                             "de_evals_per_s": st.de_evals / (ms * 1e-3), "hits": st.hits, "rays": n,
                             "de": "fp64 (an FP32 DE cannot resolve the 1e-12 pixel footprint: no ray hits)"}
-    # batched_64 with the empty-space accelerator on: the reference's default grid
-    # (64^3 x 6 cascades, safety 0.92) and a coarse one; grids built inside every step
+    # lite shading (shade_lite) of batched_64's hits after each forward: colour strip,
+    # ambient occlusion (5 DE evaluations per hit), two lights
     views = workloads.batched_64(runtime.find_formula)
     n = workloads.rays(views)
     g = runtime.GBuffer.allocate(n)
     o = runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT)
+    stops = [((0.05, 0.05, 0.22), 0.0, 0.2, 1.3), ((0.85, 0.35, 0.08), 0.5, 0.5, 1.5), ((1.0, 0.95, 0.82), 1.0, 0.8, 1.7)]
+    lights = [(abi.ND_LIGHT_GLOBAL, (0.4, 0.8, -0.45), (1.0, 0.95, 0.9), 1.2),
+              (abi.ND_LIGHT_POINT, (2.0, 2.5, -3.0), (0.6, 0.7, 1.0), 6.0)]
+    lites = [abi.make_lite(stops, lights) for _ in views]
+    ms_fwd = timed(lambda: ctx.forward(views, g, o, stream=sptr), steps, 3)
+    ms_lite = timed(lambda: (ctx.forward(views, g, o, stream=sptr), ctx.shade_lite(views, lites, g, stream=sptr)),
+                    steps, 3)
+    out["batched_64_lite"] = {"ms_per_step": ms_lite, "Mrays_per_s": n / (ms_lite * 1e-3) / 1e6,
+                              "lite_pass_ms": ms_lite - ms_fwd,
+                              "note": "forward + nd_shade_lite (colour strip, AO, 2 lights) per step"}
+    # batched_64 with the empty-space accelerator on: the reference's default grid
+    # (64^3 x 6 cascades, safety 0.92) and a coarse one; grids built inside every step
     for res in (64, 16):
         av = []
         for v in views:
@@ -409,6 +428,8 @@ def main():
     ap.add_argument("--workload", default="batched_64")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the second (1080p Mandelbox) workload")
+    ap.add_argument("--with-lite", action="store_true", help="--profile-forward: also one lite shading pass")
+    ap.add_argument("--accel-res", type=int, default=0, help="--profile-forward: accelerator grids of this size")
     ap.add_argument("--profile-forward", action="store_true",
                     help="run ONE forward of the workload through the public API and exit (for ncu captures)")
     args = ap.parse_args()
