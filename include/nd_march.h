@@ -404,9 +404,20 @@ typedef struct nd_lite_desc {
 /* Lite shading of the views of an earlier nd_march_forward with the same views:
  * in holds its depth64, normal and trap (device); lite one descriptor per view
  * (host); rgba (device, 4 floats per ray in G-buffer order) receives the colour
- * and w = 1 on a hit, 0 on a miss.  Single-instance views (no scenes). */
+ * and w = 1 on a hit, 0 on a miss.  Views without a scene (see below for scenes). */
 nd_status nd_shade_lite(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_lite_desc* lite,
                         const nd_gbuffer* in, float* rgba, void* stream);
+
+/* Lite shading after nd_march_forward_scenes (the same views, view_scene and
+ * scenes): a scene view's material is hit_material's (template.wgsl:2128-2155):
+ * each visible instance's colour stops at its own trap strip, blended instance by
+ * instance with combine_de's weight; its ambient occlusion samples the scene.
+ * instance_colors holds ND_MAX_INSTANCES descriptors per scene (scene-major; only
+ * their colour stops are read); lite[i] gives view i's lights, switches and
+ * background (and the colours of a view without a scene). */
+nd_status nd_shade_lite_scenes(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const int32_t* view_scene,
+                               const nd_scene_desc* scenes, int32_t nscenes, const nd_lite_desc* lite,
+                               const nd_lite_desc* instance_colors, const nd_gbuffer* in, float* rgba, void* stream);
 
 /* The empty-space accelerator grid of one view (its own formula; accel_res > 0),
  * as nd_march_forward builds it before the view's march (cs_build_accel,
@@ -432,11 +443,12 @@ nd_status nd_accel_grid(nd_ctx* ctx, const nd_view_desc* view, int32_t de_precis
 nd_status nd_scene_file_load(const char* json, size_t len, int32_t width, int32_t height, nd_view_desc* view,
                              nd_scene_desc* scene, int32_t* needs_scene, char* err, size_t err_len);
 
-/* The lite-shading descriptor of a scene file: the first instance's colour stops
- * (position, color, glossiness, ior), its visible point and global lights (a global
+/* The lite-shading descriptor of a scene file: instance `instance`'s colour stops
+ * (position, color, glossiness, ior), the visible point and global lights (a global
  * light's direction, a point light's position; ray lights are left out), ambient
  * occlusion and specular on, the simple pass's background colour. */
-nd_status nd_scene_file_lite(const char* json, size_t len, nd_lite_desc* lite, char* err, size_t err_len);
+nd_status nd_scene_file_lite(const char* json, size_t len, int32_t instance, nd_lite_desc* lite, char* err,
+                             size_t err_len);
 
 /* Size of a public struct by name ("nd_view_desc", ...), for binding layout checks. */
 size_t nd_sizeof(const char* name);

@@ -314,9 +314,10 @@ typedef cudaError_t (*ShadeFn)(const LaunchArgs&, const DevView&, const LaunchCo
 // --------------------------------------------------------------- lite shading
 // One thread per ray of the call (resident grid, strided): misses take the view's
 // background, hits lite_at_hit from the forward's depth64 / normal / trap.
-template <class Set, class T, bool kDir64>
+template <class Set, class T, bool kDir64, bool kScenes = false>
 __global__ void __launch_bounds__(128, MinBlocks<T>::value)
-    lite_kernel(const __grid_constant__ LaunchArgs a, const nd_lite_desc* __restrict__ lites, float4* __restrict__ rgba) {
+    lite_kernel(const __grid_constant__ LaunchArgs a, const nd_lite_desc* __restrict__ lites,
+                const nd_lite_desc* __restrict__ scene_colors, float4* __restrict__ rgba) {
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.total_rays; i += stride) {
     const int vi = find_view(a.views, a.nviews, i);
@@ -330,25 +331,28 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
       continue;
     }
     float rgb[3];
-    lite_at_hit<Set, T, kDir64>(v, L, local, a.out.depth64[r], n.x, n.y, n.z, a.out.trap[r], rgb);
+    lite_at_hit<Set, T, kDir64, kScenes>(v, L, local, a.out.depth64[r], n.x, n.y, n.z, a.out.trap[r], rgb, a.scenes,
+                                         scene_colors);
     rgba[r] = make_float4(rgb[0], rgb[1], rgb[2], 1.0f);
   }
 }
 
-template <class Set, class T, bool kDir64>
-cudaError_t launch_lite(const LaunchArgs& a, const nd_lite_desc* lites, float* rgba, int num_sms, cudaStream_t s) {
+template <class Set, class T, bool kDir64, bool kScenes = false>
+cudaError_t launch_lite(const LaunchArgs& a, const nd_lite_desc* lites, const nd_lite_desc* scene_colors, float* rgba,
+                        int num_sms, cudaStream_t s) {
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lite_kernel<Set, T, kDir64>, 128, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lite_kernel<Set, T, kDir64, kScenes>, 128, 0);
   if (e != cudaSuccess) return e;
   int64_t grid = int64_t(std::max(per_sm, 1)) * num_sms;
   const int64_t needed = (a.total_rays + 127) / 128;
   if (grid > needed) grid = needed;
   if (grid <= 0) return cudaSuccess;
-  lite_kernel<Set, T, kDir64><<<unsigned(grid), 128, 0, s>>>(a, lites, reinterpret_cast<float4*>(rgba));
+  lite_kernel<Set, T, kDir64, kScenes><<<unsigned(grid), 128, 0, s>>>(a, lites, scene_colors,
+                                                                      reinterpret_cast<float4*>(rgba));
   return cudaGetLastError();
 }
 
-typedef cudaError_t (*LiteFn)(const LaunchArgs&, const nd_lite_desc*, float*, int, cudaStream_t);
+typedef cudaError_t (*LiteFn)(const LaunchArgs&, const nd_lite_desc*, const nd_lite_desc*, float*, int, cudaStream_t);
 
 // --------------------------------------------------------------- accelerator build
 // cs_build_accel (tpl:5412-5431): one thread per voxel of every accelerated view of
@@ -450,8 +454,8 @@ struct KernelTable {
   AccelBuildFn scene_accel_build_f32, scene_accel_build_f64;
   LaunchFn scene_persistent_f32_accel, scene_persistent_f64_accel;
   ShadeFn scene_shade_f32_accel, scene_shade_f64_accel;
-  // lite shading of a forward's hits
-  LiteFn lite_f32, lite_f32_dir64;
+  // lite shading of a forward's hits (with scenes: formula groups only)
+  LiteFn lite_f32, lite_f32_dir64, scene_lite_f32;
 };
 
 template <class Set, bool kWithScenes = false> KernelTable make_kernel_table() {
@@ -469,7 +473,9 @@ template <class Set, bool kWithScenes = false> KernelTable make_kernel_table() {
     t.scene_persistent_f64_accel = &launch_persistent<Set, double, true, true, true, true>;
     t.scene_shade_f32_accel = &launch_shade<Set, float, false, true, true, true>;
     t.scene_shade_f64_accel = &launch_shade<Set, double, true, true, true, true>;
+    t.scene_lite_f32 = &launch_lite<Set, float, false, true>;
   } else {
+    t.scene_lite_f32 = nullptr;
     t.scene_persistent_f32 = t.scene_persistent_f32_dir64 = t.scene_persistent_f64 = nullptr;
     t.scene_shade_f32 = t.scene_shade_f32_dir64 = t.scene_shade_f64 = nullptr;
     t.scene_accel_build_f32 = t.scene_accel_build_f64 = nullptr;

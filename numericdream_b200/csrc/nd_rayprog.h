@@ -343,6 +343,20 @@ template <class T> ND_DEV_INLINE T combine_de(int mode, T d, T di, T k) {
   return ndw::smin_nlin(d, di, k);
 }
 
+// The material weight of combine_de (tpl:1708-1730): how much of the scene so far
+// (against the new instance) a hit's material keeps; k <= SMOOTH_K_MIN is hard.
+template <class T> ND_DEV_INLINE T combine_weight(int mode, T d, T di, T k) {
+  const bool hard = k <= T(0.0001);
+  const T closer = di < d ? T(0) : T(1);
+  if (mode == ND_COMBINE_SMOOTH_MIN || mode == ND_COMBINE_SMOOTH_MIX)
+    return hard ? closer : ndw::clamp(T(0.5) + T(0.5) * (di - d) / k, T(0), T(1));
+  if (mode == ND_COMBINE_SMOOTH_MAX)
+    return hard ? (di > d ? T(0) : T(1)) : ndw::clamp(T(0.5) - T(0.5) * (di - d) / k, T(0), T(1));
+  if (mode == ND_COMBINE_SMOOTH_INV_MAX)
+    return hard ? (-di > d ? T(0) : T(1)) : T(1) - ndw::clamp(T(0.5) - T(0.5) * (d + di) / k, T(0), T(1));
+  return closer;  // union, smooth min-lin / min-nlin
+}
+
 // eval_mixed (tpl:1361-1392) with hybrid_cycle_len / hybrid_step (tpl:1335-1359),
 // distance before the instance factor; the trap follows every step.
 template <class Set, class T, bool kTrap>
@@ -1049,6 +1063,35 @@ ND_DEV_INLINE LiteMaterial lite_material(const nd_lite_desc& L, float t) {
   return of(L.colors[count - 1]);
 }
 
+// hit_material (tpl:2128-2155) of a scene, for the lite pass: every visible
+// instance's material (its colour stops at its own trap strip) blended into the
+// scene's with combine_de's weight, instance by instance.  colors: the scene's
+// ND_MAX_INSTANCES descriptors (only their stops are read).
+template <class Set, class T>
+ND_DEV_INLINE LiteMaterial scene_lite_material(const DevScene& S, const nd_lite_desc* colors, ndw::v3<T> pos) {
+  LiteMaterial m{0.8f, 0.8f, 0.85f, 0.3f, 1.5f};
+  T d = T(0);
+  bool first = true;
+  const int count = S.count > 1 ? (S.count < ND_MAX_INSTANCES ? S.count : ND_MAX_INSTANCES) : 1;
+  for (int i = 0; i < count; ++i) {
+    const DevInstance& in = S.inst[i];
+    if (in.hidden) continue;
+    const DEOut<T> di = instance_de<Set, T, true>(in, pos);
+    const LiteMaterial mi = lite_material(colors[i], trap_strip(in.trap, float(di.trap)));
+    if (first) {
+      d = di.d;
+      m = mi;
+      first = false;
+      continue;
+    }
+    const float h = float(combine_weight<T>(in.combine, d, di.d, T(in.blend_k)));
+    auto mx = [h](float b, float a) { return b * (1.0f - h) + a * h; };  // mix_material(m, mi, h)
+    m = LiteMaterial{mx(mi.r, m.r), mx(mi.g, m.g), mx(mi.b, m.b), mx(mi.gloss, m.gloss), mx(mi.ior, m.ior)};
+    d = combine_de<T>(in.combine, d, di.d, T(in.blend_k));
+  }
+  return m;
+}
+
 // fresnel_schlick (tpl:3424-3430)
 ND_DEV_INLINE float fresnel_schlick(float cos_theta, float ior) {
   const float r0root = (1.0f - ior) / (1.0f + ior);
@@ -1060,14 +1103,14 @@ ND_DEV_INLINE float fresnel_schlick(float cos_theta, float ior) {
 
 // calc_ao (tpl:1817-1840): 5 DE samples along the normal, radius clamp(0.04 t,
 // 0.003, 0.25), steps (0.2 + 0.2 i) radius, weights 0.6^i, strength 2.
-template <class Set, class T>
-ND_DEV_INLINE float calc_ao(const DevView& v, D3 pos, float nx, float ny, float nz, double t) {
+template <class Set, class T, bool kScenes = false>
+ND_DEV_INLINE float calc_ao(const DevView& v, D3 pos, float nx, float ny, float nz, double t, const DevScene* scenes) {
   const float radius = fminf(fmaxf(float(t) * 0.04f, 0.003f), 0.25f);
   float occlusion = 0.0f, weight = 1.0f;
   for (int i = 0; i < 5; ++i) {
     const float step = radius * (0.2f + 0.2f * float(i));
     const D3 q = d3(pos.x + double(nx * step), pos.y + double(ny * step), pos.z + double(nz * step));
-    const float d = float(Set::template de<T>(v.code, to_t<T>(q), v).d);
+    const float d = float(view_de<Set, T, false, kScenes>(v, to_t<T>(q), scenes).d);
     occlusion += fmaxf(step - d, 0.0f) * weight;
     weight *= 0.6f;
   }
@@ -1075,19 +1118,28 @@ ND_DEV_INLINE float calc_ao(const DevView& v, D3 pos, float nx, float ny, float 
 }
 
 // shade_lite (tpl:4424-4444) at a hit at distance t along the ray with normal n and
-// orbit-trap value trap: (1 - F) (albedo (0.15 AO + sum ndotl c) + sum specular).
-template <class Set, class T, bool kDir64>
+// orbit-trap value trap: (1 - F) (albedo (0.15 AO + sum ndotl c) + sum specular),
+// AMBIENT_INTENSITY 0.15.  A scene view takes its material from hit_material.
+template <class Set, class T, bool kDir64, bool kScenes = false>
 ND_DEV_INLINE void lite_at_hit(const DevView& v, const nd_lite_desc& L, int64_t local, double t, float nx, float ny,
-                               float nz, float trap, float* rgb) {
+                               float nz, float trap, float* rgb, const DevScene* scenes = nullptr,
+                               const nd_lite_desc* scene_colors = nullptr) {
   Dir<kDir64> dir;
   dir.set(ray_dir(v, local));
   const D3 dd = dir.get();
   const D3 pos = fmadd(d3(v.org[0], v.org[1], v.org[2]), dd, t);
-  const LiteMaterial m = lite_material(L, trap_strip(v.trap, trap));
+  LiteMaterial m;
+  if constexpr (kScenes) {
+    if (v.scene >= 0) m = scene_lite_material<Set, T>(scenes[v.scene], scene_colors + ND_MAX_INSTANCES * v.scene,
+                                                      to_t<T>(pos));
+    else m = lite_material(L, trap_strip(v.trap, trap));
+  } else {
+    m = lite_material(L, trap_strip(v.trap, trap));
+  }
   const float spec_power = 4.0f + (128.0f - 4.0f) * fminf(fmaxf(m.gloss, 0.0f), 1.0f);  // SPEC_POWER_MIN/MAX
   const float dx = float(dd.x), dy = float(dd.y), dz = float(dd.z);
   const float fresnel = fresnel_schlick(dx * nx + dy * ny + dz * nz, fmaxf(m.ior, 1.0f));
-  const float amb = 0.15f * (L.ambient_occlusion ? calc_ao<Set, T>(v, pos, nx, ny, nz, t) : 1.0f);  // AMBIENT_INTENSITY
+  const float amb = 0.15f * (L.ambient_occlusion ? calc_ao<Set, T, kScenes>(v, pos, nx, ny, nz, t, scenes) : 1.0f);
   float dr = amb, dg = amb, db = amb, sr = 0.0f, sg = 0.0f, sb = 0.0f;
   const int lights = L.light_count < ND_MAX_LIGHTS ? L.light_count : ND_MAX_LIGHTS;
   for (int i = 0; i < lights; ++i) {

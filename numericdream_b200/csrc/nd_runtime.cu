@@ -297,6 +297,32 @@ Tuned tuned_for(const std::string& key) {
   return it == g_tuned.end() ? Tuned() : it->second;
 }
 
+// The kernels' table of a call's scenes; members: the formula group's formula ids in
+// code order.
+void scene_table(const SceneInput& sc, const std::vector<int>& members, std::vector<nd::DevScene>* out) {
+  auto code_of = [&](int f) {
+    for (size_t m = 0; m < members.size(); ++m)
+      if (members[m] == f) return int(m);
+    return -1;
+  };
+  out->assign(sc.nscenes, nd::DevScene());
+  for (int k = 0; k < sc.nscenes; ++k) {
+    const nd_scene_desc& S = sc.scenes[k];
+    nd::DevScene& D = (*out)[k];
+    memset(&D, 0, sizeof(D));
+    D.count = S.instance_count;
+    D.carve_count = S.carve_count;
+    for (int i = 0; i < ND_MAX_INSTANCES && i < S.instance_count; ++i) {
+      int mcode[ND_MAX_MIXINS] = {0, 0, 0};
+      for (int j = 0; j < S.instances[i].mixin_count && j < ND_MAX_MIXINS; ++j)
+        mcode[j] = code_of(S.instances[i].mixins[j].formula);
+      D.inst[i] = nd::make_dev_instance(S.instances[i], code_of(S.instances[i].formula), mcode);
+    }
+    for (int c = 0; c < ND_MAX_CARVES; ++c)
+      for (int q = 0; q < 4; ++q) D.carves[c][q] = S.carves[c][q];
+  }
+}
+
 // Enqueue every launch of a forward call.  d_views / d_counters are device
 // buffers with room for nviews views and 2 * plans.size() counters (work counters,
 // then hit counters); d_thit / d_hits hold one entry per ray; h_views is host
@@ -353,28 +379,8 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
   }
   if (sc.nscenes > 0 && d_scenes) {
     // scenes are only accepted when one formula group covers the call: one plan
-    const std::vector<int>& members = plans[0].members;
-    auto code_of = [&](int f) {
-      for (size_t m = 0; m < members.size(); ++m)
-        if (members[m] == f) return int(m);
-      return -1;
-    };
-    std::vector<nd::DevScene> hs(sc.nscenes);
-    for (int k = 0; k < sc.nscenes; ++k) {
-      const nd_scene_desc& S = sc.scenes[k];
-      nd::DevScene& D = hs[k];
-      memset(&D, 0, sizeof(D));
-      D.count = S.instance_count;
-      D.carve_count = S.carve_count;
-      for (int i = 0; i < ND_MAX_INSTANCES && i < S.instance_count; ++i) {
-        int mcode[ND_MAX_MIXINS] = {0, 0, 0};
-        for (int j = 0; j < S.instances[i].mixin_count && j < ND_MAX_MIXINS; ++j)
-          mcode[j] = code_of(S.instances[i].mixins[j].formula);
-        D.inst[i] = nd::make_dev_instance(S.instances[i], code_of(S.instances[i].formula), mcode);
-      }
-      for (int c = 0; c < ND_MAX_CARVES; ++c)
-        for (int q = 0; q < 4; ++q) D.carves[c][q] = S.carves[c][q];
-    }
+    std::vector<nd::DevScene> hs;
+    scene_table(sc, plans[0].members, &hs);
     // from pageable memory: returns once the table is staged, so hs may go
     cudaError_t e = cudaMemcpyAsync(d_scenes, hs.data(), sizeof(nd::DevScene) * hs.size(), cudaMemcpyHostToDevice,
                                     stream);
@@ -1042,31 +1048,52 @@ nd_status nd_de_points(nd_ctx* ctx, const nd_view_desc* view, int64_t n, const d
   return ND_OK;
 }
 
-nd_status nd_shade_lite(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_lite_desc* lite,
-                        const nd_gbuffer* in, float* rgba, void* stream) {
+}  // extern "C"
+
+namespace {
+// Sorts a descriptor's colour stops by position (stable, like sortedColorOrder).
+nd_lite_desc sorted_stops(nd_lite_desc d) {
+  for (int a = 1; a < d.color_count && a < ND_MAX_COLOR_STOPS; ++a)
+    for (int b = a; b > 0 && d.colors[b - 1].position > d.colors[b].position; --b) std::swap(d.colors[b - 1], d.colors[b]);
+  return d;
+}
+
+nd_status lite_check(nd_ctx* ctx, const nd_lite_desc& L, const char* what, int i) {
+  if (L.color_count < 0 || L.color_count > ND_MAX_COLOR_STOPS || L.light_count < 0 || L.light_count > ND_MAX_LIGHTS)
+    return fail(ctx, ND_ERR_INVALID, "%s %d: color_count 0..%d, light_count 0..%d", what, i, ND_MAX_COLOR_STOPS,
+                ND_MAX_LIGHTS);
+  for (int k = 0; k < L.light_count; ++k)
+    if (L.lights[k].type != ND_LIGHT_POINT && L.lights[k].type != ND_LIGHT_GLOBAL)
+      return fail(ctx, ND_ERR_UNSUPPORTED, "%s %d light %d: only point and global lights", what, i, k);
+  return ND_OK;
+}
+
+nd_status shade_lite_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_lite_desc* lite,
+                          const nd_lite_desc* instance_colors, const nd_gbuffer* in, float* rgba, void* stream,
+                          const SceneInput& sc) {
   if (!ctx) return ND_ERR_INVALID;
   if (!lite || !rgba || (uintptr_t(rgba) & 15)) return fail(ctx, ND_ERR_INVALID, "lite descriptors and a 16-byte aligned rgba");
   if (!in || !in->depth64 || !in->normal || !in->trap)
     return fail(ctx, ND_ERR_INVALID, "lite shading reads the forward's depth64, normal and trap");
   std::vector<Launch> plans;
   int64_t total = 0;
-  nd_status s = prepare(ctx, views, nviews, in, &plans, &total);
+  nd_status s = prepare(ctx, views, nviews, in, &plans, &total, sc);
   if (s != ND_OK) return s;
-  for (int i = 0; i < nviews; ++i) {
-    const nd_lite_desc& L = lite[i];
-    if (L.color_count < 0 || L.color_count > ND_MAX_COLOR_STOPS || L.light_count < 0 || L.light_count > ND_MAX_LIGHTS)
-      return fail(ctx, ND_ERR_INVALID, "view %d: color_count 0..%d, light_count 0..%d", i, ND_MAX_COLOR_STOPS,
-                  ND_MAX_LIGHTS);
-    for (int k = 0; k < L.light_count; ++k)
-      if (L.lights[k].type != ND_LIGHT_POINT && L.lights[k].type != ND_LIGHT_GLOBAL)
-        return fail(ctx, ND_ERR_UNSUPPORTED, "view %d light %d: only point and global lights", i, k);
-  }
+  for (int i = 0; i < nviews; ++i)
+    if ((s = lite_check(ctx, lite[i], "view", i)) != ND_OK) return s;
+  if (sc.nscenes > 0 && !instance_colors)
+    return fail(ctx, ND_ERR_INVALID, "scenes need their instances' colour descriptors");
+  for (int i = 0; i < sc.nscenes * ND_MAX_INSTANCES; ++i)
+    if ((s = lite_check(ctx, instance_colors[i], "instance colour descriptor", i)) != ND_OK) return s;
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
   cudaStream_t st = (cudaStream_t)stream;
   if (ctx->have_last) cudaEventSynchronize(ctx->last_done);  // the staging buffer may feed an earlier copy
   if ((s = ensure_dev(ctx, &ctx->d_views, &ctx->views_cap, nviews, "view table")) != ND_OK) return s;
-  if ((s = ensure_dev(ctx, &ctx->d_lite, &ctx->lite_cap, nviews, "lite descriptors")) != ND_OK) return s;
+  const int nlite = nviews + sc.nscenes * ND_MAX_INSTANCES;
+  if ((s = ensure_dev(ctx, &ctx->d_lite, &ctx->lite_cap, nlite, "lite descriptors")) != ND_OK) return s;
+  if (sc.nscenes > 0 && (s = ensure_dev(ctx, &ctx->d_scenes, &ctx->scenes_cap, sc.nscenes, "scene table")) != ND_OK)
+    return s;
   if (ctx->h_views_cap < nviews) {
     if (ctx->h_views) cudaFreeHost(ctx->h_views);
     ctx->h_views = nullptr;
@@ -1078,25 +1105,29 @@ nd_status nd_shade_lite(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, 
   // views and descriptors in plan order; colour stops sorted by position
   std::vector<int64_t> out_off(nviews + 1, 0);
   for (int i = 0; i < nviews; ++i) out_off[i + 1] = out_off[i] + int64_t(views[i].spp) * views[i].tile_w * views[i].tile_h;
-  std::vector<nd_lite_desc> hl(nviews);
+  // per view in plan order, then the scenes' instance colours (scene-major)
+  std::vector<nd_lite_desc> hl(nlite);
   int base = 0;
   for (const Launch& L : plans) {
     int64_t off = 0;
     for (size_t k = 0; k < L.views.size(); ++k) {
       const int vi = L.views[k];
       ctx->h_views[base + k] = make_dev_view(views[vi], off, out_off[vi], L.codes[k]);
+      ctx->h_views[base + k].scene = sc.scene_of(vi);
       off += ctx->h_views[base + k].rays;
-      nd_lite_desc d = lite[vi];
-      for (int a = 1; a < d.color_count; ++a)
-        for (int b = a; b > 0 && d.colors[b - 1].position > d.colors[b].position; --b)
-          std::swap(d.colors[b - 1], d.colors[b]);
-      hl[base + k] = d;
+      hl[base + k] = sorted_stops(lite[vi]);
     }
     base += int(L.views.size());
   }
+  for (int i = 0; i < sc.nscenes * ND_MAX_INSTANCES; ++i) hl[nviews + i] = sorted_stops(instance_colors[i]);
   e = cudaMemcpyAsync(ctx->d_views, ctx->h_views, sizeof(DevView) * size_t(nviews), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(ctx->d_lite, hl.data(), sizeof(nd_lite_desc) * size_t(nviews), cudaMemcpyHostToDevice, st);
+    e = cudaMemcpyAsync(ctx->d_lite, hl.data(), sizeof(nd_lite_desc) * size_t(nlite), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && sc.nscenes > 0) {
+    std::vector<nd::DevScene> hs;
+    scene_table(sc, plans[0].members, &hs);
+    e = cudaMemcpyAsync(ctx->d_scenes, hs.data(), sizeof(nd::DevScene) * hs.size(), cudaMemcpyHostToDevice, st);
+  }
   if (e != cudaSuccess) return cuda_fail(ctx, e, "copy lite tables");
   base = 0;
   for (const Launch& L : plans) {
@@ -1113,9 +1144,15 @@ nd_status nd_shade_lite(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, 
     a.nviews = nv;
     a.total_rays = rays;
     a.out = *in;
+    a.scenes = sc.nscenes > 0 ? ctx->d_scenes : nullptr;
     // the shading arithmetic is f32 like the reference's; so is the DE of its AO taps
-    const nd::LiteFn fn = dir64 ? L.table.lite_f32_dir64 : L.table.lite_f32;
-    e = fn(a, ctx->d_lite + base, rgba, ctx->num_sms, st);
+    nd::LiteFn fn = dir64 ? L.table.lite_f32_dir64 : L.table.lite_f32;
+    if (sc.nscenes > 0) {
+      if (dir64) return fail(ctx, ND_ERR_UNSUPPORTED, "lite shading of scenes with FP64 ray directions");
+      fn = L.table.scene_lite_f32;
+      if (!fn) return fail(ctx, ND_ERR_UNSUPPORTED, "no scene kernels in this formula set");
+    }
+    e = fn(a, ctx->d_lite + base, ctx->d_lite + nviews, rgba, ctx->num_sms, st);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "lite shading launch");
     base += nv;
   }
@@ -1123,6 +1160,27 @@ nd_status nd_shade_lite(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, 
   if (e != cudaSuccess) return cuda_fail(ctx, e, "record event");
   ctx->have_last = true;
   return ND_OK;
+}
+}  // namespace
+
+extern "C" {
+
+nd_status nd_shade_lite(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_lite_desc* lite,
+                        const nd_gbuffer* in, float* rgba, void* stream) {
+  return shade_lite_impl(ctx, views, nviews, lite, nullptr, in, rgba, stream, SceneInput());
+}
+
+nd_status nd_shade_lite_scenes(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const int32_t* view_scene,
+                               const nd_scene_desc* scenes, int32_t nscenes, const nd_lite_desc* lite,
+                               const nd_lite_desc* instance_colors, const nd_gbuffer* in, float* rgba, void* stream) {
+  if (!ctx) return ND_ERR_INVALID;
+  if (nscenes < 0 || (nscenes > 0 && (!scenes || !view_scene)))
+    return fail(ctx, ND_ERR_INVALID, "scenes need a view_scene array and a scene array");
+  SceneInput sc;
+  sc.view_scene = view_scene;
+  sc.scenes = scenes;
+  sc.nscenes = nscenes;
+  return shade_lite_impl(ctx, views, nviews, lite, instance_colors, in, rgba, stream, sc);
 }
 
 nd_status nd_accel_grid(nd_ctx* ctx, const nd_view_desc* view, int32_t de_precision, float* grid, int64_t capacity,

@@ -455,11 +455,11 @@ struct Loader {
   }
 };
 
-// The lite-shading descriptor of a scene file: the first instance's colour stops
+// The lite-shading descriptor of a scene file: one instance's colour stops
 // (ColorStopState: position, color, glossiness, ior) and the visible point and global
 // lights (LightState.toGpu, scene_state.zig:594-612: a global light's direction, a
 // point light's position; ray lights are not part of the lite pass and are left out).
-bool load_lite(const JVal& root, nd_lite_desc* out, std::string* err) {
+bool load_lite(const JVal& root, int instance, nd_lite_desc* out, std::string* err) {
   memset(out, 0, sizeof(*out));
   out->ambient_occlusion = 1;
   out->specular = 1;
@@ -467,11 +467,11 @@ bool load_lite(const JVal& root, nd_lite_desc* out, std::string* err) {
   out->background[1] = 0.11f;
   out->background[2] = 0.13f;
   const JVal* ins = root.kind == JVal::OBJ ? root.get("instances") : nullptr;
-  if (!ins || ins->kind != JVal::ARR || ins->arr.empty()) {
-    *err = "the scene has no instances";
+  if (!ins || ins->kind != JVal::ARR || instance < 0 || size_t(instance) >= ins->arr.size()) {
+    *err = "no such instance";
     return false;
   }
-  const JVal* colors = ins->arr[0].get("colors");
+  const JVal* colors = ins->arr[instance].get("colors");
   if (colors && colors->kind == JVal::ARR)
     for (const JVal& c : colors->arr) {
       if (out->color_count >= ND_MAX_COLOR_STOPS) break;
@@ -505,7 +505,8 @@ bool load_lite(const JVal& root, nd_lite_desc* out, std::string* err) {
 
 }  // namespace
 
-extern "C" nd_status nd_scene_file_lite(const char* json, size_t len, nd_lite_desc* lite, char* err, size_t err_len) {
+extern "C" nd_status nd_scene_file_lite(const char* json, size_t len, int32_t instance, nd_lite_desc* lite, char* err,
+                                        size_t err_len) {
   std::string msg;
   JVal root;
   JsonParser p(json ? json : "", json ? len : 0);
@@ -516,7 +517,7 @@ extern "C" nd_status nd_scene_file_lite(const char* json, size_t len, nd_lite_de
   } else if (!p.parse(&root)) {
     msg = p.error();
     st = ND_ERR_INVALID;
-  } else if (!load_lite(root, lite, &msg)) {
+  } else if (!load_lite(root, instance, lite, &msg)) {
     st = ND_ERR_INVALID;
   }
   if (err && err_len) {

@@ -60,7 +60,12 @@ _SIGNATURES = {
                                        C.POINTER(abi.nd_scene_desc), C.POINTER(C.c_int32), C.c_char_p, C.c_size_t]),
     "nd_shade_lite": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(abi.nd_lite_desc),
                                   C.POINTER(abi.nd_gbuffer), C.c_void_p, C.c_void_p]),
-    "nd_scene_file_lite": (C.c_int32, [C.c_char_p, C.c_size_t, C.POINTER(abi.nd_lite_desc), C.c_char_p, C.c_size_t]),
+    "nd_scene_file_lite": (C.c_int32, [C.c_char_p, C.c_size_t, C.c_int32, C.POINTER(abi.nd_lite_desc), C.c_char_p,
+                                       C.c_size_t]),
+    "nd_shade_lite_scenes": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(C.c_int32),
+                                         C.POINTER(abi.nd_scene_desc), C.c_int32, C.POINTER(abi.nd_lite_desc),
+                                         C.POINTER(abi.nd_lite_desc), C.POINTER(abi.nd_gbuffer), C.c_void_p,
+                                         C.c_void_p]),
     "nd_march_forward_scenes": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(C.c_int32),
                                             C.POINTER(abi.nd_scene_desc), C.c_int32, C.POINTER(abi.nd_march_opts),
                                             C.POINTER(abi.nd_gbuffer), C.c_void_p]),
@@ -178,9 +183,9 @@ def load_scene_file(source, width: int = 0, height: int = 0):
     return view, (scene if needs.value else None)
 
 
-def load_scene_file_lite(source) -> abi.nd_lite_desc:
-    """nd_scene_file_lite: the lite-shading descriptor (colour stops of the first
-    instance, point and global lights) of a .dream scene (a path or the JSON text)."""
+def load_scene_file_lite(source, instance: int = 0) -> abi.nd_lite_desc:
+    """nd_scene_file_lite: the lite-shading descriptor (colour stops of one instance,
+    point and global lights) of a .dream scene (a path or the JSON text)."""
     if isinstance(source, (bytes, bytearray)):
         data = bytes(source)
     elif isinstance(source, str) and source.lstrip().startswith("{"):
@@ -190,7 +195,7 @@ def load_scene_file_lite(source) -> abi.nd_lite_desc:
             data = fh.read()
     lite = abi.nd_lite_desc()
     err = C.create_string_buffer(256)
-    st = load_library().nd_scene_file_lite(data, len(data), C.byref(lite), err, 256)
+    st = load_library().nd_scene_file_lite(data, len(data), instance, C.byref(lite), err, 256)
     if st != abi.ND_OK:
         raise NDError(st, err.value.decode())
     return lite
@@ -380,6 +385,28 @@ class Context:
         s = None if stream is None else C.c_void_p(stream)
         st = self.lib.nd_shade_lite(self.handle, arr, len(views), la, C.byref(g), rgba.data_ptr(), s)
         self._check(st, "nd_shade_lite")
+        return rgba
+
+    def shade_lite_scenes(self, views, view_scene, scenes, lites, instance_colors, gbuf: GBuffer, stream=None):
+        """nd_shade_lite_scenes: instance_colors is one list of ND_MAX_INSTANCES
+        descriptors per scene (shorter lists are padded with empty descriptors)."""
+        import torch
+
+        n = gbuf.depth.shape[0]
+        rgba = torch.empty((n, 4), dtype=torch.float32, device=gbuf.depth.device)
+        arr = (abi.nd_view_desc * len(views))(*views)
+        vs = (C.c_int32 * len(views))(*view_scene)
+        sarr = (abi.nd_scene_desc * max(1, len(scenes)))(*scenes)
+        la = (abi.nd_lite_desc * len(views))(*lites)
+        flat = []
+        for per in instance_colors:
+            flat += list(per) + [abi.nd_lite_desc()] * (abi.ND_MAX_INSTANCES - len(per))
+        ic = (abi.nd_lite_desc * max(1, len(flat)))(*flat)
+        g = gbuf.as_abi()
+        s = None if stream is None else C.c_void_p(stream)
+        st = self.lib.nd_shade_lite_scenes(self.handle, arr, len(views), vs, sarr, len(scenes), la, ic, C.byref(g),
+                                           rgba.data_ptr(), s)
+        self._check(st, "nd_shade_lite_scenes")
         return rgba
 
     def accel_grid(self, view: abi.nd_view_desc, de_precision: int = 32):

@@ -382,6 +382,56 @@ template <class R> R combine(int mode, R d, R di, R k) {
   }
 }
 
+// combine_de's material weight (tpl:1708-1730): the share of the scene so far.
+template <class R> R combine_weight(int mode, R d, R di, R k) {
+  const bool hard = k <= R(0.0001);
+  const R closer = di < d ? R(0) : R(1);
+  switch (mode) {
+    case ND_COMBINE_SMOOTH_MIN:
+    case ND_COMBINE_SMOOTH_MIX: return hard ? closer : clampv(R(0.5) + R(0.5) * (di - d) / k, R(0), R(1));
+    case ND_COMBINE_SMOOTH_MAX: return hard ? (di > d ? R(0) : R(1)) : clampv(R(0.5) - R(0.5) * (di - d) / k, R(0), R(1));
+    case ND_COMBINE_SMOOTH_INV_MAX:
+      return hard ? (-di > d ? R(0) : R(1)) : R(1) - clampv(R(0.5) - R(0.5) * (d + di) / k, R(0), R(1));
+    default: return closer;
+  }
+}
+
+// orbit_trap_to_strip (tpl:2025-2035): TRAP_MIN_SPAN 1e-4; repeat 1 fract, 2 mirror.
+template <class R> R trap_strip(R span, R offset, int repeat, R v) {
+  const R x = v / std::fmax(span, R(1e-4)) + offset;
+  if (repeat == 1) return x - std::floor(x);
+  if (repeat == 2) return R(1) - std::fabs((x * R(0.5) - std::floor(x * R(0.5))) * R(2) - R(1));
+  return clampv(x, R(0), R(1));
+}
+
+// The lite material at a strip position: sample_gradient (tpl:2003-2023) with
+// mix_material's blend (tpl:1980-2001) of colour, glossiness and ior; no stops:
+// default_material (tpl:1965-1977).  out: r, g, b, glossiness, ior.
+inline void lite_stop_material(const nd_lite_desc& L, double strip, double out[5]) {
+  auto take = [&](const nd_color_stop& c) {
+    for (int k = 0; k < 3; ++k) out[k] = c.color[k];
+    out[3] = c.glossiness;
+    out[4] = c.ior;
+  };
+  out[0] = 0.8; out[1] = 0.8; out[2] = 0.85; out[3] = 0.3; out[4] = 1.5;
+  const int count = std::min(L.color_count, ND_MAX_COLOR_STOPS);
+  if (count <= 0) return;
+  if (count == 1 || strip <= L.colors[0].position) return take(L.colors[0]);
+  if (strip >= L.colors[count - 1].position) return take(L.colors[count - 1]);
+  take(L.colors[count - 1]);
+  for (int i = 0; i < count - 1; ++i) {
+    const nd_color_stop& a = L.colors[i];
+    const nd_color_stop& b = L.colors[i + 1];
+    if (strip >= a.position && strip <= b.position) {
+      const double f = (strip - a.position) / std::max(double(b.position) - a.position, 1e-4);
+      for (int k = 0; k < 3; ++k) out[k] = b.color[k] + (a.color[k] - b.color[k]) * (1.0 - f);
+      out[3] = b.glossiness + (a.glossiness - b.glossiness) * (1.0 - f);
+      out[4] = b.ior + (a.ior - b.ior) * (1.0 - f);
+      return;
+    }
+  }
+}
+
 // scene_de (tpl:1756-1779) over an nd_scene_desc: per instance the inverse placement
 // (instance_local tpl:1597-1609: rotation frame, then per-axis signed scale with
 // |s| >= 0.001), the DE factor min|s| * clamp(step_safety, 0.001, 1)
@@ -464,6 +514,33 @@ template <class R> struct SceneEval {
     }
     o.d = o.d * factor;
     return o;
+  }
+
+  // hit_material (tpl:2128-2155) for the lite pass: each visible instance's
+  // material at its own trap strip, blended with combine_de's weight; colors: the
+  // scene's ND_MAX_INSTANCES descriptors.  out: r, g, b, glossiness, ior.
+  void material(V3<R> pos, const nd_lite_desc* colors, double out[5]) const {
+    lite_stop_material(nd_lite_desc(), 0.0, out);
+    R d = R(0);
+    bool first = true;
+    const int count = std::min(std::max(scene->instance_count, 1), ND_MAX_INSTANCES);
+    for (int i = 0; i < count; ++i) {
+      const nd_instance_desc& in = scene->instances[i];
+      if (in.hidden) continue;
+      const DE<R> di = instance(i, pos);
+      double mi[5];
+      lite_stop_material(colors[i], trap_strip<double>(in.trap.span, in.trap.offset, in.trap.repeat, double(di.trap)),
+                         mi);
+      if (first) {
+        d = di.d;
+        for (int k = 0; k < 5; ++k) out[k] = mi[k];
+        first = false;
+        continue;
+      }
+      const double h = double(combine_weight<R>(in.combine_mode, d, di.d, R(in.blend_k)));
+      for (int k = 0; k < 5; ++k) out[k] = mi[k] * (1.0 - h) + out[k] * h;
+      d = combine<R>(in.combine_mode, d, di.d, R(in.blend_k));
+    }
   }
 
   DE<R> de(V3<R> pos) const {
@@ -555,14 +632,6 @@ struct AccelGrid {
   }
 };
 
-// orbit_trap_to_strip (tpl:2025-2035): TRAP_MIN_SPAN 1e-4; repeat 1 fract, 2 mirror.
-template <class R> R trap_strip(R span, R offset, int repeat, R v) {
-  const R x = v / std::fmax(span, R(1e-4)) + offset;
-  if (repeat == 1) return x - std::floor(x);
-  if (repeat == 2) return R(1) - std::fabs((x * R(0.5) - std::floor(x * R(0.5))) * R(2) - R(1));
-  return clampv(x, R(0), R(1));
-}
-
 // fresnel_schlick (tpl:3424-3430)
 template <class R> R fresnel_schlick(R cos_theta, R ior) {
   const R r0root = (R(1) - ior) / (R(1) + ior);
@@ -610,6 +679,7 @@ template <class R> struct Tracer {
   double de_scale = 1.0;  // every DE value is multiplied by this (stability probes)
   const SceneEval<R>* scene = nullptr;  // a multi-instance scene instead of the view's formula
   const AccelGrid* accel = nullptr;     // the view's empty-space accelerator, when it has one
+  const nd_lite_desc* scene_colors = nullptr;  // lite pass: the scene instances' colour stops
 
   Tracer(const nd_view_desc& view, int k) : v(view), kind(k) {
     for (int i = 0; i < ND_MAX_PARAMS; ++i) p[i] = R(view.params[i]);
@@ -799,34 +869,10 @@ template <class R> struct Tracer {
   void lite(const nd_lite_desc& L, int64_t ray, double t, V3<double> n, double trap, double* rgb) {
     const V3<double> dir = ray_dir(ray);
     const V3<double> pos = org + dir * t;
-    const double strip = trap_strip<double>(v.trap.span, v.trap.offset, v.trap.repeat, trap);
-    double col[3] = {0.8, 0.8, 0.85}, gloss = 0.3, ior = 1.5;
-    const int count = std::min(L.color_count, ND_MAX_COLOR_STOPS);
-    auto take = [&](const nd_color_stop& c) {
-      for (int k = 0; k < 3; ++k) col[k] = c.color[k];
-      gloss = c.glossiness;
-      ior = c.ior;
-    };
-    if (count > 0) {
-      if (count == 1 || strip <= L.colors[0].position) {
-        take(L.colors[0]);
-      } else if (strip >= L.colors[count - 1].position) {
-        take(L.colors[count - 1]);
-      } else {
-        take(L.colors[count - 1]);
-        for (int i = 0; i < count - 1; ++i) {
-          const nd_color_stop& a = L.colors[i];
-          const nd_color_stop& b = L.colors[i + 1];
-          if (strip >= a.position && strip <= b.position) {
-            const double f = (strip - a.position) / std::max(double(b.position) - a.position, 1e-4);
-            for (int k = 0; k < 3; ++k) col[k] = b.color[k] + (a.color[k] - b.color[k]) * (1.0 - f);
-            gloss = b.glossiness + (a.glossiness - b.glossiness) * (1.0 - f);
-            ior = b.ior + (a.ior - b.ior) * (1.0 - f);
-            break;
-          }
-        }
-      }
-    }
+    double mat[5];
+    if (scene && scene_colors) scene->material(V3<R>(R(pos.x), R(pos.y), R(pos.z)), scene_colors, mat);
+    else lite_stop_material(L, trap_strip<double>(v.trap.span, v.trap.offset, v.trap.repeat, trap), mat);
+    const double col[3] = {mat[0], mat[1], mat[2]}, gloss = mat[3], ior = mat[4];
     const double spec_power = 4.0 + (128.0 - 4.0) * clampv(gloss, 0.0, 1.0);
     const double fresnel = fresnel_schlick(dot(dir, n), std::max(ior, 1.0));
     const double occl = L.ambient_occlusion ? ao(pos, n, t) : 1.0;

@@ -264,6 +264,47 @@ int oracle_shade_lite(const nd_view_desc* view, const char* formula_name, const 
   return 0;
 }
 
+// Lite shading of a scene view's rays from given forward outputs (as
+// oracle_shade_lite); instance_colors: ND_MAX_INSTANCES descriptors of the scene.
+int oracle_shade_lite_scene(const nd_view_desc* view, const nd_scene_desc* scene, const int32_t* kinds,
+                            const int32_t* mixin_kinds, const nd_lite_desc* lite, const nd_lite_desc* instance_colors,
+                            int precision, int64_t first, int64_t n, const double* depth64, const float* normal4,
+                            const float* trap, float* rgba) {
+  SceneEval<float> sf;
+  SceneEval<double> sd;
+  sf.scene = sd.scene = scene;
+  sf.max_dist = sd.max_dist = view->max_dist;
+  if (scene_kinds(kinds, mixin_kinds, sf, sd) != 0) return -1;
+#pragma omp parallel
+  {
+    Tracer<float> tf(*view, kinds[0]);
+    Tracer<double> td(*view, kinds[0]);
+    tf.scene = &sf;
+    td.scene = &sd;
+    tf.scene_colors = td.scene_colors = instance_colors;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i) {
+      if (!(normal4[4 * i + 3] > 0.5f)) {
+        for (int k = 0; k < 3; ++k) rgba[4 * i + k] = lite->background[k];
+        rgba[4 * i + 3] = 0.0f;
+        continue;
+      }
+      const V3<double> nn(normal4[4 * i], normal4[4 * i + 1], normal4[4 * i + 2]);
+      double rgb[3];
+      if (precision == 32) tf.lite(*lite, first + i, depth64[i], nn, trap[i], rgb);
+      else td.lite(*lite, first + i, depth64[i], nn, trap[i], rgb);
+      for (int k = 0; k < 3; ++k) rgba[4 * i + k] = float(rgb[k]);
+      rgba[4 * i + 3] = 1.0f;
+    }
+  }
+  return 0;
+}
+
+// The oracle's combine_de material weight (f32) at n inputs.
+void oracle_combine_weight(int64_t n, const int32_t* mode, const float* d, const float* di, const float* k, float* out) {
+  for (int64_t i = 0; i < n; ++i) out[i] = combine_weight<float>(mode[i], d[i], di[i], k[i]);
+}
+
 // The oracle's calc_ao at n hit points (positions, normals, t).
 int oracle_ao(const nd_view_desc* view, const char* formula_name, int precision, int64_t n, const double* pos,
               const double* nrm, const double* t, double* out) {

@@ -35,6 +35,9 @@ def lib():
                                            + [C.c_void_p] * 4)
         _LIB.oracle_ao.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int64] + [C.c_void_p] * 4
         _LIB.oracle_strip_fresnel.argtypes = [C.c_int64] + [C.c_void_p] * 6
+        _LIB.oracle_shade_lite_scene.argtypes = ([C.c_void_p] * 6 + [C.c_int, C.c_int64, C.c_int64]
+                                                 + [C.c_void_p] * 4)
+        _LIB.oracle_combine_weight.argtypes = [C.c_int64] + [C.c_void_p] * 5
         _LIB.oracle_max_threads.restype = C.c_int
     return _LIB
 
@@ -232,3 +235,33 @@ def strip_fresnel(sor, v, cosv, ior):
     lib().oracle_strip_fresnel(v.size, sor.ctypes.data, v.ctypes.data, cosv.ctypes.data, ior.ctypes.data,
                                st.ctypes.data, fr.ctypes.data)
     return st, fr
+
+
+def shade_lite_scene(view: abi.nd_view_desc, scene: abi.nd_scene_desc, names, lite: abi.nd_lite_desc, instance_colors,
+                     gbuf: dict, precision=64, first=0):
+    """The oracle's lite shading of a scene view from forward outputs; instance_colors:
+    up to ND_MAX_INSTANCES descriptors (their colour stops, sorted by position)."""
+    kinds, mk = _scene_kinds(scene, names)
+    per = list(instance_colors) + [abi.nd_lite_desc()] * (abi.ND_MAX_INSTANCES - len(instance_colors))
+    ic = (abi.nd_lite_desc * abi.ND_MAX_INSTANCES)(*per)
+    depth64 = np.ascontiguousarray(gbuf["depth64"], np.float64)
+    normal = np.ascontiguousarray(gbuf["normal"], np.float32)
+    trap = np.ascontiguousarray(gbuf["trap"], np.float32)
+    n = depth64.shape[0]
+    out = np.zeros((n, 4), np.float32)
+    rc = lib().oracle_shade_lite_scene(C.addressof(view), C.addressof(scene), kinds.ctypes.data, mk.ctypes.data,
+                                       C.addressof(lite), C.addressof(ic), precision, first, n, depth64.ctypes.data,
+                                       normal.ctypes.data, trap.ctypes.data, out.ctypes.data)
+    if rc != 0:
+        raise ValueError("oracle_shade_lite_scene refused the scene")
+    return out
+
+
+def combine_weight(mode, d, di, k):
+    """The oracle's combine_de material weight (f32) elementwise."""
+    mode = np.ascontiguousarray(mode, np.int32)
+    d, di, k = (np.ascontiguousarray(x, np.float32) for x in (d, di, k))
+    out = np.zeros(mode.size, np.float32)
+    lib().oracle_combine_weight(mode.size, mode.ctypes.data, d.ctypes.data, di.ctypes.data, k.ctypes.data,
+                                out.ctypes.data)
+    return out

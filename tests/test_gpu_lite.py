@@ -82,3 +82,36 @@ def test_lite_refusals(ctx):
     with pytest.raises(runtime.NDError) as e:
         ctx.shade_lite([v], [abi.make_lite(STOPS, LIGHTS)], g)
     assert e.value.status == abi.ND_ERR_INVALID
+
+
+def test_lite_shading_of_a_scene(ctx):
+    """A Mandelbulb on a box floor beside a sphere, each instance with its own colour
+    strip, against the oracle's hit_material blend."""
+    from oracle import pyoracle
+
+    fid = runtime.find_formula
+    bulb = abi.make_instance(fid(workloads.MANDELBULB), params=workloads.mandelbulb_params(8.0, 8),
+                             trap={"shape": abi.ND_TRAP_SPHERE, "radius": 0.8, "span": 1.0})
+    floor = abi.make_instance(fid("cube_primitive"), params=[1.0], offset=(0.0, -1.35, 0.0), scale=(6.0, 0.1, 6.0),
+                              combine_mode=abi.ND_COMBINE_SMOOTH_MIN, blend_k=0.3)
+    ball = abi.make_instance(fid("sphere_primitive"), params=[0.45], offset=(-1.4, -0.8, 0.6),
+                             trap={"shape": abi.ND_TRAP_POINT, "span": 2.0, "repeat": 1})
+    scene = abi.make_scene([bulb, floor, ball])
+    v = abi.make_view(fid(workloads.MANDELBULB), 96, 72, (0.3, 0.7, -3.6), fov_y_deg=60.0, max_steps=256)
+    colors = [abi.make_lite(STOPS), abi.make_lite([((0.3, 0.3, 0.3), 0.0, 0.1, 1.2)]),
+              abi.make_lite(list(reversed(STOPS)))]
+    lite = abi.make_lite([], LIGHTS)
+    g = runtime.GBuffer.allocate(workloads.rays([v]))
+    ctx.forward_scenes([v], [0], [scene], g, runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT))
+    rgba = ctx.shade_lite_scenes([v], [0], [scene], [lite], [colors], g).cpu().numpy()
+    out = g.numpy()
+    sorted_colors = [abi.make_lite(sorted(STOPS, key=lambda s: s[1])), colors[1],
+                     abi.make_lite(sorted(STOPS, key=lambda s: s[1]))]
+    ref = pyoracle.shade_lite_scene(v, scene, runtime.formula_name, lite, sorted_colors, out, precision=32)
+    hit = out["normal"][:, 3] > 0.5
+    assert hit.sum() > 1000
+    err = np.abs(rgba[hit, :3] - ref[hit, :3]).max(axis=1)
+    print("scene lite: hits", hit.sum(), "max err", err.max(), "p99", np.percentile(err, 99))
+    assert (err <= 2e-3).mean() >= 0.99
+    # the three materials all show up
+    assert np.ptp(rgba[hit, 2]) > 0.1
