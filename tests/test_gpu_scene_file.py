@@ -9,6 +9,8 @@ reference's own bench scenes are built."""
 import json
 import os
 
+import numpy as np
+
 import pytest
 
 from numericdream_b200 import runtime, workloads
@@ -73,3 +75,31 @@ def test_fractal_on_primitives(ctx):
     view, scene = runtime.load_scene_file(json.dumps(doc))
     assert scene is not None and scene.instance_count == 4
     _render_and_check(ctx, view, scene, min_hits=1000)
+
+
+def test_render_scene_file_to_an_image(ctx, tmp_path):
+    """The fixture scene file to a colour image (geometry + lite shading with its
+    colour stops and lights) against the oracle's lite shading of the same hits."""
+    from numericdream_b200 import abi
+    from numericdream_b200.render import render_scene_file, write_ppm
+    from oracle import pyoracle
+
+    path = os.path.join(HERE, "golden", "two_fractals.dream")
+    img, g = render_scene_file(ctx, path, 160, 90)
+    assert img.shape == (90, 160, 4)
+    hit = g["normal"][:, 3] > 0.5
+    np.testing.assert_array_equal(img.reshape(-1, 4)[:, 3], hit.astype(np.float32))
+    view, scene = runtime.load_scene_file(path, 160, 90)
+    lite = runtime.load_scene_file_lite(path, 0)
+    colors = []
+    for i in range(scene.instance_count):
+        c = runtime.load_scene_file_lite(path, i)
+        stops = sorted(((tuple(s.color), s.position, s.glossiness, s.ior) for s in c.colors[:c.color_count]),
+                       key=lambda s: s[1])
+        colors.append(abi.make_lite(stops))
+    ref = pyoracle.shade_lite_scene(view, scene, runtime.formula_name, lite, colors, g, precision=32)
+    err = np.abs(img.reshape(-1, 4)[hit, :3] - ref[hit, :3]).max(axis=1)
+    assert hit.sum() > 500 and (err <= 2e-3).mean() >= 0.99
+    out = tmp_path / "scene.ppm"
+    write_ppm(str(out), img)
+    assert out.read_bytes().startswith(b"P6 160 90 255\n") and out.stat().st_size == 14 + 160 * 90 * 3
