@@ -516,18 +516,48 @@ def main():
     time.sleep(0.3)
     views, nrays, gbuf, opts, tune, ms_batched, ms_plain, st, kms = run_workload(args.workload, args.steps,
                                                                                   args.warmup)
-    # end to end through the public call: host descriptors in, G-buffer to pinned host
-    host = {k: torch.empty(getattr(gbuf, k).shape, dtype=getattr(gbuf, k).dtype, pin_memory=True)
-            for k in ("depth", "normal", "trap", "steps")}
-    d2h = sum(t.numel() * t.element_size() for t in host.values())
+    # end to end through the public call, as a renderer streams frames: every step
+    # copies its view descriptors up (inside nd_march_forward) and reads its G-buffer
+    # back into pinned host memory; with two G-buffers the read-back of step i (on a
+    # copy stream) overlaps the march of step i + 1.  L2 flushed before every step.
+    keys = ("depth", "normal", "trap", "steps")
+    gbufs = [gbuf, runtime.GBuffer.allocate(nrays, device=dev)]
+    hosts = [{k: torch.empty(getattr(gbuf, k).shape, dtype=getattr(gbuf, k).dtype, pin_memory=True) for k in keys}
+             for _ in range(2)]
+    d2h = sum(t.numel() * t.element_size() for t in hosts[0].values())
     h2d = len(views) * runtime.load_library().nd_sizeof(b"DevView")  # the view table nd_march_forward copies
+    copy_stream = torch.cuda.Stream(device=dev)
 
-    def e2e_step():
-        ctx.forward(views, gbuf, opts, stream=sptr)
-        for k, t in host.items():
-            t.copy_(getattr(gbuf, k), non_blocking=True)
+    def e2e_run(steps):
+        done = [None, None]
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for i in range(steps):
+            k = i % 2
+            if done[k] is not None:
+                stream.wait_event(done[k])  # the buffer's previous read-back has finished
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            ctx.forward(views, gbufs[k], opts, stream=sptr)
+            marched = torch.cuda.Event()
+            marched.record(stream)
+            copy_stream.wait_event(marched)
+            with torch.cuda.stream(copy_stream):
+                for key, t in hosts[k].items():
+                    t.copy_(getattr(gbufs[k], key), non_blocking=True)
+                done[k] = torch.cuda.Event()
+                done[k].record(copy_stream)
+        stream.wait_stream(copy_stream)
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / steps
 
-    ms_e2e = timed(e2e_step, max(2, args.steps // 2), 1)
+    e2e_run(2)
+    if ws > 1:
+        torch.distributed.barrier()
+    ms_e2e = e2e_run(max(4, args.steps))
     extra = None
     if not args.no_extra and args.workload != "mandelbox_1080p":
         v2, n2, g2, _, _, ms2, ms2_plain, st2, _ = run_workload("mandelbox_1080p", max(2, args.steps // 2), 2,
@@ -585,7 +615,10 @@ def main():
                       "kind": "one plain launch per view, one thread per ray"},
             "batched_over_plain": ms_plain / ms_batched,
             "e2e": {"value": rays_total / (ms_e2e * 1e-3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e,
+                    "kind": "nd_march_forward from host view descriptors, G-buffer (depth, normal, trap, steps) read "
+                            "back to pinned host memory every step; two G-buffers, read-back of step i overlapping "
+                            "the march of step i+1"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": NCU_TRAFFIC.get(args.workload),
                          "kernel": "persistent_kernel (march); FLOPs = its DE evaluations x FLOPs per "
