@@ -80,8 +80,11 @@ struct nd_ctx {
   nd_lite_desc* d_lite = nullptr;    // lite-shading descriptors, in plan order
   int lite_cap = 0;
   bool last_trap = false;
-  DevView* h_views = nullptr;  // pinned staging
+  DevView* h_views = nullptr;  // pinned staging: two halves of h_views_cap records, forward calls alternate
   int h_views_cap = 0;
+  cudaEvent_t staged[2] = {nullptr, nullptr};  // after the call that last used each half
+  bool staged_valid[2] = {false, false};
+  uint64_t calls = 0;
   cudaStream_t last_stream = nullptr;
   cudaEvent_t last_done = nullptr;
   std::vector<cudaEvent_t> tev;  // timing events per launch plan: accelerator build start, march start,
@@ -699,6 +702,11 @@ nd_status nd_ctx_destroy(nd_ctx* ctx) {
   if (ctx->d_accel) cudaFree(ctx->d_accel);
   if (ctx->d_accel_jobs) cudaFree(ctx->d_accel_jobs);
   if (ctx->d_lite) cudaFree(ctx->d_lite);
+  for (int k = 0; k < 2; ++k)
+    if (ctx->staged[k]) {
+      if (ctx->staged_valid[k]) cudaEventSynchronize(ctx->staged[k]);
+      cudaEventDestroy(ctx->staged[k]);
+    }
   if (ctx->h_views) cudaFreeHost(ctx->h_views);
   if (ctx->last_done) cudaEventDestroy(ctx->last_done);
   for (cudaEvent_t ev : ctx->tev) cudaEventDestroy(ev);
@@ -737,8 +745,17 @@ nd_status forward_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, c
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
   cudaStream_t st = (cudaStream_t)stream;
-  // the staging buffer may still feed an earlier copy: wait for the last call
-  if (ctx->have_last) cudaEventSynchronize(ctx->last_done);
+  // The device scratch (view table, counters, hit buffers) is reused by every call:
+  // order this call after the previous one on the device (free on the same stream),
+  // without blocking the host, so that a caller can enqueue the next frame while this
+  // one runs.  The pinned staging alternates between two halves; a half is reused
+  // once the call two back, which read it, is done.
+  if (ctx->have_last && ctx->last_stream != st) cudaStreamWaitEvent(st, ctx->last_done, 0);
+  const int half = int(ctx->calls & 1);
+  for (int k = 0; k < 2; ++k)
+    if (!ctx->staged[k] && (e = cudaEventCreateWithFlags(&ctx->staged[k], cudaEventDisableTiming)) != cudaSuccess)
+      return cuda_fail(ctx, e, "staging event");
+  if (ctx->staged_valid[half]) cudaEventSynchronize(ctx->staged[half]);
   if ((s = ensure_dev(ctx, &ctx->d_views, &ctx->views_cap, nviews, "view table")) != ND_OK) return s;
   if ((s = ensure_dev(ctx, &ctx->d_counters, &ctx->counters_cap, 2 * int(plans.size()), "work counters")) != ND_OK)
     return s;
@@ -755,13 +772,18 @@ nd_status forward_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, c
     ctx->thit_cap = total;
   }
   if (ctx->h_views_cap < nviews) {
+    for (int k = 0; k < 2; ++k)
+      if (ctx->staged_valid[k]) cudaEventSynchronize(ctx->staged[k]);
+    if (ctx->have_last) cudaEventSynchronize(ctx->last_done);
     if (ctx->h_views) cudaFreeHost(ctx->h_views);
     ctx->h_views = nullptr;
     ctx->h_views_cap = 0;
-    e = cudaMallocHost((void**)&ctx->h_views, sizeof(DevView) * size_t(std::max(nviews, 64)));
+    const int cap = std::max(nviews, 64);
+    e = cudaMallocHost((void**)&ctx->h_views, 2 * sizeof(DevView) * size_t(cap));
     if (e != cudaSuccess) return cuda_fail(ctx, e, "pinned view staging");
-    ctx->h_views_cap = std::max(nviews, 64);
+    ctx->h_views_cap = cap;
   }
+  DevView* staging = ctx->h_views + size_t(half) * ctx->h_views_cap;
   int64_t voxels = 0;
   int accel_views = 0;
   for (int i = 0; i < nviews; ++i) {
@@ -791,13 +813,16 @@ nd_status forward_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, c
   int kernel = 0;
   if (sc.nscenes > 0 && (s = ensure_dev(ctx, &ctx->d_scenes, &ctx->scenes_cap, sc.nscenes, "scene table")) != ND_OK)
     return s;
-  s = enqueue(ctx, views, nviews, opts, out, st, plans, ctx->d_views, ctx->h_views, ctx->d_counters, ctx->d_thit,
+  s = enqueue(ctx, views, nviews, opts, out, st, plans, ctx->d_views, staging, ctx->d_counters, ctx->d_thit,
               ctx->d_hits, true, &kernel, ctx->tev.data(), sc, sc.nscenes > 0 ? ctx->d_scenes : nullptr,
               ctx->d_accel, ctx->d_accel_jobs);
   ctx->tev_plans = s == ND_OK ? int(plans.size()) : 0;
   if (s != ND_OK) return s;
   e = cudaEventRecord(ctx->last_done, st);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->staged[half], st);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "record event");
+  ctx->staged_valid[half] = true;
+  ++ctx->calls;
   ctx->have_last = true;
   ctx->last_stream = st;
   ctx->last_kernel = kernel;
@@ -1095,12 +1120,15 @@ nd_status shade_lite_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews
   if (sc.nscenes > 0 && (s = ensure_dev(ctx, &ctx->d_scenes, &ctx->scenes_cap, sc.nscenes, "scene table")) != ND_OK)
     return s;
   if (ctx->h_views_cap < nviews) {
+    for (int k = 0; k < 2; ++k)
+      if (ctx->staged_valid[k]) cudaEventSynchronize(ctx->staged[k]);
     if (ctx->h_views) cudaFreeHost(ctx->h_views);
     ctx->h_views = nullptr;
     ctx->h_views_cap = 0;
-    e = cudaMallocHost((void**)&ctx->h_views, sizeof(DevView) * size_t(std::max(nviews, 64)));
+    const int cap = std::max(nviews, 64);
+    e = cudaMallocHost((void**)&ctx->h_views, 2 * sizeof(DevView) * size_t(cap));
     if (e != cudaSuccess) return cuda_fail(ctx, e, "pinned view staging");
-    ctx->h_views_cap = std::max(nviews, 64);
+    ctx->h_views_cap = cap;
   }
   // views and descriptors in plan order; colour stops sorted by position
   std::vector<int64_t> out_off(nviews + 1, 0);
