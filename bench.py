@@ -520,10 +520,17 @@ def main():
     # copies its view descriptors up (inside nd_march_forward) and reads its G-buffer
     # back into pinned host memory; with two G-buffers the read-back of step i (on a
     # copy stream) overlaps the march of step i + 1.  L2 flushed before every step.
-    keys = ("depth", "normal", "trap", "steps")
-    gbufs = [gbuf, runtime.GBuffer.allocate(nrays, device=dev)]
-    hosts = [{k: torch.empty(getattr(gbuf, k).shape, dtype=getattr(gbuf, k).dtype, pin_memory=True) for k in keys}
-             for _ in range(2)]
+    # The read-back is the reference's own G-buffer formats (fr:73-76): depth R32F,
+    # normal RGBA16F (w = hit), plus the orbit trap and the step count.
+    keys = ("depth", "normal_half", "trap", "steps")
+    gbufs = []
+    for _ in range(2):
+        gb = runtime.GBuffer.allocate(nrays, device=dev)
+        gb.normal = None
+        gb.normal_half = torch.empty((nrays, 4), dtype=torch.float16, device=dev)
+        gbufs.append(gb)
+    hosts = [{k: torch.empty(getattr(gbufs[0], k).shape, dtype=getattr(gbufs[0], k).dtype, pin_memory=True)
+              for k in keys} for _ in range(2)]
     d2h = sum(t.numel() * t.element_size() for t in hosts[0].values())
     h2d = len(views) * runtime.load_library().nd_sizeof(b"DevView")  # the view table nd_march_forward copies
     copy_stream = torch.cuda.Stream(device=dev)
@@ -616,9 +623,9 @@ def main():
             "batched_over_plain": ms_plain / ms_batched,
             "e2e": {"value": rays_total / (ms_e2e * 1e-3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e,
-                    "kind": "nd_march_forward from host view descriptors, G-buffer (depth, normal, trap, steps) read "
-                            "back to pinned host memory every step; two G-buffers, read-back of step i overlapping "
-                            "the march of step i+1"},
+                    "kind": "nd_march_forward from host view descriptors, G-buffer (depth R32F, normal RGBA16F, "
+                            "trap, steps: 20 B per ray) read back to pinned host memory every step; two G-buffers, "
+                            "read-back of step i overlapping the march of step i+1"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": NCU_TRAFFIC.get(args.workload),
                          "kernel": "persistent_kernel (march); FLOPs = its DE evaluations x FLOPs per "

@@ -54,7 +54,7 @@
 extern "C" {
 #endif
 
-#define ND_ABI_VERSION 2
+#define ND_ABI_VERSION 3
 #define ND_MAX_PARAMS 16          /* fractal_renderer.zig:47 */
 #define ND_PARAM_NAME_LEN 24      /* CustomParam.name [24:0]u8, formula.zig:7 */
 
@@ -219,6 +219,8 @@ typedef struct nd_gbuffer {
   float* shadow;      /* shadow-ray visibility in [0, 1] (1 without a shadow ray) */
   double* depth64;    /* t in FP64 */
   uint32_t* evals;    /* DE evaluations spent on this ray */
+  uint16_t* normal_half; /* the normal as the reference's RGBA16F target: 4 IEEE halves per ray,
+                            w = 1 on a hit (8-byte aligned) */
 } nd_gbuffer;
 
 enum { ND_KERNEL_AUTO = 0, ND_KERNEL_PLAIN = 1, ND_KERNEL_PERSISTENT = 2 };

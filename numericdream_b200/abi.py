@@ -181,7 +181,7 @@ def make_lite(colors=(), lights=(), ambient_occlusion=True, specular=True, backg
 class nd_gbuffer(C.Structure):
     _fields_ = [("depth", C.c_void_p), ("normal", C.c_void_p), ("trap", C.c_void_p), ("steps", C.c_void_p),
                 ("iters", C.c_void_p), ("shade", C.c_void_p), ("shadow", C.c_void_p), ("depth64", C.c_void_p),
-                ("evals", C.c_void_p)]
+                ("evals", C.c_void_p), ("normal_half", C.c_void_p)]
 
 
 class nd_march_opts(C.Structure):

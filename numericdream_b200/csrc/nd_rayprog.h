@@ -24,6 +24,9 @@
 #include "nd_helpers.h"
 #include "nd_dual.h"
 #include "../../include/nd_march.h"
+#if defined(__CUDACC__)
+#include <cuda_fp16.h>
+#endif
 
 #if defined(__CUDACC__)
 #define ND_DEV_INLINE __host__ __device__ __forceinline__
@@ -42,6 +45,7 @@ ND_DEV_INLINE double rn_add(double a, double b) { return __dadd_rn(a, b); }
 ND_DEV_INLINE double fma_d(double a, double b, double c) { return __fma_rn(a, b, c); }
 ND_DEV_INLINE float load_ro(const float* p) { return __ldg(p); }
 ND_DEV_INLINE int32_t float_bits(float x) { return __float_as_int(x); }
+ND_DEV_INLINE uint16_t half_bits(float x) { return __half_as_ushort(__float2half_rn(x)); }
 #else
 // host builds of this header are compiled with -ffp-contract=off
 ND_DEV_INLINE float rn_mul(float a, float b) { return a * b; }
@@ -54,6 +58,22 @@ ND_DEV_INLINE int32_t float_bits(float x) {
   int32_t b;
   memcpy(&b, &x, sizeof(b));
   return b;
+}
+// IEEE binary16 bits of x, rounded to nearest even (host builds of the ray program)
+ND_DEV_INLINE uint16_t half_bits(float x) {
+  uint32_t u;
+  memcpy(&u, &x, sizeof(u));
+  const uint32_t sign = (u >> 16) & 0x8000u, ax = u & 0x7fffffffu;
+  if (ax >= 0x7f800000u) return uint16_t(sign | 0x7c00u | (ax > 0x7f800000u ? 0x200u : 0u));  // inf / NaN
+  if (ax >= 0x477ff000u) return uint16_t(sign | 0x7c00u);                                      // overflow
+  if (ax < 0x38800000u) {                                                                      // subnormal / 0
+    if (ax < 0x33000000u) return uint16_t(sign);
+    const uint32_t e = ax >> 23, m = (ax & 0x7fffffu) | 0x800000u;
+    const uint32_t shift = 126u - e, q = m >> shift, rem = m & ((1u << shift) - 1u), half = 1u << (shift - 1u);
+    return uint16_t(sign | (q + ((rem > half || (rem == half && (q & 1u))) ? 1u : 0u)));
+  }
+  const uint32_t q = (ax - 0x38000000u) >> 13, rem = ax & 0x1fffu;
+  return uint16_t(sign | (q + ((rem > 0x1000u || (rem == 0x1000u && (q & 1u))) ? 1u : 0u)));
 }
 #endif
 
@@ -598,6 +618,14 @@ struct RayResult {
   bool hit;
 };
 
+// The normal as the reference's RGBA16F target (fr:73-76): four halves, w = hit.
+ND_DEV_INLINE void write_normal_half(const nd_gbuffer& g, int64_t r, float nx, float ny, float nz, bool hit) {
+  struct alignas(8) H4 {
+    uint16_t x, y, z, w;
+  };
+  reinterpret_cast<H4*>(g.normal_half)[r] = H4{half_bits(nx), half_bits(ny), half_bits(nz), uint16_t(hit ? 0x3c00u : 0u)};
+}
+
 // Outputs of the march; t_hit (FP64 t on a hit, -1 on a miss) feeds the trap pass.
 ND_DEV_INLINE void write_result(const nd_gbuffer& g, double* t_hit, int64_t r, const RayResult& o) {
   // r is the G-buffer index (view out_offset + ray index inside the view)
@@ -609,6 +637,7 @@ ND_DEV_INLINE void write_result(const nd_gbuffer& g, double* t_hit, int64_t r, c
     };
     reinterpret_cast<F4*>(g.normal)[r] = F4{o.nx, o.ny, o.nz, o.hit ? 1.0f : 0.0f};
   }
+  if (g.normal_half) write_normal_half(g, r, o.nx, o.ny, o.nz, o.hit);
   if (g.steps) g.steps[r] = o.steps;
   if (g.shade) g.shade[r] = o.shade;
   if (g.shadow) g.shadow[r] = o.shadow;
@@ -1016,6 +1045,7 @@ ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, c
     };
     reinterpret_cast<F4*>(g.normal)[r] = F4{gx, gy, gz, 1.0f};
   }
+  if (g.normal_half) write_normal_half(g, r, gx, gy, gz, true);
   if (g.shade) g.shade[r] = lambert(v, dir.get(), gx, gy, gz, vis);
   if (g.shadow) g.shadow[r] = vis;
   if (g.evals) g.evals[r] += uint32_t(taps + sev);

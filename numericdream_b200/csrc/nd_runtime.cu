@@ -516,8 +516,8 @@ nd_status prepare(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const 
   if (!views || nviews <= 0 || nviews > kMaxViews) return fail(ctx, ND_ERR_INVALID, "nviews %d out of range", nviews);
   if (!out || !out->depth) return fail(ctx, ND_ERR_INVALID, "the G-buffer needs at least a depth pointer");
   if ((out->normal && (uintptr_t(out->normal) & 15)) || (out->depth64 && (uintptr_t(out->depth64) & 7)) ||
-      (uintptr_t(out->depth) & 3))
-    return fail(ctx, ND_ERR_INVALID, "misaligned G-buffer pointer (normal needs 16 bytes)");
+      (out->normal_half && (uintptr_t(out->normal_half) & 7)) || (uintptr_t(out->depth) & 3))
+    return fail(ctx, ND_ERR_INVALID, "misaligned G-buffer pointer (normal needs 16 bytes, normal_half 8)");
   int64_t t = 0;
   for (int i = 0; i < nviews; ++i) {
     nd_status s = validate_view(ctx, views[i], i);
@@ -1332,7 +1332,7 @@ extern "C" nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t
   if (nviews > kNoAllocMaxViews) return ND_ERR_INVALID;
   if (out->trap || out->iters) return ND_ERR_UNSUPPORTED;  // the trap pass needs per-ray scratch
   if ((out->normal && (uintptr_t(out->normal) & 15)) || (out->depth64 && (uintptr_t(out->depth64) & 7)) ||
-      (uintptr_t(out->depth) & 3))
+      (out->normal_half && (uintptr_t(out->normal_half) & 7)) || (uintptr_t(out->depth) & 3))
     return ND_ERR_INVALID;
   if (opts && opts->de_precision != 0 && opts->de_precision != 32 && opts->de_precision != 64) return ND_ERR_INVALID;
   int64_t total = 0;

@@ -239,6 +239,7 @@ class GBuffer:
     shadow: "object" = None
     depth64: "object" = None
     evals: "object" = None
+    normal_half: "object" = None  # (n, 4) float16: the reference's RGBA16F normal target
 
     @staticmethod
     def allocate(n: int, device="cuda", full: bool = True) -> "GBuffer":
@@ -258,14 +259,14 @@ class GBuffer:
 
     def as_abi(self) -> abi.nd_gbuffer:
         g = abi.nd_gbuffer()
-        for f in ("depth", "normal", "trap", "steps", "iters", "shade", "shadow", "depth64", "evals"):
+        for f in ("depth", "normal", "trap", "steps", "iters", "shade", "shadow", "depth64", "evals", "normal_half"):
             t = getattr(self, f)
             setattr(g, f, None if t is None else t.data_ptr())
         return g
 
     def numpy(self) -> dict:
         out = {}
-        for f in ("depth", "normal", "trap", "steps", "iters", "shade", "shadow", "depth64", "evals"):
+        for f in ("depth", "normal", "trap", "steps", "iters", "shade", "shadow", "depth64", "evals", "normal_half"):
             t = getattr(self, f)
             if t is not None:
                 out[f] = t.cpu().numpy()

@@ -41,3 +41,15 @@ def test_back_to_back_forwards(ctx, two_streams):
             np.testing.assert_array_equal(got[k], w[k], err_msg=f"frame {i}: {k}")
     st = ctx.stats()
     assert st.rays == workloads.rays(frames[-1]) and st.timeouts == 0
+
+
+def test_rgba16f_normal_output(ctx):
+    """normal_half holds the f32 normal rounded to IEEE halves (w = hit), as the
+    reference's RGBA16F normal target."""
+    views = _frames()[0]
+    n = workloads.rays(views)
+    g = runtime.GBuffer.allocate(n)
+    g.normal_half = torch.empty((n, 4), dtype=torch.float16, device="cuda")
+    ctx.forward(views, g, runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT))
+    out = g.numpy()
+    np.testing.assert_array_equal(out["normal_half"].view(np.uint16), out["normal"].astype(np.float16).view(np.uint16))
