@@ -497,3 +497,17 @@ class FractalRenderer:
         g = GBuffer.allocate(n, device=torch.device("cuda", self.ctx.device), full=full)
         self.ctx.forward(views, g, opts, stream=stream)
         return g
+
+    def render_to_image(self, scene_file, width: int = 0, height: int = 0) -> bytes:
+        """renderToImage (fractal_renderer.zig:3548) for this pass: a .dream scene's
+        geometry and lite colour as width x height RGBA8 (colour clamped to [0, 1];
+        the reference's tone mapping and post effects are not part of this pass)."""
+        import numpy as np
+
+        from .render import render_scene_file
+
+        img, _ = render_scene_file(self.ctx, scene_file, width, height)
+        rgba = np.empty(img.shape, np.uint8)
+        rgba[..., :3] = (np.clip(img[..., :3], 0.0, 1.0) * 255.0 + 0.5).astype(np.uint8)
+        rgba[..., 3] = 255
+        return rgba.tobytes()

@@ -103,3 +103,15 @@ def test_render_scene_file_to_an_image(ctx, tmp_path):
     out = tmp_path / "scene.ppm"
     write_ppm(str(out), img)
     assert out.read_bytes().startswith(b"P6 160 90 255\n") and out.stat().st_size == 14 + 160 * 90 * 3
+
+
+def test_fractal_renderer_render_to_image(ctx):
+    from numericdream_b200.runtime import FractalRenderer
+
+    r = FractalRenderer(0)
+    try:
+        data = r.render_to_image(os.path.join(HERE, "golden", "two_fractals.dream"), 64, 36)
+    finally:
+        r.ctx.close()
+    img = np.frombuffer(data, np.uint8).reshape(36, 64, 4)
+    assert (img[..., 3] == 255).all() and img[..., :3].std() > 1.0
