@@ -578,6 +578,12 @@ def main():
     if not args.no_extra and ws == 1:
         diff = differentiation_step(ctx, stream, sptr, timed, max(2, args.steps // 2))
         other = small_and_deepzoom(ctx, sptr, timed, max(2, args.steps // 2))
+    measured_fp32 = None
+    if rank == 0:
+        try:
+            measured_fp32 = ctx.measure_fp32_peak(20.0)
+        except runtime.NDError:
+            measured_fp32 = None
     clk = clocks.stop()
     gnp = gbuf.numpy() if rank == 0 else None
 
@@ -591,7 +597,8 @@ def main():
 
         flops_per_eval, per = opcount.flops_per_eval_for(views)
         flops = st.march_evals * flops_per_eval  # the march kernel's evaluations
-        peak = opcount.fp32_peak_tflops(clk.get("sm_mhz") or clk.get("sm_max_mhz"))
+        nominal = opcount.fp32_peak_tflops(clk.get("sm_mhz") or clk.get("sm_max_mhz"))
+        peak = measured_fp32 if measured_fp32 else nominal
         achieved = flops / (kms[0] * 1e-3) / 1e12
         cpu, err = None, None
         if not args.no_cpu:
@@ -632,8 +639,10 @@ def main():
                                    "evaluation, over its CUDA-event time",
                          "kernel_ms": kms[0], "shade_pass_ms": kms[1],
                          "flops_per_eval": flops_per_eval, "sfu_per_eval": per["sfu"],
-                         "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 x sampled SM clock (not in "
-                                        "MEASURED_PEAKS.json)"},
+                         "peak_source": ("measured: nd_measure_fp32_peak, independent FFMA chains on this GPU "
+                                         "(CUDA events); FP32 is not in MEASURED_PEAKS.json")
+                         if measured_fp32 else "nominal: 148 SMs x 128 FP32 lanes x 2 x sampled SM clock",
+                         "peak_nominal": nominal},
             "error_vs_fp64": err, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": 2 * args.steps,
             "stats": {"de_evals": st.de_evals, "march": st.march_evals, "normal": st.normal_evals,

@@ -452,6 +452,11 @@ nd_status nd_scene_file_load(const char* json, size_t len, int32_t width, int32_
 nd_status nd_scene_file_lite(const char* json, size_t len, int32_t instance, nd_lite_desc* lite, char* err,
                              size_t err_len);
 
+/* Measures the device's FP32 FMA throughput (the roofline of the march, whose DE
+ * code is scalar FP32): a resident grid of independent fused multiply-add chains for
+ * about `ms` milliseconds; *tflops = 2 x FMAs / CUDA-event time. */
+nd_status nd_measure_fp32_peak(nd_ctx* ctx, double ms, double* tflops);
+
 /* Size of a public struct by name ("nd_view_desc", ...), for binding layout checks. */
 size_t nd_sizeof(const char* name);
 

@@ -1211,6 +1211,61 @@ nd_status nd_shade_lite_scenes(nd_ctx* ctx, const nd_view_desc* views, int32_t n
   return shade_lite_impl(ctx, views, nviews, lite, instance_colors, in, rgba, stream, sc);
 }
 
+}  // extern "C"
+
+namespace {
+// 8 independent FMA chains per thread (enough to cover the FMA latency at full
+// occupancy); the sum goes to out so that nothing is eliminated.
+__global__ void __launch_bounds__(256) fp32_peak_kernel(int iters, float b, float c, float* out) {
+  float a0 = threadIdx.x * 1e-7f, a1 = a0 + 1e-7f, a2 = a0 + 2e-7f, a3 = a0 + 3e-7f;
+  float a4 = a0 + 4e-7f, a5 = a0 + 5e-7f, a6 = a0 + 6e-7f, a7 = a0 + 7e-7f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      a0 = fmaf(a0, b, c); a1 = fmaf(a1, b, c); a2 = fmaf(a2, b, c); a3 = fmaf(a3, b, c);
+      a4 = fmaf(a4, b, c); a5 = fmaf(a5, b, c); a6 = fmaf(a6, b, c); a7 = fmaf(a7, b, c);
+    }
+  }
+  const float s = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+  if (s == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;  // never true for these inputs
+}
+}  // namespace
+
+extern "C" {
+
+nd_status nd_measure_fp32_peak(nd_ctx* ctx, double ms, double* tflops) {
+  if (!ctx || !tflops || !(ms > 0)) return fail(ctx, ND_ERR_INVALID, "bad nd_measure_fp32_peak arguments");
+  cudaSetDevice(ctx->device);
+  const int blocks = ctx->num_sms * 8, threads = 256;
+  float* out = nullptr;
+  cudaError_t e = cudaMalloc((void**)&out, sizeof(float) * size_t(blocks) * threads);
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&a);
+  if (e == cudaSuccess) e = cudaEventCreate(&b);
+  double best = 0.0;
+  int iters = 256;
+  for (int rep = 0; e == cudaSuccess && rep < 8; ++rep) {
+    cudaEventRecord(a, nullptr);
+    fp32_peak_kernel<<<blocks, threads>>>(iters, 0.999999f, 1e-7f, out);
+    cudaEventRecord(b, nullptr);
+    e = cudaEventSynchronize(b);
+    if (e != cudaSuccess) break;
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, a, b);
+    const double flops = 2.0 * 8.0 * 16.0 * double(iters) * blocks * threads;
+    if (t > 0.25 * ms) best = std::max(best, flops / (double(t) * 1e-3) / 1e12);
+    // grow toward `ms` at most 100x per run, and never past 2^20 iterations (about 1 s)
+    if (t < ms) iters = int(std::min<double>(double(iters) * std::min(100.0, std::max(2.0, ms / std::max(double(t), 1e-3))),
+                                             double(1 << 20)));
+  }
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  if (out) cudaFree(out);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "nd_measure_fp32_peak");
+  *tflops = best;
+  return ND_OK;
+}
+
 nd_status nd_accel_grid(nd_ctx* ctx, const nd_view_desc* view, int32_t de_precision, float* grid, int64_t capacity,
                         float* prm, int64_t* count) {
   if (!ctx || !view || !grid || !prm || !count) return fail(ctx, ND_ERR_INVALID, "bad nd_accel_grid arguments");

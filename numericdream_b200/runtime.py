@@ -66,6 +66,7 @@ _SIGNATURES = {
                                          C.POINTER(abi.nd_scene_desc), C.c_int32, C.POINTER(abi.nd_lite_desc),
                                          C.POINTER(abi.nd_lite_desc), C.POINTER(abi.nd_gbuffer), C.c_void_p,
                                          C.c_void_p]),
+    "nd_measure_fp32_peak": (C.c_int32, [C.c_void_p, C.c_double, C.POINTER(C.c_double)]),
     "nd_march_forward_scenes": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(C.c_int32),
                                             C.POINTER(abi.nd_scene_desc), C.c_int32, C.POINTER(abi.nd_march_opts),
                                             C.POINTER(abi.nd_gbuffer), C.c_void_p]),
@@ -425,6 +426,13 @@ class Context:
                                     prm.ctypes.data, C.byref(n))
         self._check(st, "nd_accel_grid")
         return grid.cpu().numpy().reshape(levels, res, res, res), prm
+
+    def measure_fp32_peak(self, ms: float = 20.0) -> float:
+        """nd_measure_fp32_peak: the device's FP32 FMA throughput in TFLOP/s."""
+        out = C.c_double()
+        st = self.lib.nd_measure_fp32_peak(self.handle, ms, C.byref(out))
+        self._check(st, "nd_measure_fp32_peak")
+        return out.value
 
     def stats(self) -> abi.nd_stats:
         out = abi.nd_stats()
