@@ -320,6 +320,13 @@ nd_status nd_orbit_view(const nd_orbit_camera* cam, nd_view_desc* view);
 nd_status nd_march_forward_scenes(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews,
                                   const int32_t* view_scene, const nd_scene_desc* scenes, int32_t nscenes,
                                   const nd_march_opts* opts, const nd_gbuffer* out, void* stream);
+/* nd_graph_capture for a scene call: the graph owns device copies of the view and
+ * scene tables, so the caller may change or free views, view_scene and scenes after
+ * the capture; replays march the captured scenes. */
+nd_status nd_graph_capture_scenes(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews,
+                                  const int32_t* view_scene, const nd_scene_desc* scenes, int32_t nscenes,
+                                  const nd_march_opts* opts, const nd_gbuffer* out, void* stream,
+                                  nd_graph** graph);
 
 /* Gradient of an image loss with respect to formula @params and the orbit pose.
  * No counterpart in the reference (it has no gradients).  views/cams (HOST) are the

@@ -105,6 +105,7 @@ struct nd_graph {
   int32_t* d_hits = nullptr;
   float* d_accel = nullptr;
   nd::AccelJob* d_accel_jobs = nullptr;
+  nd::DevScene* d_scenes = nullptr;
   bool trap = false;
 };
 
@@ -380,7 +381,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
                                     stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "copy accelerator jobs");
   }
-  if (sc.nscenes > 0 && d_scenes) {
+  if (copy_views && sc.nscenes > 0 && d_scenes) {
     // scenes are only accepted when one formula group covers the call: one plan
     std::vector<nd::DevScene> hs;
     scene_table(sc, plans[0].members, &hs);
@@ -959,17 +960,22 @@ nd_status nd_autotune(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, co
   return ND_OK;
 }
 
+}  // extern "C"
+
+namespace {
 // Captures one forward call (work-counter and stats resets plus every launch)
-// into a CUDA graph.  The graph owns a device copy of the view table, so it can
-// be replayed while the caller changes its own descriptors.
-nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_march_opts* opts,
-                           const nd_gbuffer* out, void* stream, nd_graph** graph) {
+// into a CUDA graph.  The graph owns device copies of the view table and of the
+// scene table, so it can be replayed while the caller changes its own descriptors.
+nd_status graph_capture_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_march_opts* opts,
+                             const nd_gbuffer* out, void* stream, nd_graph** graph, const SceneInput& sc) {
   if (!graph) return ND_ERR_INVALID;
   *graph = nullptr;
   std::vector<Launch> plans;
   int64_t total = 0;
-  nd_status s = prepare(ctx, views, nviews, out, &plans, &total);
+  nd_status s = prepare(ctx, views, nviews, out, &plans, &total, sc);
   if (s != ND_OK) return s;
+  if (opts && opts->de_precision != 0 && opts->de_precision != 32 && opts->de_precision != 64)
+    return fail(ctx, ND_ERR_INVALID, "de_precision must be 32 or 64");
   cudaSetDevice(ctx->device);
   nd_graph* g = new nd_graph();
   g->ctx = ctx;
@@ -987,6 +993,7 @@ nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
   if (e == cudaSuccess && voxels > 0) e = cudaMalloc((void**)&g->d_accel, sizeof(float) * size_t(voxels));
   if (e == cudaSuccess && accel_views > 0)
     e = cudaMalloc((void**)&g->d_accel_jobs, sizeof(nd::AccelJob) * size_t(accel_views));
+  if (e == cudaSuccess && sc.nscenes > 0) e = cudaMalloc((void**)&g->d_scenes, sizeof(nd::DevScene) * size_t(sc.nscenes));
   if (e != cudaSuccess) {
     nd_graph_destroy(g);
     return cuda_fail(ctx, e, "graph buffers");
@@ -1008,7 +1015,7 @@ nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
     return cuda_fail(ctx, e, "begin capture");
   }
   s = enqueue(ctx, views, nviews, opts, out, cap, plans, g->d_views, hv.data(), g->d_counters, g->d_thit,
-              g->d_hits, false, nullptr, nullptr, SceneInput(), nullptr, g->d_accel, g->d_accel_jobs, &jobs);
+              g->d_hits, false, nullptr, nullptr, sc, g->d_scenes, g->d_accel, g->d_accel_jobs, &jobs);
   cudaGraph_t gr = nullptr;
   e = cudaStreamEndCapture(cap, &gr);
   cudaStreamDestroy(cap);
@@ -1021,6 +1028,11 @@ nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
   e = cudaMemcpy(g->d_views, hv.data(), sizeof(DevView) * size_t(nviews), cudaMemcpyHostToDevice);
   if (e == cudaSuccess && !jobs.empty())
     e = cudaMemcpy(g->d_accel_jobs, jobs.data(), sizeof(nd::AccelJob) * jobs.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && sc.nscenes > 0) {
+    std::vector<nd::DevScene> hs;
+    scene_table(sc, plans[0].members, &hs);
+    e = cudaMemcpy(g->d_scenes, hs.data(), sizeof(nd::DevScene) * hs.size(), cudaMemcpyHostToDevice);
+  }
   if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, gr, 0);
   if (e != cudaSuccess) {
     nd_graph_destroy(g);
@@ -1029,6 +1041,28 @@ nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
   (void)st;
   *graph = g;
   return ND_OK;
+}
+}  // namespace
+
+extern "C" {
+
+nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_march_opts* opts,
+                           const nd_gbuffer* out, void* stream, nd_graph** graph) {
+  return graph_capture_impl(ctx, views, nviews, opts, out, stream, graph, SceneInput());
+}
+
+nd_status nd_graph_capture_scenes(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const int32_t* view_scene,
+                                  const nd_scene_desc* scenes, int32_t nscenes, const nd_march_opts* opts,
+                                  const nd_gbuffer* out, void* stream, nd_graph** graph) {
+  if (graph) *graph = nullptr;
+  if (!ctx) return ND_ERR_INVALID;
+  if (nscenes < 0 || (nscenes > 0 && (!scenes || !view_scene)))
+    return fail(ctx, ND_ERR_INVALID, "scenes need a view_scene array and a scene array");
+  SceneInput sc;
+  sc.view_scene = view_scene;
+  sc.scenes = scenes;
+  sc.nscenes = nscenes;
+  return graph_capture_impl(ctx, views, nviews, opts, out, stream, graph, sc);
 }
 
 nd_status nd_graph_launch(nd_graph* g, void* stream) {
@@ -1040,6 +1074,8 @@ nd_status nd_graph_launch(nd_graph* g, void* stream) {
   e = cudaEventRecord(g->ctx->last_done, (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(g->ctx, e, "record event");
   g->ctx->have_last = true;
+  // a later forward on another stream waits for this replay (it shares the stats block)
+  g->ctx->last_stream = (cudaStream_t)stream;
   g->ctx->last_trap = g->trap;
   return ND_OK;
 }
@@ -1055,6 +1091,7 @@ nd_status nd_graph_destroy(nd_graph* g) {
   if (g->d_hits) cudaFree(g->d_hits);
   if (g->d_accel) cudaFree(g->d_accel);
   if (g->d_accel_jobs) cudaFree(g->d_accel_jobs);
+  if (g->d_scenes) cudaFree(g->d_scenes);
   delete g;
   return ND_OK;
 }

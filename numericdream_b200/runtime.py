@@ -48,6 +48,10 @@ _SIGNATURES = {
     "nd_graph_capture": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32,
                                      C.POINTER(abi.nd_march_opts), C.POINTER(abi.nd_gbuffer), C.c_void_p,
                                      C.POINTER(C.c_void_p)]),
+    "nd_graph_capture_scenes": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32,
+                                            C.POINTER(C.c_int32), C.POINTER(abi.nd_scene_desc), C.c_int32,
+                                            C.POINTER(abi.nd_march_opts), C.POINTER(abi.nd_gbuffer), C.c_void_p,
+                                            C.POINTER(C.c_void_p)]),
     "nd_graph_launch": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "nd_graph_destroy": (C.c_int32, [C.c_void_p]),
     "nd_sizeof": (C.c_size_t, [C.c_char_p]),
@@ -456,6 +460,20 @@ class Context:
         st = self.lib.nd_graph_capture(self.handle, arr, len(views), C.byref(opts) if opts is not None else None,
                                        C.byref(g), s, C.byref(h))
         self._check(st, "nd_graph_capture")
+        return Graph(self, h)
+
+    def capture_scenes(self, views, view_scene, scenes, gbuf: GBuffer, opts=None, stream=None) -> "Graph":
+        """nd_graph_capture_scenes: a graph of forward_scenes(views, view_scene, scenes)."""
+        arr = (abi.nd_view_desc * len(views))(*views)
+        vs = (C.c_int32 * len(views))(*view_scene)
+        sarr = (abi.nd_scene_desc * max(1, len(scenes)))(*scenes)
+        g = gbuf.as_abi()
+        h = C.c_void_p()
+        s = None if stream is None else C.c_void_p(stream)
+        st = self.lib.nd_graph_capture_scenes(self.handle, arr, len(views), vs, sarr, len(scenes),
+                                              C.byref(opts) if opts is not None else None, C.byref(g), s,
+                                              C.byref(h))
+        self._check(st, "nd_graph_capture_scenes")
         return Graph(self, h)
 
 

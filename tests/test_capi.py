@@ -26,7 +26,8 @@ def test_header_declares_the_abi():
     for must in ("nd_formula_register", "nd_formula_params", "nd_ctx_create", "nd_ctx_destroy",
                  "nd_march_forward", "nd_last_stats", "nd_autotune", "nd_graph_capture", "nd_graph_launch",
                  "nd_march_backward", "nd_march_forward_noalloc", "nd_march_forward_scenes", "nd_accel_grid",
-                 "nd_scene_file_load", "nd_scene_file_lite", "nd_shade_lite", "nd_shade_lite_scenes"):
+                 "nd_scene_file_load", "nd_scene_file_lite", "nd_shade_lite", "nd_shade_lite_scenes",
+                 "nd_graph_capture_scenes"):
         assert must in names
 
 

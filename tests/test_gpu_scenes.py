@@ -159,3 +159,39 @@ def test_formulas_outside_one_set_are_refused(ctx):
     with pytest.raises(runtime.NDError) as e:
         ctx.forward_scenes([v], [0], [abi.make_scene([a, b])], g)
     assert e.value.status == abi.ND_ERR_UNSUPPORTED
+
+
+def test_graph_replay_of_a_scene_call(ctx):
+    """nd_graph_capture_scenes: a replay writes what the direct scene call wrote, and
+    keeps marching the captured scenes after the caller's tables change."""
+    import torch
+
+    box = workloads.mandelbox_params(-1.5, 10)
+    bulb = workloads.mandelbulb_params(8.0, 8)
+    a = abi.make_instance(_fid(workloads.MANDELBOX), params=box, offset=(-0.9, 0.0, 0.0), scale=(0.3, 0.3, 0.3))
+    b = abi.make_instance(_fid(workloads.MANDELBULB), params=bulb, offset=(0.7, 0.0, 0.0), scale=(0.8, 0.8, 0.8),
+                          combine_mode=abi.ND_COMBINE_SMOOTH_MIN, blend_k=0.15)
+    scenes = [abi.make_scene([a, b], carves=[(0.7, 0.0, -0.7, 0.35)])]
+    v_plain = abi.make_view(_fid(workloads.MANDELBOX), 48, 48, (0.0, 0.0, -4.5), fov_y_deg=60.0,
+                            params=box, max_steps=256)
+    views = [_view(64), v_plain]
+    view_scene = [0, -1]
+    opts = runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT)
+    g1, _ = _forward(ctx, views, view_scene, scenes)
+    gb = runtime.GBuffer.allocate(workloads.rays(views))
+    graph = ctx.capture_scenes(views, view_scene, scenes, gb, opts)
+    try:
+        # the caller's scene table changes after the capture; the graph keeps its copy
+        scenes[0].instances[0].offset[0] = 5.0
+        for _ in range(2):
+            graph.launch()
+            torch.cuda.synchronize()
+            g2 = gb.numpy()
+            for k in ("depth64", "steps", "evals", "trap", "normal"):
+                np.testing.assert_array_equal(g1[k], g2[k], err_msg=k)
+        assert ctx.stats().rays == workloads.rays(views)
+    finally:
+        graph.close()
+    with pytest.raises(runtime.NDError) as e:
+        ctx.capture_scenes(views, [0, 1], scenes, gb, opts)
+    assert e.value.status == abi.ND_ERR_INVALID
