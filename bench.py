@@ -315,6 +315,13 @@ def profile_forward(args):
     for v in views:
         if args.accel_res:
             v.accel_res, v.accel_levels, v.accel_safety = args.accel_res, 6, 0.92
+        if args.formula:
+            # the same cameras against another formula at its @param defaults (with
+            # sphere_primitive: the cost of the ray program around a one-step DE)
+            v.formula = runtime.find_formula(args.formula)
+            defaults = [p.default_value for p in runtime.formula_params(v.formula)]
+            for i in range(16):
+                v.params[i] = defaults[i] if i < len(defaults) else 0.0
     g = runtime.GBuffer.allocate(workloads.rays(views))
     ctx.forward(views, g, runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, refill_threshold=4))
     if args.with_lite:
@@ -430,6 +437,7 @@ def main():
     ap.add_argument("--no-extra", action="store_true", help="skip the second (1080p Mandelbox) workload")
     ap.add_argument("--with-lite", action="store_true", help="--profile-forward: also one lite shading pass")
     ap.add_argument("--accel-res", type=int, default=0, help="--profile-forward: accelerator grids of this size")
+    ap.add_argument("--formula", default="", help="--profile-forward: every view's formula replaced by this one")
     ap.add_argument("--profile-forward", action="store_true",
                     help="run ONE forward of the workload through the public API and exit (for ncu captures)")
     args = ap.parse_args()

@@ -102,6 +102,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
   const unsigned lt_mask = (1u << lane) - 1u;
   Lane<T, kDir64> L;
   L.item = -1;
+  L.view = 0;
   L.phase = PH_DONE;
   L.evals = 0;
   L.hit = false;
@@ -143,8 +144,8 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     }
   };
   while (true) {
-    const bool done = L.item >= 0 && L.phase == PH_DONE;
-    const unsigned free_lanes = __ballot_sync(full, L.item < 0 || done);
+    // an idle lane (item < 0) is always in PH_DONE, so phase alone tells busy lanes
+    const unsigned free_lanes = __ballot_sync(full, L.phase == PH_DONE);
     const int nfree = __popc(free_lanes);
     const bool have_work = !exhausted || wnext < wend;
     if (!have_work && free_lanes == full) {
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
         const int r = __popc(idle & lt_mask);
         if (r < used) {
           const int32_t it = r < avail ? wnext + r : base + (r - avail);
-          L.view = kBatched ? find_view(a.views, a.nviews, it) : 0;
+          L.view = kBatched ? find_view_from(a.views, a.nviews, it, L.view) : 0;
           const DevView& v = kBatched ? a.views[L.view] : single;
           L.start(v, it, L.view, true);
           if (L.phase == PH_DONE) L.finish(v, a.out, a.t_hit, 1.0f);
@@ -194,7 +195,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
         break;
       }
     }
-    if (L.item >= 0 && L.phase != PH_DONE) {
+    if (L.phase != PH_DONE) {
       const DevView& v = kBatched ? a.views[L.view] : single;
       bool probe = true;
       if constexpr (kAccel) {

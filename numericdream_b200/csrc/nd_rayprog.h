@@ -678,6 +678,17 @@ ND_DEV_INLINE int find_view(const DevView* views, int nviews, int64_t item) {
   return lo;
 }
 
+// find_view, checking first the view a lane marched last: a warp takes runs of
+// consecutive rays, so a new ray is usually in the same view.  The same result as
+// find_view (the one non-empty view whose ray range holds item).
+ND_DEV_INLINE int find_view_from(const DevView* views, int nviews, int64_t item, int hint) {
+  if (hint >= 0 && hint < nviews) {
+    const int64_t lo = views[hint].ray_offset;
+    if (item >= lo && item - lo < views[hint].rays) return hint;
+  }
+  return find_view(views, nviews, item);
+}
+
 // --------------------------------------------------------------- normals
 // estimate_normal (tpl:1783-1804) and the 6-tap central difference, one tap at a
 // time: the position of tap k around the hit p, the accumulation of its DE value,
@@ -899,12 +910,11 @@ template <class T, bool kDir64> struct Lane {
         return;
       }
       if (probing && on_hit) {
-        // a plain sphere-tracing step (no verify refinement): advance by d
+        // a plain sphere-tracing step (no verify refinement): advance by d.  march_to
+        // also sets hi, refines and resolved here; with on_hit none of them is read
+        // before the bisection's entry sets them again, so the lane leaves them.
         a = t;
         t = t + d;
-        b = t;
-        k = 0;
-        resolved = false;
         ++i;
         if (t > v.max_dist || i >= v.max_steps || n >= v.max_samples) finish(v, g, t_hit, 1.0f);
         return;
