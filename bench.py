@@ -305,13 +305,19 @@ def reference_arm(args):
 
 
 def profile_forward(args):
-    """One forward of the workload (persistent march + shade pass), nothing timed."""
+    """One forward of the workload (persistent march + shade pass) for a profiler;
+    with --repeat N, N more forwards after it, reporting the median of the march
+    kernel's CUDA-event times (L2 flushed before each)."""
     import torch
 
     from numericdream_b200 import abi, runtime, workloads
 
     ctx = runtime.Context(0)
     views = build_views(args.workload, runtime.find_formula)
+    if args.views_of:
+        views = [v for v in views if runtime.formula_name(v.formula) == args.views_of]
+        if not views:
+            raise SystemExit(f"no view of {args.views_of} in {args.workload}")
     for v in views:
         if args.accel_res:
             v.accel_res, v.accel_levels, v.accel_safety = args.accel_res, 6, 0.92
@@ -323,15 +329,28 @@ def profile_forward(args):
             for i in range(16):
                 v.params[i] = defaults[i] if i < len(defaults) else 0.0
     g = runtime.GBuffer.allocate(workloads.rays(views))
-    ctx.forward(views, g, runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, refill_threshold=4))
+    opts = runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, refill_threshold=4)
+    ctx.forward(views, g, opts)
+    march_ms = []
+    if args.repeat > 0:
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        for _ in range(args.repeat):
+            flush.fill_(1)
+            ctx.forward(views, g, opts)
+            march_ms.append(ctx.stats().march_ms)
     if args.with_lite:
         lite = abi.make_lite([((0.05, 0.05, 0.22), 0.0, 0.2, 1.3), ((1.0, 0.95, 0.82), 1.0, 0.8, 1.7)],
                              [(abi.ND_LIGHT_GLOBAL, (0.4, 0.8, -0.45), (1.0, 0.95, 0.9), 1.2)])
         ctx.shade_lite(views, [lite] * len(views), g)
     torch.cuda.synchronize()
     st = ctx.stats()
-    print(json.dumps({"workload": args.workload, "rays": workloads.rays(views), "de_evals": st.de_evals,
-                      "march_evals": st.march_evals, "normal_evals": st.normal_evals, "hits": st.hits}))
+    line = {"workload": args.workload, "views": len(views), "rays": workloads.rays(views), "de_evals": st.de_evals,
+            "march_evals": st.march_evals, "normal_evals": st.normal_evals, "hits": st.hits}
+    if march_ms:
+        m = sorted(march_ms)[len(march_ms) // 2]
+        line.update({"march_ms_median": m, "sm_ns_per_march_eval": m * 1e6 * torch.cuda.get_device_properties(0).multi_processor_count
+                                              / max(st.march_evals, 1)})
+    print(json.dumps(line))
     ctx.close()
     return 0
 
@@ -438,6 +457,8 @@ def main():
     ap.add_argument("--with-lite", action="store_true", help="--profile-forward: also one lite shading pass")
     ap.add_argument("--accel-res", type=int, default=0, help="--profile-forward: accelerator grids of this size")
     ap.add_argument("--formula", default="", help="--profile-forward: every view's formula replaced by this one")
+    ap.add_argument("--views-of", default="", help="--profile-forward: only the views of this formula")
+    ap.add_argument("--repeat", type=int, default=0, help="--profile-forward: timed forwards after the first")
     ap.add_argument("--profile-forward", action="store_true",
                     help="run ONE forward of the workload through the public API and exit (for ncu captures)")
     args = ap.parse_args()
