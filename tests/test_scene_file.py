@@ -138,3 +138,85 @@ def test_scene_file_lite(ndlib):
     # a scene without stops or lights: the default material, no lights
     bare = runtime.load_scene_file_lite(_minimal())
     assert (bare.color_count, bare.light_count) == (0, 0)
+
+
+class _GuardedText:
+    """Bytes placed so that they end where an inaccessible page begins: a parser that
+    reads one byte past the length it was given faults at once."""
+
+    def __init__(self, data: bytes):
+        import ctypes as C
+
+        self.C = C
+        libc = C.CDLL(None, use_errno=True)
+        libc.mmap.restype = C.c_void_p
+        libc.mmap.argtypes = [C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_long]
+        libc.mprotect.argtypes = [C.c_void_p, C.c_size_t, C.c_int]
+        libc.munmap.argtypes = [C.c_void_p, C.c_size_t]
+        self.libc = libc
+        page = 4096
+        self.size = ((len(data) + page - 1) // page + 1) * page
+        base = libc.mmap(None, self.size, 3, 0x22, -1, 0)  # PROT_READ|WRITE, MAP_PRIVATE|ANONYMOUS
+        assert base not in (None, C.c_void_p(-1).value)
+        assert libc.mprotect(base + self.size - page, page, 0) == 0  # PROT_NONE
+        self.base = base
+        self.addr = base + self.size - page - len(data)
+        C.memmove(self.addr, data, len(data))
+        self.n = len(data)
+
+    def ptr(self):
+        return self.C.cast(self.addr, self.C.c_char_p)
+
+    def close(self):
+        self.libc.munmap(self.base, self.size)
+
+
+def test_mutated_scene_files_never_crash(ndlib):
+    """Seeded byte mutations and truncations of the fixture: the loader returns a status
+    (or a scene) for every one; the first 400 sit against an inaccessible page, so a
+    read past the given length would fault the test process."""
+    import ctypes as C
+    import random
+
+    src = open(SCENE, "rb").read()
+    rng = random.Random(12345)
+    alphabet = b'{}[]",:0123456789.-eE ntfulrasx\\'
+    outcomes = {"ok": 0, "error": 0}
+    for trial in range(3000):
+        s = bytearray(src)
+        for _ in range(rng.randint(1, 6)):
+            i = rng.randrange(len(s))
+            op = rng.random()
+            if op < 0.3:
+                del s[i:i + rng.randint(1, 20)]
+            elif op < 0.6:
+                s.insert(i, rng.choice(alphabet))
+            elif op < 0.8:
+                s[i] = rng.choice(alphabet)
+            else:
+                j = rng.randrange(len(s))
+                s[i:i] = s[j:j + rng.randint(1, 40)]
+        if rng.random() < 0.2:
+            s = s[:rng.randrange(len(s))]
+        if trial < 400:
+            g = _GuardedText(bytes(s))
+            try:
+                view, scene, needs = abi.nd_view_desc(), abi.nd_scene_desc(), C.c_int32()
+                err = C.create_string_buffer(256)
+                st = ndlib.nd_scene_file_load(g.ptr(), g.n, 64, 48, C.byref(view), C.byref(scene),
+                                              C.byref(needs), err, 256)
+                lite = abi.nd_lite_desc()
+                st2 = ndlib.nd_scene_file_lite(g.ptr(), g.n, 0, C.byref(lite), err, 256)
+                assert st in (abi.ND_OK, abi.ND_ERR_INVALID, abi.ND_ERR_UNSUPPORTED, abi.ND_ERR_NOT_FOUND)
+                assert st2 in (abi.ND_OK, abi.ND_ERR_INVALID, abi.ND_ERR_UNSUPPORTED, abi.ND_ERR_NOT_FOUND)
+            finally:
+                g.close()
+        for load in (lambda: runtime.load_scene_file(bytes(s), 64, 48),
+                     lambda: runtime.load_scene_file_lite(bytes(s), rng.randint(-1, 4))):
+            try:
+                load()
+                outcomes["ok"] += 1
+            except runtime.NDError as e:
+                assert e.status in (abi.ND_ERR_INVALID, abi.ND_ERR_UNSUPPORTED, abi.ND_ERR_NOT_FOUND)
+                outcomes["error"] += 1
+    assert outcomes["ok"] > 0 and outcomes["error"] > 0
