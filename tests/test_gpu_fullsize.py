@@ -1,0 +1,163 @@
+"""batched_64 at its full size (64 views of 64..1024 pixels a side, 7,199,703 rays, the
+benchmark's workload), checked through properties that need no oracle run of every ray:
+
+* two forwards write identical G-buffers (no state carries over between calls);
+* the same views in reverse order give every view the same bits (batching couples no
+  two views: a ray's march depends on its own view only);
+* internal consistency: per-ray evaluation counts sum to the launch's march, normal
+  and shadow counters; a hit has depth = float(depth64) > 0 and normal.w = 1, a miss
+  depth 0 and normal.w = 0; a miss reports max_steps probe steps, a hit at most that;
+* seeded runs of 96 consecutive rays from every view against the FP64 oracle under the
+  boundary-case policy of tests/parity_util.py, with the parity tests' depth, normal
+  and trap tolerances over stable short rays both runs hit.
+
+Edge cases beside it: an empty tile and a one-pixel tile inside a batch, and
+max_steps 0."""
+
+import numpy as np
+import pytest
+
+from numericdream_b200 import abi, runtime, workloads
+from tests.parity_util import compare, policy_check
+
+pytestmark = pytest.mark.gpu
+
+RUN = 96
+
+
+def _forward(ctx, views):
+    g = runtime.GBuffer.allocate(workloads.rays(views))
+    ctx.forward(views, g, runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT))
+    st = ctx.stats()
+    return g.numpy(), st
+
+
+def _offsets(views):
+    off = [0]
+    for v in views:
+        off.append(off[-1] + abi.rays_of(v))
+    return off
+
+
+@pytest.fixture(scope="module")
+def full(ctx):
+    views = workloads.batched_64(runtime.find_formula)
+    assert workloads.rays(views) == 7199703
+    g, st = _forward(ctx, views)
+    return views, g, st
+
+
+def test_full_size_forward_is_deterministic(ctx, full):
+    views, g1, st1 = full
+    g2, st2 = _forward(ctx, views)
+    for k in g1:
+        np.testing.assert_array_equal(g1[k], g2[k], err_msg=k)
+    assert (st1.de_evals, st1.hits, st1.rays) == (st2.de_evals, st2.hits, st2.rays)
+    assert st1.timeouts == 0
+
+
+def test_view_order_does_not_change_any_view(ctx, full):
+    views, g1, _ = full
+    rev = list(reversed(views))
+    g2, _ = _forward(ctx, rev)
+    o1, o2 = _offsets(views), _offsets(rev)
+    n = len(views)
+    for i in range(n):
+        j = n - 1 - i
+        for k in ("depth64", "steps", "evals", "normal", "trap", "iters", "shade"):
+            np.testing.assert_array_equal(g1[k][o1[i]:o1[i + 1]], g2[k][o2[j]:o2[j + 1]], err_msg=f"view {i} {k}")
+
+
+def test_full_size_internal_consistency(full):
+    views, g, st = full
+    assert st.rays == workloads.rays(views)
+    assert int(g["evals"].astype(np.int64).sum()) == st.march_evals + st.normal_evals + st.shadow_evals
+    hit = g["normal"][:, 3] > 0.5
+    assert int(hit.sum()) == st.hits
+    assert np.all(g["normal"][:, 3][~hit] == 0.0)
+    assert np.all(g["depth"][hit] > 0) and np.all(g["depth"][~hit] == 0)
+    np.testing.assert_array_equal(g["depth"][hit], g["depth64"][hit].astype(np.float32))
+    off = _offsets(views)
+    for i, v in enumerate(views):
+        s = g["steps"][off[i]:off[i + 1]].astype(np.int64)
+        h = hit[off[i]:off[i + 1]]
+        assert np.all(s[~h] == v.max_steps) and np.all(s[h] <= v.max_steps), i
+
+
+def test_sampled_rays_of_every_view_match_the_oracle(full):
+    from oracle import pyoracle
+
+    views, g, _ = full
+    rng = np.random.default_rng(2024)
+    off = _offsets(views)
+    parts_gpu, parts_base, parts_unstable = [], [], []
+    for i, v in enumerate(views):
+        n = abi.rays_of(v)
+        first = int(rng.integers(0, max(n - RUN, 1)))
+        m = min(RUN, n - first)
+        name = runtime.formula_name(v.formula)
+        base = pyoracle.render(v, name, 64, first=first, n=m)
+        lo = pyoracle.render(v, name, 64, first=first, n=m, de_scale=1.0 - pyoracle.STABILITY_DELTA)
+        hi = pyoracle.render(v, name, 64, first=first, n=m, de_scale=1.0 + pyoracle.STABILITY_DELTA)
+        h = [o["normal"][:, 3] > 0.5 for o in (base, lo, hi)]
+        unstable = (h[0] != h[1]) | (h[0] != h[2])
+        unstable |= (base["steps"] != lo["steps"]) | (base["steps"] != hi["steps"])
+        parts_gpu.append({k: a[off[i] + first:off[i] + first + m] for k, a in g.items()})
+        parts_base.append(base)
+        parts_unstable.append(unstable)
+    gpu = {k: np.concatenate([p[k] for p in parts_gpu]) for k in parts_gpu[0]}
+    base = {k: np.concatenate([p[k] for p in parts_base]) for k in parts_base[0]}
+    unstable = np.concatenate(parts_unstable)
+    pol = policy_check(gpu, base, unstable, agg_tol=0.05)
+    strict = pol.pop("strict_mask")
+    print("policy:", pol)
+    assert pol["ok"], pol
+    c = compare(gpu, base, mask=strict)
+    print("vs oracle f64 (stable short rays):", c)
+    assert c["hits_ref"] >= 500
+    assert c["depth_rel_p99"] <= 1e-4
+    assert c["normal_deg_p99"] <= 2.0
+    assert c["trap_abs_p99"] <= 1e-3
+
+
+def _small_view(name, size, cam, params, **kw):
+    return abi.make_view(runtime.find_formula(name), size, size, cam, fov_y_deg=60.0, params=params, **kw)
+
+
+def test_empty_and_one_ray_views_in_a_batch(ctx):
+    """A view with an empty tile contributes no rays and changes no other view; a
+    one-pixel tile marches its one ray like the same pixel of the whole frame."""
+    a = _small_view(workloads.MANDELBOX, 48, (0.0, 0.0, -4.5), workloads.mandelbox_params(-1.5, 10), max_steps=256)
+    b = _small_view(workloads.MANDELBULB, 40, (0.0, 0.4, -2.6), workloads.mandelbulb_params(8.0, 8), max_steps=256)
+    empty = abi.nd_view_desc.from_buffer_copy(b)
+    empty.tile_w = empty.tile_h = 0
+    one = abi.nd_view_desc.from_buffer_copy(b)
+    one.tile_x, one.tile_y, one.tile_w, one.tile_h = 20, 17, 1, 1
+    ref, _ = _forward(ctx, [a, b])
+    g, st = _forward(ctx, [a, empty, b, one])
+    na, nb = abi.rays_of(a), abi.rays_of(b)
+    assert abi.rays_of(empty) == 0 and st.rays == na + nb + 1
+    for k in ("depth64", "steps", "evals", "normal", "trap"):
+        np.testing.assert_array_equal(g[k][:na + nb], ref[k], err_msg=k)
+        # pixel (20, 17) of b is ray 17 * 40 + 20 of b's frame
+        np.testing.assert_array_equal(g[k][na + nb], ref[k][na + 17 * 40 + 20], err_msg=k)
+
+
+def test_zero_max_steps(ctx):
+    """max_steps 0: march_to's sample loop still runs (its bound counts the bisection
+    budget too), so each ray takes one DE sample at the camera and ends as a miss with
+    0 probe steps, as in the oracle."""
+    from oracle import pyoracle
+
+    v = _small_view(workloads.MANDELBULB, 24, (0.0, 0.0, -2.5), workloads.mandelbulb_params(8.0, 8), max_steps=0)
+    base = pyoracle.render(v, workloads.MANDELBULB, 64)
+    assert np.all(base["normal"][:, 3] == 0) and np.all(base["steps"] == 0) and np.all(base["evals"] == 1)
+    for kernel in (abi.ND_KERNEL_PERSISTENT, abi.ND_KERNEL_PLAIN):
+        g = runtime.GBuffer.allocate(abi.rays_of(v))
+        ctx.forward([v], g, runtime.make_opts(kernel=kernel))
+        out = g.numpy()
+        assert ctx.stats().march_evals == abi.rays_of(v)
+        np.testing.assert_array_equal(out["normal"][:, 3], base["normal"][:, 3])
+        np.testing.assert_array_equal(out["steps"], base["steps"].astype(out["steps"].dtype))
+        np.testing.assert_array_equal(out["evals"], base["evals"].astype(out["evals"].dtype))
+        assert np.all(out["depth"] == 0)
