@@ -10,9 +10,11 @@ benchmark's workload), checked through properties that need no oracle run of eve
 * seeded runs of 96 consecutive rays from every view against the FP64 oracle under the
   boundary-case policy of tests/parity_util.py; over stable short rays both runs hit
   beyond t = 1e-3, depth p99 relative error <= 1e-4 (as in the parity tests), normal
-  p99 <= 4 degrees and trap p99 <= 2e-3 (the parity tests' 2 degrees and 1e-3 hold on
-  their own views; this mix of 64 random cameras includes far and grazing hits, where
-  the central difference divides the FP32 DE's rounding noise by a small h = eps(t)).
+  p99 <= 4 degrees and trap p99 <= 2e-3 over the mix (measured on a B200: Mandelbulb
+  and Menger hits agree to 0.1 degree and 3e-5; the Mandelbox and pseudo-Kleinian
+  views reach 4.1 and 4.4 degrees and traps 2e-3 and 7e-3 at p99, because their folds,
+  the box fold's clamp and the lattice wrap's round, make the DE's gradient jump where
+  a tap or an iterate crosses a fold; FP32 rounding moves points across them).
   Some of these cameras sit inside a pseudo-Kleinian lattice, where a ray hits at its
   first samples: there depth is a few epsilon and the normal is the gradient inside
   the solid, so those hits are compared through the policy's hit and step counts only.
