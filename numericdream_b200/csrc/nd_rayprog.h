@@ -513,9 +513,9 @@ ND_DEV_INLINE D3 fmadd(D3 o, D3 d, double t) {
 // cameras whose neighbouring pixels differ by less than an FP32 ulp.
 template <bool kDir64> struct Dir;
 template <> struct Dir<false> {
-  float x, y, z;
-  ND_DEV_INLINE void set(D3 d) { x = float(d.x); y = float(d.y); z = float(d.z); }
-  ND_DEV_INLINE D3 get() const { return D3{double(x), double(y), double(z)}; }
+  double x, y, z;  // the f32-rounded direction, held widened
+  ND_DEV_INLINE void set(D3 d) { x = double(float(d.x)); y = double(float(d.y)); z = double(float(d.z)); }
+  ND_DEV_INLINE D3 get() const { return D3{x, y, z}; }
 };
 template <> struct Dir<true> {
   double x, y, z;
