@@ -20,6 +20,7 @@
 #pragma once
 
 #include <stdint.h>
+#include <type_traits>
 
 #include "nd_helpers.h"
 #include "nd_dual.h"
@@ -532,6 +533,14 @@ template <> ND_DEV_INLINE double march_eps<double>(const DevView& v, double t) {
   return rn_add(rn_mul(double(v.eps_coef), t), double(v.eps_floor));
 }
 
+// d < eps(t) for a DE value d: an f32 DE value against the f32 epsilon compares the
+// same as their widened doubles, so the FP32 DE path tests in f32 and leaves the
+// epsilon's widening to the rarer branches that need it in FP64.
+template <class T> ND_DEV_INLINE bool below_eps(const T& d, double dd, const DevView& v, double t) {
+  if constexpr (std::is_same<T, float>::value) return d < rn_add(rn_mul(v.eps_coef, float(t)), v.eps_floor);
+  else return dd < march_eps<T>(v, t);
+}
+
 // accel_skip (tpl:428-447): the safe skip recorded for the finest cascade cell that
 // holds p, 0 outside every cascade.  The cascades are nested around the camera, so
 // "finest cascade holding p" is found from p's Chebyshev distance m to the camera
@@ -884,10 +893,11 @@ template <class T, bool kDir64> struct Lane {
       const int refine_budget = on_hit ? 0 : v.refine;
       const int bisect_budget = on_hit ? v.refine : 0;
       const double st = probing ? t : 0.5 * (a + b);
-      const double e = march_eps<T>(v, st);
+      const bool below = below_eps<T>(de.d, d, v, st);
       ++n;
       if (bisecting) {
-        if (d < e) {
+        const double e = march_eps<T>(v, st);
+        if (below) {
           b = st;
         } else {
           a = st;
@@ -897,8 +907,8 @@ template <class T, bool kDir64> struct Lane {
         else if (n >= v.max_samples) finish(v, g, t_hit, 1.0f);  // march_to's loop ran out: a miss
         return;
       }
-      if (d < e) {
-        if (on_hit && bisect_budget > 0 && (v.exact_hit ? st > a : st - a > e)) {
+      if (below) {
+        if (on_hit && bisect_budget > 0 && (v.exact_hit ? st > a : st - a > march_eps<T>(v, st))) {
           bisecting = true;
           probing = false;
           b = st;
