@@ -149,14 +149,18 @@ def cpu_sample(views, target_rays, seed=0, run=64):
     return out
 
 
-def run_cpu(views, seconds_budget=15.0, with_fp64=False):
+def run_cpu(views, seconds_budget=15.0, with_fp64=False, names=None):
     """The oracle's FP32 march on all host cores over a bounded sample (timed), and
-    optionally the FP64 oracle on the same sample (for the error figures)."""
-    from numericdream_b200 import runtime
+    optionally the FP64 oracle on the same sample (for the error figures).  names:
+    formula names by id (default: the CUDA library's registry)."""
     from oracle import pyoracle
 
     cores = pyoracle.max_threads()
-    names = [runtime.formula_name(v.formula) for v in views]
+    if names is None:
+        from numericdream_b200 import runtime
+
+        names = runtime.formula_names()
+    names = [names[v.formula] for v in views]
     t0 = time.perf_counter()
     nr = 0
     for vi, first, n in cpu_sample(views, 2048, seed=1):
@@ -195,19 +199,23 @@ def reference_lib():
     return lib
 
 
-def run_cpu_reference(lib, views, seconds_budget=15.0):
+def run_cpu_reference(lib, views, seconds_budget=15.0, names=None):
     """The reference's own fs_simple primary pass (march_to and estimate_normal of its
     shader template, translated mechanically and compiled for the host; FP32 like the
-    reference) on all host cores over a bounded, seeded sample of the views' rays."""
+    reference) on all host cores over a bounded, seeded sample of the views' rays.
+    names: formula names by id (default: the CUDA library's registry)."""
     import ctypes as C
 
     import numpy as np
 
-    from numericdream_b200 import runtime
     from oracle import pyoracle
 
     cores = pyoracle.max_threads()
-    names = [runtime.formula_name(v.formula).encode() for v in views]
+    if names is None:
+        from numericdream_b200 import runtime
+
+        names = runtime.formula_names()
+    names = [names[v.formula].encode() for v in views]
 
     def run(chunks):
         rays = evals = 0
@@ -261,25 +269,38 @@ def error_stats(views, gbuf_np, cpu):
             "note": "all sampled rays incl. rounding-unstable ones; hits with t > 1e-3"}
 
 
+def build_manifest_names():
+    """Formula names in formula-id order, from the build's manifest (the CUDA library
+    numbers its formulas in this order), so that the reference arm resolves names
+    without loading the CUDA library."""
+    path = os.path.join(ROOT, "numericdream_b200", "_generated", "manifest.json")
+    with open(path) as fh:
+        return json.load(fh)["formulas"]
+
+
 def reference_arm(args):
     ws, rank, _ = _dist_env()
     if rank != 0:
         return 0
-    from numericdream_b200 import runtime
-
     try:
-        runtime.load_library()
-    except ImportError as e:
+        names = build_manifest_names()
+    except (OSError, ValueError, KeyError) as e:
         print(json.dumps({"impl": "reference", "unavailable": f"formula table not built: {e}"}))
         return 0
-    views = build_views(args.workload, runtime.find_formula)
+    views = build_views(args.workload, names.index)
     per, res = [], None
     budget = max(2.0, 60.0 / max(args.steps + args.warmup, 1))
     ref = reference_lib()
+    t_all = []
     for i in range(args.warmup + args.steps):
-        res = run_cpu_reference(ref, views, seconds_budget=budget) if ref else run_cpu(views, seconds_budget=budget)
+        t0 = time.perf_counter()
+        if ref:
+            res = run_cpu_reference(ref, views, seconds_budget=budget, names=names)
+        else:
+            res = run_cpu(views, seconds_budget=budget, names=names)
         if i >= args.warmup:
             per.append(res)
+            t_all.append(time.perf_counter() - t0)
     v = sum(r["rays_per_s"] for r in per) / len(per) / 1e6
     if ref:
         kind = "reference"
@@ -291,8 +312,12 @@ def reference_arm(args):
         kind = "port"
         note = ("the reference's march restated on the CPU (FP32, all host threads); the reference app itself "
                 "runs only through WebGPU, unavailable on this box")
+    # a step is one bounded sample of the workload: its wall time, and the whole
+    # workload's time at the measured rate
     line = {"metric": METRIC, "value": v, "unit": "Mrays/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(r["rays"] for r in per) / len(per) / (v * 1e6),
+            "sample_wall_ms_per_step": 1e3 * sum(t_all) / len(t_all), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config_of(args.workload, views, 1),
             "de_evals_per_s": sum(r["evals_per_s"] for r in per) / len(per),

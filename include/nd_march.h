@@ -34,8 +34,6 @@
  *       FreeCamera's basis (src/app/camera.zig:98-112) for an orbit pose.
  *   nd_march_backward
  *       no reference counterpart (the reference has no gradients).
- *   nd_march_backward
- *       no reference counterpart (the reference has no gradients).
  *
  * Conventions: every call returns an nd_status and never aborts.  The caller owns
  * every buffer; G-buffer pointers are DEVICE pointers, descriptors are HOST
@@ -360,11 +358,24 @@ nd_status nd_march_backward(nd_ctx* ctx, const nd_view_desc* views, const nd_orb
  * Limits: at most 64 views and 2^31-1 rays per call; trap and iters outputs are
  * not available here (they need per-ray scratch) and return ND_ERR_UNSUPPORTED.
  * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  Every call shares the one array: calls
+ * first call before any stream capture (a call in a new CUDA context, e.g. after
+ * cudaDeviceReset, repeats that look-up).  Every call shares the one array: calls
  * that overlap on the GPU (different streams, or host threads) race, so serialise
- * them.  views is a HOST array; the G-buffer pointers are DEVICE pointers. */
+ * them.  views is a HOST array; the G-buffer pointers are DEVICE pointers.  The
+ * call returns once the work is enqueued; a failure's message is kept per host
+ * thread (nd_march_forward_noalloc_stats reads it). */
 nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t nviews, const nd_march_opts* opts,
                                    const nd_gbuffer* out, void* stream);
+
+/* Statistics of the last nd_march_forward_noalloc call on the current device (rays,
+ * DE evaluations, hits, refills, watchdog expiries), read from the library's
+ * scratch array once `stream`'s work is done (synchronises the stream; allocates
+ * nothing).  Returns ND_ERR_TIMEOUT when the device watchdog stopped the march
+ * (opts->watchdog_ms): the G-buffer slots of the rays it did not finish are then
+ * not written.  err (nullable) receives the message of the calling thread's last
+ * failed nd_march_forward_noalloc call, or of the timeout.  No counterpart in the
+ * reference, like the entry point it reports on. */
+nd_status nd_march_forward_noalloc_stats(void* stream, nd_stats* out, char* err, size_t err_len);
 
 /* DE of view->formula (with view->params and view->trap) at n points: pts is a
  * DEVICE array of 3n doubles; de, trap (nullable) and iters (nullable) are DEVICE

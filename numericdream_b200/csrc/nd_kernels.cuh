@@ -109,11 +109,10 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
   L.lazy = true;
   L.pending = 0;
   uint32_t rays = 0, hits = 0, ev_m = 0, ev_n = 0, ev_s = 0, refills = 0;
-  bool exhausted = false;
   const int64_t deadline = __shfl_sync(full, globaltimer_ns(), 0) + a.deadline_ns;
   int tick = 0;
-  const int32_t total = int32_t(a.total_rays);
-  int32_t wnext = 0, wend = 0;  // warp-uniform: taken but not yet started rays [wnext, wend)
+  const int32_t total = int32_t(a.total_rays);  // < 2^31 (checked by the host)
+  WarpRuns runs;  // warp-uniform
   const int thr = a.refill_threshold;
   const bool defer = a.hit_list != nullptr;
   // Finished rays keep their lane until the next refill: their outputs are written
@@ -147,7 +146,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     // an idle lane (item < 0) is always in PH_DONE, so phase alone tells busy lanes
     const unsigned free_lanes = __ballot_sync(full, L.phase == PH_DONE);
     const int nfree = __popc(free_lanes);
-    const bool have_work = !exhausted || wnext < wend;
+    const bool have_work = runs.have_work();
     if (!have_work && free_lanes == full) {
       retire();
       break;
@@ -155,34 +154,21 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     if (have_work && nfree != 0 && (nfree >= thr || free_lanes == full)) {
       retire();
       const unsigned idle = __ballot_sync(full, L.item < 0);
-      const int nidle = __popc(idle);
-      int avail = wend - wnext;
-      int32_t base = 0, nnew = 0;
-      if (avail < nidle && !exhausted) {
-        // enough whole runs to fill every idle lane
-        const int take = ((nidle - avail + a.chunk - 1) / a.chunk) * a.chunk;
-        if (lane == 0) base = int32_t(atomicAdd(a.counter, (unsigned long long)take));
-        base = __shfl_sync(full, base, 0);
-        ++refills;
-        nnew = base < total ? min(take, total - base) : 0;
-        if (int64_t(base) + take >= int64_t(total)) exhausted = true;
-      }
-      const int used = min(nidle, avail + nnew);
+      const WarpRuns::Claim c = runs.claim(__popc(idle), a.chunk, total, [&](int take) {
+        unsigned long long got = 0;
+        if (lane == 0) got = atomicAdd(a.counter, (unsigned long long)take);
+        return uint64_t(__shfl_sync(full, got, 0));
+      });
+      refills += c.fetched ? 1u : 0u;
       if (L.item < 0) {
         const int r = __popc(idle & lt_mask);
-        if (r < used) {
-          const int32_t it = r < avail ? wnext + r : base + (r - avail);
+        if (r < c.used) {
+          const int32_t it = c.item(r);
           L.view = kBatched ? find_view_from(a.views, a.nviews, it, L.view) : 0;
           const DevView& v = kBatched ? a.views[L.view] : single;
           L.start(v, it, L.view, true);
           if (L.phase == PH_DONE) L.finish(v, a.out, a.t_hit, 1.0f);
         }
-      }
-      if (used <= avail) {
-        wnext += used;
-      } else {
-        wnext = base + (used - avail);
-        wend = base + nnew;
       }
       continue;  // lanes that finished at once go back through the bookkeeping
     }

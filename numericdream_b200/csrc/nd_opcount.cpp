@@ -59,4 +59,54 @@ int nd_opcount(const nd_view_desc* views, int nviews, int64_t rays_per_view, dou
   return 0;
 }
 
+// Host run of the persistent kernel's work-list bookkeeping (WarpRuns, the same
+// code the kernel runs) with a plain 64-bit counter standing in for the device
+// atomic: `warps` warps claim rays for a pseudo-random number of idle lanes
+// (1..32), round after round from a pseudo-random first warp, until every warp has
+// run dry.  The counter starts at `start` (as if the rays before it were handed out
+// already).  Each ray index handed out in [start, total) is counted in
+// seen[index - start] (the caller zeroes seen); out[0] = rays handed out, out[1] = smallest index, out[2] = largest
+// index, out[3] = final counter value, out[4] = claims.  Returns 0.
+int nd_sim_work_runs(int32_t total, int32_t warps, int32_t chunk, int64_t start, uint64_t seed, uint8_t* seen,
+                     int64_t* out) {
+  std::vector<nd::WarpRuns> w(size_t(warps > 0 ? warps : 0));
+  uint64_t counter = uint64_t(start), s = seed | 1u;
+  int64_t handed = 0, lo = INT64_MAX, hi = INT64_MIN, claims = 0;
+  auto rnd = [&s]() {
+    s ^= s << 13;
+    s ^= s >> 7;
+    s ^= s << 17;
+    return s;
+  };
+  for (bool busy = true; busy;) {
+    busy = false;
+    const size_t off = size_t(rnd() % (w.size() ? w.size() : 1));
+    for (size_t k = 0; k < w.size(); ++k) {
+      nd::WarpRuns& r = w[(k + off) % w.size()];
+      if (!r.have_work()) continue;
+      busy = true;
+      const int nidle = 1 + int(rnd() % 32);
+      const nd::WarpRuns::Claim c = r.claim(nidle, chunk, total, [&](int take) {
+        const uint64_t got = counter;
+        counter += uint64_t(take);
+        ++claims;
+        return got;
+      });
+      for (int i = 0; i < c.used; ++i) {
+        const int64_t it = c.item(i);
+        ++handed;
+        lo = it < lo ? it : lo;
+        hi = it > hi ? it : hi;
+        if (it >= start && it < total && seen) ++seen[it - start];
+      }
+    }
+  }
+  out[0] = handed;
+  out[1] = lo;
+  out[2] = hi;
+  out[3] = int64_t(counter);
+  out[4] = claims;
+  return 0;
+}
+
 }  // extern "C"

@@ -740,6 +740,56 @@ ND_DEV_INLINE void normal_finish(float& gx, float& gy, float& gz) {
 // Normal taps of a view (4 tetrahedral or 6 central-difference evaluations).
 ND_DEV_INLINE uint32_t normal_taps(const DevView& v) { return v.normal_mode == ND_NORMAL_CENTRAL ? 6u : 4u; }
 
+// --------------------------------------------------------------- work runs
+// A warp's share of the persistent kernel's work list: it takes runs of `chunk`
+// consecutive ray indices from a 64-bit global counter (one atomicAdd per claim,
+// fetch() returns the counter before the add, the same value on every lane) and
+// hands them to its idle lanes.  Every warp may add one more run after the list is
+// used up, so the counter ends above the ray total by up to warps x the largest
+// claim; it is compared with the total in 64 bits before any narrowing, and only
+// indices below the total (< 2^31) become 32-bit ray indices.
+struct WarpRuns {
+  int32_t next = 0, end = 0;  // taken but not yet started: [next, end)
+  bool exhausted = false;     // the counter has passed the total
+
+  ND_DEV_INLINE bool have_work() const { return !exhausted || next < end; }
+
+  // Rays for `nidle` idle lanes.  After the call, idle lane r (by rank) with
+  // r < used starts ray first_old + r when r < avail, else base + (r - avail).
+  struct Claim {
+    int32_t avail, first_old, base, used;
+    bool fetched;
+    ND_DEV_INLINE int32_t item(int r) const { return r < avail ? first_old + r : base + (r - avail); }
+  };
+  template <class Fetch> ND_DEV_INLINE Claim claim(int nidle, int chunk, int32_t total, Fetch fetch) {
+    Claim c;
+    c.avail = end - next;
+    c.first_old = next;
+    c.base = 0;
+    c.fetched = false;
+    int32_t nnew = 0;
+    if (c.avail < nidle && !exhausted) {
+      // enough whole runs to fill every idle lane
+      const int take = ((nidle - c.avail + chunk - 1) / chunk) * chunk;
+      const uint64_t got = fetch(take);
+      c.fetched = true;
+      if (got < uint64_t(total)) {
+        c.base = int32_t(got);
+        nnew = total - c.base < take ? total - c.base : take;
+      }
+      if (got + uint64_t(take) >= uint64_t(total)) exhausted = true;
+    }
+    c.used = nidle < c.avail + nnew ? nidle : c.avail + nnew;
+    if (c.used <= c.avail) {
+      next += c.used;
+    } else {
+      next = c.base + (c.used - c.avail);
+      end = c.base + nnew;
+    }
+    return c;
+  }
+};
+
 // --------------------------------------------------------------- the ray program
 enum Phase : int { PH_MARCH = 0, PH_NORMAL = 1, PH_SHADOW = 2, PH_DONE = 3 };
 

@@ -40,12 +40,14 @@ uint64_t fnv1a64(const char* s, size_t n) {
   return h;
 }
 
-void copy_str(char* out, size_t out_len, const std::string& s) {
+void copy_str(char* out, size_t out_len, const char* s, size_t len) {
   if (!out || out_len == 0) return;
-  const size_t n = std::min(out_len - 1, s.size());
-  memcpy(out, s.data(), n);
+  const size_t n = std::min(out_len - 1, len);
+  memcpy(out, s, n);
   out[n] = 0;
 }
+void copy_str(char* out, size_t out_len, const std::string& s) { copy_str(out, out_len, s.data(), s.size()); }
+void copy_str(char* out, size_t out_len, const char* s) { copy_str(out, out_len, s, strlen(s)); }
 
 // Per-(formula set) tuned launch parameters, filled by nd_autotune.
 struct Tuned {
@@ -111,15 +113,17 @@ struct nd_graph {
 
 namespace {
 
+// The message of the last failure of a context-free call (nd_march_forward_noalloc),
+// per host thread.
+thread_local char g_noctx_err[256] = "";
+
 nd_status fail(nd_ctx* ctx, nd_status s, const char* fmt, ...) {
-  if (ctx) {
-    char buf[512];
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(buf, sizeof(buf), fmt, ap);
-    va_end(ap);
-    ctx->err = buf;
-  }
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(ctx ? buf : g_noctx_err, ctx ? sizeof(buf) : sizeof(g_noctx_err), fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = buf;
   return s;
 }
 
@@ -1385,31 +1389,69 @@ struct NoAllocScratch {
 
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
-NoAllocScratch* g_noalloc_ptr[kNoAllocMaxDevices] = {};  // device address per device
+// Per device: the scratch array's device address and the SM count, and the id of
+// the CUDA context they were looked up in.  A host that resets the device
+// (cudaDeviceReset) or re-creates its primary context gets a new context in which
+// the library's module, and with it the array, may sit elsewhere: a call in a
+// context other than the recorded one repeats the set-up.
+NoAllocScratch* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 int g_noalloc_sms[kNoAllocMaxDevices] = {};
+unsigned long long g_noalloc_ctx[kNoAllocMaxDevices] = {};
+
+// The id of the calling thread's current CUDA context (driver entry points looked up
+// through the runtime, so the library needs no link to the driver library); 0 when
+// the driver cannot tell.
+unsigned long long current_context_id() {
+  typedef int (*GetCurrent)(void**);
+  typedef int (*GetId)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  });
+  void* c = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&c) != 0 || !c || get_id(c, &id) != 0) return 0;
+  return id;
+}
 
 }  // namespace
 
 // The scratch array.  In host code this name is only a stand-in: its device
-// address comes from cudaGetSymbolAddress, once per device.
+// address comes from cudaGetSymbolAddress, once per device (and context).
 static __device__ __align__(256) unsigned char g_nd_noalloc_scratch[sizeof(NoAllocScratch)];
 
 namespace {
 
-// First call on a device: look up the device address of the scratch array and
-// the SM count, with that device current.
+// First call on a device (in its current context): look up the device address of
+// the scratch array and the SM count, with that device current.
 nd_status noalloc_setup(int dev, NoAllocScratch** ptr, int* sms) {
-  if (dev < 0 || dev >= kNoAllocMaxDevices) return ND_ERR_UNSUPPORTED;
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return fail(nullptr, ND_ERR_UNSUPPORTED, "device %d: at most %d devices", dev, kNoAllocMaxDevices);
+  // 0 when no context is current yet on this thread: the set-up below makes the
+  // device's primary context current (cudaGetSymbolAddress loads the module)
+  const unsigned long long ctx = current_context_id();
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+  if (!g_noalloc_ptr[dev] || ctx != g_noalloc_ctx[dev] || ctx == 0) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_nd_noalloc_scratch);
-    if (e != cudaSuccess || !p) return ND_ERR_CUDA;
+    if (e != cudaSuccess || !p)
+      return fail(nullptr, ND_ERR_CUDA, "scratch address on device %d: %s", dev, cudaGetErrorString(e));
     int n = 0;
     e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess || n <= 0) return ND_ERR_CUDA;
+    if (e != cudaSuccess || n <= 0) return fail(nullptr, ND_ERR_CUDA, "SM count of device %d", dev);
     g_noalloc_sms[dev] = n;
     g_noalloc_ptr[dev] = static_cast<NoAllocScratch*>(p);
+    g_noalloc_ctx[dev] = current_context_id();
   }
   *ptr = g_noalloc_ptr[dev];
   *sms = g_noalloc_sms[dev];
@@ -1420,23 +1462,32 @@ nd_status noalloc_setup(int dev, NoAllocScratch** ptr, int* sms) {
 
 extern "C" nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t nviews, const nd_march_opts* opts,
                                               const nd_gbuffer* out, void* stream) {
-  if (!views || nviews <= 0 || !out || !out->depth) return ND_ERR_INVALID;
-  if (nviews > kNoAllocMaxViews) return ND_ERR_INVALID;
-  if (out->trap || out->iters) return ND_ERR_UNSUPPORTED;  // the trap pass needs per-ray scratch
+  g_noctx_err[0] = 0;
+  if (!views || nviews <= 0 || !out || !out->depth)
+    return fail(nullptr, ND_ERR_INVALID, "needs views, nviews > 0 and a G-buffer with a depth pointer");
+  if (nviews > kNoAllocMaxViews)
+    return fail(nullptr, ND_ERR_INVALID, "%d views: this entry point takes at most %d per call", nviews,
+                kNoAllocMaxViews);
+  if (out->trap || out->iters)
+    return fail(nullptr, ND_ERR_UNSUPPORTED, "trap and iters outputs need per-ray scratch: use nd_march_forward");
   if ((out->normal && (uintptr_t(out->normal) & 15)) || (out->depth64 && (uintptr_t(out->depth64) & 7)) ||
       (out->normal_half && (uintptr_t(out->normal_half) & 7)) || (uintptr_t(out->depth) & 3))
-    return ND_ERR_INVALID;
-  if (opts && opts->de_precision != 0 && opts->de_precision != 32 && opts->de_precision != 64) return ND_ERR_INVALID;
+    return fail(nullptr, ND_ERR_INVALID, "misaligned G-buffer pointer (normal needs 16 bytes, normal_half 8)");
+  if (opts && opts->de_precision != 0 && opts->de_precision != 32 && opts->de_precision != 64)
+    return fail(nullptr, ND_ERR_INVALID, "de_precision must be 32 or 64");
   int64_t total = 0;
   for (int i = 0; i < nviews; ++i) {
     const nd_status s = validate_view(nullptr, views[i], i);
     if (s != ND_OK) return s;
-    if (views[i].accel_res > 0) return ND_ERR_UNSUPPORTED;  // the accelerator grid needs device memory
+    if (views[i].accel_res > 0)
+      return fail(nullptr, ND_ERR_UNSUPPORTED, "view %d: the accelerator grid needs device memory", i);
     total += int64_t(views[i].spp) * views[i].tile_w * views[i].tile_h;
-    if (total > int64_t(0x7fffffff)) return ND_ERR_INVALID;
+    if (total > int64_t(0x7fffffff))
+      return fail(nullptr, ND_ERR_INVALID, "more than 2^31-1 rays: this entry point takes at most 2^31-1 per call");
   }
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return ND_ERR_CUDA;
+  cudaError_t ge = cudaGetDevice(&dev);
+  if (ge != cudaSuccess) return fail(nullptr, ND_ERR_CUDA, "current device: %s", cudaGetErrorString(ge));
   NoAllocScratch* scratch = nullptr;
   int sms = 0;
   nd_status s = noalloc_setup(dev, &scratch, &sms);
@@ -1493,7 +1544,7 @@ extern "C" nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t
       ++nlaunch;
     }
   }
-  if (nv != nviews) return ND_ERR_INVALID;
+  if (nv != nviews) return fail(nullptr, ND_ERR_INVALID, "view planning failed");
 
   // view table: G-buffer offsets in call order, work-item offsets per launch
   int64_t out_off[kNoAllocMaxViews + 1];
@@ -1519,7 +1570,7 @@ extern "C" nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t
   cudaError_t e = cudaMemcpyAsync(scratch->views, host, sizeof(DevView) * size_t(nv), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(scratch->counters, 0, sizeof(unsigned long long) * size_t(nlaunch), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(&scratch->stats, 0, sizeof(Stats), st);
-  if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? ND_ERR_OOM : ND_ERR_CUDA;
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "scratch set-up");
   const int prec = (opts && opts->de_precision == 64) ? 64 : 32;
   for (int l = 0; l < nlaunch; ++l) {
     if (rays[l] <= 0) continue;
@@ -1544,7 +1595,43 @@ extern "C" nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t
     c.num_sms = sms;
     LaunchFn fn = pick(tables[l], ND_KERNEL_PERSISTENT, prec, n > 1, dir64);
     e = fn(a, host[first[l]], c, st);
-    if (e != cudaSuccess) return ND_ERR_CUDA;
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "kernel launch");
+  }
+  return ND_OK;
+}
+
+// Statistics of the last nd_march_forward_noalloc call enqueued on the current
+// device, read from the scratch array after the stream's work is done; the message
+// of the calling thread's last failed call goes to err.
+extern "C" nd_status nd_march_forward_noalloc_stats(void* stream, nd_stats* out, char* err, size_t err_len) {
+  copy_str(err, err_len, g_noctx_err);
+  if (!out) return ND_ERR_INVALID;
+  memset(out, 0, sizeof(*out));
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return ND_ERR_CUDA;
+  NoAllocScratch* scratch = nullptr;
+  int sms = 0;
+  nd_status s = noalloc_setup(dev, &scratch, &sms);
+  if (s != ND_OK) return s;
+  Stats h;
+  cudaStream_t st = (cudaStream_t)stream;
+  e = cudaMemcpyAsync(&h, &scratch->stats, sizeof(Stats), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "read scratch statistics");
+  out->rays = h.rays;
+  out->de_evals = h.de_evals;
+  out->march_evals = h.march_evals;
+  out->normal_evals = h.normal_evals;
+  out->shadow_evals = h.shadow_evals;
+  out->hits = h.hits;
+  out->refills = h.refills;
+  out->timeouts = h.timeouts;
+  out->kernel = ND_KERNEL_PERSISTENT;
+  if (h.timeouts) {
+    fail(nullptr, ND_ERR_TIMEOUT, "the device watchdog stopped %u warps", h.timeouts);
+    copy_str(err, err_len, g_noctx_err);
+    return ND_ERR_TIMEOUT;
   }
   return ND_OK;
 }

@@ -55,3 +55,22 @@ def fp32_peak_tflops(sm_mhz=None, sms: int = SM_COUNT_B200) -> float:
     """Nominal FP32 FMA peak: SMs x 128 lanes x 2 FLOPs x SM clock."""
     mhz = float(sm_mhz) if sm_mhz else 1965.0
     return sms * FP32_LANES_PER_SM * 2 * mhz * 1e6 / 1e12
+
+
+def sim_work_runs(total: int, warps: int, chunk: int, start: int = 0, seed: int = 1):
+    """The persistent kernel's work-list bookkeeping (WarpRuns) run on the host with a
+    plain counter in place of the device atomic.  Returns (summary dict, per-ray count
+    of how often each index in [start, total) was handed out)."""
+    import numpy as np
+
+    lib = _load()
+    if not hasattr(lib, "_sim_ready"):
+        lib.nd_sim_work_runs.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_uint64, C.c_void_p,
+                                         C.POINTER(C.c_int64)]
+        lib.nd_sim_work_runs.restype = C.c_int
+        lib._sim_ready = True
+    seen = np.zeros(max(total - start, 0), dtype=np.uint8)
+    out = (C.c_int64 * 5)()
+    lib.nd_sim_work_runs(total, warps, chunk, start, seed, seen.ctypes.data if seen.size else None, out)
+    keys = ["handed", "lowest", "highest", "counter", "claims"]
+    return {k: int(out[i]) for i, k in enumerate(keys)}, seen

@@ -74,6 +74,9 @@ _SIGNATURES = {
     "nd_march_forward_scenes": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(C.c_int32),
                                             C.POINTER(abi.nd_scene_desc), C.c_int32, C.POINTER(abi.nd_march_opts),
                                             C.POINTER(abi.nd_gbuffer), C.c_void_p]),
+    "nd_march_forward_noalloc": (C.c_int32, [C.POINTER(abi.nd_view_desc), C.c_int32, C.POINTER(abi.nd_march_opts),
+                                             C.POINTER(abi.nd_gbuffer), C.c_void_p]),
+    "nd_march_forward_noalloc_stats": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_stats), C.c_char_p, C.c_size_t]),
     "nd_march_backward": (C.c_int32, [C.c_void_p, C.POINTER(abi.nd_view_desc), C.POINTER(abi.nd_orbit_camera),
                                       C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(abi.nd_gbuffer),
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(abi.nd_march_opts),

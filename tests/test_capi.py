@@ -90,3 +90,23 @@ def test_status_strings(ndlib):
     assert ndlib.nd_status_string(0) == b"ND_OK"
     assert ndlib.nd_status_string(4) == b"ND_ERR_TIMEOUT"
     assert ndlib.nd_abi_version() == 3
+
+
+def test_noalloc_rejections_carry_a_message(ndlib):
+    # rejected before any CUDA call: runs without a GPU.  The message of the calling
+    # thread's last failed call comes back through nd_march_forward_noalloc_stats.
+    fid = runtime.find_formula("mandelbrot")
+    v = abi.make_view(fid, 8, 8, (0.0, 0.0, -2.5))
+    g = abi.nd_gbuffer()
+    g.depth = 256  # never dereferenced: the call is rejected first
+    err = C.create_string_buffer(256)
+    st = abi.nd_stats()
+    too_many = (abi.nd_view_desc * 65)(*([v] * 65))
+    assert ndlib.nd_march_forward_noalloc(too_many, 65, None, C.byref(g), None) == abi.ND_ERR_INVALID
+    ndlib.nd_march_forward_noalloc_stats(None, C.byref(st), err, 256)
+    assert b"at most 64" in err.value
+    g.trap = 512
+    one = (abi.nd_view_desc * 1)(v)
+    assert ndlib.nd_march_forward_noalloc(one, 1, None, C.byref(g), None) == abi.ND_ERR_UNSUPPORTED
+    ndlib.nd_march_forward_noalloc_stats(None, C.byref(st), err, 256)
+    assert b"per-ray scratch" in err.value

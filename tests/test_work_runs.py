@@ -1,0 +1,35 @@
+"""The persistent kernel's work list: warps take runs of consecutive ray indices from
+a 64-bit counter (WarpRuns in csrc/nd_rayprog.h).  These tests run that same code on
+the host with a plain counter standing in for the device atomic."""
+
+import pytest
+
+from numericdream_b200 import opcount
+
+# resident warps of a full B200 launch: 148 SMs x 7 blocks x 4 warps
+WARPS = 148 * 7 * 4
+
+
+def check(total, warps, chunk, start, seed=1):
+    s, seen = opcount.sim_work_runs(total, warps, chunk, start, seed)
+    assert s["handed"] == total - start
+    assert s["lowest"] == start and s["highest"] == total - 1
+    assert (seen == 1).all(), "a ray index was handed out twice or never"
+    assert s["counter"] >= total
+    return s
+
+
+def test_largest_launch_hands_out_every_ray_once():
+    # the largest launch the host accepts: 2^31 - 1 rays.  Every warp adds one more
+    # run after the list is used up, so the counter ends above 2^31 - 1; none of
+    # those values may come back as a (negative) ray index.
+    total = 2**31 - 1
+    for chunk in (1, 17, 64):
+        s = check(total, WARPS, chunk, start=total - 300_000, seed=chunk)
+        assert s["counter"] > 2**31, "the run did not go past 2^31 (nothing exercised)"
+
+
+@pytest.mark.parametrize("total,warps,chunk", [(1, 1, 1), (1, 37, 64), (1000, 37, 1), (1000, 37, 64),
+                                               (65536, 4, 16), (4097, WARPS, 1)])
+def test_small_launches(total, warps, chunk):
+    check(total, warps, chunk, start=0, seed=total + chunk)

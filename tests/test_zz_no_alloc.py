@@ -104,3 +104,34 @@ def test_noalloc_rejects_what_it_cannot_serve(ndlib):
     small = _gbuf(n * 65)
     g2 = small.as_abi()
     assert fn(too_many, 65, None, C.byref(g2), None) == abi.ND_ERR_INVALID
+
+
+def test_noalloc_reports_a_watchdog_expiry(ndlib):
+    # nd_march_forward_noalloc_stats reads the scratch array's statistics block: a
+    # march stopped by a 1 ms watchdog budget comes back as ND_ERR_TIMEOUT, and the
+    # next call with the default budget runs to the end again
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    fid = runtime.find_formula(workloads.MANDELBOX)
+    views = [abi.make_view(fid, 512, 512, workloads.reference_initial_camera(), fov_y_deg=90.0,
+                           params=workloads.mandelbox_params(-1.5, 30), max_steps=4096, eps_coef=1e-7,
+                           eps_floor=0.0, normal_mode=abi.ND_NORMAL_CENTRAL, normal_h_coef=1e-7)]
+    n = workloads.rays(views)
+    fn = _noalloc(ndlib)
+    stats = ndlib.nd_march_forward_noalloc_stats
+    arr = (abi.nd_view_desc * 1)(*views)
+    gb = _gbuf(n)
+    g = gb.as_abi()
+    st = abi.nd_stats()
+    err = C.create_string_buffer(256)
+    short = runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, de_precision=64, watchdog_ms=1)
+    assert fn(arr, 1, C.byref(short), C.byref(g), None) == abi.ND_OK
+    assert stats(None, C.byref(st), err, 256) == abi.ND_ERR_TIMEOUT
+    assert st.timeouts > 0 and st.rays < n
+    assert b"watchdog" in err.value
+    normal = runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, de_precision=64)
+    assert fn(arr, 1, C.byref(normal), C.byref(g), None) == abi.ND_OK
+    assert stats(None, C.byref(st), err, 256) == abi.ND_OK
+    assert st.timeouts == 0 and st.rays == n
