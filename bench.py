@@ -237,8 +237,39 @@ def run_cpu_reference(lib, views, seconds_budget=15.0, names=None):
     return {"rays_per_s": rays / dt, "evals_per_s": evals / dt, "rays": rays, "seconds": dt, "cores": cores}
 
 
-def error_stats(views, gbuf_np, cpu):
-    """GPU output against the FP64 oracle on the sampled rays (hits of both)."""
+def sampled_errors(views, gbuf, target_rays, seed, names=None, run=64, de_precision=64, min_t=1e-3, chunks=None):
+    """The G-buffer (device tensors) against the FP64 oracle on seeded runs of `run`
+    consecutive rays over every view (about target_rays rays): the same statistics
+    as error_stats, plus the oracle's time.  Only the sampled slices are copied."""
+    import numpy as np
+
+    from numericdream_b200 import abi
+    from oracle import pyoracle
+
+    if names is None:
+        from numericdream_b200 import runtime
+
+        names = runtime.formula_names()
+    offs = [0]
+    for v in views:
+        offs.append(offs[-1] + abi.rays_of(v))
+    if chunks is None:
+        chunks = cpu_sample(views, target_rays, seed=seed, run=run)
+    t0 = time.perf_counter()
+    refs, gpus = [], []
+    for vi, first, cnt in chunks:
+        refs.append(pyoracle.render(views[vi], names[views[vi].formula], precision=de_precision, first=first, n=cnt))
+        sl = slice(offs[vi] + first, offs[vi] + first + cnt)
+        gpus.append({"normal": gbuf.normal[sl].cpu().numpy(), "depth64": gbuf.depth64[sl].cpu().numpy()})
+    dt = time.perf_counter() - t0
+    out = error_stats(views, None, {"chunks": chunks, "fp64": refs}, gpu_parts=gpus, min_t=min_t)
+    out["oracle_seconds"] = dt
+    return out
+
+
+def error_stats(views, gbuf_np, cpu, gpu_parts=None, min_t=1e-3):
+    """GPU output against the FP64 oracle on the sampled rays (hits of both, beyond
+    t = min_t)."""
     import numpy as np
 
     from numericdream_b200 import abi
@@ -247,16 +278,20 @@ def error_stats(views, gbuf_np, cpu):
     for v in views:
         offs.append(offs[-1] + abi.rays_of(v))
     rel, ang, mism, n = [], [], 0, 0
-    for (vi, first, cnt), ref in zip(cpu["chunks"], cpu["fp64"]):
-        sl = slice(offs[vi] + first, offs[vi] + first + cnt)
-        gh = gbuf_np["normal"][sl, 3] > 0.5
+    for k, ((vi, first, cnt), ref) in enumerate(zip(cpu["chunks"], cpu["fp64"])):
+        if gpu_parts is not None:
+            gn, gd = gpu_parts[k]["normal"], gpu_parts[k]["depth64"]
+        else:
+            sl = slice(offs[vi] + first, offs[vi] + first + cnt)
+            gn, gd = gbuf_np["normal"][sl], gbuf_np["depth64"][sl]
+        gh = gn[:, 3] > 0.5
         rh = ref["normal"][:, 3] > 0.5
         mism += int((gh != rh).sum())
         n += cnt
-        both = gh & rh & (ref["depth64"] > 1e-3)
+        both = gh & rh & (ref["depth64"] > min_t)
         if both.any():
-            rel.append(np.abs(gbuf_np["depth64"][sl][both] - ref["depth64"][both]) / ref["depth64"][both])
-            a = gbuf_np["normal"][sl][both, :3].astype(np.float64)
+            rel.append(np.abs(gd[both] - ref["depth64"][both]) / ref["depth64"][both])
+            a = gn[both, :3].astype(np.float64)
             b = ref["normal"][both, :3].astype(np.float64)
             c = np.clip((a * b).sum(1) / np.maximum(np.linalg.norm(a, axis=1) * np.linalg.norm(b, axis=1), 1e-30), -1, 1)
             ang.append(np.degrees(np.arccos(c)))
@@ -266,7 +301,7 @@ def error_stats(views, gbuf_np, cpu):
             "depth_rel_p99": float(np.percentile(rel, 99)), "depth_rel_max": float(rel.max()),
             "depth_rel_frac_over_1e-4": float((rel > 1e-4).mean()),
             "normal_deg_p99": float(np.percentile(ang, 99)), "normal_deg_max": float(ang.max()),
-            "note": "all sampled rays incl. rounding-unstable ones; hits with t > 1e-3"}
+            "note": f"all sampled rays incl. rounding-unstable ones; hits with t > {min_t:g}"}
 
 
 def build_manifest_names():
@@ -380,9 +415,12 @@ def profile_forward(args):
     return 0
 
 
-def small_and_deepzoom(ctx, sptr, timed, steps):
+def small_and_deepzoom(ctx, sptr, timed, steps, with_errors=True):
     """The single-view Mandelbulb 256x256 (persistent and plain) and the deep-zoom frame
-    (Mandelbox, 30 iterations, 4096x4096 in 16 tiles of 1024x1024, FP64 DE)."""
+    (Mandelbox, 30 iterations, 4096x4096 in 16 tiles of 1024x1024, FP64 DE), each with
+    its depth and normal error against the FP64 oracle."""
+    import torch
+
     from numericdream_b200 import abi, runtime, workloads
 
     out = {}
@@ -393,6 +431,10 @@ def small_and_deepzoom(ctx, sptr, timed, steps):
         o = runtime.make_opts(kernel=kern)
         ms = timed(lambda: ctx.forward(v, g, o, stream=sptr), steps, 3)
         out[f"mandelbulb_256_{label}"] = {"ms_per_step": ms, "Mrays_per_s": n / (ms * 1e-3) / 1e6}
+        if label == "persistent" and with_errors:
+            torch.cuda.synchronize()
+            # every ray of the view against the FP64 oracle
+            out["mandelbulb_256_persistent"]["error_vs_fp64"] = sampled_errors(v, g, 0, 0, chunks=[(0, 0, n)])
     views = workloads.deepzoom_4096(runtime.find_formula, ctx)
     n = workloads.rays(views)
     g = runtime.GBuffer.allocate(n)
@@ -402,6 +444,10 @@ def small_and_deepzoom(ctx, sptr, timed, steps):
     out["deepzoom_4096"] = {"ms_per_frame": ms, "Mrays_per_s": n / (ms * 1e-3) / 1e6,
                             "de_evals_per_s": st.de_evals / (ms * 1e-3), "hits": st.hits, "rays": n,
                             "de": "fp64 (an FP32 DE cannot resolve the 1e-12 pixel footprint: no ray hits)"}
+    if with_errors:
+        torch.cuda.synchronize()
+        # hits lie at t ~ 1e-5 here: no t floor
+        out["deepzoom_4096"]["error_vs_fp64"] = sampled_errors(views, g, 8192, 5, min_t=0.0)
     # lite shading (shade_lite) of batched_64's hits after each forward: colour strip,
     # ambient occlusion (5 DE evaluations per hit), two lights
     views = workloads.batched_64(runtime.find_formula)
@@ -627,11 +673,14 @@ def main():
                  "value": n2 * ws / (ms2 * 1e-3) / 1e6, "unit": "Mrays/s", "ms_per_step": ms2,
                  "de_evals_per_s": st2.de_evals * ws / (ms2 * 1e-3),
                  "plain": n2 * ws / (ms2_plain * 1e-3) / 1e6, "batched_over_plain": ms2_plain / ms2}
+        if rank == 0 and not args.no_cpu:
+            torch.cuda.synchronize()
+            extra["error_vs_fp64"] = sampled_errors(v2, g2, 32768, 9)
         del g2
     diff = other = None
     if not args.no_extra and ws == 1:
         diff = differentiation_step(ctx, stream, sptr, timed, max(2, args.steps // 2))
-        other = small_and_deepzoom(ctx, sptr, timed, max(2, args.steps // 2))
+        other = small_and_deepzoom(ctx, sptr, timed, max(2, args.steps // 2), with_errors=not args.no_cpu)
     measured_fp32 = None
     if rank == 0:
         try:
