@@ -112,24 +112,32 @@ class ClockSampler:
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_views(name, resolve, rank=0):
-    from numericdream_b200 import workloads
+def build_views(name, resolve, world=1, rank=0, names=None):
+    """The workload's views; with world > 1, rank `rank`'s share of the one batch
+    (views cut into tiles and balanced over the ranks: numericdream_b200.shard)."""
+    from numericdream_b200 import shard, workloads
 
     if name == "batched_64":
-        return workloads.batched_64(resolve, seed=7 + 1000 * rank)
-    if name == "mandelbox_1080p":
-        return workloads.mandelbox_1080p(resolve, seed=1234 + rank)
-    if name == "mandelbulb_256":
-        return workloads.mandelbulb_256(resolve)
-    raise SystemExit(f"unknown workload {name}")
+        views = workloads.batched_64(resolve, seed=7)
+    elif name == "mandelbox_1080p":
+        views = workloads.mandelbox_1080p(resolve, seed=1234)
+    elif name == "mandelbulb_256":
+        views = workloads.mandelbulb_256(resolve)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return shard.rank_views(views, world, rank, names) if world > 1 else views
 
 
-def config_of(name, views, ws):
+def config_of(name, views, ws, rays_total=None):
     from numericdream_b200 import workloads
 
-    return {"workload": name, "views": len(views), "rays_per_step_per_gpu": workloads.rays(views),
-            "max_steps": int(max(v.max_steps for v in views)), "de": "fp32 (fast math)", "t": "fp64",
-            "l2": "flushed between steps (256 MiB write)", "parallelism": f"shards{ws}" if ws > 1 else "single"}
+    c = {"workload": name, "views": len(views), "rays_per_step": rays_total or workloads.rays(views),
+         "max_steps": int(max(v.max_steps for v in views)), "de": "fp32 (fast math)", "t": "fp64",
+         "l2": "flushed between steps (256 MiB write)", "parallelism": f"shards{ws}" if ws > 1 else "single"}
+    if ws > 1:
+        c["sharding"] = ("one batch per step, its views cut into tiles and balanced over the ranks "
+                         "(longest-processing-time first); rank 0's share: %d tiles" % len(views))
+    return c
 
 
 def cpu_sample(views, target_rays, seed=0, run=64):
@@ -535,6 +543,16 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and not args.profile_forward:
+        # one process per GPU: start the ranks under torch.distributed.run
+        import socket
+
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+        return subprocess.call(cmd)
     if args.profile_forward:
         return profile_forward(args)
 
@@ -551,6 +569,8 @@ def main():
 
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if ws != args.gpus and rank == 0:
+            print(f"note: --gpus {args.gpus} but WORLD_SIZE {ws}; running {ws} ranks", file=sys.stderr)
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     ctx = runtime.Context(local)
@@ -582,8 +602,18 @@ def main():
             torch.distributed.barrier()
         return total / steps
 
+    def over_ranks(times, counts):
+        """Times: the max over ranks; counts: the sum over ranks."""
+        if ws == 1:
+            return list(times), list(counts)
+        t = torch.tensor(times, dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        c = torch.tensor(counts, dtype=torch.int64, device=dev)
+        torch.distributed.all_reduce(c)
+        return t.tolist(), [int(x) for x in c.tolist()]
+
     def run_workload(name, steps, warmup, tune=True):
-        views = build_views(name, runtime.find_formula, rank)
+        views = build_views(name, runtime.find_formula, ws, rank, runtime.formula_names())
         nrays = workloads.rays(views)
         gbuf = runtime.GBuffer.allocate(nrays, device=dev)
         tr = ctx.autotune(views, gbuf) if tune else None
@@ -633,6 +663,7 @@ def main():
               for k in keys} for _ in range(2)]
     d2h = sum(t.numel() * t.element_size() for t in hosts[0].values())
     h2d = len(views) * runtime.load_library().nd_sizeof(b"DevView")  # the view table nd_march_forward copies
+    _, (d2h, h2d) = over_ranks([], [d2h, h2d])  # the whole job's copies per step
     copy_stream = torch.cuda.Stream(device=dev)
 
     def e2e_run(steps):
@@ -669,10 +700,11 @@ def main():
     if not args.no_extra and args.workload != "mandelbox_1080p":
         v2, n2, g2, _, _, ms2, ms2_plain, st2, _ = run_workload("mandelbox_1080p", max(2, args.steps // 2), 2,
                                                                 tune=False)
-        extra = {"workload": "mandelbox_1080p (1920x1080 x 4 spp, shadow rays)", "rays_per_step": n2,
-                 "value": n2 * ws / (ms2 * 1e-3) / 1e6, "unit": "Mrays/s", "ms_per_step": ms2,
-                 "de_evals_per_s": st2.de_evals * ws / (ms2 * 1e-3),
-                 "plain": n2 * ws / (ms2_plain * 1e-3) / 1e6, "batched_over_plain": ms2_plain / ms2}
+        (ms2, ms2_plain), (n2_all, de2_all) = over_ranks([ms2, ms2_plain], [n2, st2.de_evals])
+        extra = {"workload": "mandelbox_1080p (1920x1080 x 4 spp, shadow rays)", "rays_per_step": n2_all,
+                 "value": n2_all / (ms2 * 1e-3) / 1e6, "unit": "Mrays/s", "ms_per_step": ms2,
+                 "de_evals_per_s": de2_all / (ms2 * 1e-3),
+                 "plain": n2_all / (ms2_plain * 1e-3) / 1e6, "batched_over_plain": ms2_plain / ms2}
         if rank == 0 and not args.no_cpu:
             torch.cuda.synchronize()
             extra["error_vs_fp64"] = sampled_errors(v2, g2, 32768, 9)
@@ -690,11 +722,9 @@ def main():
     clk = clocks.stop()
     gnp = gbuf.numpy() if rank == 0 else None
 
-    if ws > 1:
-        t = torch.tensor([ms_batched, ms_plain, ms_e2e], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_batched, ms_plain, ms_e2e = t.tolist()
-    rays_total = nrays * ws
+    # rays: the sum over ranks (each marched its share of the one batch); times: the max
+    (ms_batched, ms_plain, ms_e2e), (rays_total, de_all) = over_ranks([ms_batched, ms_plain, ms_e2e],
+                                                                      [nrays, st.de_evals])
     if rank == 0:
         from numericdream_b200 import opcount
 
@@ -725,9 +755,9 @@ def main():
         line = {
             "metric": METRIC, "value": rays_total / (ms_batched * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded views, no dataset)",
-            "config": config_of(args.workload, views, ws),
-            "de_evals_per_s": st.de_evals * ws / (ms_batched * 1e-3),
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded views, no dataset)",
+            "config": config_of(args.workload, views, ws, rays_total),
+            "de_evals_per_s": de_all / (ms_batched * 1e-3),
             "plain": {"value": rays_total / (ms_plain * 1e-3) / 1e6, "unit": "Mrays/s", "ms_per_step": ms_plain,
                       "kind": "one plain launch per view, one thread per ray"},
             "batched_over_plain": ms_plain / ms_batched,

@@ -151,6 +151,9 @@ def generate(verbose=False):
 #include "formulas/{tf.name}.inc"
 {_traits(tf)}
 nd::KernelTable nd_kernels_{tf.namespace}() {{ return nd::make_kernel_table<nd::FormulaSet<F_{tf.namespace}>>(); }}
+int32_t nd_iterations_{tf.namespace}(const float* p) {{
+  return F_{tf.namespace}::iterations<float, nd::ParamRef<float>>(nd::ParamRef<float>{{p}});
+}}
 """)
         units.append(unit)
     groups = []
@@ -195,7 +198,8 @@ extern "C" void ndop_{tf.namespace}(const nd::DevView* v, int64_t ray, ndw::OpCo
     # registry
     lines = ['// formula registry (generated)', '#include "nd_registry.h"', "", "namespace {"]
     for tf in formulas:
-        lines.append(f"}}  // namespace\nnd::KernelTable nd_kernels_{tf.namespace}();\nnamespace {{")
+        lines.append(f"}}  // namespace\nnd::KernelTable nd_kernels_{tf.namespace}();\n"
+                     f"int32_t nd_iterations_{tf.namespace}(const float*);\nnamespace {{")
     for gname, _ in groups:
         lines.append(f"}}  // namespace\nnd::KernelTable nd_group_{gname}();\nnamespace {{")
     lines.append("}  // namespace")
@@ -206,9 +210,9 @@ extern "C" void ndop_{tf.namespace}(const nd::DevView* v, int64_t ray, ndw::OpCo
             ps.append(f"{{{_cpp_str(p.name)}, {p.min!r}f, {p.max!r}f, {p.default!r}f, {1 if p.integral else 0}}}")
         plist = ", ".join(ps) if ps else ""
         lines.append(f"  {{{_cpp_str(tf.name)}, 0x{tf.source_hash:016x}ull, {len(tf.params)}, {{{plist}}}, "
-                     f"&nd_kernels_{tf.namespace}}},")
+                     f"&nd_kernels_{tf.namespace}, &nd_iterations_{tf.namespace}}},")
     if not formulas:
-        lines.append('  {"", 0ull, 0, {}, nullptr},')
+        lines.append('  {"", 0ull, 0, {}, nullptr, nullptr},')
     lines.append("};")
     lines.append(f"const int nd_formula_entry_count = {len(formulas)};")
     lines.append("const nd::GroupEntry nd_group_entries[] = {")

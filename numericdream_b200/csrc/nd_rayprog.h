@@ -578,19 +578,26 @@ ND_DEV_INLINE float accel_skip(const DevView& v, float px, float py, float pz) {
 ND_DEV_INLINE void ray_uv(const DevView& v, int64_t local, double* ux, double* uy) {
   const int64_t npix = int64_t(v.tile_w) * v.tile_h;
   int px, py;
+  int64_t sample;
   if (local < 0x80000000ll && npix < 0x80000000ll) {
     // 32-bit division (a 64-bit one is a long software routine on the GPU)
-    const uint32_t pix = uint32_t(local) % uint32_t(npix);
+    const uint32_t s = uint32_t(local) / uint32_t(npix);
+    const uint32_t pix = uint32_t(local) - s * uint32_t(npix);
+    sample = s;
     px = v.tile_x + int(pix % uint32_t(v.tile_w));
     py = v.tile_y + int(pix / uint32_t(v.tile_w));
   } else {
-    const int64_t pix = local % npix;
+    sample = local / npix;
+    const int64_t pix = local - sample * npix;
     px = v.tile_x + int(pix % v.tile_w);
     py = v.tile_y + int(pix / v.tile_w);
   }
   double jx = 0.5, jy = 0.5;
   if (v.spp > 1) {
-    const uint64_t h = splitmix64(v.seed ^ splitmix64(uint64_t(local)));
+    // keyed by the sample's place in the whole frame (sample, row, column), so that
+    // a view cut into tiles draws the same rays as the view itself
+    const uint64_t key = (uint64_t(sample) * uint64_t(v.height) + uint64_t(py)) * uint64_t(v.width) + uint64_t(px);
+    const uint64_t h = splitmix64(v.seed ^ splitmix64(key));
     jx = double(uint32_t(h) >> 8) * (1.0 / 16777216.0);
     jy = double(uint32_t(h >> 32) >> 8) * (1.0 / 16777216.0);
   }

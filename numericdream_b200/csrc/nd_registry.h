@@ -20,6 +20,7 @@ struct FormulaEntry {
   int nparams;
   ParamEntry params[ND_MAX_PARAMS];
   KernelTable (*kernels)();
+  int32_t (*iterations)(const float* params);  // de_iterations(p) on the host
 };
 
 // A set of formulas compiled into one kernel (mixed-formula batches).

@@ -219,6 +219,14 @@ std::vector<int> view_formulas(const nd_view_desc& v, int scene, const SceneInpu
   return f;
 }
 
+// de_iterations() of a formula at a view's parameters, clamped like the kernels'.
+double view_iterations(int formula, const float* params) {
+  const nd::FormulaEntry& f = nd_formula_entries[formula];
+  if (!f.iterations) return 1.0;
+  const int32_t n = f.iterations(params);
+  return double(n < 1 ? 1 : (n > nd::kMaxIterations ? nd::kMaxIterations : n));
+}
+
 nd_status plan(nd_ctx* ctx, const nd_view_desc* views, int nviews, std::vector<Launch>* out,
                const SceneInput& sc = SceneInput()) {
   std::vector<int> distinct;
@@ -252,7 +260,11 @@ nd_status plan(nd_ctx* ctx, const nd_view_desc* views, int nviews, std::vector<L
     Launch L;
     L.table = G.kernels();
     L.members.assign(G.members, G.members + G.count);
-    // order the views by formula code so that warps stay formula-uniform
+    // Views are grouped by formula code so that warps stay formula-uniform, and the
+    // groups go in decreasing order of their views' mean formula iteration count (a
+    // view's cost per DE evaluation): the persistent kernel hands out rays in table
+    // order, so the rays still in flight when the work list runs out, which set how
+    // long the last warps run with few lanes busy, are the cheapest ones.
     std::vector<int> order(nviews);
     for (int i = 0; i < nviews; ++i) order[i] = i;
     auto code_of = [&](int vi) {
@@ -261,7 +273,28 @@ nd_status plan(nd_ctx* ctx, const nd_view_desc* views, int nviews, std::vector<L
         if (G.members[m] == f) return m;
       return 0;
     };
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return code_of(a) < code_of(b); });
+    std::vector<double> cost_sum(G.count, 0.0);
+    std::vector<int> cost_n(G.count, 0);
+    for (int i = 0; i < nviews; ++i) {
+      double c = 0.0;
+      const int k = sc.scene_of(i);
+      if (k < 0) {
+        c = view_iterations(views[i].formula, views[i].params);
+      } else {
+        const nd_scene_desc& S = sc.scenes[k];
+        for (int j = 0; j < S.instance_count && j < ND_MAX_INSTANCES; ++j)
+          c += view_iterations(S.instances[j].formula, S.instances[j].params);
+      }
+      cost_sum[code_of(i)] += c;
+      ++cost_n[code_of(i)];
+    }
+    std::vector<int> rank(G.count);
+    for (int m = 0; m < G.count; ++m) rank[m] = m;
+    auto mean = [&](int m) { return cost_n[m] ? cost_sum[m] / cost_n[m] : 0.0; };
+    std::stable_sort(rank.begin(), rank.end(), [&](int a, int b) { return mean(a) > mean(b); });
+    std::vector<int> pos(G.count);
+    for (int r = 0; r < G.count; ++r) pos[rank[r]] = r;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return pos[code_of(a)] < pos[code_of(b)]; });
     for (int vi : order) {
       L.views.push_back(vi);
       L.codes.push_back(code_of(vi));

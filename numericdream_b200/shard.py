@@ -73,3 +73,18 @@ def shard_views(views, world: int, rank: int, names=None, max_rays_per_item: int
     costs = [estimate_cost(t, names[i] if names else None) for t, i in items]
     parts = partition(costs, world)
     return [items[j][0] for j in parts[rank]]
+
+
+def rank_views(views, world: int, rank: int, names=None) -> list:
+    """One rank's share of a batch for a multi-GPU step: the batch's views cut into
+    tiles of at most total_rays / (4 x world) rays each (at least 2^16), assigned by
+    longest-processing-time-first.  Every ray of the batch lands on exactly one rank,
+    and a tile draws the same rays as the same pixels of the uncut view (the tile
+    rectangle is in frame pixels and the sample jitter is keyed by frame position).
+    names maps a view's formula id to its name (for the cost estimate)."""
+    if world <= 1:
+        return list(views)
+    total = sum(abi.rays_of(v) for v in views)
+    per = max(1 << 16, total // (4 * world))
+    nm = [names[v.formula] for v in views] if names is not None else None
+    return shard_views(views, world, rank, names=nm, max_rays_per_item=per)

@@ -655,8 +655,9 @@ struct RayOut {
   double margin;      // smallest |d - eps| / eps over all hit decisions of the primary march
 };
 
-// Philox-free counter hash for jitter: SplitMix64 of (seed, ray) -> two floats in
-// [0, 1) with 24-bit resolution.  The CUDA library uses the same function.
+// Philox-free counter hash for jitter: SplitMix64 of (seed, key) -> two floats in
+// [0, 1) with 24-bit resolution, key = (sample * height + row) * width + column of
+// the ray in the whole frame.  The CUDA library uses the same function.
 inline uint64_t splitmix64(uint64_t x) {
   x += 0x9E3779B97F4A7C15ull;
   x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -838,7 +839,10 @@ template <class R> struct Tracer {
     const int64_t s = ray / npix, pix = ray % npix;
     const int px = v.tile_x + int(pix % v.tile_w), py = v.tile_y + int(pix / v.tile_w);
     double jx = 0.5, jy = 0.5;
-    if (v.spp > 1) jitter2(v.seed, uint64_t(s * npix + pix), &jx, &jy);
+    // the jitter is keyed by the sample's place in the whole frame (sample, row,
+    // column): a view cut into tiles draws the same rays as the view itself
+    if (v.spp > 1) jitter2(v.seed, (uint64_t(s) * uint64_t(v.height) + uint64_t(py)) * uint64_t(v.width) + uint64_t(px),
+                           &jx, &jy);
     const double ndc_x = 2.0 * (px + jx) / v.width - 1.0;
     const double ndc_y = 1.0 - 2.0 * (py + jy) / v.height;
     const double ux = ndc_x * double(v.width) / double(v.height), uy = -ndc_y;
@@ -911,7 +915,8 @@ template <class R> struct Tracer {
     const int64_t s = ray / npix, pix = ray % npix;
     const int px = v.tile_x + int(pix % v.tile_w), py = v.tile_y + int(pix / v.tile_w);
     double jx = 0.5, jy = 0.5;
-    if (v.spp > 1) jitter2(v.seed, uint64_t(s * npix + pix), &jx, &jy);
+    if (v.spp > 1) jitter2(v.seed, (uint64_t(s) * uint64_t(v.height) + uint64_t(py)) * uint64_t(v.width) + uint64_t(px),
+                           &jx, &jy);
     // camera ray: cs_wf_generate tpl:5120-5127 and fs_simple tpl:4523-4525; the tile
     // transform (fractal_renderer.zig:852-863) is folded into full-frame pixels.
     const double ndc_x = 2.0 * (px + jx) / v.width - 1.0;

@@ -83,3 +83,69 @@ def test_partition_lpt():
     assert sorted(loads) == [8, 10] or sorted(loads) == [9, 9]
     with pytest.raises(ValueError):
         shard.partition([1], 0)
+
+
+def _bench_worker(rank, world, port, q):
+    # the benchmark's own multi-GPU partition (bench.build_views with world > 1): the
+    # one batched_64 batch cut into tiles and balanced over the ranks
+    import numpy as np
+
+    import bench
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    names = bench.build_manifest_names()
+    full = bench.build_views("batched_64", names.index)
+    mine = bench.build_views("batched_64", names.index, world, rank, names)
+    index = {v.seed: i for i, v in enumerate(full)}
+    offs = np.cumsum([0] + [abi.rays_of(v) for v in full])
+    cover = torch.zeros(int(offs[-1]), dtype=torch.int32)
+    cv = cover.numpy()
+    for t in mine:
+        i = index[t.seed]
+        v = full[i]
+        block = cv[offs[i]:offs[i + 1]].reshape(v.spp, v.tile_h, v.tile_w)
+        block[:, t.tile_y - v.tile_y:t.tile_y - v.tile_y + t.tile_h, t.tile_x - v.tile_x:t.tile_x - v.tile_x + t.tile_w] += 1
+    load = torch.tensor([sum(shard.estimate_cost(t, names[t.formula]) for t in mine)], dtype=torch.float64)
+    loads = [torch.zeros(1, dtype=torch.float64) for _ in range(world)]
+    dist.all_gather(loads, load)
+    dist.all_reduce(cover)
+    if rank == 0:
+        q.put((int(cover.min()), int(cover.max()), [float(x.item()) for x in loads], len(mine)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_bench_partition_covers_the_batch_once():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_bench_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(300)
+        assert p.exitcode == 0
+    lo, hi, loads, ntiles = q.get(timeout=10)
+    assert lo == 1 and hi == 1, "a ray of the batch is marched twice or never"
+    assert max(loads) <= 1.1 * sum(loads) / world, loads
+
+
+def test_tiles_draw_the_rays_of_the_whole_view():
+    # jittered samples are keyed by their place in the frame: a view cut into tiles
+    # marches exactly the rays of the uncut view (checked with the FP64 oracle)
+    import numpy as np
+
+    from oracle import pyoracle
+
+    v = abi.make_view(0, 24, 16, (2.0, 1.0, -2.5), params=[8.0, 8.0], spp=4, seed=99)
+    whole = pyoracle.render(v, "mandelbrot", precision=64)
+    d = whole["depth64"].reshape(4, 16, 24)
+    st = whole["steps"].reshape(4, 16, 24)
+    for t in shard.split_tiles(v, 2, 2):
+        part = pyoracle.render(t, "mandelbrot", precision=64)
+        ys, xs = slice(t.tile_y, t.tile_y + t.tile_h), slice(t.tile_x, t.tile_x + t.tile_w)
+        np.testing.assert_array_equal(part["depth64"].reshape(4, t.tile_h, t.tile_w), d[:, ys, xs])
+        np.testing.assert_array_equal(part["steps"].reshape(4, t.tile_h, t.tile_w), st[:, ys, xs])
