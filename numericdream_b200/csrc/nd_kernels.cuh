@@ -119,6 +119,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
   // then, all together, instead of in the pass that ends each ray.
   auto retire = [&]() {
     int32_t hit_item = -1;
+    uint32_t hit_evals = 0;
     if (L.item >= 0 && L.phase == PH_DONE) {
       const DevView& v = kBatched ? a.views[L.view] : single;
       L.flush(v, a.out, a.t_hit);
@@ -128,7 +129,10 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
       ev_m += L.mev;
       ev_n += taps;
       ev_s += L.evals - L.mev - taps;
-      if (defer && L.hit) hit_item = L.item;
+      if (defer && L.hit) {
+        hit_item = L.item;
+        hit_evals = L.evals;
+      }
       L.item = -1;
     }
     if (defer) {
@@ -138,7 +142,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
         unsigned base = 0;
         if (lane == 0) base = atomicAdd(a.hit_count, unsigned(__popc(hm)));
         base = __shfl_sync(full, base, 0);
-        if (hit_item >= 0) a.hit_list[base + __popc(hm & lt_mask)] = hit_item;
+        if (hit_item >= 0) a.hit_list[base + __popc(hm & lt_mask)] = HitEntry{hit_item, hit_evals};
       }
     }
   };
@@ -213,14 +217,16 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   unsigned long long taps = 0, shadow = 0;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride) {
-    const int64_t it = list ? int64_t(a.hit_list[i]) : i;
+    HitEntry h{int32_t(i), 0u};
+    if (list) h = a.hit_list[i];
+    const int64_t it = h.item;
     const int vi = kBatched ? find_view(a.views, a.nviews, it) : 0;
     const DevView& v = kBatched ? a.views[vi] : single;
     const int64_t local = it - v.ray_offset;
     const double t = a.t_hit[v.out_offset + local];
     if (t < 0.0) continue;  // a miss (all-rays mode); the march wrote its outputs
     if (list) {
-      const uint32_t ev = shade_at_hit<Set, T, kDir64, kScenes, kAccel>(v, local, t, a.out, a.scenes);
+      const uint32_t ev = shade_at_hit<Set, T, kDir64, kScenes, kAccel>(v, local, t, a.out, a.scenes, h.march_evals);
       taps += ev & 0xffffu;
       shadow += ev >> 16;
     }

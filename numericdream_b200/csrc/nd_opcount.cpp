@@ -109,4 +109,12 @@ int nd_sim_work_runs(int32_t total, int32_t warps, int32_t chunk, int64_t start,
   return 0;
 }
 
+// floor(n[i] / d) by ray_uv's magic-number division (div_magic / div_by, the code the
+// kernels run) into q[i]; n[i] < 2^31.
+void nd_div_by(uint32_t d, int64_t count, const uint32_t* n, uint32_t* q) {
+  uint32_t m, s;
+  nd::div_magic(d, &m, &s);
+  for (int64_t i = 0; i < count; ++i) q[i] = nd::div_by(n[i], m, s);
+}
+
 }  // extern "C"

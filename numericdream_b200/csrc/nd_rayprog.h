@@ -124,11 +124,34 @@ struct DevView {
   float accel_inv[kAccelMaxCascades];  // 1 / cell size
   float accel_cam[3];   // the camera position the cascades are centred on (f32)
   float accel_k;        // 1 / ((res / 2 - 1) * finest cell): lookup start level
+  // n / d for 0 <= n < 2^31 as (n * m) >> s (DivMagic): d = the tile's pixels, d = its width
+  uint32_t npix_m, npix_s, width_m, width_s;
 };
+
+// Exact unsigned division by a divisor fixed per view, for dividends below 2^31:
+// with l = ceil(log2 d), m = ceil(2^(31+l) / d) < 2^32 and s = 31 + l,
+// floor(n / d) = (n m) >> s for every 0 <= n < 2^31 (the rounding error of m is
+// below d, so n m / 2^s exceeds n / d by less than 2^-l <= 1/d).  A 32-bit division
+// by a variable is a long instruction sequence on the GPU; this is one wide multiply
+// and a shift.
+ND_DEV_INLINE void div_magic(uint32_t d, uint32_t* m, uint32_t* s) {
+  uint32_t l = 0;
+  while (l < 31 && (uint64_t(1) << l) < d) ++l;
+  *s = 31 + l;
+  *m = uint32_t(((uint64_t(1) << (31 + l)) + d - 1) / (d ? d : 1));
+}
+ND_DEV_INLINE uint32_t div_by(uint32_t n, uint32_t m, uint32_t s) { return uint32_t((uint64_t(n) * m) >> s); }
 
 struct Stats {
   unsigned long long rays, de_evals, march_evals, normal_evals, shadow_evals, hits, refills;
   unsigned int timeouts, pad;
+};
+
+// One entry of the deferred shade pass's hit list: the launch-local ray index and
+// the DE evaluations its march used (the shade pass writes the ray's total once).
+struct HitEntry {
+  int32_t item;
+  uint32_t march_evals;
 };
 
 struct LaunchArgs {
@@ -145,7 +168,7 @@ struct LaunchArgs {
   int64_t deadline_ns;        // watchdog budget (globaltimer units)
   // Deferred shading: the persistent march ends a hit ray at its hit and appends it
   // to hit_list; the shade pass then evaluates the normal taps coherently.
-  int32_t* hit_list;          // launch-local ray indices of hits (nullptr: shading inline)
+  struct HitEntry* hit_list;  // hits of the launch (nullptr: shading inline)
   unsigned int* hit_count;    // entries in hit_list (zeroed before launch)
   const struct DevScene* scenes;  // multi-instance scenes of the launch's views (may be null)
 };
@@ -580,12 +603,13 @@ ND_DEV_INLINE void ray_uv(const DevView& v, int64_t local, double* ux, double* u
   int px, py;
   int64_t sample;
   if (local < 0x80000000ll && npix < 0x80000000ll) {
-    // 32-bit division (a 64-bit one is a long software routine on the GPU)
-    const uint32_t s = uint32_t(local) / uint32_t(npix);
+    // 32-bit division by the view's precomputed magic numbers
+    const uint32_t s = div_by(uint32_t(local), v.npix_m, v.npix_s);
     const uint32_t pix = uint32_t(local) - s * uint32_t(npix);
+    const uint32_t row = div_by(pix, v.width_m, v.width_s);
     sample = s;
-    px = v.tile_x + int(pix % uint32_t(v.tile_w));
-    py = v.tile_y + int(pix / uint32_t(v.tile_w));
+    px = v.tile_x + int(pix - row * uint32_t(v.tile_w));
+    py = v.tile_y + int(row);
   } else {
     sample = local / npix;
     const int64_t pix = local - sample * npix;
@@ -924,13 +948,13 @@ template <class T, bool kDir64> struct Lane {
     write_march(v, g, t_hit);
   }
 
+  // (the evaluation count goes to the shade pass with the hit, which writes the total)
   ND_DEV_INLINE void write_march(const DevView& v, const nd_gbuffer& g, double* t_hit) const {
     const int64_t r = v.out_offset + (int64_t(item) - v.ray_offset);
     g.depth[r] = float(t);
     if (t_hit) t_hit[r] = t;
     if (g.steps) g.steps[r] = uint32_t(i);
     if (g.depth64) g.depth64[r] = t;
-    if (g.evals) g.evals[r] = evals;
   }
 
   ND_DEV_INLINE void hit_at(const DevView& v, double at, const nd_gbuffer& g, double* t_hit, bool defer) {
@@ -1060,11 +1084,11 @@ ND_DEV_INLINE void trap_at_hit(const DevView& v, int64_t local, double t, const 
 // The deferred part of a hit ray: its normal taps at org + dir * t (the same
 // positions, evaluation order and float accumulation as the inline PH_NORMAL
 // phase), the shadow ray when the view has one (the steps of PH_SHADOW), and the
-// Lambert level.  Adds the evaluations to the ray's count; returns the taps in
-// the low and the shadow steps in the high 16 bits.
+// Lambert level.  Writes the ray's evaluation count (march_evals from the march plus
+// these); returns the taps in the low and the shadow steps in the high 16 bits.
 template <class Set, class T, bool kDir64, bool kScenes = false, bool kAccel = false>
 ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, const nd_gbuffer& g,
-                                    const DevScene* scenes) {
+                                    const DevScene* scenes, uint32_t march_evals) {
   Dir<kDir64> dir;
   dir.set(ray_dir(v, local));
   const D3 p = fmadd(d3(v.org[0], v.org[1], v.org[2]), dir.get(), t);
@@ -1125,7 +1149,7 @@ ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, c
   if (g.normal_half) write_normal_half(g, r, gx, gy, gz, true);
   if (g.shade) g.shade[r] = lambert(v, dir.get(), gx, gy, gz, vis);
   if (g.shadow) g.shadow[r] = vis;
-  if (g.evals) g.evals[r] += uint32_t(taps + sev);
+  if (g.evals) g.evals[r] = march_evals + uint32_t(taps + sev);
   return uint32_t(taps) | (uint32_t(sev) << 16);
 }
 

@@ -70,7 +70,7 @@ struct nd_ctx {
   int counters_cap = 0;
   Stats* d_stats = nullptr;
   double* d_thit = nullptr;    // FP64 hit distances for the shade pass
-  int32_t* d_hits = nullptr;   // hit list of the deferred shade pass
+  nd::HitEntry* d_hits = nullptr;   // hit list of the deferred shade pass
   int64_t thit_cap = 0;
   nd::DevScene* d_scenes = nullptr;  // multi-instance scene table
   int scenes_cap = 0;
@@ -104,7 +104,7 @@ struct nd_graph {
   DevView* d_views = nullptr;
   unsigned long long* d_counters = nullptr;
   double* d_thit = nullptr;
-  int32_t* d_hits = nullptr;
+  nd::HitEntry* d_hits = nullptr;
   float* d_accel = nullptr;
   nd::AccelJob* d_accel_jobs = nullptr;
   nd::DevScene* d_scenes = nullptr;
@@ -371,7 +371,7 @@ void scene_table(const SceneInput& sc, const std::vector<int>& members, std::vec
 // table is already on the device (graph replay).
 nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_march_opts* opts,
                   const nd_gbuffer* out, cudaStream_t stream, const std::vector<Launch>& plans, DevView* d_views,
-                  DevView* h_views, unsigned long long* d_counters, double* d_thit, int32_t* d_hits,
+                  DevView* h_views, unsigned long long* d_counters, double* d_thit, nd::HitEntry* d_hits,
                   bool copy_views, int* kernel_used, cudaEvent_t* tev = nullptr,
                   const SceneInput& sc = SceneInput(), nd::DevScene* d_scenes = nullptr, float* d_accel = nullptr,
                   nd::AccelJob* d_jobs = nullptr, std::vector<nd::AccelJob>* jobs_out = nullptr) {
@@ -805,7 +805,7 @@ nd_status forward_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, c
     ctx->d_hits = nullptr;
     ctx->thit_cap = 0;
     e = cudaMalloc((void**)&ctx->d_thit, sizeof(double) * size_t(total));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_hits, sizeof(int32_t) * size_t(total));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_hits, sizeof(nd::HitEntry) * size_t(total));
     if (e != cudaSuccess) return cuda_fail(ctx, e, "hit buffers");
     ctx->thit_cap = total;
   }
@@ -1020,7 +1020,7 @@ nd_status graph_capture_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nvi
   cudaError_t e = cudaMalloc((void**)&g->d_views, sizeof(DevView) * size_t(nviews));
   if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_counters, sizeof(unsigned long long) * 2 * plans.size());
   if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_thit, sizeof(double) * size_t(std::max<int64_t>(total, 1)));
-  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_hits, sizeof(int32_t) * size_t(std::max<int64_t>(total, 1)));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_hits, sizeof(nd::HitEntry) * size_t(std::max<int64_t>(total, 1)));
   int64_t voxels = 0;
   int accel_views = 0;
   for (int i = 0; i < nviews; ++i) {

@@ -33,3 +33,23 @@ def test_largest_launch_hands_out_every_ray_once():
                                                (65536, 4, 16), (4097, WARPS, 1)])
 def test_small_launches(total, warps, chunk):
     check(total, warps, chunk, start=0, seed=total + chunk)
+
+
+def test_magic_division_of_ray_indices():
+    # ray_uv divides ray indices (< 2^31) by a view's pixel count and width with a
+    # precomputed multiplier and shift; it must equal integer division everywhere
+    import ctypes as C
+
+    import numpy as np
+
+    lib = opcount._load()
+    lib.nd_div_by.argtypes = [C.c_uint32, C.c_int64, C.c_void_p, C.c_void_p]
+    rng = np.random.default_rng(5)
+    divisors = list(range(1, 3000)) + [int(x) for x in rng.integers(1, 2**31, 3000)]
+    divisors += [2**k + o for k in range(31) for o in (-1, 0, 1) if 0 < 2**k + o < 2**31]
+    for d in divisors:
+        n = np.concatenate([rng.integers(0, 2**31, 64), [0, 1, d - 1, d, d + 1, 2**31 - 1, 2**31 - 2]])
+        n = n[(n >= 0) & (n < 2**31)].astype(np.uint32)
+        q = np.zeros_like(n)
+        lib.nd_div_by(d, n.size, n.ctypes.data, q.ctypes.data)
+        np.testing.assert_array_equal(q, n // np.uint32(d), err_msg=f"d={d}")
