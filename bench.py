@@ -618,7 +618,7 @@ def main():
         gbuf = runtime.GBuffer.allocate(nrays, device=dev)
         tr = ctx.autotune(views, gbuf) if tune else None
         opts = runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT, blocks_per_sm=tr.blocks_per_sm if tr else 0,
-                                 refill_threshold=tr.refill_threshold if tr else 4)
+                                 refill_threshold=tr.refill_threshold if tr else 6, block=tr.block if tr else 0)
         graph = ctx.capture(views, gbuf, opts, stream=sptr)
         ms_p = timed(lambda: graph.launch(sptr), steps, warmup)
         st = ctx.stats()
@@ -780,7 +780,7 @@ def main():
             "gpu_launches": 2 * args.steps,
             "stats": {"de_evals": st.de_evals, "march": st.march_evals, "normal": st.normal_evals,
                       "shadow": st.shadow_evals, "trap": st.trap_evals, "hits": st.hits, "refills": st.refills},
-            "tune": {"kernel": tune.kernel, "blocks_per_sm": tune.blocks_per_sm,
+            "tune": {"kernel": tune.kernel, "block": tune.block, "blocks_per_sm": tune.blocks_per_sm,
                      "refill_threshold": tune.refill_threshold} if tune else None,
             "second_workload": extra,
             "differentiation": diff,

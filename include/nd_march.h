@@ -225,8 +225,9 @@ enum { ND_KERNEL_AUTO = 0, ND_KERNEL_PLAIN = 1, ND_KERNEL_PERSISTENT = 2 };
 
 typedef struct nd_march_opts {
   int32_t kernel;            /* ND_KERNEL_* */
-  int32_t block;             /* threads per block (0 = tuned default) */
-  int32_t blocks_per_sm;     /* persistent kernel residency (0 = tuned default) */
+  int32_t block;             /* persistent march: threads per block, 64, 128 or 256 (0 = tuned, else 128) */
+  int32_t blocks_per_sm;     /* persistent kernel residency: > 0 that many (at most what fits), < 0 that
+                                many fewer than fit, 0 = tuned default (as many as fit) */
   int32_t refill_threshold;  /* persistent: refill a warp once this many lanes idle (0 = default) */
   int32_t de_precision;      /* 32 (default) or 64: float type of the DE itself */
   int32_t watchdog_ms;       /* device watchdog per launch (0 = 10000 ms) */
@@ -284,8 +285,22 @@ nd_status nd_last_stats(nd_ctx* ctx, nd_stats* out); /* synchronises the last fo
 nd_status nd_count_rays(const nd_view_desc* views, int32_t nviews, int64_t* total);
 nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews,
                            const nd_march_opts* opts, const nd_gbuffer* out, void* stream);
+/* Times the launch configurations of the march on these views (writing into
+ * scratch_out): the plain per-view launch, and the persistent march at 64, 128 and
+ * 256 threads per block x as many resident blocks per SM as fit or two fewer x
+ * refill thresholds 3..12; each candidate's time is the median of three runs with
+ * the L2 cache flushed before each.  The winner is kept for the call's formula sets
+ * on this GPU (later forwards with opts fields 0 use it).  result->blocks_per_sm is
+ * the resident count the march runs with. */
 nd_status nd_autotune(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews,
                       const nd_gbuffer* scratch_out, nd_tune_result* result);
+/* The autotuner's winners on disk: a JSON array of entries keyed by GPU name, formula
+ * set and a hash of the formula sources, so that a later process starts tuned.  No
+ * counterpart in the reference (it paces sub-tiles by a heuristic instead, ExportPacer,
+ * fractal_renderer.zig:991).  load: ND_ERR_NOT_FOUND when the file does not exist;
+ * *loaded (nullable) receives the number of entries read. */
+nd_status nd_tune_cache_save(const char* path);
+nd_status nd_tune_cache_load(const char* path, int32_t* loaded);
 nd_status nd_graph_capture(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews,
                            const nd_march_opts* opts, const nd_gbuffer* out, void* stream, nd_graph** graph);
 nd_status nd_graph_launch(nd_graph* graph, void* stream);

@@ -94,8 +94,11 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value) plain_kernel(const _
 // tpl:5083-5105), and a warp keeps marching neighbouring pixels.  Whatever phase
 // a lane is in, each pass of the loop is one DE evaluation for every busy lane.
 
-template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, bool kAccel = false>
-__global__ void __launch_bounds__(128, MinBlocks<T>::value)
+// kBlock: threads per block (the autotuner's block-size axis); every block size is
+// compiled for the same threads per SM, and so the same registers per thread.
+template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, bool kAccel = false,
+          int kBlock = 128>
+__global__ void __launch_bounds__(kBlock, MinBlocks<T>::value * 128 / kBlock)
     persistent_kernel(const __grid_constant__ LaunchArgs a, const __grid_constant__ DevView single) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -204,44 +207,171 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
 }
 
 // --------------------------------------------------------------- shade pass
-// Work at the hit points, after the march: with a hit list (deferred shading) the
-// normal taps, the shadow ray, the Lambert level and, when asked, the orbit trap of
-// every listed hit (the shadow rays' step counts differ, the rest is coherent);
-// without one (the plain kernel) the orbit trap of every ray that hit.  It strides
-// over its work with a resident grid.
+// Work at the hit points, after the march (the wavefront surface pass, after
+// cs_wf_surface tpl:5215-5236): with a hit list (deferred shading) the normal taps,
+// the Lambert level and, when asked, the orbit trap of every listed hit.  A hit whose
+// view casts a shadow ray either marches it here (no shadow queue) or is appended to
+// the shadow queue for the shadow kernel, which finishes the ray.  Without a hit list
+// (the plain kernel) the pass computes the orbit trap of every ray that hit.  It
+// strides over its work with a resident grid, warp by warp (the queue appends are
+// warp-aggregated).
 template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, bool kAccel = false>
 __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     shade_kernel(const __grid_constant__ LaunchArgs a, const __grid_constant__ DevView single, int do_trap) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
   const bool list = a.hit_list != nullptr;
+  const bool queue = a.shadow_queue != nullptr;
   const int64_t count = list ? int64_t(*a.hit_count) : a.total_rays;
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   unsigned long long taps = 0, shadow = 0;
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride) {
-    HitEntry h{int32_t(i), 0u};
-    if (list) h = a.hit_list[i];
-    const int64_t it = h.item;
-    const int vi = kBatched ? find_view(a.views, a.nviews, it) : 0;
-    const DevView& v = kBatched ? a.views[vi] : single;
-    const int64_t local = it - v.ray_offset;
-    const double t = a.t_hit[v.out_offset + local];
-    if (t < 0.0) continue;  // a miss (all-rays mode); the march wrote its outputs
-    if (list) {
-      const uint32_t ev = shade_at_hit<Set, T, kDir64, kScenes, kAccel>(v, local, t, a.out, a.scenes, h.march_evals);
-      taps += ev & 0xffffu;
-      shadow += ev >> 16;
+  for (int64_t i0 = int64_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); i0 < count; i0 += stride) {
+    const int64_t i = i0 + lane;  // the loop bound is warp-uniform: every lane takes part in the ballot
+    bool want = false;
+    ShadowEntry e;
+    if (i < count) {
+      HitEntry h{int32_t(i), 0u};
+      if (list) h = a.hit_list[i];
+      const int64_t it = h.item;
+      const int vi = kBatched ? find_view(a.views, a.nviews, it) : 0;
+      const DevView& v = kBatched ? a.views[vi] : single;
+      const int64_t local = it - v.ray_offset;
+      const int64_t r = v.out_offset + local;
+      const double t = a.t_hit[r];
+      if (t >= 0.0) {  // (all-rays mode: a miss has t < 0 and the march wrote its outputs)
+        if (list) {
+          if (queue && casts_shadow(v)) {
+            Dir<kDir64> dir;
+            dir.set(ray_dir(v, local));
+            const Surface sf = surface_at_hit<Set, T, kDir64, kScenes>(v, dir, t, r, a.out, a.scenes);
+            const D3 so = shadow_origin(sf);
+            e = ShadowEntry{h.item, h.march_evals + uint32_t(sf.taps), sf.gx, sf.gy, sf.gz, 0, so.x, so.y, so.z};
+            want = true;
+            taps += uint32_t(sf.taps);
+          } else {
+            const uint32_t ev = shade_at_hit<Set, T, kDir64, kScenes, kAccel>(v, local, t, a.out, a.scenes,
+                                                                              h.march_evals);
+            taps += ev & 0xffffu;
+            shadow += ev >> 16;
+          }
+        }
+        if (do_trap) trap_at_hit<Set, T, kDir64, kScenes>(v, local, t, a.out, a.scenes);
+      }
     }
-    if (do_trap) trap_at_hit<Set, T, kDir64, kScenes>(v, local, t, a.out, a.scenes);
+    if (queue) {
+      const unsigned qm = __ballot_sync(full, want);
+      if (qm) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(a.shadow_count, unsigned(__popc(qm)));
+        base = __shfl_sync(full, base, 0);
+        if (want) a.shadow_queue[base + __popc(qm & ((1u << lane) - 1u))] = e;
+      }
+    }
   }
   if (list) {
     for (int o = 16; o > 0; o >>= 1) {
-      taps += __shfl_xor_sync(0xffffffffu, taps, o);
-      shadow += __shfl_xor_sync(0xffffffffu, shadow, o);
+      taps += __shfl_xor_sync(full, taps, o);
+      shadow += __shfl_xor_sync(full, shadow, o);
     }
-    if ((threadIdx.x & 31) == 0 && taps + shadow) {
+    if (lane == 0 && taps + shadow) {
       atomicAdd(&a.stats->normal_evals, taps);
       atomicAdd(&a.stats->shadow_evals, shadow);
       atomicAdd(&a.stats->de_evals, taps + shadow);
     }
+  }
+}
+
+// --------------------------------------------------------------- shadow pass
+// The queued shadow rays (cs_wf_shadow tpl:5333-5346, with visibility_march
+// tpl:2294-2341 for an opaque scene): a persistent kernel in which every lane
+// marches one shadow ray, one DE evaluation per pass, and the warp refills its
+// finished lanes from the queue by ballot and popc rank (WarpRuns, as the primary
+// march), so that shadow rays of very different lengths do not idle the warp.  The
+// arithmetic is shadow_visibility's, step for step, so the inline and the queued
+// pass give the same bits.  At the end of a ray: the visibility, the Lambert level
+// and the ray's evaluation count.
+template <class Set, class T, bool kScenes = false>
+__global__ void __launch_bounds__(128, MinBlocks<T>::value) shadow_kernel(const __grid_constant__ LaunchArgs a) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const int32_t total = int32_t(*a.shadow_count);
+  WarpRuns runs;
+  // this lane's shadow ray
+  bool busy = false;
+  int32_t qi = -1, view = 0, k = 0, sev = 0;
+  double ox = 0.0, oy = 0.0, oz = 0.0, dist = 0.0, res = 1.0;
+  uint32_t steps_sum = 0;
+  const int64_t deadline = __shfl_sync(full, globaltimer_ns(), 0) + a.deadline_ns;
+  int tick = 0;
+  const int thr = a.refill_threshold;
+  auto finish = [&](float vis) {
+    const ShadowEntry& e = a.shadow_queue[qi];
+    const DevView& v = a.views[view];
+    const int64_t r = v.out_offset + (int64_t(e.item) - v.ray_offset);
+    // a view that casts shadow rays uses its light for the Lambert term (no ray direction)
+    finish_at_hit(v, D3{0.0, 0.0, 0.0}, e.nx, e.ny, e.nz, vis, e.evals + uint32_t(sev), r, a.out);
+    steps_sum += uint32_t(sev);
+    busy = false;
+  };
+  while (true) {
+    const unsigned free_lanes = __ballot_sync(full, !busy);
+    const int nfree = __popc(free_lanes);
+    const bool have_work = runs.have_work();
+    if (!have_work && free_lanes == full) break;
+    if (have_work && nfree != 0 && (nfree >= thr || free_lanes == full)) {
+      const WarpRuns::Claim c = runs.claim(nfree, a.chunk, total, [&](int take) {
+        unsigned long long got = 0;
+        if (lane == 0) got = atomicAdd(a.shadow_counter, (unsigned long long)take);
+        return uint64_t(__shfl_sync(full, got, 0));
+      });
+      if (!busy) {
+        const int rk = __popc(free_lanes & lt_mask);
+        if (rk < c.used) {
+          qi = c.item(rk);
+          const ShadowEntry& e = a.shadow_queue[qi];
+          view = find_view_from(a.views, a.nviews, e.item, view);
+          ox = e.ox;
+          oy = e.oy;
+          oz = e.oz;
+          dist = kShadowBias;
+          res = 1.0;
+          k = 0;
+          sev = 0;
+          busy = true;
+        }
+      }
+      continue;
+    }
+    if (((++tick) & 63) == 0) {
+      const int64_t now = __shfl_sync(full, globaltimer_ns(), 0);
+      if (now > deadline) {
+        if (lane == 0) atomicAdd(&a.stats->timeouts, 1u);
+        break;
+      }
+    }
+    if (busy) {
+      const DevView& v = a.views[view];
+      const D3 q = fmadd(d3(ox, oy, oz), d3(v.light[0], v.light[1], v.light[2]), dist);
+      const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(q), a.scenes);
+      ++sev;
+      const double d = double(de.d);
+      if (d < kShadowHitEps) {
+        finish(0.0f);
+      } else {
+        res = fmin(res, double(v.shadow_k) * d / dist);
+        dist += fmax(d, kShadowMinStep);
+        ++k;
+        const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
+        if (k >= steps || dist >= 2.0 * v.max_dist) finish(float(fmin(fmax(res, 0.0), 1.0)));
+      }
+    }
+  }
+  unsigned long long s = steps_sum;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(full, s, o);
+  if (lane == 0 && s) {
+    atomicAdd(&a.stats->shadow_evals, s);
+    atomicAdd(&a.stats->de_evals, s);
   }
 }
 
@@ -262,16 +392,26 @@ cudaError_t launch_plain(const LaunchArgs& a, const DevView& single, const Launc
   return cudaGetLastError();
 }
 
-template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, bool kAccel = false>
+// Blocks per SM of a resident grid: the most that fit (c.blocks_per_sm 0), that many
+// less (c.blocks_per_sm < 0), or the requested count clamped to what fits, so that
+// every block of the persistent grid is resident at once.
+template <class K> cudaError_t resident_blocks(K kernel, int block, int want, int* per_sm) {
+  int fit = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, kernel, block, 0);
+  if (e != cudaSuccess) return e;
+  fit = std::max(fit, 1);
+  *per_sm = want > 0 ? std::min(want, fit) : std::max(1, fit + want);
+  return cudaSuccess;
+}
+
+template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, bool kAccel = false,
+          int kBlock = 128>
 cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const LaunchConfig& c, cudaStream_t s) {
-  const int block = 128;
-  int per_sm = c.blocks_per_sm;
-  if (per_sm <= 0) {
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, persistent_kernel<Set, T, kDir64, kBatched, kScenes, kAccel>, block, 0);
-    if (e != cudaSuccess) return e;
-    if (per_sm <= 0) per_sm = 1;
-  }
+  const int block = kBlock;
+  int per_sm = 0;
+  cudaError_t e = resident_blocks(persistent_kernel<Set, T, kDir64, kBatched, kScenes, kAccel, kBlock>, block,
+                                  c.blocks_per_sm, &per_sm);
+  if (e != cudaSuccess) return e;
   int64_t grid = int64_t(per_sm) * c.num_sms;
   const int64_t needed = (a.total_rays + block - 1) / block;
   if (grid > needed) grid = needed;
@@ -281,11 +421,22 @@ cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const 
   LaunchArgs b = a;
   const int64_t warps = grid * (block / 32);
   b.chunk = int32_t(std::max<int64_t>(1, std::min<int64_t>(64, a.total_rays / (warps * 4))));
-  persistent_kernel<Set, T, kDir64, kBatched, kScenes, kAccel><<<unsigned(grid), block, 0, s>>>(b, single);
+  persistent_kernel<Set, T, kDir64, kBatched, kScenes, kAccel, kBlock><<<unsigned(grid), block, 0, s>>>(b, single);
   return cudaGetLastError();
 }
 
 typedef cudaError_t (*LaunchFn)(const LaunchArgs&, const DevView&, const LaunchConfig&, cudaStream_t);
+
+// Blocks per SM a persistent launch would use (the clamp above) for the FP32 batched
+// march at a block size: what the autotuner reports.
+template <class Set, int kBlock> int resident_f32_batched(int want) {
+  int per_sm = 0;
+  if (resident_blocks(persistent_kernel<Set, float, false, true, false, false, kBlock>, kBlock, want, &per_sm) !=
+      cudaSuccess)
+    return 0;
+  return per_sm;
+}
+typedef int (*ResidentFn)(int);
 
 template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, bool kAccel = false>
 cudaError_t launch_shade(const LaunchArgs& a, const DevView& single, const LaunchConfig& c, int do_trap,
@@ -303,6 +454,26 @@ cudaError_t launch_shade(const LaunchArgs& a, const DevView& single, const Launc
 }
 
 typedef cudaError_t (*ShadeFn)(const LaunchArgs&, const DevView&, const LaunchConfig&, int, cudaStream_t);
+
+// The shadow pass over a launch's shadow queue: a resident grid (its size cannot
+// depend on the queue length, which the surface pass writes on the device), runs of
+// up to 16 queue entries per warp claim.
+template <class Set, class T, bool kScenes = false>
+cudaError_t launch_shadow(const LaunchArgs& a, const LaunchConfig& c, cudaStream_t s) {
+  int per_sm = 0;
+  cudaError_t e = resident_blocks(shadow_kernel<Set, T, kScenes>, 128, c.blocks_per_sm, &per_sm);
+  if (e != cudaSuccess) return e;
+  int64_t grid = int64_t(per_sm) * c.num_sms;
+  const int64_t needed = (a.total_rays + 127) / 128;  // at most one queue entry per ray
+  if (grid > needed) grid = needed;
+  if (grid <= 0) return cudaSuccess;
+  LaunchArgs b = a;
+  b.chunk = 16;
+  shadow_kernel<Set, T, kScenes><<<unsigned(grid), 128, 0, s>>>(b);
+  return cudaGetLastError();
+}
+
+typedef cudaError_t (*ShadowFn)(const LaunchArgs&, const LaunchConfig&, cudaStream_t);
 
 // --------------------------------------------------------------- lite shading
 // One thread per ray of the call (resident grid, strided): misses take the view's
@@ -432,6 +603,9 @@ typedef cudaError_t (*DePointsFn)(const DevView&, int64_t, const double*, double
 struct KernelTable {
   LaunchFn plain_f32, plain_f32_dir64, plain_f64;
   LaunchFn persistent_f32, persistent_f32_batched, persistent_f32_dir64, persistent_f32_dir64_batched;
+  // the FP32 march at 64 and 256 threads per block (the default is 128), single and batched
+  LaunchFn persistent_f32_b64, persistent_f32_b256, persistent_f32_batched_b64, persistent_f32_batched_b256;
+  ResidentFn resident_b64, resident_b128, resident_b256;
   LaunchFn persistent_f64, persistent_f64_batched;
   ShadeFn shade_f32, shade_f32_batched, shade_f32_dir64, shade_f32_dir64_batched, shade_f64, shade_f64_batched;
   DePointsFn de_points_f32, de_points_f64;
@@ -449,6 +623,8 @@ struct KernelTable {
   ShadeFn scene_shade_f32_accel, scene_shade_f64_accel;
   // lite shading of a forward's hits (with scenes: formula groups only)
   LiteFn lite_f32, lite_f32_dir64, scene_lite_f32;
+  // the wavefront shadow pass (FP32 or FP64 DE; with scenes: formula groups only)
+  ShadowFn shadow_f32, shadow_f64, scene_shadow_f32, scene_shadow_f64;
 };
 
 template <class Set, bool kWithScenes = false> KernelTable make_kernel_table() {
@@ -467,7 +643,10 @@ template <class Set, bool kWithScenes = false> KernelTable make_kernel_table() {
     t.scene_shade_f32_accel = &launch_shade<Set, float, false, true, true, true>;
     t.scene_shade_f64_accel = &launch_shade<Set, double, true, true, true, true>;
     t.scene_lite_f32 = &launch_lite<Set, float, false, true>;
+    t.scene_shadow_f32 = &launch_shadow<Set, float, true>;
+    t.scene_shadow_f64 = &launch_shadow<Set, double, true>;
   } else {
+    t.scene_shadow_f32 = t.scene_shadow_f64 = nullptr;
     t.scene_lite_f32 = nullptr;
     t.scene_persistent_f32 = t.scene_persistent_f32_dir64 = t.scene_persistent_f64 = nullptr;
     t.scene_shade_f32 = t.scene_shade_f32_dir64 = t.scene_shade_f64 = nullptr;
@@ -475,6 +654,8 @@ template <class Set, bool kWithScenes = false> KernelTable make_kernel_table() {
     t.scene_persistent_f32_accel = t.scene_persistent_f64_accel = nullptr;
     t.scene_shade_f32_accel = t.scene_shade_f64_accel = nullptr;
   }
+  t.shadow_f32 = &launch_shadow<Set, float>;
+  t.shadow_f64 = &launch_shadow<Set, double>;
   t.lite_f32 = &launch_lite<Set, float, false>;
   t.lite_f32_dir64 = &launch_lite<Set, float, true>;
   t.accel_build_f32 = &launch_accel_build<Set, float, false>;
@@ -486,6 +667,13 @@ template <class Set, bool kWithScenes = false> KernelTable make_kernel_table() {
   t.plain_f32 = &launch_plain<Set, float, false>;
   t.plain_f32_dir64 = &launch_plain<Set, float, true>;
   t.plain_f64 = &launch_plain<Set, double, true>;
+  t.persistent_f32_b64 = &launch_persistent<Set, float, false, false, false, false, 64>;
+  t.persistent_f32_b256 = &launch_persistent<Set, float, false, false, false, false, 256>;
+  t.persistent_f32_batched_b64 = &launch_persistent<Set, float, false, true, false, false, 64>;
+  t.persistent_f32_batched_b256 = &launch_persistent<Set, float, false, true, false, false, 256>;
+  t.resident_b64 = &resident_f32_batched<Set, 64>;
+  t.resident_b128 = &resident_f32_batched<Set, 128>;
+  t.resident_b256 = &resident_f32_batched<Set, 256>;
   t.persistent_f32 = &launch_persistent<Set, float, false, false>;
   t.persistent_f32_batched = &launch_persistent<Set, float, false, true>;
   t.persistent_f32_dir64 = &launch_persistent<Set, float, true, false>;

@@ -154,6 +154,19 @@ struct HitEntry {
   uint32_t march_evals;
 };
 
+// One entry of the shadow queue (the wavefront shadow pass, after cs_wf_shadow
+// tpl:5333-5346): a hit whose view casts a shadow ray, with what the surface pass
+// computed for it: the shadow ray's origin (hit + normal x SHADOW_BIAS, FP64), the
+// unit normal (for the Lambert level once the visibility is known) and the DE
+// evaluations the ray has used so far (march + normal taps).
+struct ShadowEntry {
+  int32_t item;
+  uint32_t evals;
+  float nx, ny, nz;
+  int32_t pad;
+  double ox, oy, oz;
+};
+
 struct LaunchArgs {
   const DevView* views;       // device
   int32_t nviews;
@@ -171,6 +184,12 @@ struct LaunchArgs {
   struct HitEntry* hit_list;  // hits of the launch (nullptr: shading inline)
   unsigned int* hit_count;    // entries in hit_list (zeroed before launch)
   const struct DevScene* scenes;  // multi-instance scenes of the launch's views (may be null)
+  // Wavefront shadow pass: the surface pass appends hits whose view casts a shadow
+  // ray to shadow_queue; a persistent shadow kernel then marches them with the same
+  // warp-ballot refill as the primary march (nullptr: shadow rays inline).
+  ShadowEntry* shadow_queue;
+  unsigned int* shadow_count;           // entries in shadow_queue (zeroed before launch)
+  unsigned long long* shadow_counter;   // the shadow kernel's work counter (zeroed before launch)
 };
 
 // --------------------------------------------------------------- orbit trap
@@ -1081,65 +1100,41 @@ ND_DEV_INLINE void trap_at_hit(const DevView& v, int64_t local, double t, const 
   if (g.iters) g.iters[r] = uint32_t(de.iters);
 }
 
-// The deferred part of a hit ray: its normal taps at org + dir * t (the same
-// positions, evaluation order and float accumulation as the inline PH_NORMAL
-// phase), the shadow ray when the view has one (the steps of PH_SHADOW), and the
-// Lambert level.  Writes the ray's evaluation count (march_evals from the march plus
-// these); returns the taps in the low and the shadow steps in the high 16 bits.
-template <class Set, class T, bool kDir64, bool kScenes = false, bool kAccel = false>
-ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, const nd_gbuffer& g,
-                                    const DevScene* scenes, uint32_t march_evals) {
-  Dir<kDir64> dir;
-  dir.set(ray_dir(v, local));
-  const D3 p = fmadd(d3(v.org[0], v.org[1], v.org[2]), dir.get(), t);
-  const int taps = int(normal_taps(v));
+// The deferred part of a hit ray, in three pieces: surface_at_hit (the normal taps
+// at org + dir * t: the same positions, evaluation order and float accumulation as
+// the inline PH_NORMAL phase; writes the normal), shadow_visibility (the shadow ray
+// when the view has one: the steps of PH_SHADOW) and finish_at_hit (the Lambert
+// level, the visibility and the ray's evaluation count).  shade_at_hit chains them;
+// with a shadow queue the surface pass queues the shadow ray instead and the shadow
+// kernel finishes the ray.
+
+// Does the view cast a shadow ray from its hits? (visibility_march's loop runs)
+ND_DEV_INLINE bool casts_shadow(const DevView& v) {
+  const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
+  return v.shadow && steps > 0 && kShadowBias < 2.0 * v.max_dist;
+}
+
+struct Surface {
+  D3 p;              // the hit point
+  float gx, gy, gz;  // unit normal
+  int taps;
+};
+
+template <class Set, class T, bool kDir64, bool kScenes = false>
+ND_DEV_INLINE Surface surface_at_hit(const DevView& v, const Dir<kDir64>& dir, double t, int64_t r,
+                                     const nd_gbuffer& g, const DevScene* scenes) {
+  Surface s;
+  s.p = fmadd(d3(v.org[0], v.org[1], v.org[2]), dir.get(), t);
+  s.taps = int(normal_taps(v));
   float gx = 0.0f, gy = 0.0f, gz = 0.0f;
-  for (int k = 0; k < taps; ++k) {
-    const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(normal_tap_pos<T>(v, p, t, k)), scenes);
+  for (int k = 0; k < s.taps; ++k) {
+    const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(normal_tap_pos<T>(v, s.p, t, k)), scenes);
     normal_accumulate(v, k, double(de.d), gx, gy, gz);
   }
   normal_finish(gx, gy, gz);
-  // visibility_march (tpl:2294-2341) toward the light, opaque scene
-  float vis = 1.0f;
-  int k = 0, sev = 0;  // shadow steps, shadow DE evaluations
-  const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
-  if (v.shadow && steps > 0 && kShadowBias < 2.0 * v.max_dist) {
-    const D3 so = fmadd(p, d3(gx, gy, gz), kShadowBias);
-    const D3 L = d3(v.light[0], v.light[1], v.light[2]);
-    double a = kShadowBias, res = 1.0;
-    while (true) {
-      const D3 q = fmadd(so, L, a);
-      if constexpr (kAccel) {
-        // visibility_march tpl:2297-2303: a recorded safe jump instead of an evaluation
-        const double skip = double(accel_skip(v, float(q.x), float(q.y), float(q.z)));
-        if (skip > kShadowMinStep && double(v.shadow_k) * skip >= res * a) {
-          a += skip;
-          ++k;
-          if (k >= steps || a >= 2.0 * v.max_dist) {
-            vis = float(fmin(fmax(res, 0.0), 1.0));
-            break;
-          }
-          continue;
-        }
-      }
-      const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(q), scenes);
-      ++sev;
-      const double d = double(de.d);
-      if (d < kShadowHitEps) {
-        vis = 0.0f;
-        ++k;
-        break;
-      }
-      res = fmin(res, double(v.shadow_k) * d / a);
-      a += fmax(d, kShadowMinStep);
-      ++k;
-      if (k >= steps || a >= 2.0 * v.max_dist) {
-        vis = float(fmin(fmax(res, 0.0), 1.0));
-        break;
-      }
-    }
-  }
-  const int64_t r = v.out_offset + local;
+  s.gx = gx;
+  s.gy = gy;
+  s.gz = gz;
   if (g.normal) {
     struct alignas(16) F4 {
       float x, y, z, w;
@@ -1147,10 +1142,77 @@ ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, c
     reinterpret_cast<F4*>(g.normal)[r] = F4{gx, gy, gz, 1.0f};
   }
   if (g.normal_half) write_normal_half(g, r, gx, gy, gz, true);
-  if (g.shade) g.shade[r] = lambert(v, dir.get(), gx, gy, gz, vis);
+  return s;
+}
+
+// The origin of a hit's shadow ray (visibility_march is started at hit + n * bias).
+ND_DEV_INLINE D3 shadow_origin(const Surface& s) { return fmadd(s.p, d3(s.gx, s.gy, s.gz), kShadowBias); }
+
+// visibility_march (tpl:2294-2341) toward the light from `so`, opaque scene: the
+// visibility, with the DE evaluations in *sev.
+template <class Set, class T, bool kScenes = false, bool kAccel = false>
+ND_DEV_INLINE float shadow_visibility(const DevView& v, D3 so, const DevScene* scenes, int* sev) {
+  float vis = 1.0f;
+  int k = 0;
+  *sev = 0;
+  const int steps = v.max_steps < kShadowMaxSteps ? v.max_steps : kShadowMaxSteps;
+  const D3 L = d3(v.light[0], v.light[1], v.light[2]);
+  double a = kShadowBias, res = 1.0;
+  while (true) {
+    const D3 q = fmadd(so, L, a);
+    if constexpr (kAccel) {
+      // visibility_march tpl:2297-2303: a recorded safe jump instead of an evaluation
+      const double skip = double(accel_skip(v, float(q.x), float(q.y), float(q.z)));
+      if (skip > kShadowMinStep && double(v.shadow_k) * skip >= res * a) {
+        a += skip;
+        ++k;
+        if (k >= steps || a >= 2.0 * v.max_dist) {
+          vis = float(fmin(fmax(res, 0.0), 1.0));
+          break;
+        }
+        continue;
+      }
+    }
+    const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(q), scenes);
+    ++*sev;
+    const double d = double(de.d);
+    if (d < kShadowHitEps) {
+      vis = 0.0f;
+      break;
+    }
+    res = fmin(res, double(v.shadow_k) * d / a);
+    a += fmax(d, kShadowMinStep);
+    ++k;
+    if (k >= steps || a >= 2.0 * v.max_dist) {
+      vis = float(fmin(fmax(res, 0.0), 1.0));
+      break;
+    }
+  }
+  return vis;
+}
+
+// The outputs a hit ray's shading ends with.
+ND_DEV_INLINE void finish_at_hit(const DevView& v, D3 dir, float gx, float gy, float gz, float vis, uint32_t evals,
+                                 int64_t r, const nd_gbuffer& g) {
+  if (g.shade) g.shade[r] = lambert(v, dir, gx, gy, gz, vis);
   if (g.shadow) g.shadow[r] = vis;
-  if (g.evals) g.evals[r] = march_evals + uint32_t(taps + sev);
-  return uint32_t(taps) | (uint32_t(sev) << 16);
+  if (g.evals) g.evals[r] = evals;
+}
+
+// All of it inline: normal, shadow ray, Lambert.  Returns the taps in the low and
+// the shadow steps in the high 16 bits.
+template <class Set, class T, bool kDir64, bool kScenes = false, bool kAccel = false>
+ND_DEV_INLINE uint32_t shade_at_hit(const DevView& v, int64_t local, double t, const nd_gbuffer& g,
+                                    const DevScene* scenes, uint32_t march_evals) {
+  Dir<kDir64> dir;
+  dir.set(ray_dir(v, local));
+  const int64_t r = v.out_offset + local;
+  const Surface s = surface_at_hit<Set, T, kDir64, kScenes>(v, dir, t, r, g, scenes);
+  float vis = 1.0f;
+  int sev = 0;
+  if (casts_shadow(v)) vis = shadow_visibility<Set, T, kScenes, kAccel>(v, shadow_origin(s), scenes, &sev);
+  finish_at_hit(v, dir.get(), s.gx, s.gy, s.gz, vis, march_evals + uint32_t(s.taps + sev), r, g);
+  return uint32_t(s.taps) | (uint32_t(sev) << 16);
 }
 
 // --------------------------------------------------------------- lite shading

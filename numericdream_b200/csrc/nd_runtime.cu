@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "nd_json.h"
 #include "nd_registry.h"
 #include "nd_view.h"
 
@@ -27,6 +28,9 @@ namespace {
 
 constexpr int kMaxViews = 1 << 16;
 constexpr int64_t kMaxRays = int64_t(1) << 40;
+// Device counters per launch plan: the work counter, the hit count, the shadow-queue
+// count and the shadow pass's work counter.
+constexpr int kCountersPerPlan = 4;
 
 const char* kStatusNames[] = {"ND_OK",          "ND_ERR_INVALID", "ND_ERR_COMPILE",     "ND_ERR_OOM",
                               "ND_ERR_TIMEOUT", "ND_ERR_CUDA",    "ND_ERR_UNSUPPORTED", "ND_ERR_NOT_FOUND"};
@@ -49,20 +53,24 @@ void copy_str(char* out, size_t out_len, const char* s, size_t len) {
 void copy_str(char* out, size_t out_len, const std::string& s) { copy_str(out, out_len, s.data(), s.size()); }
 void copy_str(char* out, size_t out_len, const char* s) { copy_str(out, out_len, s, strlen(s)); }
 
-// Per-(formula set) tuned launch parameters, filled by nd_autotune.
+// Tuned launch parameters per (GPU, formula set), filled by nd_autotune and by
+// nd_tune_cache_load.  blocks_per_sm: 0 = as many as fit, < 0 = that many fewer.
 struct Tuned {
   int kernel = ND_KERNEL_PERSISTENT;
+  int block = 128;
   int blocks_per_sm = 0;
-  int refill_threshold = 8;
+  int refill_threshold = 6;
+  double rays_per_s = 0.0;  // measured by the tuning run
 };
 std::mutex g_tune_mu;
-std::map<std::string, Tuned> g_tuned;
+std::map<std::string, Tuned> g_tuned;  // key: tune_key()
 
 }  // namespace
 
 struct nd_ctx {
   int device = 0;
   int num_sms = 0;
+  std::string gpu_name;  // cudaDeviceProp::name (the tuning cache's key)
   std::string err;
   DevView* d_views = nullptr;
   int views_cap = 0;
@@ -72,6 +80,8 @@ struct nd_ctx {
   double* d_thit = nullptr;    // FP64 hit distances for the shade pass
   nd::HitEntry* d_hits = nullptr;   // hit list of the deferred shade pass
   int64_t thit_cap = 0;
+  nd::ShadowEntry* d_shadowq = nullptr;  // shadow queue of the wavefront shadow pass
+  int64_t shadowq_cap = 0;
   nd::DevScene* d_scenes = nullptr;  // multi-instance scene table
   int scenes_cap = 0;
   float* d_accel = nullptr;          // accelerator grids of the views that have one
@@ -105,6 +115,7 @@ struct nd_graph {
   unsigned long long* d_counters = nullptr;
   double* d_thit = nullptr;
   nd::HitEntry* d_hits = nullptr;
+  nd::ShadowEntry* d_shadowq = nullptr;
   float* d_accel = nullptr;
   nd::AccelJob* d_accel_jobs = nullptr;
   nd::DevScene* d_scenes = nullptr;
@@ -325,11 +336,32 @@ nd_status plan(nd_ctx* ctx, const nd_view_desc* views, int nviews, std::vector<L
   return ND_OK;
 }
 
-LaunchFn pick(const KernelTable& t, int kernel, int prec, bool batched, bool dir64) {
+LaunchFn pick(const KernelTable& t, int kernel, int prec, bool batched, bool dir64, int block = 128) {
   if (kernel == ND_KERNEL_PLAIN) return prec == 64 ? t.plain_f64 : (dir64 ? t.plain_f32_dir64 : t.plain_f32);
   if (prec == 64) return batched ? t.persistent_f64_batched : t.persistent_f64;
   if (dir64) return batched ? t.persistent_f32_dir64_batched : t.persistent_f32_dir64;
+  // block sizes other than 128 exist for the FP32 march (the autotuner's axis)
+  if (block == 64 && (batched ? t.persistent_f32_batched_b64 : t.persistent_f32_b64))
+    return batched ? t.persistent_f32_batched_b64 : t.persistent_f32_b64;
+  if (block == 256 && (batched ? t.persistent_f32_batched_b256 : t.persistent_f32_b256))
+    return batched ? t.persistent_f32_batched_b256 : t.persistent_f32_b256;
   return batched ? t.persistent_f32_batched : t.persistent_f32;
+}
+
+// The tuning key of a launch plan on a context's GPU: the GPU's name, the formula
+// set, and a hash of the set's formula sources (an edited formula is tuned anew).
+std::string tune_key(const nd_ctx* ctx, const Launch& L) {
+  uint64_t h = 0xCBF29CE484222325ull;
+  for (int f : L.members) {
+    const uint64_t x = nd_formula_entries[f].source_hash;
+    for (int b = 0; b < 8; ++b) {
+      h ^= (x >> (8 * b)) & 0xffu;
+      h *= 0x100000001B3ull;
+    }
+  }
+  char hex[20];
+  snprintf(hex, sizeof(hex), "%016llx", (unsigned long long)h);
+  return ctx->gpu_name + "|" + L.key + "|" + hex;
 }
 
 Tuned tuned_for(const std::string& key) {
@@ -365,16 +397,18 @@ void scene_table(const SceneInput& sc, const std::vector<int>& members, std::vec
 }
 
 // Enqueue every launch of a forward call.  d_views / d_counters are device
-// buffers with room for nviews views and 2 * plans.size() counters (work counters,
-// then hit counters); d_thit / d_hits hold one entry per ray; h_views is host
-// staging (pinned when owned by the context).  When views_ready is true the view
+// buffers with room for nviews views and kCountersPerPlan * plans.size() counters
+// (work counters, hit counters, shadow-queue counts, shadow work counters);
+// d_thit / d_hits / d_shadowq hold one entry per ray; h_views is host staging
+// (pinned when owned by the context).  When views_ready is true the view
 // table is already on the device (graph replay).
 nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_march_opts* opts,
                   const nd_gbuffer* out, cudaStream_t stream, const std::vector<Launch>& plans, DevView* d_views,
                   DevView* h_views, unsigned long long* d_counters, double* d_thit, nd::HitEntry* d_hits,
                   bool copy_views, int* kernel_used, cudaEvent_t* tev = nullptr,
                   const SceneInput& sc = SceneInput(), nd::DevScene* d_scenes = nullptr, float* d_accel = nullptr,
-                  nd::AccelJob* d_jobs = nullptr, std::vector<nd::AccelJob>* jobs_out = nullptr) {
+                  nd::AccelJob* d_jobs = nullptr, std::vector<nd::AccelJob>* jobs_out = nullptr,
+                  nd::ShadowEntry* d_shadowq = nullptr) {
   const int prec = (opts && opts->de_precision == 64) ? 64 : 32;
   // global output offsets in call order
   std::vector<int64_t> out_off(nviews + 1, 0);
@@ -433,7 +467,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
   }
   cudaError_t e = cudaMemsetAsync(ctx->d_stats, 0, sizeof(Stats), stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "clear stats");
-  e = cudaMemsetAsync(d_counters, 0, sizeof(unsigned long long) * 2 * plans.size(), stream);
+  e = cudaMemsetAsync(d_counters, 0, sizeof(unsigned long long) * kCountersPerPlan * plans.size(), stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "clear work counters");
   base = 0;
   int used = 0;
@@ -445,7 +479,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
     int64_t rays = 0;
     for (int k = 0; k < nv; ++k) rays += h_views[base + k].rays;
     if (rays > 0) {
-      const Tuned tu = tuned_for(L.key);
+      const Tuned tu = tuned_for(tune_key(ctx, L));
       int kernel = opts && opts->kernel ? opts->kernel : tu.kernel;
       const bool accel = plan_voxels[p] > 0;
       if (accel && kernel == ND_KERNEL_PLAIN) {
@@ -472,7 +506,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       a.deadline_ns = int64_t(wd) * 1000000;
       LaunchConfig c;
       c.kernel = kernel;
-      c.block = 128;
+      c.block = opts && opts->block ? opts->block : tu.block;
       c.blocks_per_sm = opts && opts->blocks_per_sm ? opts->blocks_per_sm : tu.blocks_per_sm;
       c.num_sms = ctx->num_sms;
       bool dir64 = false;
@@ -507,7 +541,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
         }
       } else {
         const bool batched = nv > 1;
-        LaunchFn fn = pick(L.table, kernel, prec, batched, dir64);
+        LaunchFn fn = pick(L.table, kernel, prec, batched, dir64, c.block);
         if (scn) {
           fn = prec == 64 ? T.scene_persistent_f64 : (dir64 ? T.scene_persistent_f32_dir64 : T.scene_persistent_f32);
           if (!fn) return fail(ctx, ND_ERR_UNSUPPORTED, "no scene kernels in this formula set");
@@ -520,6 +554,15 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
         if (defer) {
           a.hit_list = d_hits + ray_base;
           a.hit_count = reinterpret_cast<unsigned int*>(d_counters + plans.size() + p);
+        }
+        // the wavefront shadow pass: shadow rays queued by the surface pass and marched
+        // by the persistent shadow kernel (the accelerator's shadow skips run inline)
+        bool shadows = false;
+        for (int k = 0; k < nv; ++k) shadows |= nd::casts_shadow(h_views[base + k]);
+        if (defer && !accel && shadows && d_shadowq) {
+          a.shadow_queue = d_shadowq + ray_base;
+          a.shadow_count = reinterpret_cast<unsigned int*>(d_counters + 2 * plans.size() + p);
+          a.shadow_counter = d_counters + 3 * plans.size() + p;
         }
         e = fn(a, h_views[base], c, stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
@@ -537,6 +580,15 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
                    : (prec == 64 ? T.shade_f64_accel : T.shade_f32_accel);
         e = sf(a, h_views[base], c, want_trap ? 1 : 0, stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "shade pass launch");
+        if (a.shadow_queue) {
+          nd::ShadowFn hf = scn ? (prec == 64 ? T.scene_shadow_f64 : T.scene_shadow_f32)
+                                : (prec == 64 ? T.shadow_f64 : T.shadow_f32);
+          if (!hf) return fail(ctx, ND_ERR_UNSUPPORTED, "no shadow kernels in this formula set");
+          LaunchConfig sc2 = c;
+          sc2.blocks_per_sm = 0;
+          e = hf(a, sc2, stream);
+          if (e != cudaSuccess) return cuda_fail(ctx, e, "shadow pass launch");
+        }
       }
       if (tev) cudaEventRecord(tev[4 * p + 3], stream);
       used = kernel;
@@ -716,6 +768,11 @@ nd_status nd_ctx_create(int32_t device, nd_ctx** out) {
   ctx->device = device;
   e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) {
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, device);
+    if (e == cudaSuccess) ctx->gpu_name = prop.name;
+  }
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_stats, sizeof(Stats));
   if (e == cudaSuccess) e = cudaMemset(ctx->d_stats, 0, sizeof(Stats));
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->last_done, cudaEventDisableTiming);
@@ -736,6 +793,7 @@ nd_status nd_ctx_destroy(nd_ctx* ctx) {
   if (ctx->d_stats) cudaFree(ctx->d_stats);
   if (ctx->d_thit) cudaFree(ctx->d_thit);
   if (ctx->d_hits) cudaFree(ctx->d_hits);
+  if (ctx->d_shadowq) cudaFree(ctx->d_shadowq);
   if (ctx->d_scenes) cudaFree(ctx->d_scenes);
   if (ctx->d_accel) cudaFree(ctx->d_accel);
   if (ctx->d_accel_jobs) cudaFree(ctx->d_accel_jobs);
@@ -780,6 +838,8 @@ nd_status forward_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, c
   if (s != ND_OK) return s;
   if (opts && opts->de_precision != 0 && opts->de_precision != 32 && opts->de_precision != 64)
     return fail(ctx, ND_ERR_INVALID, "de_precision must be 32 or 64");
+  if (opts && opts->block != 0 && opts->block != 64 && opts->block != 128 && opts->block != 256)
+    return fail(ctx, ND_ERR_INVALID, "block must be 0, 64, 128 or 256");
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
   cudaStream_t st = (cudaStream_t)stream;
@@ -795,8 +855,19 @@ nd_status forward_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, c
       return cuda_fail(ctx, e, "staging event");
   if (ctx->staged_valid[half]) cudaEventSynchronize(ctx->staged[half]);
   if ((s = ensure_dev(ctx, &ctx->d_views, &ctx->views_cap, nviews, "view table")) != ND_OK) return s;
-  if ((s = ensure_dev(ctx, &ctx->d_counters, &ctx->counters_cap, 2 * int(plans.size()), "work counters")) != ND_OK)
+  if ((s = ensure_dev(ctx, &ctx->d_counters, &ctx->counters_cap, kCountersPerPlan * int(plans.size()),
+                      "work counters")) != ND_OK)
     return s;
+  bool any_shadow = false;
+  for (int i = 0; i < nviews; ++i) any_shadow |= views[i].shadow != 0;
+  if (any_shadow && ctx->shadowq_cap < total) {
+    if (ctx->d_shadowq) cudaFree(ctx->d_shadowq);
+    ctx->d_shadowq = nullptr;
+    ctx->shadowq_cap = 0;
+    e = cudaMalloc((void**)&ctx->d_shadowq, sizeof(nd::ShadowEntry) * size_t(total));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "shadow queue");
+    ctx->shadowq_cap = total;
+  }
   const bool want_trap = out->trap || out->iters;
   if (ctx->thit_cap < total) {
     if (ctx->d_thit) cudaFree(ctx->d_thit);
@@ -853,7 +924,7 @@ nd_status forward_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, c
     return s;
   s = enqueue(ctx, views, nviews, opts, out, st, plans, ctx->d_views, staging, ctx->d_counters, ctx->d_thit,
               ctx->d_hits, true, &kernel, ctx->tev.data(), sc, sc.nscenes > 0 ? ctx->d_scenes : nullptr,
-              ctx->d_accel, ctx->d_accel_jobs);
+              ctx->d_accel, ctx->d_accel_jobs, nullptr, any_shadow ? ctx->d_shadowq : nullptr);
   ctx->tev_plans = s == ND_OK ? int(plans.size()) : 0;
   if (s != ND_OK) return s;
   e = cudaEventRecord(ctx->last_done, st);
@@ -925,7 +996,11 @@ nd_status nd_last_stats(nd_ctx* ctx, nd_stats* out) {
 }
 
 // Times every candidate launch configuration on the given views (writing into
-// scratch_out) and keeps the fastest for this formula set.
+// scratch_out) and keeps the fastest for this call's formula sets.  Candidates: the
+// plain per-view launch, and the persistent march at 64, 128 and 256 threads per
+// block (FP32 DE; 128 otherwise) x as many blocks per SM as fit or two fewer x refill
+// thresholds 3, 4, 6, 8 and 12.  Each candidate runs once to warm up, then three
+// times with the L2 cache flushed before each run; its time is the median.
 nd_status nd_autotune(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const nd_gbuffer* scratch_out,
                       nd_tune_result* result) {
   std::vector<Launch> plans;
@@ -933,67 +1008,161 @@ nd_status nd_autotune(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, co
   nd_status s = prepare(ctx, views, nviews, scratch_out, &plans, &total);
   if (s != ND_OK) return s;
   cudaSetDevice(ctx->device);
+  bool any_accel = false;
+  bool block_axis = true;  // every plan has the FP32 block-size variants
+  for (int i = 0; i < nviews; ++i) any_accel |= nd::accel_voxels_of(views[i]) > 0;
+  for (const Launch& L : plans) block_axis &= L.table.persistent_f32_batched_b64 && L.table.persistent_f32_batched_b256;
+  struct Cand {
+    int kernel, block, per_sm, thr;
+  };
+  std::vector<Cand> cands;
+  if (!any_accel) cands.push_back({ND_KERNEL_PLAIN, 128, 0, 1});  // the accelerator runs on the persistent kernel
+  const int blocks[3] = {64, 128, 256};
+  for (int b : blocks) {
+    if (b != 128 && !block_axis) continue;
+    for (int per_sm : {0, -2})
+      for (int thr : {3, 4, 6, 8, 12}) cands.push_back({ND_KERNEL_PERSISTENT, b, per_sm, thr});
+  }
   cudaStream_t st;
   cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "stream");
-  cudaEvent_t a, b;
-  cudaEventCreate(&a);
-  cudaEventCreate(&b);
-  struct Cand {
-    int kernel, per_sm, thr;
-  };
-  std::vector<Cand> cands;
-  bool any_accel = false;
-  for (int i = 0; i < nviews; ++i) any_accel |= nd::accel_voxels_of(views[i]) > 0;
-  if (!any_accel) cands.push_back({ND_KERNEL_PLAIN, 0, 1});  // the accelerator runs on the persistent kernel
-  for (int per_sm : {0, 4, 8})
-    for (int thr : {1, 4, 8, 16, 24})
-      cands.push_back({ND_KERNEL_PERSISTENT, per_sm, thr});
+  // a buffer larger than the L2 cache, written before every timed run
+  const size_t flush_bytes = size_t(256) << 20;
+  void* flush = nullptr;
+  e = cudaMalloc(&flush, flush_bytes);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(st);
+    return cuda_fail(ctx, e, "autotune L2 flush buffer");
+  }
+  cudaEvent_t ev[2];
+  cudaEventCreate(&ev[0]);
+  cudaEventCreate(&ev[1]);
   double best = 1e30;
   Cand bc = cands[any_accel ? 0 : 1];
   for (const Cand& c : cands) {
     nd_march_opts o;
     memset(&o, 0, sizeof(o));
     o.kernel = c.kernel;
+    o.block = c.block;
     o.blocks_per_sm = c.per_sm;
     o.refill_threshold = c.thr;
-    float ms = 0;
     s = nd_march_forward(ctx, views, nviews, &o, scratch_out, st);  // warm-up
     if (s != ND_OK) break;
-    cudaEventRecord(a, st);
-    s = nd_march_forward(ctx, views, nviews, &o, scratch_out, st);
-    if (s != ND_OK) break;
-    cudaEventRecord(b, st);
-    e = cudaEventSynchronize(b);
-    if (e != cudaSuccess) {
-      s = cuda_fail(ctx, e, "autotune run");
-      break;
+    float runs[3];
+    for (int r = 0; r < 3 && s == ND_OK; ++r) {
+      cudaMemsetAsync(flush, r, flush_bytes, st);
+      cudaEventRecord(ev[0], st);
+      s = nd_march_forward(ctx, views, nviews, &o, scratch_out, st);
+      cudaEventRecord(ev[1], st);
+      e = cudaEventSynchronize(ev[1]);
+      if (s == ND_OK && e != cudaSuccess) s = cuda_fail(ctx, e, "autotune run");
+      if (s == ND_OK) cudaEventElapsedTime(&runs[r], ev[0], ev[1]);
     }
-    cudaEventElapsedTime(&ms, a, b);
-    if (ms < best) {
-      best = ms;
+    if (s != ND_OK) break;
+    std::sort(runs, runs + 3);
+    if (runs[1] < best) {
+      best = runs[1];
       bc = c;
     }
   }
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  cudaFree(flush);
   cudaStreamDestroy(st);
   if (s != ND_OK) return s;
   Tuned t;
   t.kernel = bc.kernel;
+  t.block = bc.block;
   t.blocks_per_sm = bc.per_sm;
   t.refill_threshold = bc.thr;
+  t.rays_per_s = best > 0 ? double(total) / (best * 1e-3) : 0.0;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    for (const Launch& L : plans) g_tuned[L.key] = t;
+    for (const Launch& L : plans) g_tuned[tune_key(ctx, L)] = t;
   }
   if (result) {
     result->kernel = t.kernel;
-    result->block = 128;
-    result->blocks_per_sm = t.blocks_per_sm;
+    result->block = t.block;
+    // the blocks per SM the persistent march runs with (as many as fit, or fewer)
+    int resident = 0;
+    if (t.kernel == ND_KERNEL_PERSISTENT && !plans.empty()) {
+      const KernelTable& T = plans[0].table;
+      nd::ResidentFn rf = t.block == 64 ? T.resident_b64 : (t.block == 256 ? T.resident_b256 : T.resident_b128);
+      if (rf) resident = rf(t.blocks_per_sm);
+    }
+    result->blocks_per_sm = resident;
     result->refill_threshold = t.refill_threshold;
-    result->rays_per_s = best > 0 ? double(total) / (best * 1e-3) : 0.0;
+    result->rays_per_s = t.rays_per_s;
   }
+  return ND_OK;
+}
+
+// The tuning cache on disk: one JSON array of the tuned entries of every GPU and
+// formula set (key: GPU name | formula set | hash of the formula sources).
+nd_status nd_tune_cache_save(const char* path) {
+  if (!path) return ND_ERR_INVALID;
+  std::string out = "[\n";
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    bool first = true;
+    for (const auto& kv : g_tuned) {
+      std::string key;
+      for (char ch : kv.first) {
+        if (ch == '"' || ch == '\\') key += '\\';
+        key += ch;
+      }
+      char buf[512];
+      snprintf(buf, sizeof(buf),
+               "%s {\"key\": \"%s\", \"kernel\": %d, \"block\": %d, \"blocks_per_sm\": %d, "
+               "\"refill_threshold\": %d, \"rays_per_s\": %.6g}",
+               first ? "" : ",\n", key.c_str(), kv.second.kernel, kv.second.block, kv.second.blocks_per_sm,
+               kv.second.refill_threshold, kv.second.rays_per_s);
+      out += buf;
+      first = false;
+    }
+  }
+  out += "\n]\n";
+  FILE* f = fopen(path, "wb");
+  if (!f) return ND_ERR_INVALID;
+  const bool ok = fwrite(out.data(), 1, out.size(), f) == out.size();
+  return (fclose(f) == 0 && ok) ? ND_OK : ND_ERR_INVALID;
+}
+
+nd_status nd_tune_cache_load(const char* path, int32_t* loaded) {
+  if (loaded) *loaded = 0;
+  if (!path) return ND_ERR_INVALID;
+  FILE* f = fopen(path, "rb");
+  if (!f) return ND_ERR_NOT_FOUND;
+  std::string text;
+  char buf[4096];
+  size_t n;
+  while ((n = fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, n);
+  fclose(f);
+  nd_json::JVal root;
+  nd_json::JsonParser p(text.data(), text.size());
+  if (!p.parse(&root) || root.kind != nd_json::JVal::ARR) return ND_ERR_INVALID;
+  int count = 0;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (const nd_json::JVal& e : root.arr) {
+    const nd_json::JVal* key = e.get("key");
+    if (!key || key->kind != nd_json::JVal::STR) continue;
+    auto num = [&](const char* k, double d) {
+      const nd_json::JVal* v = e.get(k);
+      return v && v->kind == nd_json::JVal::NUM ? v->num : d;
+    };
+    Tuned t;
+    t.kernel = int(num("kernel", ND_KERNEL_PERSISTENT));
+    t.block = int(num("block", 128));
+    t.blocks_per_sm = int(num("blocks_per_sm", 0));
+    t.refill_threshold = int(num("refill_threshold", 6));
+    t.rays_per_s = num("rays_per_s", 0.0);
+    if ((t.kernel != ND_KERNEL_PLAIN && t.kernel != ND_KERNEL_PERSISTENT) ||
+        (t.block != 64 && t.block != 128 && t.block != 256) || t.refill_threshold < 1 || t.refill_threshold > 32)
+      continue;
+    g_tuned[key->str] = t;
+    ++count;
+  }
+  if (loaded) *loaded = count;
   return ND_OK;
 }
 
@@ -1018,9 +1187,14 @@ nd_status graph_capture_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nvi
   g->ctx = ctx;
   g->trap = out->trap || out->iters;
   cudaError_t e = cudaMalloc((void**)&g->d_views, sizeof(DevView) * size_t(nviews));
-  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_counters, sizeof(unsigned long long) * 2 * plans.size());
+  if (e == cudaSuccess)
+    e = cudaMalloc((void**)&g->d_counters, sizeof(unsigned long long) * kCountersPerPlan * plans.size());
   if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_thit, sizeof(double) * size_t(std::max<int64_t>(total, 1)));
   if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_hits, sizeof(nd::HitEntry) * size_t(std::max<int64_t>(total, 1)));
+  bool any_shadow = false;
+  for (int i = 0; i < nviews; ++i) any_shadow |= views[i].shadow != 0;
+  if (e == cudaSuccess && any_shadow)
+    e = cudaMalloc((void**)&g->d_shadowq, sizeof(nd::ShadowEntry) * size_t(std::max<int64_t>(total, 1)));
   int64_t voxels = 0;
   int accel_views = 0;
   for (int i = 0; i < nviews; ++i) {
@@ -1052,7 +1226,7 @@ nd_status graph_capture_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nvi
     return cuda_fail(ctx, e, "begin capture");
   }
   s = enqueue(ctx, views, nviews, opts, out, cap, plans, g->d_views, hv.data(), g->d_counters, g->d_thit,
-              g->d_hits, false, nullptr, nullptr, sc, g->d_scenes, g->d_accel, g->d_accel_jobs, &jobs);
+              g->d_hits, false, nullptr, nullptr, sc, g->d_scenes, g->d_accel, g->d_accel_jobs, &jobs, g->d_shadowq);
   cudaGraph_t gr = nullptr;
   e = cudaStreamEndCapture(cap, &gr);
   cudaStreamDestroy(cap);
@@ -1126,6 +1300,7 @@ nd_status nd_graph_destroy(nd_graph* g) {
   if (g->d_counters) cudaFree(g->d_counters);
   if (g->d_thit) cudaFree(g->d_thit);
   if (g->d_hits) cudaFree(g->d_hits);
+  if (g->d_shadowq) cudaFree(g->d_shadowq);
   if (g->d_accel) cudaFree(g->d_accel);
   if (g->d_accel_jobs) cudaFree(g->d_accel_jobs);
   if (g->d_scenes) cudaFree(g->d_scenes);

@@ -52,6 +52,8 @@ _SIGNATURES = {
                                             C.POINTER(C.c_int32), C.POINTER(abi.nd_scene_desc), C.c_int32,
                                             C.POINTER(abi.nd_march_opts), C.POINTER(abi.nd_gbuffer), C.c_void_p,
                                             C.POINTER(C.c_void_p)]),
+    "nd_tune_cache_save": (C.c_int32, [C.c_char_p]),
+    "nd_tune_cache_load": (C.c_int32, [C.c_char_p, C.POINTER(C.c_int32)]),
     "nd_graph_launch": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "nd_graph_destroy": (C.c_int32, [C.c_void_p]),
     "nd_sizeof": (C.c_size_t, [C.c_char_p]),
@@ -282,9 +284,9 @@ class GBuffer:
 
 
 def make_opts(kernel=abi.ND_KERNEL_AUTO, blocks_per_sm=0, refill_threshold=0, de_precision=32, watchdog_ms=0,
-              accel_chain=0):
+              accel_chain=0, block=0):
     o = abi.nd_march_opts()
-    o.kernel, o.blocks_per_sm, o.refill_threshold = kernel, blocks_per_sm, refill_threshold
+    o.kernel, o.blocks_per_sm, o.refill_threshold, o.block = kernel, blocks_per_sm, refill_threshold, block
     o.de_precision, o.watchdog_ms, o.accel_chain = de_precision, watchdog_ms, accel_chain
     return o
 
@@ -454,6 +456,22 @@ class Context:
         st = self.lib.nd_autotune(self.handle, arr, len(views), C.byref(g), C.byref(r))
         self._check(st, "nd_autotune")
         return r
+
+    @staticmethod
+    def tune_cache_save(path: str):
+        """nd_tune_cache_save: the autotuner's winners (every context, every GPU) to a JSON file."""
+        st = load_library().nd_tune_cache_save(path.encode())
+        if st != abi.ND_OK:
+            raise NDError(st, f"nd_tune_cache_save({path!r})")
+
+    @staticmethod
+    def tune_cache_load(path: str) -> int:
+        """nd_tune_cache_load: read winners saved earlier; returns the entries read."""
+        n = C.c_int32()
+        st = load_library().nd_tune_cache_load(path.encode(), C.byref(n))
+        if st != abi.ND_OK:
+            raise NDError(st, f"nd_tune_cache_load({path!r})")
+        return n.value
 
     def capture(self, views, gbuf: GBuffer, opts=None, stream=None) -> "Graph":
         arr = (abi.nd_view_desc * len(views))(*views)

@@ -46,9 +46,10 @@ STEPS = (1e-5, 3e-5, 1e-6)  # the reference step first
 CONVERGED = 1e-4      # FD(1e-5) vs FD(3e-5) and FD(1e-6), relative
 PER_RAY_TOL = 1e-3    # adjoint vs converged FD, relative, per ray
 SUM_TOL = 1e-3        # sum over converged rays, relative to the sum of |FD|
-# The FP32 adjoint: its DE carries ~1e-3 relative rounding near the surface, and it
-# cannot tell jumps of the DE below 1e-2 of eps from roots (see nd_adjoint.cuh)
-SUM_TOL_FP32 = 1e-2
+# The FP32 adjoint (the one the differentiation benchmark times) is held to the
+# same 1e-3 relative target on its median and on the sum over converged rays; its DE
+# carries ~1e-3 relative rounding near the surface, so single rays may exceed it
+SUM_TOL_FP32 = 1e-3
 NAMES = ("power", "bailout", "yaw", "pitch", "dist")
 
 
@@ -207,7 +208,10 @@ def test_adjoint_fp32_matches_converged_fd_sum(study):
         assert median <= 1e-3, f"{name}: median relative error {median:.2e}"
         assert sum_err <= SUM_TOL_FP32, f"{name}: sum over converged rays off by {sum_err:.2e}"
     # the production path: FP32 forward, FP32 adjoint (hit distances differ by the FP32 DE's error)
-    _compare(study, _per_ray(study, study["g32"], 32), "fp32 forward + fp32 adjoint")
+    rows = _compare(study, _per_ray(study, study["g32"], 32), "fp32 forward + fp32 adjoint")
+    for name, n, within, median, sum_err in rows:
+        assert median <= 1e-3, f"fp32 forward: {name}: median relative error {median:.2e}"
+        assert sum_err <= SUM_TOL_FP32, f"fp32 forward: {name}: sum over converged rays off by {sum_err:.2e}"
 
 
 def test_bailout_gradient_is_zero(study):
