@@ -47,6 +47,14 @@ __device__ __forceinline__ void flush_stats(Stats* s, unsigned long long rays, u
 template <class T> struct MinBlocks {
   static constexpr int value = sizeof(T) == 4 ? 7 : 4;
 };
+// The batched FP32 march that defers its shading (the forward calls) carries no
+// normal or shadow state and fits in fewer registers.
+#ifndef ND_MARCH_MIN_BLOCKS_F32
+#define ND_MARCH_MIN_BLOCKS_F32 7
+#endif
+template <class T, bool kBatched, bool kDefer> struct MarchBlocks {
+  static constexpr int value = (sizeof(T) == 4 && kBatched && kDefer) ? ND_MARCH_MIN_BLOCKS_F32 : MinBlocks<T>::value;
+};
 
 // --------------------------------------------------------------- plain kernel
 // The reference's per-pixel program as a plain per-view launch: one thread per
@@ -96,9 +104,12 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value) plain_kernel(const _
 
 // kBlock: threads per block (the autotuner's block-size axis); every block size is
 // compiled for the same threads per SM, and so the same registers per thread.
+// kDefer: hit rays end at their hit and go to the hit list for the surface pass (the
+// forward calls); without it (the no-allocation entry point, which has no per-ray
+// scratch) the normal and shadow phases run inside the march.
 template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, bool kAccel = false,
-          int kBlock = 128>
-__global__ void __launch_bounds__(kBlock, MinBlocks<T>::value * 128 / kBlock)
+          int kBlock = 128, bool kDefer = true>
+__global__ void __launch_bounds__(kBlock, MarchBlocks<T, kBatched, kDefer>::value * 128 / kBlock)
     persistent_kernel(const __grid_constant__ LaunchArgs a, const __grid_constant__ DevView single) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -117,7 +128,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::value * 128 / kBlock)
   const int32_t total = int32_t(a.total_rays);  // < 2^31 (checked by the host)
   WarpRuns runs;  // warp-uniform
   const int thr = a.refill_threshold;
-  const bool defer = a.hit_list != nullptr;
+  constexpr bool defer = kDefer;
   // Finished rays keep their lane until the next refill: their outputs are written
   // then, all together, instead of in the pass that ends each ray.
   auto retire = [&]() {
@@ -125,20 +136,25 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::value * 128 / kBlock)
     uint32_t hit_evals = 0;
     if (L.item >= 0 && L.phase == PH_DONE) {
       const DevView& v = kBatched ? a.views[L.view] : single;
-      L.flush(v, a.out, a.t_hit);
+      if constexpr (kDefer) {
+        L.flush_deferred(v, a.out, a.t_hit);
+        ev_m += L.evals;
+        if (L.hit) {
+          hit_item = L.item;
+          hit_evals = L.evals;
+        }
+      } else {
+        L.flush(v, a.out, a.t_hit);
+        const uint32_t taps = L.hit ? normal_taps(v) : 0u;
+        ev_m += L.mev;
+        ev_n += taps;
+        ev_s += L.evals - L.mev - taps;
+      }
       ++rays;
       hits += L.hit ? 1 : 0;
-      const uint32_t taps = (L.hit && !defer) ? normal_taps(v) : 0u;
-      ev_m += L.mev;
-      ev_n += taps;
-      ev_s += L.evals - L.mev - taps;
-      if (defer && L.hit) {
-        hit_item = L.item;
-        hit_evals = L.evals;
-      }
       L.item = -1;
     }
-    if (defer) {
+    if constexpr (defer) {
       // append the retired hits to the shade pass's list, one atomic per warp
       const unsigned hm = __ballot_sync(full, hit_item >= 0);
       if (hm) {
@@ -199,7 +215,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::value * 128 / kBlock)
       }
       if (probe && L.phase != PH_DONE) {
         const DEOut<T> de = view_de<Set, T, false, kScenes>(v, to_t<T>(L.sample_pos(v)), a.scenes);
-        L.advance(v, de, a.out, a.t_hit, defer);
+        L.template advance<kDefer>(v, de, a.out, a.t_hit, kDefer);
       }
     }
   }
@@ -405,12 +421,14 @@ template <class K> cudaError_t resident_blocks(K kernel, int block, int want, in
 }
 
 template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, bool kAccel = false,
-          int kBlock = 128>
+          int kBlock = 128, bool kDefer = true>
 cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const LaunchConfig& c, cudaStream_t s) {
   const int block = kBlock;
+  // the deferred march needs the hit list, the inline one must not get one
+  if ((a.hit_list != nullptr) != kDefer || (kDefer && !a.t_hit)) return cudaErrorInvalidValue;
   int per_sm = 0;
-  cudaError_t e = resident_blocks(persistent_kernel<Set, T, kDir64, kBatched, kScenes, kAccel, kBlock>, block,
-                                  c.blocks_per_sm, &per_sm);
+  cudaError_t e = resident_blocks(persistent_kernel<Set, T, kDir64, kBatched, kScenes, kAccel, kBlock, kDefer>,
+                                  block, c.blocks_per_sm, &per_sm);
   if (e != cudaSuccess) return e;
   int64_t grid = int64_t(per_sm) * c.num_sms;
   const int64_t needed = (a.total_rays + block - 1) / block;
@@ -421,7 +439,8 @@ cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const 
   LaunchArgs b = a;
   const int64_t warps = grid * (block / 32);
   b.chunk = int32_t(std::max<int64_t>(1, std::min<int64_t>(64, a.total_rays / (warps * 4))));
-  persistent_kernel<Set, T, kDir64, kBatched, kScenes, kAccel, kBlock><<<unsigned(grid), block, 0, s>>>(b, single);
+  persistent_kernel<Set, T, kDir64, kBatched, kScenes, kAccel, kBlock, kDefer><<<unsigned(grid), block, 0, s>>>(b,
+                                                                                                         single);
   return cudaGetLastError();
 }
 
@@ -603,10 +622,14 @@ typedef cudaError_t (*DePointsFn)(const DevView&, int64_t, const double*, double
 struct KernelTable {
   LaunchFn plain_f32, plain_f32_dir64, plain_f64;
   LaunchFn persistent_f32, persistent_f32_batched, persistent_f32_dir64, persistent_f32_dir64_batched;
-  // the FP32 march at 64 and 256 threads per block (the default is 128), single and batched
+  // the FP32 march at 64 and 256 threads per block (the default is 128), single and
+  // batched (formula groups only; null in single-formula tables)
   LaunchFn persistent_f32_b64, persistent_f32_b256, persistent_f32_batched_b64, persistent_f32_batched_b256;
   ResidentFn resident_b64, resident_b128, resident_b256;
   LaunchFn persistent_f64, persistent_f64_batched;
+  // the march with its normal and shadow phases inline (no hit list): the
+  // no-allocation entry point
+  LaunchFn inline_f32, inline_f32_batched, inline_f32_dir64, inline_f32_dir64_batched, inline_f64, inline_f64_batched;
   ShadeFn shade_f32, shade_f32_batched, shade_f32_dir64, shade_f32_dir64_batched, shade_f64, shade_f64_batched;
   DePointsFn de_points_f32, de_points_f64;
   AdjointFn adjoint_f32, adjoint_f32_batched, adjoint_f64, adjoint_f64_batched;
@@ -667,13 +690,25 @@ template <class Set, bool kWithScenes = false> KernelTable make_kernel_table() {
   t.plain_f32 = &launch_plain<Set, float, false>;
   t.plain_f32_dir64 = &launch_plain<Set, float, true>;
   t.plain_f64 = &launch_plain<Set, double, true>;
-  t.persistent_f32_b64 = &launch_persistent<Set, float, false, false, false, false, 64>;
-  t.persistent_f32_b256 = &launch_persistent<Set, float, false, false, false, false, 256>;
-  t.persistent_f32_batched_b64 = &launch_persistent<Set, float, false, true, false, false, 64>;
-  t.persistent_f32_batched_b256 = &launch_persistent<Set, float, false, true, false, false, 256>;
-  t.resident_b64 = &resident_f32_batched<Set, 64>;
+  if constexpr (kWithScenes) {
+    t.persistent_f32_b64 = &launch_persistent<Set, float, false, false, false, false, 64>;
+    t.persistent_f32_b256 = &launch_persistent<Set, float, false, false, false, false, 256>;
+    t.persistent_f32_batched_b64 = &launch_persistent<Set, float, false, true, false, false, 64>;
+    t.persistent_f32_batched_b256 = &launch_persistent<Set, float, false, true, false, false, 256>;
+    t.resident_b64 = &resident_f32_batched<Set, 64>;
+    t.resident_b256 = &resident_f32_batched<Set, 256>;
+  } else {
+    t.persistent_f32_b64 = t.persistent_f32_b256 = t.persistent_f32_batched_b64 = t.persistent_f32_batched_b256 =
+        nullptr;
+    t.resident_b64 = t.resident_b256 = nullptr;
+  }
   t.resident_b128 = &resident_f32_batched<Set, 128>;
-  t.resident_b256 = &resident_f32_batched<Set, 256>;
+  t.inline_f32 = &launch_persistent<Set, float, false, false, false, false, 128, false>;
+  t.inline_f32_batched = &launch_persistent<Set, float, false, true, false, false, 128, false>;
+  t.inline_f32_dir64 = &launch_persistent<Set, float, true, false, false, false, 128, false>;
+  t.inline_f32_dir64_batched = &launch_persistent<Set, float, true, true, false, false, 128, false>;
+  t.inline_f64 = &launch_persistent<Set, double, true, false, false, false, 128, false>;
+  t.inline_f64_batched = &launch_persistent<Set, double, true, true, false, false, 128, false>;
   t.persistent_f32 = &launch_persistent<Set, float, false, false>;
   t.persistent_f32_batched = &launch_persistent<Set, float, false, true>;
   t.persistent_f32_dir64 = &launch_persistent<Set, float, true, false>;

@@ -947,6 +947,27 @@ template <class T, bool kDir64> struct Lane {
     pending = 0;
   }
 
+  // The outputs of a miss (write_finish with hit = false and visibility 1).
+  ND_DEV_INLINE void write_miss(const DevView& v, const nd_gbuffer& g, double* t_hit) const {
+    RayResult r;
+    r.hit = false;
+    r.t = t;
+    r.steps = uint32_t(v.max_steps);
+    r.evals = evals;
+    r.nx = r.ny = r.nz = 0.0f;
+    r.shadow = 1.0f;
+    r.shade = 0.0f;
+    write_result(g, t_hit, v.out_offset + (int64_t(item) - v.ray_offset), r);
+  }
+
+  // flush for a march that defers all shading (advance<true>): a lane that finished
+  // without a hit is a miss, one with a hit waits for the surface pass.
+  ND_DEV_INLINE void flush_deferred(const DevView& v, const nd_gbuffer& g, double* t_hit) {
+    if (pending == 1) write_miss(v, g, t_hit);
+    else if (pending == 2) write_march(v, g, t_hit);
+    pending = 0;
+  }
+
   ND_DEV_INLINE void begin_normal(double at) {
     mev = evals;
     t = at;
@@ -976,18 +997,29 @@ template <class T, bool kDir64> struct Lane {
     if (g.depth64) g.depth64[r] = t;
   }
 
+  template <bool kDeferOnly>
   ND_DEV_INLINE void hit_at(const DevView& v, double at, const nd_gbuffer& g, double* t_hit, bool defer) {
-    begin_normal(at);
-    if (defer) finish_march(v, g, t_hit);
+    if constexpr (kDeferOnly) {
+      // the ray ends at its hit; the normal and shadow phases are the surface pass's
+      t = at;
+      hit = true;
+      finish_march(v, g, t_hit);
+    } else {
+      begin_normal(at);
+      if (defer) finish_march(v, g, t_hit);
+    }
   }
 
   // Consume one DE result; sets phase = PH_DONE (outputs written) when finished.
   // With defer_shade a hit ends the ray (finish_march) instead of entering PH_NORMAL.
+  // kDeferOnly: a march that always defers its shading (every lane is in PH_MARCH or
+  // done), compiled without the normal and shadow phases.
+  template <bool kDeferOnly = false>
   ND_DEV_INLINE void advance(const DevView& v, const DEOut<T>& de, const nd_gbuffer& g, double* t_hit,
                              bool defer_shade = false) {
     ++evals;
     const double d = double(de.d);
-    if (phase == PH_MARCH) {
+    if (kDeferOnly || phase == PH_MARCH) {
       // one pass of march_to's sample loop (tpl:1881-1960); a = lo, b = hi
       const bool on_hit = v.verify == 0;
       const int refine_budget = on_hit ? 0 : v.refine;
@@ -1003,7 +1035,7 @@ template <class T, bool kDir64> struct Lane {
           a = st;
         }
         ++k;
-        if ((b - a <= e && !v.exact_hit) || k >= bisect_budget) hit_at(v, b, g, t_hit, defer_shade);
+        if ((b - a <= e && !v.exact_hit) || k >= bisect_budget) hit_at<kDeferOnly>(v, b, g, t_hit, defer_shade);
         else if (n >= v.max_samples) finish(v, g, t_hit, 1.0f);  // march_to's loop ran out: a miss
         return;
       }
@@ -1016,7 +1048,7 @@ template <class T, bool kDir64> struct Lane {
           if (n >= v.max_samples) finish(v, g, t_hit, 1.0f);
           return;
         }
-        hit_at(v, st, g, t_hit, defer_shade);
+        hit_at<kDeferOnly>(v, st, g, t_hit, defer_shade);
         return;
       }
       if (probing && on_hit) {
@@ -1053,6 +1085,7 @@ template <class T, bool kDir64> struct Lane {
       if (n >= v.max_samples) finish(v, g, t_hit, 1.0f);
       return;
     }
+    if constexpr (kDeferOnly) return;
     if (phase == PH_NORMAL) {
       normal_accumulate(v, k, d, gx, gy, gz);
       ++k;

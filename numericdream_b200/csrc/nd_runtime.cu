@@ -1801,7 +1801,12 @@ extern "C" nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t
     c.block = 128;
     c.blocks_per_sm = opts ? opts->blocks_per_sm : 0;
     c.num_sms = sms;
-    LaunchFn fn = pick(tables[l], ND_KERNEL_PERSISTENT, prec, n > 1, dir64);
+    // the inline march (normal and shadow phases in the march: no hit list here)
+    const KernelTable& T = tables[l];
+    const bool batched = n > 1;
+    LaunchFn fn = prec == 64 ? (batched ? T.inline_f64_batched : T.inline_f64)
+                             : dir64 ? (batched ? T.inline_f32_dir64_batched : T.inline_f32_dir64)
+                                     : (batched ? T.inline_f32_batched : T.inline_f32);
     e = fn(a, host[first[l]], c, st);
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "kernel launch");
   }
