@@ -11,7 +11,9 @@
  *       + assembleShaderSource (fractal_renderer.zig:725-760) + stampFormulaCodes (:2882):
  *       a formula source becomes an integer formula code.  Formula files are
  *       translated from WGSL to CUDA at build time; registering a source looks up
- *       its compiled code by the source hash, as CodeTable.find does (:585-590).
+ *       its compiled code by the source hash, as CodeTable.find does (:585-590), and
+ *       a source the build did not compile is translated and compiled then, as the
+ *       reference's compileWorker does (:1609).
  *   nd_formula_params
  *       formula.parseFormulaParams / CustomParam  (src/app/formula.zig:6-13, :147-157)
  *   nd_view_desc
@@ -271,6 +273,16 @@ const char* nd_status_string(nd_status s);
 nd_status nd_formula_count(int32_t* n);
 nd_status nd_formula_find(const char* name, nd_formula_id* out);
 nd_status nd_formula_name(nd_formula_id id, char* out, size_t out_len);
+/* A formula source (WGSL) to a formula id.  A source compiled into the build (same
+ * bytes) is found by its hash.  Any other source is compiled now: the build's
+ * translator and nvcc turn it into a small library of its forward kernels (march,
+ * surface and shadow passes, DE at points; FP32 and FP64 DE; no accelerator, lite
+ * shading or adjoint for it), which is loaded and gets the next id (name
+ * "user_<hash>"); this takes seconds, like the reference's shader compile, so call it
+ * from a worker thread as the reference does.  Needs a Python interpreter with this
+ * package (ND_PYTHON, default python3) and nvcc; temporary files go under ND_RTC_DIR
+ * (default /tmp).  A source the translator or nvcc refuses returns ND_ERR_COMPILE
+ * with the message in err.  Thread-safe (one compile at a time). */
 nd_status nd_formula_register(const char* wgsl_src, size_t len, nd_formula_id* out, char* err, size_t err_len);
 nd_status nd_formula_params(nd_formula_id id, nd_param_info* out, int32_t* n);
 nd_status nd_view_defaults(nd_formula_id id, nd_view_desc* out);

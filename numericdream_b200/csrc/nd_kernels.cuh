@@ -6,6 +6,8 @@
 
 #include <cuda_runtime.h>
 
+#include <string.h>
+
 #include <algorithm>
 
 #include "nd_rayprog.h"
@@ -650,8 +652,12 @@ struct KernelTable {
   ShadowFn shadow_f32, shadow_f64, scene_shadow_f32, scene_shadow_f64;
 };
 
-template <class Set, bool kWithScenes = false> KernelTable make_kernel_table() {
+// kForwardOnly: the table of a formula compiled at run time (nd_formula_register):
+// the forward march, its surface and shadow passes and the DE at points, FP32 and
+// FP64; no accelerator, lite shading or adjoint (their entries are null).
+template <class Set, bool kWithScenes = false, bool kForwardOnly = false> KernelTable make_kernel_table() {
   KernelTable t;
+  memset(&t, 0, sizeof(t));
   if constexpr (kWithScenes) {
     t.scene_persistent_f32 = &launch_persistent<Set, float, false, true, true>;
     t.scene_persistent_f32_dir64 = &launch_persistent<Set, float, true, true, true>;
@@ -679,14 +685,16 @@ template <class Set, bool kWithScenes = false> KernelTable make_kernel_table() {
   }
   t.shadow_f32 = &launch_shadow<Set, float>;
   t.shadow_f64 = &launch_shadow<Set, double>;
-  t.lite_f32 = &launch_lite<Set, float, false>;
-  t.lite_f32_dir64 = &launch_lite<Set, float, true>;
-  t.accel_build_f32 = &launch_accel_build<Set, float, false>;
-  t.accel_build_f64 = &launch_accel_build<Set, double, false>;
-  t.persistent_f32_accel = &launch_persistent<Set, float, false, true, false, true>;
-  t.persistent_f64_accel = &launch_persistent<Set, double, true, true, false, true>;
-  t.shade_f32_accel = &launch_shade<Set, float, false, true, false, true>;
-  t.shade_f64_accel = &launch_shade<Set, double, true, true, false, true>;
+  if constexpr (!kForwardOnly) {
+    t.lite_f32 = &launch_lite<Set, float, false>;
+    t.lite_f32_dir64 = &launch_lite<Set, float, true>;
+    t.accel_build_f32 = &launch_accel_build<Set, float, false>;
+    t.accel_build_f64 = &launch_accel_build<Set, double, false>;
+    t.persistent_f32_accel = &launch_persistent<Set, float, false, true, false, true>;
+    t.persistent_f64_accel = &launch_persistent<Set, double, true, true, false, true>;
+    t.shade_f32_accel = &launch_shade<Set, float, false, true, false, true>;
+    t.shade_f64_accel = &launch_shade<Set, double, true, true, false, true>;
+  }
   t.plain_f32 = &launch_plain<Set, float, false>;
   t.plain_f32_dir64 = &launch_plain<Set, float, true>;
   t.plain_f64 = &launch_plain<Set, double, true>;
@@ -723,10 +731,12 @@ template <class Set, bool kWithScenes = false> KernelTable make_kernel_table() {
   t.shade_f64_batched = &launch_shade<Set, double, true, true>;
   t.de_points_f32 = &launch_de_points<Set, float>;
   t.de_points_f64 = &launch_de_points<Set, double>;
-  t.adjoint_f32 = &launch_adjoint<Set, float, false>;
-  t.adjoint_f32_batched = &launch_adjoint<Set, float, true>;
-  t.adjoint_f64 = &launch_adjoint<Set, double, false>;
-  t.adjoint_f64_batched = &launch_adjoint<Set, double, true>;
+  if constexpr (!kForwardOnly) {
+    t.adjoint_f32 = &launch_adjoint<Set, float, false>;
+    t.adjoint_f32_batched = &launch_adjoint<Set, float, true>;
+    t.adjoint_f64 = &launch_adjoint<Set, double, false>;
+    t.adjoint_f64_batched = &launch_adjoint<Set, double, true>;
+  }
   return t;
 }
 

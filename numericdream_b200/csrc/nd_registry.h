@@ -35,5 +35,11 @@ struct GroupEntry {
 
 extern const nd::FormulaEntry nd_formula_entries[];
 extern const int nd_formula_entry_count;
+
+// Every formula the library knows: the build-time table (ids 0 .. nd_formula_entry_count
+// - 1), then the formulas nd_formula_register compiled at run time.  nd_formula_at
+// returns nullptr for an id out of range.
+const nd::FormulaEntry* nd_formula_at(int id);
+int nd_formula_total();
 extern const nd::GroupEntry nd_group_entries[];
 extern const int nd_group_entry_count;

@@ -1,11 +1,14 @@
 // C-ABI implementation (include/nd_march.h): formula registry, contexts, view
 // validation, launch planning, statistics, autotuning and CUDA-graph capture.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 #include <stdarg.h>
+#include <stdlib.h>
 #include <stdio.h>
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <complex>
 #include <map>
 #include <mutex>
@@ -146,7 +149,7 @@ nd_status cuda_fail(nd_ctx* ctx, cudaError_t e, const char* what) {
 bool finite(double x) { return x == x && x < 1e300 && x > -1e300; }
 
 nd_status validate_view(nd_ctx* ctx, const nd_view_desc& v, int idx) {
-  if (v.formula < 0 || v.formula >= nd_formula_entry_count)
+  if (v.formula < 0 || v.formula >= nd_formula_total())
     return fail(ctx, ND_ERR_NOT_FOUND, "view %d: unknown formula id %d", idx, v.formula);
   if (v.width <= 0 || v.height <= 0 || v.tile_w < 0 || v.tile_h < 0 || v.tile_x < 0 || v.tile_y < 0 ||
       int64_t(v.tile_x) + v.tile_w > v.width || int64_t(v.tile_y) + v.tile_h > v.height)
@@ -203,7 +206,7 @@ struct Launch {
 std::string set_key(const std::vector<int>& formulas) {
   std::string k;
   for (int f : formulas) {
-    k += nd_formula_entries[f].name;
+    k += nd_formula_at(f)->name;
     k += "+";
   }
   return k;
@@ -232,7 +235,7 @@ std::vector<int> view_formulas(const nd_view_desc& v, int scene, const SceneInpu
 
 // de_iterations() of a formula at a view's parameters, clamped like the kernels'.
 double view_iterations(int formula, const float* params) {
-  const nd::FormulaEntry& f = nd_formula_entries[formula];
+  const nd::FormulaEntry& f = (*nd_formula_at(formula));
   if (!f.iterations) return 1.0;
   const int32_t n = f.iterations(params);
   return double(n < 1 ? 1 : (n > nd::kMaxIterations ? nd::kMaxIterations : n));
@@ -248,7 +251,7 @@ nd_status plan(nd_ctx* ctx, const nd_view_desc* views, int nviews, std::vector<L
   out->clear();
   if (distinct.size() == 1 && !any_scene) {
     Launch L;
-    L.table = nd_formula_entries[distinct[0]].kernels();
+    L.table = nd_formula_at(distinct[0])->kernels();
     L.members = distinct;
     for (int i = 0; i < nviews; ++i) {
       L.views.push_back(i);
@@ -316,14 +319,14 @@ nd_status plan(nd_ctx* ctx, const nd_view_desc* views, int nviews, std::vector<L
   }
   if (any_scene) {
     std::string names;
-    for (int f : distinct) names += std::string(names.empty() ? "" : ", ") + nd_formula_entries[f].name;
+    for (int f : distinct) names += std::string(names.empty() ? "" : ", ") + nd_formula_at(f)->name;
     return fail(ctx, ND_ERR_UNSUPPORTED, "the call's formulas (%s) are not in one compiled formula group "
                 "(build with ND_GROUPS)", names.c_str());
   }
   // otherwise one launch per formula
   for (int f : distinct) {
     Launch L;
-    L.table = nd_formula_entries[f].kernels();
+    L.table = nd_formula_at(f)->kernels();
     L.members = {f};
     for (int i = 0; i < nviews; ++i)
       if (views[i].formula == f) {
@@ -353,7 +356,7 @@ LaunchFn pick(const KernelTable& t, int kernel, int prec, bool batched, bool dir
 std::string tune_key(const nd_ctx* ctx, const Launch& L) {
   uint64_t h = 0xCBF29CE484222325ull;
   for (int f : L.members) {
-    const uint64_t x = nd_formula_entries[f].source_hash;
+    const uint64_t x = nd_formula_at(f)->source_hash;
     for (int b = 0; b < 8; ++b) {
       h ^= (x >> (8 * b)) & 0xffu;
       h *= 0x100000001B3ull;
@@ -536,6 +539,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
         // the plain baseline: one launch per view, one thread per ray
         for (int k = 0; k < nv; ++k) {
           LaunchFn fn = pick(L.table, kernel, prec, false, h_views[base + k].dir64 != 0);
+          if (!fn) return fail(ctx, ND_ERR_UNSUPPORTED, "no plain kernel for this formula set");
           e = fn(a, h_views[base + k], c, stream);
           if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
         }
@@ -564,6 +568,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
           a.shadow_count = reinterpret_cast<unsigned int*>(d_counters + 2 * plans.size() + p);
           a.shadow_counter = d_counters + 3 * plans.size() + p;
         }
+        if (!fn) return fail(ctx, ND_ERR_UNSUPPORTED, "no persistent kernel for this formula set");
         e = fn(a, h_views[base], c, stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
       }
@@ -578,6 +583,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
         if (accel)
           sf = scn ? (prec == 64 ? T.scene_shade_f64_accel : T.scene_shade_f32_accel)
                    : (prec == 64 ? T.shade_f64_accel : T.shade_f32_accel);
+        if (!sf) return fail(ctx, ND_ERR_UNSUPPORTED, "no shade kernel for this formula set");
         e = sf(a, h_views[base], c, want_trap ? 1 : 0, stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "shade pass launch");
         if (a.shadow_queue) {
@@ -627,11 +633,11 @@ nd_status prepare(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const 
                   ND_MAX_CARVES);
     for (int j = 0; j < S.instance_count; ++j) {
       const nd_instance_desc& in = S.instances[j];
-      if (in.formula < 0 || in.formula >= nd_formula_entry_count || in.mixin_count < 0 ||
+      if (in.formula < 0 || in.formula >= nd_formula_total() || in.mixin_count < 0 ||
           in.mixin_count > ND_MAX_MIXINS || in.combine_mode < ND_COMBINE_UNION || in.combine_mode > ND_COMBINE_SMOOTH_MIX)
         return fail(ctx, ND_ERR_INVALID, "scene %d instance %d: bad formula, mixin count or combine mode", k, j);
       for (int m = 0; m < in.mixin_count; ++m)
-        if (in.mixins[m].formula < 0 || in.mixins[m].formula >= nd_formula_entry_count)
+        if (in.mixins[m].formula < 0 || in.mixins[m].formula >= nd_formula_total())
           return fail(ctx, ND_ERR_INVALID, "scene %d instance %d mixin %d: bad formula", k, j, m);
     }
   }
@@ -639,6 +645,110 @@ nd_status prepare(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, const 
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------- run-time formulas
+// Formulas that nd_formula_register compiled at run time, after the build-time table.
+// An entry is written completely before the count that publishes it, and entries are
+// never removed (their libraries stay loaded), so readers need no lock.
+namespace {
+constexpr int kMaxRuntimeFormulas = 256;
+nd::FormulaEntry g_rt_entries[kMaxRuntimeFormulas];
+std::atomic<int> g_rt_count{0};
+std::mutex g_rt_mu;  // one compile at a time
+
+std::string shell_quote(const std::string& s) {
+  std::string q = "'";
+  for (char c : s) q += (c == '\'') ? std::string("'\\''") : std::string(1, c);
+  return q + "'";
+}
+
+// The compile worker: the build's translator and nvcc, run as a child process
+// (numericdream_b200/rtc.py beside this library) into a temporary directory, then the
+// resulting library loaded and its entry published.  ND_PYTHON names the Python
+// interpreter (default python3); ND_RTC_DIR the parent of the temporary directories
+// (default /tmp).
+nd_status runtime_compile(const char* src, size_t len, uint64_t hash, nd_formula_id* out, std::string* msg) {
+  std::lock_guard<std::mutex> lk(g_rt_mu);
+  const int have = g_rt_count.load(std::memory_order_acquire);
+  for (int i = 0; i < have; ++i)  // compiled by another thread while this one waited
+    if (g_rt_entries[i].source_hash == hash) {
+      *out = nd_formula_entry_count + i;
+      return ND_OK;
+    }
+  if (have >= kMaxRuntimeFormulas) {
+    *msg = "too many formulas compiled at run time (at most 256)";
+    return ND_ERR_COMPILE;
+  }
+  Dl_info info;
+  if (!dladdr(reinterpret_cast<void*>(&runtime_compile), &info) || !info.dli_fname) {
+    *msg = "cannot locate the library to find its formula compiler";
+    return ND_ERR_COMPILE;
+  }
+  std::string pkg = info.dli_fname;
+  pkg = pkg.substr(0, pkg.find_last_of('/'));
+  const std::string root = pkg.substr(0, pkg.find_last_of('/'));
+  const char* base = getenv("ND_RTC_DIR");
+  std::string tmpl = std::string(base && *base ? base : "/tmp") + "/nd_rtc_XXXXXX";
+  std::vector<char> dirbuf(tmpl.begin(), tmpl.end());
+  dirbuf.push_back(0);
+  if (!mkdtemp(dirbuf.data())) {
+    *msg = "cannot create a directory under " + tmpl;
+    return ND_ERR_COMPILE;
+  }
+  const std::string dir = dirbuf.data();
+  FILE* f = fopen((dir + "/formula.wgsl").c_str(), "wb");
+  if (!f || fwrite(src, 1, len, f) != len) {
+    if (f) fclose(f);
+    *msg = "cannot write the formula source to " + dir;
+    return ND_ERR_COMPILE;
+  }
+  fclose(f);
+  const char* py = getenv("ND_PYTHON");
+  const std::string cmd = "cd " + shell_quote(root) + " && " + shell_quote(py && *py ? py : "python3") +
+                          " -m numericdream_b200.rtc " + shell_quote(dir + "/formula.wgsl") + " " + shell_quote(dir) +
+                          " > " + shell_quote(dir + "/log.txt") + " 2>&1";
+  const int rc = system(cmd.c_str());
+  if (rc != 0) {
+    std::string text;
+    FILE* e = fopen((dir + "/error.txt").c_str(), "rb");
+    if (!e) e = fopen((dir + "/log.txt").c_str(), "rb");
+    if (e) {
+      char buf[1024];
+      size_t n;
+      while ((n = fread(buf, 1, sizeof(buf), e)) > 0 && text.size() < 8192) text.append(buf, n);
+      fclose(e);
+    }
+    *msg = text.empty() ? "the formula compiler failed (" + cmd + ")" : text;
+    return ND_ERR_COMPILE;
+  }
+  void* lib = dlopen((dir + "/formula.so").c_str(), RTLD_NOW | RTLD_LOCAL);
+  if (!lib) {
+    const char* de = dlerror();
+    *msg = std::string("cannot load the compiled formula: ") + (de ? de : "?");
+    return ND_ERR_COMPILE;
+  }
+  typedef const nd::FormulaEntry* (*EntryFn)();
+  EntryFn fn = reinterpret_cast<EntryFn>(dlsym(lib, "nd_rtc_entry"));
+  const nd::FormulaEntry* e = fn ? fn() : nullptr;
+  if (!e || e->source_hash != hash) {
+    *msg = "the compiled formula library does not match the source";
+    return ND_ERR_COMPILE;
+  }
+  g_rt_entries[have] = *e;
+  g_rt_count.store(have + 1, std::memory_order_release);
+  *out = nd_formula_entry_count + have;
+  return ND_OK;
+}
+}  // namespace
+
+const nd::FormulaEntry* nd_formula_at(int id) {
+  if (id >= 0 && id < nd_formula_entry_count) return &nd_formula_entries[id];
+  const int k = id - nd_formula_entry_count;
+  if (k >= 0 && k < g_rt_count.load(std::memory_order_acquire)) return &g_rt_entries[k];
+  return nullptr;
+}
+
+int nd_formula_total() { return nd_formula_entry_count + g_rt_count.load(std::memory_order_acquire); }
 
 extern "C" {
 
@@ -651,14 +761,14 @@ const char* nd_status_string(nd_status s) {
 
 nd_status nd_formula_count(int32_t* n) {
   if (!n) return ND_ERR_INVALID;
-  *n = nd_formula_entry_count;
+  *n = nd_formula_total();
   return ND_OK;
 }
 
 nd_status nd_formula_find(const char* name, nd_formula_id* out) {
   if (!name || !out) return ND_ERR_INVALID;
-  for (int i = 0; i < nd_formula_entry_count; ++i)
-    if (strcmp(nd_formula_entries[i].name, name) == 0) {
+  for (int i = 0; i < nd_formula_total(); ++i)
+    if (strcmp(nd_formula_at(i)->name, name) == 0) {
       *out = i;
       return ND_OK;
     }
@@ -666,17 +776,19 @@ nd_status nd_formula_find(const char* name, nd_formula_id* out) {
 }
 
 nd_status nd_formula_name(nd_formula_id id, char* out, size_t out_len) {
-  if (id < 0 || id >= nd_formula_entry_count) return ND_ERR_NOT_FOUND;
+  if (id < 0 || id >= nd_formula_total()) return ND_ERR_NOT_FOUND;
   if (!out || out_len == 0) return ND_ERR_INVALID;
-  copy_str(out, out_len, nd_formula_entries[id].name);
+  copy_str(out, out_len, nd_formula_at(id)->name);
   return ND_OK;
 }
 
-// The reference compiles a formula source into the scene's shader module and
-// reports errors into FormulaState.formula_error (formula.zig:73-77, 170-181).
-// Here sources are compiled at build time; registering a source checks the
-// contract functions like missingContractFn and then finds the compiled code by
-// the source hash (CodeTable.find, fractal_renderer.zig:585-590).
+// The reference compiles a formula source into the scene's shader module on a worker
+// thread (rebuildAsync, fractal_renderer.zig:2951; compileWorker :1609) and reports
+// errors into FormulaState.formula_error (formula.zig:73-77, 170-181).  Registering a
+// source checks the contract functions like missingContractFn, then finds compiled
+// code by the source hash (CodeTable.find, fractal_renderer.zig:585-590): the
+// build-time formulas, then those compiled earlier at run time.  A new source is
+// compiled now (runtime_compile) and gets the next id.
 nd_status nd_formula_register(const char* src, size_t len, nd_formula_id* out, char* err, size_t err_len) {
   if (!src || !out) {
     copy_str(err, err_len, "null argument");
@@ -695,22 +807,22 @@ nd_status nd_formula_register(const char* src, size_t len, nd_formula_id* out, c
     return ND_ERR_COMPILE;
   }
   const uint64_t h = fnv1a64(src, len);
-  for (int i = 0; i < nd_formula_entry_count; ++i)
-    if (nd_formula_entries[i].source_hash == h) {
+  for (int i = 0; i < nd_formula_total(); ++i)
+    if (nd_formula_at(i)->source_hash == h) {
       *out = i;
       copy_str(err, err_len, "");
       return ND_OK;
     }
-  copy_str(err, err_len,
-           "formula source is not compiled into this build: add the file to the build's formula directory "
-           "(ND_FORMULA_DIRS) and rebuild");
-  return ND_ERR_COMPILE;
+  std::string msg;
+  const nd_status st = runtime_compile(src, len, h, out, &msg);
+  copy_str(err, err_len, msg);
+  return st;
 }
 
 nd_status nd_formula_params(nd_formula_id id, nd_param_info* out, int32_t* n) {
-  if (id < 0 || id >= nd_formula_entry_count) return ND_ERR_NOT_FOUND;
+  if (id < 0 || id >= nd_formula_total()) return ND_ERR_NOT_FOUND;
   if (!n) return ND_ERR_INVALID;
-  const nd::FormulaEntry& f = nd_formula_entries[id];
+  const nd::FormulaEntry& f = (*nd_formula_at(id));
   if (out) {
     for (int i = 0; i < f.nparams; ++i) {
       memset(&out[i], 0, sizeof(nd_param_info));
@@ -728,7 +840,7 @@ nd_status nd_formula_params(nd_formula_id id, nd_param_info* out, int32_t* n) {
 // Defaults of the reference's render settings (render_precision.zig:3-30,
 // scene_state.zig:192-210) with the formula's @param defaults packed in.
 nd_status nd_view_defaults(nd_formula_id id, nd_view_desc* v) {
-  if (id < 0 || id >= nd_formula_entry_count) return ND_ERR_NOT_FOUND;
+  if (id < 0 || id >= nd_formula_total()) return ND_ERR_NOT_FOUND;
   if (!v) return ND_ERR_INVALID;
   memset(v, 0, sizeof(*v));
   v->cam_pos[2] = -3.0;
@@ -738,7 +850,7 @@ nd_status nd_view_defaults(nd_formula_id id, nd_view_desc* v) {
   v->width = v->height = v->tile_w = v->tile_h = 256;
   v->formula = id;
   v->spp = 1;
-  const nd::FormulaEntry& f = nd_formula_entries[id];
+  const nd::FormulaEntry& f = (*nd_formula_at(id));
   for (int i = 0; i < f.nparams; ++i) v->params[i] = f.params[i].default_value;
   v->trap.shape = ND_TRAP_POINT;
   v->trap.mode = ND_TRAP_MIN;
@@ -1311,12 +1423,13 @@ nd_status nd_graph_destroy(nd_graph* g) {
 nd_status nd_de_points(nd_ctx* ctx, const nd_view_desc* view, int64_t n, const double* pts, double* de,
                        double* trap, uint32_t* iters, int32_t de_precision, void* stream) {
   if (!ctx || !view || n < 0 || (n > 0 && (!pts || !de))) return fail(ctx, ND_ERR_INVALID, "bad nd_de_points arguments");
-  if (view->formula < 0 || view->formula >= nd_formula_entry_count)
+  if (view->formula < 0 || view->formula >= nd_formula_total())
     return fail(ctx, ND_ERR_NOT_FOUND, "unknown formula id %d", view->formula);
   cudaSetDevice(ctx->device);
   const DevView v = make_dev_view(*view, 0, 0, 0);
-  const KernelTable t = nd_formula_entries[view->formula].kernels();
+  const KernelTable t = nd_formula_at(view->formula)->kernels();
   const nd::DePointsFn fn = de_precision == 64 ? t.de_points_f64 : t.de_points_f32;
+  if (!fn) return fail(ctx, ND_ERR_UNSUPPORTED, "no DE kernel for this formula");
   cudaError_t e = fn(v, n, pts, de, trap, iters, (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "nd_de_points launch");
   return ND_OK;
@@ -1424,6 +1537,7 @@ nd_status shade_lite_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews
     a.scenes = sc.nscenes > 0 ? ctx->d_scenes : nullptr;
     // the shading arithmetic is f32 like the reference's; so is the DE of its AO taps
     nd::LiteFn fn = dir64 ? L.table.lite_f32_dir64 : L.table.lite_f32;
+    if (!fn) return fail(ctx, ND_ERR_UNSUPPORTED, "no lite shading kernels for this formula set");
     if (sc.nscenes > 0) {
       if (dir64) return fail(ctx, ND_ERR_UNSUPPORTED, "lite shading of scenes with FP64 ray directions");
       fn = L.table.scene_lite_f32;
@@ -1528,8 +1642,9 @@ nd_status nd_accel_grid(nd_ctx* ctx, const nd_view_desc* view, int32_t de_precis
   nd::place_accel(v, *view, grid);
   for (int l = 0; l < nd::kAccelMaxCascades; ++l)
     for (int a = 0; a < 4; ++a) prm[4 * l + a] = l < v.accel_levels ? v.accel_prm[l][a] : 0.0f;
-  const KernelTable t = nd_formula_entries[view->formula].kernels();
+  const KernelTable t = nd_formula_at(view->formula)->kernels();
   const nd::AccelBuildFn fn = de_precision == 64 ? t.accel_build_f64 : t.accel_build_f32;
+  if (!fn) return fail(ctx, ND_ERR_UNSUPPORTED, "no accelerator kernels for this formula");
   DevView* dv = nullptr;
   nd::AccelJob* dj = nullptr;
   nd::AccelJob job;
@@ -1726,7 +1841,7 @@ extern "C" nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t
   }
   int nv = 0;
   if (ndistinct == 1 || group >= 0) {
-    tables[0] = group >= 0 ? nd_group_entries[group].kernels() : nd_formula_entries[distinct[0]].kernels();
+    tables[0] = group >= 0 ? nd_group_entries[group].kernels() : nd_formula_at(distinct[0])->kernels();
     nlaunch = 1;
     const int gcount = group >= 0 ? nd_group_entries[group].count : 1;
     for (int m = 0; m < gcount; ++m)  // views ordered by formula code
@@ -1741,7 +1856,7 @@ extern "C" nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t
       }
   } else {
     for (int k = 0; k < ndistinct; ++k) {
-      tables[nlaunch] = nd_formula_entries[distinct[k]].kernels();
+      tables[nlaunch] = nd_formula_at(distinct[k])->kernels();
       for (int i = 0; i < nviews; ++i)
         if (views[i].formula == distinct[k]) {
           order[nv] = i;
@@ -1807,6 +1922,7 @@ extern "C" nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t
     LaunchFn fn = prec == 64 ? (batched ? T.inline_f64_batched : T.inline_f64)
                              : dir64 ? (batched ? T.inline_f32_dir64_batched : T.inline_f32_dir64)
                                      : (batched ? T.inline_f32_batched : T.inline_f32);
+    if (!fn) return fail(nullptr, ND_ERR_UNSUPPORTED, "no inline march kernel for this formula set");
     e = fn(a, host[first[l]], c, st);
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "kernel launch");
   }
@@ -2000,6 +2116,10 @@ extern "C" nd_status nd_march_backward(nd_ctx* ctx, const nd_view_desc* views, c
     const KernelTable& kt = plans[p].table;
     const nd::AdjointFn fn = prec == 64 ? (nv > 1 ? kt.adjoint_f64_batched : kt.adjoint_f64)
                                         : (nv > 1 ? kt.adjoint_f32_batched : kt.adjoint_f32);
+    if (!fn) {
+      e = cudaErrorNotSupported;
+      break;
+    }
     e = fn(a, hv[first[p]], st);
   }
   // the host staging vectors are pageable: wait for the copies before they go away

@@ -77,10 +77,10 @@ struct Loader {
     if (stem.size() > 5 && stem.compare(stem.size() - 5, 5, ".wgsl") == 0) stem.resize(stem.size() - 5);
     if (stem.empty()) stem = "mandelbrot";
     *id = -1;
-    for (int i = 0; i < nd_formula_entry_count; ++i)
-      if (stem == nd_formula_entries[i].name) *id = i;
+    for (int i = 0; i < nd_formula_total(); ++i)
+      if (stem == nd_formula_at(i)->name) *id = i;
     if (*id < 0) return fail(std::string(what) + ": formula \"" + stem + "\" is not in this build");
-    const nd::FormulaEntry& e = nd_formula_entries[*id];
+    const nd::FormulaEntry& e = (*nd_formula_at(*id));
     for (int k = 0; k < ND_MAX_PARAMS; ++k) params[k] = k < e.nparams ? e.params[k].default_value : 0.0f;
     const JVal* saved = f->get("params");
     if (saved && saved->kind == JVal::ARR)

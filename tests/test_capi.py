@@ -68,12 +68,15 @@ def test_register_rejects_bad_sources(ndlib):
     with pytest.raises(runtime.FormulaError) as e:
         runtime.register_formula("fn de_iterations(p: Params) -> i32 { return 1; }")
     assert "de_step" in str(e.value)
+    # all three contract functions, but one names a value that does not exist: the
+    # translator refuses it and its message comes back
     with pytest.raises(runtime.FormulaError) as e:
         runtime.register_formula(
             "fn de_iterations(p: Params) -> i32 { return 1; }\n"
             "fn de_step(carry: IterCarry, pos: vec3f, p: Params) -> IterCarry { return carry; }\n"
-            "fn de_finalize(carry: IterCarry) -> f32 { return 0.0; }\n")
+            "fn de_finalize(carry: IterCarry) -> f32 { return undefined_value; }\n")
     assert e.value.status == abi.ND_ERR_COMPILE
+    assert "undefined_value" in str(e.value)
 
 
 def test_register_finds_compiled_sources(ndlib):
