@@ -46,9 +46,11 @@ if ROOT not in sys.path:
 
 METRIC = "Mrays/s & DE-evals/s on 1 B200, batched vs plain, at stated FP64 error"
 
-# DRAM bytes of one batched persistent launch (march kernel), from
-# ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum on this workload.
-NCU_TRAFFIC = {"batched_64": 335.2e6}
+# DRAM bytes (read + write) of one forward's kernels on each workload, from
+# ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum (one capture per workload;
+# the summary and its command are in profiles/).
+NCU_TRAFFIC = {"batched_64": {"march": 333.6e6, "surface": 384.0e6},
+               "mandelbox_1080p": {"march": 367.3e6, "surface": 532.1e6, "shadow": 330.4e6}}
 
 
 def _dist_env():
@@ -767,7 +769,11 @@ def main():
                             "trap, steps: 20 B per ray) read back to pinned host memory every step; two G-buffers, "
                             "read-back of step i overlapping the march of step i+1"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": NCU_TRAFFIC.get(args.workload),
+                         "frac": achieved / peak,
+                         "traffic": NCU_TRAFFIC.get(args.workload, {}).get("march"),
+                         "traffic_forward": sum(NCU_TRAFFIC.get(args.workload, {}).values()) or None,
+                         "traffic_note": "DRAM bytes per launch of the march (traffic) and of the whole forward, "
+                                         "march + surface pass (traffic_forward), from one ncu capture",
                          "kernel": "persistent_kernel (march); FLOPs = its DE evaluations x FLOPs per "
                                    "evaluation, over its CUDA-event time",
                          "kernel_ms": kms[0], "shade_pass_ms": kms[1],

@@ -257,23 +257,31 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
       const int64_t r = v.out_offset + local;
       const double t = a.t_hit[r];
       if (t >= 0.0) {  // (all-rays mode: a miss has t < 0 and the march wrote its outputs)
+        // one call site per kind of DE evaluation (normal taps, shadow steps, trap), so
+        // that the formula set's code appears three times in the kernel
+        Dir<kDir64> dir;
+        dir.set(ray_dir(v, local));
         if (list) {
-          if (queue && casts_shadow(v)) {
-            Dir<kDir64> dir;
-            dir.set(ray_dir(v, local));
-            const Surface sf = surface_at_hit<Set, T, kDir64, kScenes>(v, dir, t, r, a.out, a.scenes);
+          const Surface sf = surface_at_hit<Set, T, kDir64, kScenes>(v, dir, t, r, a.out, a.scenes);
+          taps += uint32_t(sf.taps);
+          float vis = 1.0f;
+          int sev = 0;
+          if (casts_shadow(v)) {
             const D3 so = shadow_origin(sf);
-            e = ShadowEntry{h.item, h.march_evals + uint32_t(sf.taps), sf.gx, sf.gy, sf.gz, 0, so.x, so.y, so.z};
-            want = true;
-            taps += uint32_t(sf.taps);
-          } else {
-            const uint32_t ev = shade_at_hit<Set, T, kDir64, kScenes, kAccel>(v, local, t, a.out, a.scenes,
-                                                                              h.march_evals);
-            taps += ev & 0xffffu;
-            shadow += ev >> 16;
+            if (queue) {
+              e = ShadowEntry{h.item, h.march_evals + uint32_t(sf.taps), sf.gx, sf.gy, sf.gz, 0, so.x, so.y, so.z};
+              want = true;
+            } else {
+              vis = shadow_visibility<Set, T, kScenes, kAccel>(v, so, a.scenes, &sev);
+              shadow += uint32_t(sev);
+            }
           }
+          if (!want)
+            finish_at_hit(v, dir.get(), sf.gx, sf.gy, sf.gz, vis, h.march_evals + uint32_t(sf.taps + sev), r, a.out);
         }
-        if (do_trap) trap_at_hit<Set, T, kDir64, kScenes>(v, local, t, a.out, a.scenes);
+        if (do_trap)
+          trap_at_point<Set, T, kScenes>(v, fmadd(d3(v.org[0], v.org[1], v.org[2]), dir.get(), t), r, a.out,
+                                         a.scenes);
       }
     }
     if (queue) {

@@ -1121,16 +1121,21 @@ namespace nd {
 
 // The orbit trap and changed-iteration count at a ray's hit point: the formula
 // wrapper with its trap (formula_N) evaluated once at org + dir * t_hit.
+// p: the hit point, r: the ray's G-buffer slot.
+template <class Set, class T, bool kScenes = false>
+ND_DEV_INLINE void trap_at_point(const DevView& v, D3 p, int64_t r, const nd_gbuffer& g, const DevScene* scenes) {
+  const DEOut<T> de = view_de<Set, T, true, kScenes>(v, to_t<T>(p), scenes);
+  if (g.trap) g.trap[r] = float(de.trap);
+  if (g.iters) g.iters[r] = uint32_t(de.iters);
+}
+
 template <class Set, class T, bool kDir64, bool kScenes = false>
 ND_DEV_INLINE void trap_at_hit(const DevView& v, int64_t local, double t, const nd_gbuffer& g,
                                const DevScene* scenes) {
   Dir<kDir64> dir;
   dir.set(ray_dir(v, local));
   const D3 p = fmadd(d3(v.org[0], v.org[1], v.org[2]), dir.get(), t);
-  const DEOut<T> de = view_de<Set, T, true, kScenes>(v, to_t<T>(p), scenes);
-  const int64_t r = v.out_offset + local;
-  if (g.trap) g.trap[r] = float(de.trap);
-  if (g.iters) g.iters[r] = uint32_t(de.iters);
+  trap_at_point<Set, T, kScenes>(v, p, v.out_offset + local, g, scenes);
 }
 
 // The deferred part of a hit ray, in three pieces: surface_at_hit (the normal taps
