@@ -277,6 +277,30 @@ def sampled_errors(views, gbuf, target_rays, seed, names=None, run=64, de_precis
     return out
 
 
+def deepzoom_normal_floor(views, target_rays, seed):
+    """The FP64 oracle's own normal noise at the deep-zoom camera: the angle between its
+    normals and those of the same oracle compiled with fused multiply-adds (results
+    that differ by rounding only), on the same sampled rays."""
+    import numpy as np
+
+    from numericdream_b200 import runtime
+    from oracle import pyoracle
+
+    names = runtime.formula_names()
+    angles = []
+    for vi, first, cnt in cpu_sample(views, target_rays, seed=seed):
+        v = views[vi]
+        a = pyoracle.render(v, names[v.formula], precision=64, first=first, n=cnt)
+        b = pyoracle.render(v, names[v.formula], precision=64, first=first, n=cnt, fma=True)
+        both = (a["normal"][:, 3] > 0.5) & (b["normal"][:, 3] > 0.5)
+        x, y = a["normal"][both, :3].astype(np.float64), b["normal"][both, :3].astype(np.float64)
+        c = (x * y).sum(1) / np.maximum(np.linalg.norm(x, axis=1) * np.linalg.norm(y, axis=1), 1e-300)
+        angles.append(np.degrees(np.arccos(np.clip(c, -1.0, 1.0))))
+    ang = np.concatenate(angles) if angles else np.zeros(1)
+    return {"normal_deg_p50": float(np.percentile(ang, 50)), "normal_deg_p99": float(np.percentile(ang, 99)),
+            "note": "FP64 oracle against the same oracle compiled with FMA contraction, same sampled rays"}
+
+
 def error_stats(views, gbuf_np, cpu, gpu_parts=None, min_t=1e-3):
     """GPU output against the FP64 oracle on the sampled rays (hits of both, beyond
     t = min_t)."""
@@ -458,6 +482,7 @@ def small_and_deepzoom(ctx, sptr, timed, steps, with_errors=True):
         torch.cuda.synchronize()
         # hits lie at t ~ 1e-5 here: no t floor
         out["deepzoom_4096"]["error_vs_fp64"] = sampled_errors(views, g, 8192, 5, min_t=0.0)
+        out["deepzoom_4096"]["normal_noise_floor"] = deepzoom_normal_floor(views, 8192, 5)
     # lite shading (shade_lite) of batched_64's hits after each forward: colour strip,
     # ambient occlusion (5 DE evaluations per hit), two lights
     views = workloads.batched_64(runtime.find_formula)

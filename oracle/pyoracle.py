@@ -11,35 +11,46 @@ from numericdream_b200 import abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
+_LIB_FMA = None
 
 
-def lib():
-    global _LIB
+def lib(fma: bool = False):
+    """The oracle library; fma=True: the same code compiled with fused multiply-adds."""
+    global _LIB, _LIB_FMA
+    from . import build_oracle
+
+    if fma:
+        if _LIB_FMA is None:
+            _LIB_FMA = _setup(C.CDLL(build_oracle.build(fma=True)))
+        return _LIB_FMA
     if _LIB is None:
-        from . import build_oracle
-        path = build_oracle.build()  # rebuilt only when a source is newer than the library
-        _LIB = C.CDLL(path)
-        _LIB.oracle_formula_index.argtypes = [C.c_char_p]
-        _LIB.oracle_de.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p,
-                                   C.c_void_p, C.c_void_p]
-        _LIB.oracle_render.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_int64, C.c_int64] + [C.c_void_p] * 10 + [C.c_double]
-        _LIB.oracle_render_scene.argtypes = ([C.c_void_p] * 4 + [C.c_int, C.c_int, C.c_int64, C.c_int64]
-                                             + [C.c_void_p] * 10 + [C.c_double])
-        _LIB.oracle_scene_de.argtypes = ([C.c_void_p] * 3 + [C.c_double, C.c_int, C.c_int64] + [C.c_void_p] * 4)
-        _LIB.oracle_accel_grid.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_void_p, C.c_int64,
-                                           C.c_void_p]
-        _LIB.oracle_accel_grid.restype = C.c_int64
-        _LIB.oracle_march_dirs.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p]
-        _LIB.oracle_combine.argtypes = [C.c_int64] + [C.c_void_p] * 5
-        _LIB.oracle_shade_lite.argtypes = ([C.c_void_p, C.c_char_p, C.c_void_p, C.c_int, C.c_int64, C.c_int64]
-                                           + [C.c_void_p] * 4)
-        _LIB.oracle_ao.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int64] + [C.c_void_p] * 4
-        _LIB.oracle_strip_fresnel.argtypes = [C.c_int64] + [C.c_void_p] * 6
-        _LIB.oracle_shade_lite_scene.argtypes = ([C.c_void_p] * 6 + [C.c_int, C.c_int64, C.c_int64]
-                                                 + [C.c_void_p] * 4)
-        _LIB.oracle_combine_weight.argtypes = [C.c_int64] + [C.c_void_p] * 5
-        _LIB.oracle_max_threads.restype = C.c_int
+        _LIB = _setup(C.CDLL(build_oracle.build()))  # rebuilt only when a source is newer than the library
     return _LIB
+
+
+def _setup(L):
+    L.oracle_formula_index.argtypes = [C.c_char_p]
+    L.oracle_de.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p,
+                            C.c_void_p, C.c_void_p]
+    L.oracle_render.argtypes = ([C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_int64, C.c_int64] + [C.c_void_p] * 10
+                                + [C.c_double])
+    L.oracle_render_scene.argtypes = ([C.c_void_p] * 4 + [C.c_int, C.c_int, C.c_int64, C.c_int64]
+                                      + [C.c_void_p] * 10 + [C.c_double])
+    L.oracle_scene_de.argtypes = ([C.c_void_p] * 3 + [C.c_double, C.c_int, C.c_int64] + [C.c_void_p] * 4)
+    L.oracle_accel_grid.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_void_p, C.c_int64,
+                                       C.c_void_p]
+    L.oracle_accel_grid.restype = C.c_int64
+    L.oracle_march_dirs.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p]
+    L.oracle_combine.argtypes = [C.c_int64] + [C.c_void_p] * 5
+    L.oracle_shade_lite.argtypes = ([C.c_void_p, C.c_char_p, C.c_void_p, C.c_int, C.c_int64, C.c_int64]
+                                       + [C.c_void_p] * 4)
+    L.oracle_ao.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int64] + [C.c_void_p] * 4
+    L.oracle_strip_fresnel.argtypes = [C.c_int64] + [C.c_void_p] * 6
+    L.oracle_shade_lite_scene.argtypes = ([C.c_void_p] * 6 + [C.c_int, C.c_int64, C.c_int64]
+                                             + [C.c_void_p] * 4)
+    L.oracle_combine_weight.argtypes = [C.c_int64] + [C.c_void_p] * 5
+    L.oracle_max_threads.restype = C.c_int
+    return L
 
 
 def has_formula(name: str) -> bool:
@@ -78,13 +89,15 @@ def _outputs(n):
     }
 
 
-def render(view: abi.nd_view_desc, formula_name: str, precision=64, nthreads=0, first=0, n=None, de_scale=1.0):
-    """Trace rays [first, first+n) of one view; returns a dict of numpy arrays."""
+def render(view: abi.nd_view_desc, formula_name: str, precision=64, nthreads=0, first=0, n=None, de_scale=1.0,
+           fma=False):
+    """Trace rays [first, first+n) of one view; returns a dict of numpy arrays.  fma:
+    with the oracle compiled with fused multiply-adds (differs by rounding only)."""
     total = abi.rays_of(view)
     if n is None:
         n = total - first
     out = _outputs(n)
-    rc = lib().oracle_render(C.addressof(view), formula_name.encode(), precision, nthreads, first, n,
+    rc = lib(fma).oracle_render(C.addressof(view), formula_name.encode(), precision, nthreads, first, n,
                              *[out[k].ctypes.data for k in _KEYS], de_scale)
     if rc != 0:
         raise ValueError(f"oracle has no formula {formula_name!r}")
