@@ -54,7 +54,7 @@
 extern "C" {
 #endif
 
-#define ND_ABI_VERSION 3
+#define ND_ABI_VERSION 4
 #define ND_MAX_PARAMS 16          /* fractal_renderer.zig:47 */
 #define ND_PARAM_NAME_LEN 24      /* CustomParam.name [24:0]u8, formula.zig:7 */
 
@@ -151,6 +151,15 @@ typedef struct nd_view_desc {
   int32_t accel_res;
   int32_t accel_levels;
   float accel_safety;     /* every recorded skip is multiplied by this */
+  /* The formula image of a formula that declares `// @image` (read through
+   * image_info / image_sample, template.wgsl:1111-1191; HeightMaps, src/gpu/height_maps.zig):
+   * DEVICE pointer to image_width x image_height texels of 4 words as nd_image_prepare
+   * writes them, and the image's per-channel slope bound from nd_image_prepare.
+   * NULL: no image (the formula sees size 0, as the reference does with none loaded). */
+  const uint32_t* image_texels;
+  int32_t image_width;
+  int32_t image_height;
+  float image_slope[4];
 } nd_view_desc;
 
 /* A scene of up to four fractal instances combined by distance (scene_de,
@@ -501,6 +510,18 @@ nd_status nd_scene_file_lite(const char* json, size_t len, int32_t instance, nd_
  * code is scalar FP32): a resident grid of independent fused multiply-add chains for
  * about `ms` milliseconds; *tflops = 2 x FMAs / CUDA-event time. */
 nd_status nd_measure_fp32_peak(nd_ctx* ctx, double ms, double* tflops);
+
+/* A formula image from its pixels, as the reference prepares a height map after
+ * decoding it (height_maps.zig:264-320): rgba (HOST, width x height x 4 floats, row
+ * major, top row first) holds R, G, B premultiplied by alpha and alpha, each in [0, 1]
+ * (the reference's 8- and 16-bit decode; HDR images normalised to [0, 1] with alpha 1).
+ * Each channel is quantised to 16 bits; per texel the change to its right and lower
+ * neighbours bounds the slope, its running maximum within 8 + 2 and 64 + 2 texels
+ * (max-filter dilation) becomes the near and far slope codes.  texels (HOST, 4 words
+ * per texel) receives the layout image_sample reads; slope (HOST, 4 floats) the
+ * largest slope per channel (times 1.001).  Copy texels to the device and set the
+ * view's image fields.  Sizes up to 2048 x 2048 (the reference's max_edge). */
+nd_status nd_image_prepare(const float* rgba, int32_t width, int32_t height, uint32_t* texels, float* slope);
 
 /* Size of a public struct by name ("nd_view_desc", ...), for binding layout checks. */
 size_t nd_sizeof(const char* name);

@@ -47,6 +47,8 @@ class nd_view_desc(C.Structure):
         ("hq_footprint_px", C.c_float), ("normal_mode", C.c_int32), ("normal_h_coef", C.c_float),
         ("shadow", C.c_int32), ("light_dir", C.c_float * 3), ("shadow_k", C.c_float), ("step_safety", C.c_float),
         ("flags", C.c_int32), ("accel_res", C.c_int32), ("accel_levels", C.c_int32), ("accel_safety", C.c_float),
+        ("image_texels", C.c_void_p), ("image_width", C.c_int32), ("image_height", C.c_int32),
+        ("image_slope", C.c_float * 4),
     ]
 
 

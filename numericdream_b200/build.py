@@ -271,10 +271,12 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         fheaders[u] = headers + incs
     runtime = os.path.join(CSRC, "nd_runtime.cu")
     scene_file = os.path.join(CSRC, "nd_scene_file.cu")
-    all_units = units + [reg, runtime, scene_file]
+    image = os.path.join(CSRC, "nd_image.cu")
+    all_units = units + [reg, runtime, scene_file, image]
     fheaders[reg] = headers
     fheaders[runtime] = headers
     fheaders[scene_file] = headers
+    fheaders[image] = headers
     jobs = jobs or max(1, os.cpu_count() or 1)
     objs = []
     errors = []

@@ -6,6 +6,8 @@
 // below), because formula files call these names and must see the same results.
 #pragma once
 
+#include <utility>
+
 #include "nd_wgsl.h"
 
 namespace ndw {
@@ -189,6 +191,111 @@ template <class T> ND_HD_INLINE T smix(T a, T b, T k) {
   if (k <= T(0.0001)) return min(a, b);
   const T h = clamp(T(0.5) + T(0.5) * (b - a) / k, T(0), T(1));
   return mix(b, a, h);
+}
+
+// ------------------------------------------------------------------ formula images
+// The image a formula declares with `// @image` and reads through image_info() and
+// image_sample() (template.wgsl:1111-1191).  The texels are prepared on the host by
+// nd_image_prepare, four 32-bit words per texel (IMAGE_TEXEL_WORDS): red and green as
+// u16 in word 0, blue and alpha in word 1 (R, G, B premultiplied by alpha, then alpha,
+// each in [0, 1]), and in words 2 and 3 the per-channel bounds on the change per texel
+// within IMAGE_SLOPE_RADIUS_NEAR and _FAR texels as u8 codes (image_slope_decode).
+// The reference finds a formula's image through a slot index into one shared buffer;
+// here a view carries a pointer to its image, and the formula's parameter accessor
+// carries it to image_info().
+struct ImageRef {
+  const uint32_t* texels;  // nullptr: no image (image_info reports size 0)
+  uint32_t width, height;
+  float slope[4];          // per channel: the largest change between neighbouring texels
+};
+
+template <class T> struct ImageInfo {  // ImageInfo, tpl:1142-1146
+  uint32_t base;                       // 0: the texels pointer replaces the shared buffer's offset
+  v2<uint32_t> size;
+  v4<T> slope;
+  const uint32_t* texels;
+};
+template <class T> struct ImageSample {  // ImageSample, tpl:1158-1162
+  v4<T> value;
+  v4<T> near;
+  v4<T> far;
+};
+
+// The accessor's image when it has one (ParamRef of a view in a kernel); the host
+// builds of the formula code (op counting) and the dual-number accessor of the adjoint
+// see no image.
+template <class P, class = void> struct HasImage {
+  static constexpr bool value = false;
+};
+template <class P> struct HasImage<P, decltype(void(std::declval<const P&>().image()))> {
+  static constexpr bool value = true;
+};
+template <class P> ND_HD_INLINE const ImageRef* image_of(const P& p) {
+#if defined(__CUDA_ARCH__)
+  if constexpr (HasImage<P>::value) return p.image();
+#endif
+  (void)p;
+  return nullptr;
+}
+
+ND_HD_INLINE uint32_t image_word(const uint32_t* w, uint32_t i) {
+#if defined(__CUDA_ARCH__)
+  return __ldg(w + i);
+#else
+  return w[i];
+#endif
+}
+
+// image_info (tpl:1148-1155)
+template <class T, class P> ND_HD_INLINE ImageInfo<T> image_info(const P& p) {
+  const ImageRef* im = image_of(p);
+  if (!im || !im->texels) return ImageInfo<T>{0u, v2<uint32_t>(0u, 0u), v4<T>(T(0)), nullptr};
+  return ImageInfo<T>{0u, v2<uint32_t>(im->width, im->height),
+                      v4<T>(T(im->slope[0]), T(im->slope[1]), T(im->slope[2]), T(im->slope[3])), im->texels};
+}
+
+// image_slope_decode (tpl:1164-1168): code c in 1..255 is the bound 2^((c - 255) / 16 + 1),
+// 0 is no change.
+template <class T> ND_HD_INLINE v4<T> image_slope_decode(uint32_t packed) {
+  const T c[4] = {T(packed & 0xffu), T((packed >> 8) & 0xffu), T((packed >> 16) & 0xffu), T(packed >> 24)};
+  v4<T> out;
+  for (int k = 0; k < 4; ++k) {
+    const T s = exp2((c[k] - T(255.0)) / T(16.0) + T(1.0));
+    out[k] = c[k] == T(0) ? T(0) : s;
+  }
+  return out;
+}
+
+// image_texel (tpl:1170-1176)
+template <class T> ND_HD_INLINE ImageSample<T> image_texel(const ImageInfo<T>& info, uint32_t x, uint32_t y) {
+  const uint32_t i = info.base + (y * info.size.x + x) * 4u;
+  const uint32_t rg = image_word(info.texels, i), ba = image_word(info.texels, i + 1u);
+  const T scale = T(1.0f / 65535.0f);  // IMAGE_U16_SCALE, an f32 constant
+  const v4<T> value = v4<T>(T(rg & 0xffffu), T(rg >> 16), T(ba & 0xffffu), T(ba >> 16)) * scale;
+  return ImageSample<T>{value, image_slope_decode<T>(image_word(info.texels, i + 2u)),
+                        image_slope_decode<T>(image_word(info.texels, i + 3u))};
+}
+
+// image_mix (tpl:1178-1180): mix of every field with one weight
+template <class T> ND_HD_INLINE ImageSample<T> image_mix(const ImageSample<T>& a, const ImageSample<T>& b, T t) {
+  const v4<T> w(t);
+  return ImageSample<T>{mix(a.value, b.value, w), mix(a.near, b.near, w), mix(a.far, b.far, w)};
+}
+
+// image_sample (tpl:1182-1191): bilinear at uv in [0, 1]^2, clamped at the edges;
+// zeros without an image.
+template <class T> ND_HD_INLINE ImageSample<T> image_sample(const ImageInfo<T>& info, v2<T> uv) {
+  if (info.size.x == 0u || info.size.y == 0u || !info.texels)
+    return ImageSample<T>{v4<T>(T(0)), v4<T>(T(0)), v4<T>(T(0))};
+  const v2<uint32_t> last = v2<uint32_t>(info.size.x - 1u, info.size.y - 1u);
+  const T tx = clamp(uv.x * T(info.size.x) - T(0.5), T(0), T(last.x));
+  const T ty = clamp(uv.y * T(info.size.y) - T(0.5), T(0), T(last.y));
+  const uint32_t x0 = min(to_u32(tx), last.x), y0 = min(to_u32(ty), last.y);
+  const uint32_t x1 = min(x0 + 1u, last.x), y1 = min(y0 + 1u, last.y);
+  const T fx = tx - T(x0), fy = ty - T(y0);
+  const ImageSample<T> top = image_mix(image_texel(info, x0, y0), image_texel(info, x1, y0), fx);
+  const ImageSample<T> bottom = image_mix(image_texel(info, x0, y1), image_texel(info, x1, y1), fx);
+  return image_mix(top, bottom, fy);
 }
 
 }  // namespace ndw

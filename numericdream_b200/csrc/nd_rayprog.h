@@ -124,6 +124,7 @@ struct DevView {
   float accel_inv[kAccelMaxCascades];  // 1 / cell size
   float accel_cam[3];   // the camera position the cascades are centred on (f32)
   float accel_k;        // 1 / ((res / 2 - 1) * finest cell): lookup start level
+  ndw::ImageRef image;  // the formula image (texels nullptr: none)
   // n / d for 0 <= n < 2^31 as (n * m) >> s (DivMagic): d = the tile's pixels, d = its width
   uint32_t npix_m, npix_s, width_m, width_s;
 };
@@ -258,7 +259,9 @@ template <class T> struct DEOut {
 // Parameter access for formula code: p[i] reads the view's packed params.
 template <class T> struct ParamRef {
   const float* v;
+  const ndw::ImageRef* img = nullptr;  // the view's formula image (image_info)
   ND_HD_INLINE T operator[](int i) const { return T(v[i]); }
+  ND_HD_INLINE const ndw::ImageRef* image() const { return img; }
 };
 
 // formula_N (fractal_renderer.zig:490-512) + the single-instance scene_de
@@ -312,8 +315,9 @@ ND_DEV_INLINE DEOut<T> formula_de_p(ndw::v3<T> pos, const PR& p, const nd_trap_d
 }
 
 template <class F, class T, bool kTrap>
-ND_DEV_INLINE DEOut<T> formula_de(ndw::v3<T> pos, const float* params, const nd_trap_desc& trap, float factor) {
-  return formula_de_p<F, T, kTrap, ParamRef<T>>(pos, ParamRef<T>{params}, trap, factor);
+ND_DEV_INLINE DEOut<T> formula_de(ndw::v3<T> pos, const float* params, const nd_trap_desc& trap, float factor,
+                                  const ndw::ImageRef* image = nullptr) {
+  return formula_de_p<F, T, kTrap, ParamRef<T>>(pos, ParamRef<T>{params, image}, trap, factor);
 }
 
 // A compile-time list of formulas; code selects one (warp-uniform in practice,
@@ -326,7 +330,7 @@ template <class... Fs> struct FormulaSet;
 template <class F> struct FormulaSet<F> {
   template <class T, bool kTrap = false>
   static ND_DEV_INLINE DEOut<T> de(int, ndw::v3<T> pos, const DevView& v) {
-    return formula_de<F, T, kTrap>(pos, v.params, v.trap, v.factor);
+    return formula_de<F, T, kTrap>(pos, v.params, v.trap, v.factor, &v.image);
   }
   template <class T, class PR>
   static ND_DEV_INLINE DEOut<T> de_with(int, ndw::v3<T> pos, const PR& p, const DevView& v) {
@@ -350,7 +354,7 @@ template <class F> struct FormulaSet<F> {
 template <class F, class G, class... Rest> struct FormulaSet<F, G, Rest...> {
   template <class T, bool kTrap = false>
   static ND_DEV_INLINE DEOut<T> de(int code, ndw::v3<T> pos, const DevView& v) {
-    if (code == 0) return formula_de<F, T, kTrap>(pos, v.params, v.trap, v.factor);
+    if (code == 0) return formula_de<F, T, kTrap>(pos, v.params, v.trap, v.factor, &v.image);
     return FormulaSet<G, Rest...>::template de<T, kTrap>(code - 1, pos, v);
   }
   template <class T, class PR>

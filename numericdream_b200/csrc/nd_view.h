@@ -68,6 +68,10 @@ inline DevView make_dev_view(const nd_view_desc& v, int64_t ray_offset, int64_t 
   const double rn = sqrt(v.right[0] * v.right[0] + v.right[1] * v.right[1] + v.right[2] * v.right[2]);
   const double un = sqrt(v.up[0] * v.up[0] + v.up[1] * v.up[1] + v.up[2] * v.up[2]);
   d.dir64 = ((v.flags & ND_VIEW_DIR64) != 0 || std::max(rn, un) < 1e-3) ? 1 : 0;
+  d.image.texels = v.image_texels;
+  d.image.width = v.image_texels ? uint32_t(v.image_width) : 0u;
+  d.image.height = v.image_texels ? uint32_t(v.image_height) : 0u;
+  for (int i = 0; i < 4; ++i) d.image.slope[i] = v.image_slope[i];
   // ray_uv's 32-bit path divides by the tile's pixel count and width (both < 2^31 there)
   const int64_t npix = int64_t(v.tile_w) * v.tile_h;
   div_magic(uint32_t(npix > 0 && npix < 0x80000000ll ? npix : 1), &d.npix_m, &d.npix_s);

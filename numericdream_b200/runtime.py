@@ -52,6 +52,7 @@ _SIGNATURES = {
                                             C.POINTER(C.c_int32), C.POINTER(abi.nd_scene_desc), C.c_int32,
                                             C.POINTER(abi.nd_march_opts), C.POINTER(abi.nd_gbuffer), C.c_void_p,
                                             C.POINTER(C.c_void_p)]),
+    "nd_image_prepare": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
     "nd_tune_cache_save": (C.c_int32, [C.c_char_p]),
     "nd_tune_cache_load": (C.c_int32, [C.c_char_p, C.POINTER(C.c_int32)]),
     "nd_graph_launch": (C.c_int32, [C.c_void_p, C.c_void_p]),
@@ -162,6 +163,24 @@ def register_formula(source: str) -> int:
     if st != abi.ND_OK:
         raise FormulaError(st, err.value.decode())
     return out.value
+
+
+def prepare_image(rgba):
+    """nd_image_prepare: a formula image's texels (uint32, 4 per texel) and per-channel
+    slope bound from rgba, a (height, width, 4) float array of R, G, B premultiplied by
+    alpha and alpha in [0, 1]."""
+    import numpy as np
+
+    a = np.ascontiguousarray(rgba, dtype=np.float32)
+    if a.ndim != 3 or a.shape[2] != 4:
+        raise ValueError("rgba must be (height, width, 4)")
+    h, w = a.shape[:2]
+    texels = np.zeros(h * w * 4, dtype=np.uint32)
+    slope = np.zeros(4, dtype=np.float32)
+    st = load_library().nd_image_prepare(a.ctypes.data, w, h, texels.ctypes.data, slope.ctypes.data)
+    if st != abi.ND_OK:
+        raise NDError(st, f"nd_image_prepare({w}x{h})")
+    return texels, slope
 
 
 def formula_params(fid: int) -> list:

@@ -11,8 +11,6 @@ estimated cost so the slowest rank finishes as early as possible.
 
 from __future__ import annotations
 
-import copy
-
 from . import abi
 
 # relative DE cost of one ray per formula (DE evaluations x FLOPs per evaluation,
@@ -32,7 +30,7 @@ def split_tiles(view: abi.nd_view_desc, tiles_x: int, tiles_y: int) -> list:
             d = y0 + (h * (ty + 1)) // tiles_y
             if b <= a or d <= c:
                 continue
-            t = copy.copy(view)
+            t = type(view).from_buffer_copy(view)
             t.tile_x, t.tile_y, t.tile_w, t.tile_h = a, c, b - a, d - c
             out.append(t)
     return out

@@ -598,7 +598,13 @@ F32, I32, U32, BOOL, AINT, AFLOAT = S("f32"), S("i32"), S("u32"), S("bool"), S("
 VOID = Ty("void")
 PARAMS = Ty("params")
 CARRY = Ty("st", name="IterCarry")
-STRUCT_FIELDS = {"IterCarry": {"z": V(3, "f32"), "dr": F32}}
+IMAGE_INFO = Ty("st", name="ImageInfo")
+IMAGE_SAMPLE = Ty("st", name="ImageSample")
+# struct types a formula may use: its carry, and the image sampler's records
+# (ImageInfo / ImageSample, template.wgsl:1142-1162)
+STRUCT_FIELDS = {"IterCarry": {"z": V(3, "f32"), "dr": F32},
+                 "ImageInfo": {"base": U32, "size": V(2, "u32"), "slope": V(4, "f32")},
+                 "ImageSample": {"value": V(4, "f32"), "near": V(4, "f32"), "far": V(4, "f32")}}
 
 _SHORT_TYPES = {
     "f32": F32, "i32": I32, "u32": U32, "bool": BOOL,
@@ -606,7 +612,7 @@ _SHORT_TYPES = {
     "vec2i": V(2, "i32"), "vec3i": V(3, "i32"), "vec4i": V(4, "i32"),
     "vec2u": V(2, "u32"), "vec3u": V(3, "u32"), "vec4u": V(4, "u32"),
     "mat2x2f": M(2, 2), "mat3x3f": M(3, 3), "mat4x4f": M(4, 4),
-    "IterCarry": CARRY, "Params": PARAMS,
+    "IterCarry": CARRY, "Params": PARAMS, "ImageInfo": IMAGE_INFO, "ImageSample": IMAGE_SAMPLE,
 }
 
 _CPP_SCALAR = {"f32": "T", "i32": "int32_t", "u32": "uint32_t", "bool": "bool"}
@@ -683,6 +689,8 @@ TEMPLATE_CONSTS = {
     "SPATIAL_PRIME_Z": (83492791, U32),
     "BULB_BAILOUT": (2.0, AFLOAT),
     "SMOOTH_K_MIN": (0.0001, AFLOAT),
+    "IMAGE_SLOPE_RADIUS_NEAR": (8.0, AFLOAT),   # tpl:1124-1125
+    "IMAGE_SLOPE_RADIUS_FAR": (64.0, AFLOAT),
 }
 
 V3F, V4F, V2F = V(3, "f32"), V(4, "f32"), V(2, "f32")
@@ -1166,7 +1174,8 @@ class FormulaCompiler:
         if name in ("f32", "i32", "u32", "bool") and e.targs is None:
             return self.scalar_conv(name, args, line)
         ctor_ty = None
-        if name in _SHORT_TYPES and e.targs is None and name not in ("Params", "IterCarry"):
+        if name in _SHORT_TYPES and e.targs is None and name not in ("Params", "IterCarry", "ImageInfo",
+                                                                        "ImageSample"):
             ctor_ty = _SHORT_TYPES[name]
         elif name in ("vec2", "vec3", "vec4"):
             n = int(name[3])
@@ -1188,6 +1197,13 @@ class FormulaCompiler:
             if dr.ty != F32:
                 raise TranslateError("IterCarry.dr must be f32", line)
             return TE(CARRY, f"ndw::IterCarry<T>{{{z.code}, {dr.code}}}")
+        if name == "ImageSample":
+            if len(args) != 3:
+                raise TranslateError("ImageSample(value, near, far) takes three arguments", line)
+            conv = [self.convert(a, V4F, line) for a in args]
+            return TE(IMAGE_SAMPLE, f"ndw::ImageSample<T>{{{', '.join(c.code for c in conv)}}}")
+        if name in ("image_info", "image_sample"):
+            return self.image_call(name, args, line)
         if name == "bitcast":
             return self.bitcast(e, args)
         if name in self.fn_sigs:
@@ -1471,8 +1487,29 @@ class FormulaCompiler:
                 a = self._abstract_to_scalar(a, "u32", line)
             return TE(a.ty, f"ndw::{name}({a.code})")
         if name.startswith("image_") or name in ("textureSample", "textureLoad"):
-            raise TranslateError(f"'{name}' (formula images) is not supported yet", line)
+            raise TranslateError(f"'{name}' is not part of the formula image interface", line)
         raise TranslateError(f"unknown function '{name}'", line)
+
+    def image_call(self, name, args, line):
+        """The formula image interface (template.wgsl:1126-1191): image_info() and
+        image_sample(info, uv).  The reference selects the image through the private
+        g_image_slot its wrapper sets; here the image travels with the parameter
+        accessor, so the calling function must have its Params parameter in scope."""
+        self.features.add("image")
+        if name == "image_info":
+            if args:
+                raise TranslateError("image_info() takes no arguments", line)
+            for sc in reversed(self.scopes):
+                for te in sc.values():
+                    if te.ty.kind == "params":
+                        return TE(IMAGE_INFO, f"ndw::image_info<T>({te.code})")
+            raise TranslateError("image_info() needs the function's Params parameter in scope", line)
+        if len(args) != 2:
+            raise TranslateError("image_sample(info, uv) takes two arguments", line)
+        if args[0].ty != IMAGE_INFO:
+            raise TranslateError("image_sample's first argument must be an ImageInfo", line)
+        uv = self.convert(args[1], V(2, "f32"), line)
+        return TE(IMAGE_SAMPLE, f"ndw::image_sample<T>({args[0].code}, {uv.code})")
 
     # ---- statements
     def block(self, stmts, indent) -> list[str]:
@@ -1728,8 +1765,7 @@ def translate(source: str, name: str) -> TranslatedFormula:
     missing = missing_contract_fn(source)
     if missing is not None:
         raise TranslateError(f"formula is missing `{missing}`")
-    if image_directive(source) is not None:
-        raise TranslateError("formula images (@image) are not supported yet")
+
     toks = lex(source)
     fns, consts = Parser(toks).module()
     ns = "ndf_" + _sanitize(name)

@@ -206,7 +206,121 @@ template <class R> struct CubePrim {
   }
 };
 
-enum FormulaKind { F_MANDELBULB = 0, F_MANDELBOX, F_MENGER3, F_PSEUDOKLEINIAN, F_SPHERE, F_CUBE, F_COUNT };
+// The formula image of an `// @image` formula (the image sampler, tpl:1111-1191):
+// host texels of 4 words each (u16 R, G | u16 B, A | u8 near-slope codes | u8
+// far-slope codes), set by oracle_set_image; empty: no image (size 0).
+struct OracleImage {
+  std::vector<uint32_t> texels;
+  uint32_t w = 0, h = 0;
+  float slope[4] = {0, 0, 0, 0};
+};
+inline OracleImage& oracle_image() {
+  static OracleImage img;
+  return img;
+}
+
+template <class R> struct ImageSampleR {
+  R value[4], near[4], far[4];
+};
+// image_slope_decode (tpl:1164-1168)
+template <class R> void slope_decode(uint32_t packed, R out[4]) {
+  for (int k = 0; k < 4; ++k) {
+    const R c = R((packed >> (8 * k)) & 0xffu);
+    out[k] = c == R(0) ? R(0) : R(std::exp2((c - R(255)) / R(16) + R(1)));
+  }
+}
+// image_texel (tpl:1170-1176)
+template <class R> ImageSampleR<R> image_texel_r(const OracleImage& im, uint32_t x, uint32_t y) {
+  const uint32_t* t = &im.texels[size_t(y * im.w + x) * 4];
+  ImageSampleR<R> s;
+  const R scale = R(1.0f / 65535.0f);
+  const uint32_t ch[4] = {t[0] & 0xffffu, t[0] >> 16, t[1] & 0xffffu, t[1] >> 16};
+  for (int k = 0; k < 4; ++k) s.value[k] = R(ch[k]) * scale;
+  slope_decode<R>(t[2], s.near);
+  slope_decode<R>(t[3], s.far);
+  return s;
+}
+template <class R> ImageSampleR<R> image_mix_r(const ImageSampleR<R>& a, const ImageSampleR<R>& b, R t) {
+  ImageSampleR<R> o;
+  for (int k = 0; k < 4; ++k) {
+    o.value[k] = a.value[k] * (R(1) - t) + b.value[k] * t;
+    o.near[k] = a.near[k] * (R(1) - t) + b.near[k] * t;
+    o.far[k] = a.far[k] * (R(1) - t) + b.far[k] * t;
+  }
+  return o;
+}
+// image_sample (tpl:1182-1191): bilinear, clamped at the edges
+template <class R> ImageSampleR<R> image_sample_r(const OracleImage& im, R u, R v) {
+  const uint32_t lx = im.w - 1, ly = im.h - 1;
+  const R tx = std::fmin(std::fmax(u * R(im.w) - R(0.5), R(0)), R(lx));
+  const R ty = std::fmin(std::fmax(v * R(im.h) - R(0.5), R(0)), R(ly));
+  const uint32_t x0 = std::min(uint32_t(tx), lx), y0 = std::min(uint32_t(ty), ly);
+  const uint32_t x1 = std::min(x0 + 1, lx), y1 = std::min(y0 + 1, ly);
+  const R fx = tx - R(x0), fy = ty - R(y0);
+  const ImageSampleR<R> top = image_mix_r(image_texel_r<R>(im, x0, y0), image_texel_r<R>(im, x1, y0), fx);
+  const ImageSampleR<R> bottom = image_mix_r(image_texel_r<R>(im, x0, y1), image_texel_r<R>(im, x1, y1), fx);
+  return image_mix_r(top, bottom, fy);
+}
+
+// Height map: formulas/heightmap_primitive.wgsl:14-62 with the image sampler above.
+template <class R> struct HeightMap {
+  static int iterations(const R*) { return 1; }  // primitive_de_iterations (tpl:1096)
+  static R dot4(const R a[4], const R b[4]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3]; }
+  static Carry<R> step(Carry<R> c, V3<R>, const R* p) {
+    const R size = std::fmax(p[0], R(1e-4));
+    const V3<R> q = c.z / (size * std::fmax(std::fabs(c.dr), R(1e-6)));
+    const R lift = p[1];
+    const R base = std::fmax(p[2], R(0));
+    const bool up = lift >= R(0);
+    const R w[4] = {p[3], p[4], p[5], p[6]};
+    R k[4];
+    if (p[7] > R(0.5)) {
+      k[0] = -w[0]; k[1] = -w[1]; k[2] = -w[2];
+      const R one[4] = {1, 1, 1, 1};
+      k[3] = dot4(w, one);
+    } else {
+      for (int i = 0; i < 4; ++i) k[i] = w[i];
+    }
+    const OracleImage& im = oracle_image();
+    R halfx = 1, halfy = 1, texel = 0, h_lo = 0, h_hi = 0;
+    ImageSampleR<R> s;
+    for (int i = 0; i < 4; ++i) s.value[i] = s.near[i] = s.far[i] = R(0);
+    R slope[4] = {0, 0, 0, 0};
+    if (im.w > 0 && im.h > 0 && !im.texels.empty()) {
+      for (int i = 0; i < 4; ++i) slope[i] = R(im.slope[i]);
+      const R dx = R(im.w), dy = R(im.h), m = std::fmax(dx, dy);
+      halfx = dx / m;
+      halfy = dy / m;
+      texel = R(2) / m;
+      s = image_sample_r<R>(im, q.x / halfx * R(0.5) + R(0.5), q.z / halfy * R(0.5) + R(0.5));
+      h_lo = std::fmin(R(0), k[3] + (std::fmin(k[0], R(0)) + std::fmin(k[1], R(0)) + std::fmin(k[2], R(0))));
+      h_hi = std::fmax(R(0), k[3] + (std::fmax(k[0], R(0)) + std::fmax(k[1], R(0)) + std::fmax(k[2], R(0))));
+    }
+    const R top = lift * dot4(k, s.value);
+    const R dyv = up ? q.y - top : top - q.y;
+    const R flat_side = up ? -base - q.y : q.y - base;
+    const R ak[4] = {std::fabs(k[0]), std::fabs(k[1]), std::fabs(k[2]), std::fabs(k[3])};
+    const R per_texel = std::fabs(lift) / std::fmax(texel, R(1e-6));
+    const R g[3] = {per_texel * dot4(ak, slope), per_texel * dot4(ak, s.near), per_texel * dot4(ak, s.far)};
+    R cc[3];
+    for (int i = 0; i < 3; ++i) cc[i] = dyv / std::sqrt(R(1) + g[i] * g[i]);
+    const R nearw = R(8) * texel, farw = R(64) * texel;  // IMAGE_SLOPE_RADIUS_NEAR / _FAR
+    const R c_near = std::fmin(std::fmax(cc[1], -nearw), nearw);
+    const R c_far = std::fmin(std::fmax(cc[2], -farw), farw);
+    const R curved = dyv >= R(0) ? std::fmax(cc[0], std::fmax(c_near, c_far)) : std::fmin(cc[0], std::fmin(c_near, c_far));
+    const R t_min = std::fmin(lift * h_lo, lift * h_hi), t_max = std::fmax(lift * h_lo, lift * h_hi);
+    const R lo = up ? -base : std::fmin(t_min, base);
+    const R hi = up ? std::fmax(t_max, -base) : base;
+    const V3<R> e(std::fabs(q.x) - halfx, std::fmax(lo - q.y, q.y - hi), std::fabs(q.z) - halfy);
+    const R bounds = len(vmax(e, R(0))) + std::fmin(std::fmax(e.x, std::fmax(e.y, e.z)), R(0));
+    const R d = std::fmax(std::fmax(curved, flat_side), bounds);
+    const R elevation = std::fmin(std::fmax((q.y - lo) / std::fmax(hi - lo, R(1e-4)), R(0)), R(1));
+    return Carry<R>{V3<R>(R(0), elevation, R(0)), d * size};
+  }
+  static R finalize(Carry<R> c) { return c.dr; }
+};
+
+enum FormulaKind { F_MANDELBULB = 0, F_MANDELBOX, F_MENGER3, F_PSEUDOKLEINIAN, F_SPHERE, F_CUBE, F_HEIGHTMAP, F_COUNT };
 
 inline int formula_index(const char* name) {
   const std::string n(name ? name : "");
@@ -216,6 +330,7 @@ inline int formula_index(const char* name) {
   if (n == "pseudokleinian_kleinian") return F_PSEUDOKLEINIAN;
   if (n == "sphere_primitive") return F_SPHERE;
   if (n == "cube_primitive") return F_CUBE;
+  if (n == "heightmap_primitive") return F_HEIGHTMAP;
   return -1;
 }
 
@@ -311,6 +426,7 @@ template <class R> DE<R> eval_de(int kind, V3<R> pos, const R* p, const nd_trap_
     case F_MENGER3: return formula_de<R, Menger3<R>>(pos, p, trap, factor);
     case F_PSEUDOKLEINIAN: return formula_de<R, PseudoKleinian<R>>(pos, p, trap, factor);
     case F_SPHERE: return formula_de<R, SpherePrim<R>>(pos, p, trap, factor);
+    case F_HEIGHTMAP: return formula_de<R, HeightMap<R>>(pos, p, trap, factor);
     default: return formula_de<R, CubePrim<R>>(pos, p, trap, factor);
   }
 }
@@ -323,6 +439,7 @@ template <class R> Carry<R> step_kind(int kind, Carry<R> c, V3<R> pos, const R* 
     case F_MENGER3: return Menger3<R>::step(c, pos, p);
     case F_PSEUDOKLEINIAN: return PseudoKleinian<R>::step(c, pos, p);
     case F_SPHERE: return SpherePrim<R>::step(c, pos, p);
+    case F_HEIGHTMAP: return HeightMap<R>::step(c, pos, p);
     default: return CubePrim<R>::step(c, pos, p);
   }
 }
@@ -333,6 +450,7 @@ template <class R> R finalize_kind(int kind, Carry<R> c) {
     case F_MENGER3: return Menger3<R>::finalize(c);
     case F_PSEUDOKLEINIAN: return PseudoKleinian<R>::finalize(c);
     case F_SPHERE: return SpherePrim<R>::finalize(c);
+    case F_HEIGHTMAP: return HeightMap<R>::finalize(c);
     default: return CubePrim<R>::finalize(c);
   }
 }

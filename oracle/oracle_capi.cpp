@@ -69,6 +69,21 @@ int64_t oracle_accel_grid(const nd_view_desc* view, const char* formula_name, in
 
 int oracle_formula_index(const char* name) { return formula_index(name); }
 
+// The formula image `// @image` formulas read (texels as nd_image_prepare writes them);
+// texels NULL clears it.
+int oracle_set_image(const uint32_t* texels, int32_t w, int32_t h, const float* slope) {
+  OracleImage& im = oracle_image();
+  im.texels.clear();
+  im.w = im.h = 0;
+  for (int k = 0; k < 4; ++k) im.slope[k] = 0.0f;
+  if (!texels || w <= 0 || h <= 0) return 0;
+  im.texels.assign(texels, texels + size_t(w) * size_t(h) * 4);
+  im.w = uint32_t(w);
+  im.h = uint32_t(h);
+  for (int k = 0; k < 4; ++k) im.slope[k] = slope ? slope[k] : 0.0f;
+  return 0;
+}
+
 // DE (and trap, changed-iteration count) of a formula at n points, in FP64
 // (precision 64) or FP32 (precision 32).
 int oracle_de(const char* name, const float* params, const nd_trap_desc* trap, int precision, int64_t n,

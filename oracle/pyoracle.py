@@ -50,7 +50,22 @@ def _setup(L):
                                              + [C.c_void_p] * 4)
     L.oracle_combine_weight.argtypes = [C.c_int64] + [C.c_void_p] * 5
     L.oracle_max_threads.restype = C.c_int
+    L.oracle_set_image.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]
     return L
+
+
+def set_image(texels=None, width=0, height=0, slope=None):
+    """The formula image `// @image` formulas read (texels as nd_image_prepare writes
+    them: uint32, 4 per texel); None clears it.  Both oracle builds get it."""
+    keep = []
+    for fma in (False, True):
+        if texels is None:
+            lib(fma).oracle_set_image(None, 0, 0, None)
+            continue
+        t = np.ascontiguousarray(texels, dtype=np.uint32)
+        sl = np.ascontiguousarray(slope, dtype=np.float32)
+        keep += [t, sl]
+        lib(fma).oracle_set_image(t.ctypes.data, int(width), int(height), sl.ctypes.data)
 
 
 def has_formula(name: str) -> bool:

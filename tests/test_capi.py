@@ -92,7 +92,7 @@ def test_register_finds_compiled_sources(ndlib):
 def test_status_strings(ndlib):
     assert ndlib.nd_status_string(0) == b"ND_OK"
     assert ndlib.nd_status_string(4) == b"ND_ERR_TIMEOUT"
-    assert ndlib.nd_abi_version() == 3
+    assert ndlib.nd_abi_version() == 4
 
 
 def test_noalloc_rejections_carry_a_message(ndlib):
