@@ -461,10 +461,15 @@ def small_and_deepzoom(ctx, sptr, timed, steps, with_errors=True):
     v = workloads.mandelbulb_256(runtime.find_formula)
     n = workloads.rays(v)
     g = runtime.GBuffer.allocate(n)
-    for label, kern in (("persistent", abi.ND_KERNEL_PERSISTENT), ("plain", abi.ND_KERNEL_PLAIN)):
+    # "auto": the default options, which run the plain launch for one view that fits in
+    # one round of the persistent grid
+    for label, kern in (("persistent", abi.ND_KERNEL_PERSISTENT), ("plain", abi.ND_KERNEL_PLAIN),
+                        ("auto", abi.ND_KERNEL_AUTO)):
         o = runtime.make_opts(kernel=kern)
         ms = timed(lambda: ctx.forward(v, g, o, stream=sptr), steps, 3)
         out[f"mandelbulb_256_{label}"] = {"ms_per_step": ms, "Mrays_per_s": n / (ms * 1e-3) / 1e6}
+        if label == "auto":
+            out["mandelbulb_256_auto"]["kernel"] = "plain" if ctx.stats().kernel == abi.ND_KERNEL_PLAIN else "persistent"
         if label == "persistent" and with_errors:
             torch.cuda.synchronize()
             # every ray of the view against the FP64 oracle

@@ -235,7 +235,9 @@ typedef struct nd_gbuffer {
 enum { ND_KERNEL_AUTO = 0, ND_KERNEL_PLAIN = 1, ND_KERNEL_PERSISTENT = 2 };
 
 typedef struct nd_march_opts {
-  int32_t kernel;            /* ND_KERNEL_* */
+  int32_t kernel;            /* ND_KERNEL_*; AUTO = the tuned kernel, else the persistent one, but
+                                the plain launch for one view with no more rays than the
+                                persistent grid has threads (nothing to refill) */
   int32_t block;             /* persistent march: threads per block, 64, 128 or 256 (0 = tuned, else 128) */
   int32_t blocks_per_sm;     /* persistent kernel residency: > 0 that many (at most what fits), < 0 that
                                 many fewer than fit, 0 = tuned default (as many as fit) */

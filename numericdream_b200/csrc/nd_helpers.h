@@ -6,6 +6,7 @@
 // below), because formula files call these names and must see the same results.
 #pragma once
 
+#include <type_traits>
 #include <utility>
 
 #include "nd_wgsl.h"
@@ -67,7 +68,27 @@ template <class T> ND_HD_INLINE v4<T> sphere_invert_offset(v3<T> z, T dr, v3<T> 
 }
 
 // template.wgsl:987-991: wrap into the cube of side `cell` centred at the origin.
+#if defined(__CUDA_ARCH__) && !defined(ND_OPCOUNT_BUILD)
+// The FP32 DE on the device: the lattice index k = round(p / cell) comes from adding
+// 1.5 * 2^23 in a fused multiply-add, where the float spacing is 1 so the addition
+// itself rounds half to even, and subtracting it again.  Two FMA-pipe instructions
+// replace the multiply and the FRND of the rounding unit, which the iteration keeps
+// busy with its reciprocals.  k is always an integer, so p - k cell is always a lattice
+// translate of p; it is the nearest one for |p / cell| < 2^22, and rounds the exact
+// product p / cell where the generic form rounds it first.
+__device__ __forceinline__ float lattice_index(float x, float inv_cell) {
+  const float shift = 12582912.0f;  // 1.5 * 2^23
+  return __fadd_rn(__fmaf_rn(x, inv_cell, shift), -shift);
+}
+#endif
 template <class T> ND_HD_INLINE v3<T> lattice_wrap(v3<T> p, T cell) {
+#if defined(__CUDA_ARCH__) && !defined(ND_OPCOUNT_BUILD)
+  if constexpr (std::is_same<T, float>::value) {
+    const float inv = 1.0f / cell;
+    return v3<float>(fmaf(-lattice_index(p.x, inv), cell, p.x), fmaf(-lattice_index(p.y, inv), cell, p.y),
+                     fmaf(-lattice_index(p.z, inv), cell, p.z));
+  }
+#endif
   return p - round(p / cell) * cell;
 }
 

@@ -64,6 +64,7 @@ struct Tuned {
   int blocks_per_sm = 0;
   int refill_threshold = 6;
   double rays_per_s = 0.0;  // measured by the tuning run
+  bool tuned = false;       // false: the defaults above, no tuning run or cache entry
 };
 std::mutex g_tune_mu;
 std::map<std::string, Tuned> g_tuned;  // key: tune_key()
@@ -485,6 +486,13 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       const Tuned tu = tuned_for(tune_key(ctx, L));
       int kernel = opts && opts->kernel ? opts->kernel : tu.kernel;
       const bool accel = plan_voxels[p] > 0;
+      // Untuned, one view with no more rays than the persistent grid has lanes runs the
+      // plain launch: with one ray per lane there is nothing to refill, and the plain
+      // loop has no ballot per pass and no second pass for the normals (10 % faster on
+      // a 256 x 256 Mandelbulb).
+      if (!(opts && opts->kernel) && !tu.tuned && nv == 1 && !accel && sc.nscenes == 0 && L.table.resident_b128 &&
+          rays <= int64_t(L.table.resident_b128(0)) * ctx->num_sms * 128)
+        kernel = ND_KERNEL_PLAIN;
       if (accel && kernel == ND_KERNEL_PLAIN) {
         if (opts && opts->kernel == ND_KERNEL_PLAIN)
           return fail(ctx, ND_ERR_UNSUPPORTED, "the empty-space accelerator runs on the persistent kernel only");
@@ -1188,6 +1196,7 @@ nd_status nd_autotune(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, co
   t.blocks_per_sm = bc.per_sm;
   t.refill_threshold = bc.thr;
   t.rays_per_s = best > 0 ? double(total) / (best * 1e-3) : 0.0;
+  t.tuned = true;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     for (const Launch& L : plans) g_tuned[tune_key(ctx, L)] = t;
@@ -1268,6 +1277,7 @@ nd_status nd_tune_cache_load(const char* path, int32_t* loaded) {
     t.blocks_per_sm = int(num("blocks_per_sm", 0));
     t.refill_threshold = int(num("refill_threshold", 6));
     t.rays_per_s = num("rays_per_s", 0.0);
+    t.tuned = true;
     if ((t.kernel != ND_KERNEL_PLAIN && t.kernel != ND_KERNEL_PERSISTENT) ||
         (t.block != 64 && t.block != 128 && t.block != 256) || t.refill_threshold < 1 || t.refill_threshold > 32)
       continue;

@@ -75,3 +75,26 @@ def test_autotune_picks_a_resident_configuration_and_caches_it(ctx, tmp_path):
     with pytest.raises(runtime.NDError) as err:
         runtime.Context.tune_cache_load(str(tmp_path / "missing.json"))
     assert err.value.status == abi.ND_ERR_NOT_FOUND
+
+
+def test_untuned_single_small_view_runs_the_plain_launch():
+    """With no tuning entry, one view with no more rays than the persistent grid has
+    threads runs the plain launch (one ray per thread, nothing to refill) with the plain
+    launch's results; several views run the persistent march."""
+    c = runtime.Context(0)
+    try:
+        small = workloads.mandelbulb_256(runtime.find_formula)
+        n = workloads.rays(small)
+        g = runtime.GBuffer.allocate(n)
+        c.forward(small, g, runtime.make_opts())
+        assert c.stats().kernel == abi.ND_KERNEL_PLAIN
+        auto = g.numpy()
+        c.forward(small, g, runtime.make_opts(kernel=abi.ND_KERNEL_PLAIN))
+        plain = g.numpy()
+        for k in ("depth64", "steps", "evals", "normal", "trap", "shade"):
+            np.testing.assert_array_equal(auto[k], plain[k], err_msg=k)
+        views = _views()
+        c.forward(views, runtime.GBuffer.allocate(workloads.rays(views)), runtime.make_opts())
+        assert c.stats().kernel == abi.ND_KERNEL_PERSISTENT
+    finally:
+        c.close()
