@@ -395,9 +395,9 @@ nd_status nd_march_backward(nd_ctx* ctx, const nd_view_desc* views, const nd_orb
  * about 28 KB inside the library, present on every GPU that loads it.
  * Limits: at most 64 views and 2^31-1 rays per call; trap and iters outputs are
  * not available here (they need per-ray scratch) and return ND_ERR_UNSUPPORTED.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture (a call in a new CUDA context, e.g. after
- * cudaDeviceReset, repeats that look-up).  Every call shares the one array: calls
+ * The call cannot be captured into a CUDA graph (it copies the view table from its
+ * own stack frame): on a capturing stream it returns ND_ERR_UNSUPPORTED.  The first
+ * call in a CUDA context looks up the array's device address.  Every call shares the one array: calls
  * that overlap on the GPU (different streams, or host threads) race, so serialise
  * them.  views is a HOST array; the G-buffer pointers are DEVICE pointers.  The
  * call returns once the work is enqueued; a failure's message is kept per host

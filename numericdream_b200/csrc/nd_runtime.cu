@@ -1818,6 +1818,13 @@ extern "C" nd_status nd_march_forward_noalloc(const nd_view_desc* views, int32_t
     if (total > int64_t(0x7fffffff))
       return fail(nullptr, ND_ERR_INVALID, "more than 2^31-1 rays: this entry point takes at most 2^31-1 per call");
   }
+  // the view table is copied from this call's stack, which a captured graph would
+  // read again at replay, after the frame is gone
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t ce = cudaStreamIsCapturing((cudaStream_t)stream, &cap);
+  if (ce != cudaSuccess) return fail(nullptr, ND_ERR_CUDA, "stream capture status: %s", cudaGetErrorString(ce));
+  if (cap != cudaStreamCaptureStatusNone)
+    return fail(nullptr, ND_ERR_UNSUPPORTED, "this entry point cannot be captured into a CUDA graph");
   int dev = 0;
   cudaError_t ge = cudaGetDevice(&dev);
   if (ge != cudaSuccess) return fail(nullptr, ND_ERR_CUDA, "current device: %s", cudaGetErrorString(ge));

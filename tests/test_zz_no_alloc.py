@@ -135,3 +135,31 @@ def test_noalloc_reports_a_watchdog_expiry(ndlib):
     assert fn(arr, 1, C.byref(normal), C.byref(g), None) == abi.ND_OK
     assert stats(None, C.byref(st), err, 256) == abi.ND_OK
     assert st.timeouts == 0 and st.rays == n
+
+
+def test_noalloc_refuses_stream_capture(ndlib):
+    # the call copies its view table from its own stack frame, which a graph replay
+    # would read after the frame is gone: on a capturing stream it enqueues nothing
+    # and returns ND_ERR_UNSUPPORTED
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    fn = _noalloc(ndlib)
+    views = _views_single()
+    gb = _gbuf(workloads.rays(views))
+    g = gb.as_abi()
+    arr = (abi.nd_view_desc * 1)(*views)
+    side = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    x = torch.zeros(4, device="cuda")
+    with torch.cuda.graph(graph, stream=side, capture_error_mode="relaxed"):
+        status = fn(arr, 1, None, C.byref(g), C.c_void_p(side.cuda_stream))
+        x += 1.0
+    assert status == abi.ND_ERR_UNSUPPORTED
+    graph.replay()
+    torch.cuda.synchronize()
+    assert float(x[0]) == 1.0
+    # outside a capture the same call runs
+    assert fn(arr, 1, None, C.byref(g), None) == abi.ND_OK
+    torch.cuda.synchronize()
