@@ -1,11 +1,13 @@
 // C-ABI implementation (include/nd_march.h): formula registry, contexts, view
 // validation, launch planning, statistics, autotuning and CUDA-graph capture.
 #include <cuda_runtime.h>
+#include <dirent.h>
 #include <dlfcn.h>
 #include <stdarg.h>
 #include <stdlib.h>
 #include <stdio.h>
 #include <string.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <atomic>
@@ -670,6 +672,22 @@ std::string shell_quote(const std::string& s) {
   return q + "'";
 }
 
+// Removes a compile directory and everything in it (files and the one level of
+// subdirectories the compile worker makes).  A loaded library stays mapped after its
+// file is gone.
+void remove_tree(const std::string& path) {
+  if (DIR* d = opendir(path.c_str())) {
+    while (const dirent* ent = readdir(d)) {
+      const std::string name = ent->d_name;
+      if (name == "." || name == "..") continue;
+      const std::string sub = path + "/" + name;
+      if (unlink(sub.c_str()) != 0) remove_tree(sub);
+    }
+    closedir(d);
+  }
+  rmdir(path.c_str());
+}
+
 // The compile worker: the build's translator and nvcc, run as a child process
 // (numericdream_b200/rtc.py beside this library) into a temporary directory, then the
 // resulting library loaded and its entry published.  ND_PYTHON names the Python
@@ -708,6 +726,7 @@ nd_status runtime_compile(const char* src, size_t len, uint64_t hash, nd_formula
   if (!f || fwrite(src, 1, len, f) != len) {
     if (f) fclose(f);
     *msg = "cannot write the formula source to " + dir;
+    remove_tree(dir);
     return ND_ERR_COMPILE;
   }
   fclose(f);
@@ -727,9 +746,11 @@ nd_status runtime_compile(const char* src, size_t len, uint64_t hash, nd_formula
       fclose(e);
     }
     *msg = text.empty() ? "the formula compiler failed (" + cmd + ")" : text;
+    remove_tree(dir);
     return ND_ERR_COMPILE;
   }
   void* lib = dlopen((dir + "/formula.so").c_str(), RTLD_NOW | RTLD_LOCAL);
+  remove_tree(dir);  // the loaded library stays mapped
   if (!lib) {
     const char* de = dlerror();
     *msg = std::string("cannot load the compiled formula: ") + (de ? de : "?");
@@ -739,6 +760,7 @@ nd_status runtime_compile(const char* src, size_t len, uint64_t hash, nd_formula
   EntryFn fn = reinterpret_cast<EntryFn>(dlsym(lib, "nd_rtc_entry"));
   const nd::FormulaEntry* e = fn ? fn() : nullptr;
   if (!e || e->source_hash != hash) {
+    dlclose(lib);
     *msg = "the compiled formula library does not match the source";
     return ND_ERR_COMPILE;
   }
@@ -1227,17 +1249,29 @@ nd_status nd_tune_cache_save(const char* path) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     bool first = true;
     for (const auto& kv : g_tuned) {
+      // the key as a JSON string (any length; quotes, backslashes and control
+      // characters escaped)
       std::string key;
       for (char ch : kv.first) {
-        if (ch == '"' || ch == '\\') key += '\\';
-        key += ch;
+        if (ch == '"' || ch == '\\') {
+          key += '\\';
+          key += ch;
+        } else if (static_cast<unsigned char>(ch) < 0x20) {
+          char esc[8];
+          snprintf(esc, sizeof(esc), "\\u%04x", unsigned(static_cast<unsigned char>(ch)));
+          key += esc;
+        } else {
+          key += ch;
+        }
       }
-      char buf[512];
+      char buf[256];
       snprintf(buf, sizeof(buf),
-               "%s {\"key\": \"%s\", \"kernel\": %d, \"block\": %d, \"blocks_per_sm\": %d, "
-               "\"refill_threshold\": %d, \"rays_per_s\": %.6g}",
-               first ? "" : ",\n", key.c_str(), kv.second.kernel, kv.second.block, kv.second.blocks_per_sm,
-               kv.second.refill_threshold, kv.second.rays_per_s);
+               "\", \"kernel\": %d, \"block\": %d, \"blocks_per_sm\": %d, \"refill_threshold\": %d, "
+               "\"rays_per_s\": %.6g}",
+               kv.second.kernel, kv.second.block, kv.second.blocks_per_sm, kv.second.refill_threshold,
+               kv.second.rays_per_s);
+      out += first ? " {\"key\": \"" : ",\n {\"key\": \"";
+      out += key;
       out += buf;
       first = false;
     }

@@ -48,3 +48,17 @@ def test_translator_errors_come_back_as_compile_errors(ndlib):
     with pytest.raises(runtime.FormulaError) as e:
         runtime.register_formula(unknown)
     assert e.value.status == abi.ND_ERR_COMPILE and "no_such_helper" in str(e.value)
+
+
+def test_the_compile_directory_is_removed(ndlib, tmp_path, monkeypatch):
+    # ND_RTC_DIR holds the temporary compile directories; after a compile that failed
+    # and one that succeeded (its library loaded), none is left
+    monkeypatch.setenv("ND_RTC_DIR", str(tmp_path))
+    bad = edited_source().replace("let power = p[0];", "let power = p[0] * ;")
+    with pytest.raises(runtime.FormulaError):
+        runtime.register_formula(bad)
+    assert os.listdir(tmp_path) == []
+    src = edited_source().replace("default=7.5", "default=7.25")
+    fid = runtime.register_formula(src)
+    assert runtime.formula_params(fid)[0].default_value == 7.25
+    assert os.listdir(tmp_path) == []
