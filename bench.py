@@ -387,7 +387,7 @@ def reference_arm(args):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sum(r["rays"] for r in per) / len(per) / (v * 1e6),
             "sample_wall_ms_per_step": 1e3 * sum(t_all) / len(t_all), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded views, no dataset)",
             "config": config_of(args.workload, views, 1),
             "de_evals_per_s": sum(r["evals_per_s"] for r in per) / len(per),
             "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": res["cores"], "kind": kind,
