@@ -49,8 +49,8 @@ METRIC = "Mrays/s & DE-evals/s on 1 B200, batched vs plain, at stated FP64 error
 # DRAM bytes (read + write) of one forward's kernels on each workload, from
 # ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum (one capture per workload;
 # the summary and its command are in profiles/).
-NCU_TRAFFIC = {"batched_64": {"march": 333.6e6, "surface": 384.0e6},
-               "mandelbox_1080p": {"march": 367.3e6, "surface": 532.1e6, "shadow": 330.4e6}}
+NCU_TRAFFIC = {"batched_64": {"march": 297.0e6, "surface": 402.2e6},
+               "mandelbox_1080p": {"march": 318.8e6, "surface": 502.9e6, "shadow": 333.7e6}}
 
 
 def _dist_env():

@@ -136,14 +136,17 @@ __global__ void __launch_bounds__(kBlock, MarchBlocks<T, kBatched, kDefer>::valu
   auto retire = [&]() {
     int32_t hit_item = -1;
     uint32_t hit_evals = 0;
+    double hit_t = 0.0;
     if (L.item >= 0 && L.phase == PH_DONE) {
       const DevView& v = kBatched ? a.views[L.view] : single;
       if constexpr (kDefer) {
-        L.flush_deferred(v, a.out, a.t_hit);
+        // the hit distance travels in the hit list: no per-ray distance array
+        L.flush_deferred(v, a.out, nullptr);
         ev_m += L.evals;
         if (L.hit) {
           hit_item = L.item;
           hit_evals = L.evals;
+          hit_t = L.t;
         }
       } else {
         L.flush(v, a.out, a.t_hit);
@@ -163,7 +166,7 @@ __global__ void __launch_bounds__(kBlock, MarchBlocks<T, kBatched, kDefer>::valu
         unsigned base = 0;
         if (lane == 0) base = atomicAdd(a.hit_count, unsigned(__popc(hm)));
         base = __shfl_sync(full, base, 0);
-        if (hit_item >= 0) a.hit_list[base + __popc(hm & lt_mask)] = HitEntry{hit_item, hit_evals};
+        if (hit_item >= 0) a.hit_list[base + __popc(hm & lt_mask)] = HitEntry{hit_item, hit_evals, hit_t};
       }
     }
   };
@@ -248,14 +251,14 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::value)
     bool want = false;
     ShadowEntry e;
     if (i < count) {
-      HitEntry h{int32_t(i), 0u};
+      HitEntry h{int32_t(i), 0u, 0.0};
       if (list) h = a.hit_list[i];
       const int64_t it = h.item;
       const int vi = kBatched ? find_view(a.views, a.nviews, it) : 0;
       const DevView& v = kBatched ? a.views[vi] : single;
       const int64_t local = it - v.ray_offset;
       const int64_t r = v.out_offset + local;
-      const double t = a.t_hit[r];
+      const double t = list ? h.t : a.t_hit[r];
       if (t >= 0.0) {  // (all-rays mode: a miss has t < 0 and the march wrote its outputs)
         // one call site per kind of DE evaluation (normal taps, shadow steps, trap), so
         // that the formula set's code appears three times in the kernel
@@ -435,7 +438,7 @@ template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, 
 cudaError_t launch_persistent(const LaunchArgs& a, const DevView& single, const LaunchConfig& c, cudaStream_t s) {
   const int block = kBlock;
   // the deferred march needs the hit list, the inline one must not get one
-  if ((a.hit_list != nullptr) != kDefer || (kDefer && !a.t_hit)) return cudaErrorInvalidValue;
+  if ((a.hit_list != nullptr) != kDefer) return cudaErrorInvalidValue;
   int per_sm = 0;
   cudaError_t e = resident_blocks(persistent_kernel<Set, T, kDir64, kBatched, kScenes, kAccel, kBlock, kDefer>,
                                   block, c.blocks_per_sm, &per_sm);

@@ -148,11 +148,14 @@ struct Stats {
   unsigned int timeouts, pad;
 };
 
-// One entry of the deferred shade pass's hit list: the launch-local ray index and
-// the DE evaluations its march used (the shade pass writes the ray's total once).
+// One entry of the deferred shade pass's hit list: the launch-local ray index, the DE
+// evaluations its march used (the shade pass writes the ray's total once) and the FP64
+// hit distance.  The surface pass reads its hits in list order, 16 B each and
+// coalesced, instead of fetching each hit's distance from a per-ray array.
 struct HitEntry {
   int32_t item;
   uint32_t march_evals;
+  double t;
 };
 
 // One entry of the shadow queue (the wavefront shadow pass, after cs_wf_shadow
