@@ -96,5 +96,10 @@ def test_untuned_single_small_view_runs_the_plain_launch():
         views = _views()
         c.forward(views, runtime.GBuffer.allocate(workloads.rays(views)), runtime.make_opts())
         assert c.stats().kernel == abi.ND_KERNEL_PERSISTENT
+        # one view with more rays than the grid has threads: the persistent march
+        big = workloads.mandelbox_1080p(runtime.find_formula)
+        assert len(big) == 1
+        c.forward(big, runtime.GBuffer.allocate(workloads.rays(big)), runtime.make_opts())
+        assert c.stats().kernel == abi.ND_KERNEL_PERSISTENT
     finally:
         c.close()
