@@ -312,13 +312,15 @@ nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nview
  * scratch_out): the plain per-view launch, and the persistent march at 64, 128 and
  * 256 threads per block x as many resident blocks per SM as fit or two fewer x
  * refill thresholds 3..12; each candidate's time is the median of three runs with
- * the L2 cache flushed before each.  The winner is kept for the call's formula sets
- * on this GPU (later forwards with opts fields 0 use it).  result->blocks_per_sm is
- * the resident count the march runs with. */
+ * the L2 cache flushed before each.  The candidates run the FP32 DE; the winner is
+ * kept for the call's formula sets on this GPU and the FP32 DE (later FP32 forwards
+ * with opts fields 0 use it; FP64-DE forwards keep the defaults).
+ * result->blocks_per_sm is the resident count the march runs with. */
 nd_status nd_autotune(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews,
                       const nd_gbuffer* scratch_out, nd_tune_result* result);
 /* The autotuner's winners on disk: a JSON array of entries keyed by GPU name, formula
- * set and a hash of the formula sources, so that a later process starts tuned.  No
+ * set, a hash of the formula sources and the DE precision, so that a later process
+ * starts tuned.  No
  * counterpart in the reference (it paces sub-tiles by a heuristic instead, ExportPacer,
  * fractal_renderer.zig:991).  load: ND_ERR_NOT_FOUND when the file does not exist;
  * *loaded (nullable) receives the number of entries read. */

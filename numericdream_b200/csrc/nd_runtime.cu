@@ -355,8 +355,10 @@ LaunchFn pick(const KernelTable& t, int kernel, int prec, bool batched, bool dir
 }
 
 // The tuning key of a launch plan on a context's GPU: the GPU's name, the formula
-// set, and a hash of the set's formula sources (an edited formula is tuned anew).
-std::string tune_key(const nd_ctx* ctx, const Launch& L) {
+// set, a hash of the set's formula sources (an edited formula is tuned anew) and the
+// DE precision (the FP64 kernels fit fewer blocks per SM than the FP32 ones, so a
+// residency tuned for one does not carry over to the other).
+std::string tune_key(const nd_ctx* ctx, const Launch& L, int prec) {
   uint64_t h = 0xCBF29CE484222325ull;
   for (int f : L.members) {
     const uint64_t x = nd_formula_at(f)->source_hash;
@@ -367,7 +369,7 @@ std::string tune_key(const nd_ctx* ctx, const Launch& L) {
   }
   char hex[20];
   snprintf(hex, sizeof(hex), "%016llx", (unsigned long long)h);
-  return ctx->gpu_name + "|" + L.key + "|" + hex;
+  return ctx->gpu_name + "|" + L.key + "|" + hex + (prec == 64 ? "|fp64" : "|fp32");
 }
 
 Tuned tuned_for(const std::string& key) {
@@ -485,7 +487,7 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
     int64_t rays = 0;
     for (int k = 0; k < nv; ++k) rays += h_views[base + k].rays;
     if (rays > 0) {
-      const Tuned tu = tuned_for(tune_key(ctx, L));
+      const Tuned tu = tuned_for(tune_key(ctx, L, prec));
       int kernel = opts && opts->kernel ? opts->kernel : tu.kernel;
       const bool accel = plan_voxels[p] > 0;
       // Untuned, one view with no more rays than the persistent grid has lanes runs the
@@ -1221,7 +1223,7 @@ nd_status nd_autotune(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, co
   t.tuned = true;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    for (const Launch& L : plans) g_tuned[tune_key(ctx, L)] = t;
+    for (const Launch& L : plans) g_tuned[tune_key(ctx, L, 32)] = t;  // the candidates ran the FP32 DE
   }
   if (result) {
     result->kernel = t.kernel;
@@ -1241,7 +1243,7 @@ nd_status nd_autotune(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, co
 }
 
 // The tuning cache on disk: one JSON array of the tuned entries of every GPU and
-// formula set (key: GPU name | formula set | hash of the formula sources).
+// formula set (key: GPU name | formula set | hash of the formula sources | precision).
 nd_status nd_tune_cache_save(const char* path) {
   if (!path) return ND_ERR_INVALID;
   std::string out = "[\n";

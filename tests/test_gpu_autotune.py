@@ -71,6 +71,10 @@ def test_autotune_picks_a_resident_configuration_and_caches_it(ctx, tmp_path):
     import torch
 
     assert torch.cuda.get_device_name(0) in e["key"]
+    # the winner is the FP32 DE's: an FP64-DE forward of the same formulas, whose
+    # kernels fit fewer blocks per SM, keeps the defaults
+    assert e["key"].endswith("|fp32")
+    assert not any(x["key"].endswith("|fp64") for x in entries)
     assert runtime.Context.tune_cache_load(path) == len(entries)
     with pytest.raises(runtime.NDError) as err:
         runtime.Context.tune_cache_load(str(tmp_path / "missing.json"))
