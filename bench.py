@@ -51,6 +51,9 @@ METRIC = "Mrays/s & DE-evals/s on 1 B200, batched vs plain, at stated FP64 error
 # the summary and its command are in profiles/).
 NCU_TRAFFIC = {"batched_64": {"march": 297.0e6, "surface": 402.2e6},
                "mandelbox_1080p": {"march": 318.8e6, "surface": 502.9e6, "shadow": 333.7e6}}
+# The march kernel's share of issue slots busy on batched_64 (ncu --set full, one
+# capture; the summary and its command are in profiles/).
+NCU_ISSUE = {"batched_64": 0.874}
 
 
 def _dist_env():
@@ -809,6 +812,10 @@ def main():
                          "traffic_forward": sum(NCU_TRAFFIC.get(args.workload, {}).values()) or None,
                          "traffic_note": "DRAM bytes per launch of the march (traffic) and of the whole forward, "
                                          "march + surface pass (traffic_forward), from one ncu capture",
+                         "issue_active": NCU_ISSUE.get(args.workload),
+                         "issue_note": "the march's share of issue slots busy (ncu smsp__issue_active, one "
+                                       "capture): the bound of this scalar, branchy code, whose FP32 "
+                                       "add/mul/fma are under half of the instructions it issues",
                          "kernel": "persistent_kernel (march); FLOPs = its DE evaluations x FLOPs per "
                                    "evaluation, over its CUDA-event time",
                          "kernel_ms": kms[0], "shade_pass_ms": kms[1],
