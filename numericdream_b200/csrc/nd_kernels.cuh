@@ -54,8 +54,13 @@ template <class T> struct MinBlocks {
 #ifndef ND_MARCH_MIN_BLOCKS_F32
 #define ND_MARCH_MIN_BLOCKS_F32 7
 #endif
+#ifndef ND_MARCH_MIN_BLOCKS_F64
+#define ND_MARCH_MIN_BLOCKS_F64 4
+#endif
 template <class T, bool kBatched, bool kDefer> struct MarchBlocks {
-  static constexpr int value = (sizeof(T) == 4 && kBatched && kDefer) ? ND_MARCH_MIN_BLOCKS_F32 : MinBlocks<T>::value;
+  static constexpr int value = (sizeof(T) == 4 && kBatched && kDefer) ? ND_MARCH_MIN_BLOCKS_F32
+                               : (sizeof(T) == 8 && kDefer)            ? ND_MARCH_MIN_BLOCKS_F64
+                                                                       : MinBlocks<T>::value;
 };
 
 // --------------------------------------------------------------- plain kernel
