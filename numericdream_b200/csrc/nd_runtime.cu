@@ -99,6 +99,10 @@ struct nd_ctx {
   int lite_cap = 0;
   bool last_trap = false;
   DevView* h_views = nullptr;  // pinned staging: two halves of h_views_cap records, forward calls alternate
+  DevView* d_fviews = nullptr;  // the forward's device view table: two halves of fviews_half records, alternating
+  int fviews_half = 0;          // like the staging
+  cudaStream_t upload = nullptr;  // the view-table uploads of forward calls
+  cudaEvent_t uploaded[2] = {nullptr, nullptr};  // after the upload into each half
   int h_views_cap = 0;
   cudaEvent_t staged[2] = {nullptr, nullptr};  // after the call that last used each half
   bool staged_valid[2] = {false, false};
@@ -192,6 +196,44 @@ template <class T> nd_status ensure_dev(nd_ctx* ctx, T** p, int* cap, int need, 
   cudaError_t e = cudaMalloc((void**)p, sizeof(T) * size_t(n));
   if (e != cudaSuccess) return cuda_fail(ctx, e, what);
   *cap = n;
+  return ND_OK;
+}
+
+// The pinned view staging (two halves, forward calls alternate).  Growing it waits for
+// every call that may still read the old one.
+nd_status ensure_staging(nd_ctx* ctx, int nviews) {
+  if (ctx->h_views_cap >= nviews) return ND_OK;
+  for (int k = 0; k < 2; ++k)
+    if (ctx->staged_valid[k]) cudaEventSynchronize(ctx->staged[k]);
+  if (ctx->have_last) cudaEventSynchronize(ctx->last_done);
+  if (ctx->h_views) cudaFreeHost(ctx->h_views);
+  ctx->h_views = nullptr;
+  ctx->h_views_cap = 0;
+  const int cap = std::max(nviews, 64);
+  cudaError_t e = cudaMallocHost((void**)&ctx->h_views, 2 * sizeof(DevView) * size_t(cap));
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "pinned view staging");
+  ctx->h_views_cap = cap;
+  return ND_OK;
+}
+
+// The forward's device view table (two halves, used like the staging's), its upload
+// stream and the events that order each half's upload before the march.
+nd_status ensure_forward_views(nd_ctx* ctx, int nviews) {
+  cudaError_t e = cudaSuccess;
+  if (!ctx->upload && (e = cudaStreamCreateWithFlags(&ctx->upload, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_fail(ctx, e, "upload stream");
+  for (int k = 0; k < 2; ++k)
+    if (!ctx->uploaded[k] && (e = cudaEventCreateWithFlags(&ctx->uploaded[k], cudaEventDisableTiming)) != cudaSuccess)
+      return cuda_fail(ctx, e, "upload event");
+  if (ctx->fviews_half >= nviews) return ND_OK;
+  if (ctx->have_last) cudaEventSynchronize(ctx->last_done);
+  if (ctx->d_fviews) cudaFree(ctx->d_fviews);
+  ctx->d_fviews = nullptr;
+  ctx->fviews_half = 0;
+  const int half = std::max(nviews, 64);
+  e = cudaMalloc((void**)&ctx->d_fviews, 2 * sizeof(DevView) * size_t(half));
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "view table");
+  ctx->fviews_half = half;
   return ND_OK;
 }
 
@@ -404,6 +446,12 @@ void scene_table(const SceneInput& sc, const std::vector<int>& members, std::vec
   }
 }
 
+// Zeroes two word arrays (a statistics block and a call's counters).
+__global__ void clear_words(unsigned long long* __restrict__ a, int na, unsigned long long* __restrict__ b, int nb) {
+  for (int i = threadIdx.x; i < na; i += blockDim.x) a[i] = 0ull;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) b[i] = 0ull;
+}
+
 // Enqueue every launch of a forward call.  d_views / d_counters are device
 // buffers with room for nviews views and kCountersPerPlan * plans.size() counters
 // (work counters, hit counters, shadow-queue counts, shadow work counters);
@@ -416,7 +464,8 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
                   bool copy_views, int* kernel_used, cudaEvent_t* tev = nullptr,
                   const SceneInput& sc = SceneInput(), nd::DevScene* d_scenes = nullptr, float* d_accel = nullptr,
                   nd::AccelJob* d_jobs = nullptr, std::vector<nd::AccelJob>* jobs_out = nullptr,
-                  nd::ShadowEntry* d_shadowq = nullptr) {
+                  nd::ShadowEntry* d_shadowq = nullptr, cudaStream_t upload = nullptr,
+                  cudaEvent_t uploaded = nullptr) {
   const int prec = (opts && opts->de_precision == 64) ? 64 : 32;
   // global output offsets in call order
   std::vector<int64_t> out_off(nviews + 1, 0);
@@ -470,13 +519,24 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
     if (e != cudaSuccess) return cuda_fail(ctx, e, "copy scenes");
   }
   if (copy_views && base > 0) {
-    cudaError_t e = cudaMemcpyAsync(d_views, h_views, sizeof(DevView) * size_t(base), cudaMemcpyHostToDevice, stream);
+    // on the upload stream when there is one (the march waits for it there)
+    cudaStream_t cs = upload && uploaded ? upload : stream;
+    cudaError_t e = cudaMemcpyAsync(d_views, h_views, sizeof(DevView) * size_t(base), cudaMemcpyHostToDevice, cs);
+    if (e == cudaSuccess && cs != stream) {
+      e = cudaEventRecord(uploaded, cs);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, uploaded, 0);
+    }
     if (e != cudaSuccess) return cuda_fail(ctx, e, "copy view table");
   }
-  cudaError_t e = cudaMemsetAsync(ctx->d_stats, 0, sizeof(Stats), stream);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "clear stats");
-  e = cudaMemsetAsync(d_counters, 0, sizeof(unsigned long long) * kCountersPerPlan * plans.size(), stream);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "clear work counters");
+  // the statistics block and the counters: one small kernel instead of two memsets
+  // (every command a forward enqueues is fetched over the bus, which a caller's
+  // device-to-host read-back of an earlier frame may be keeping busy)
+  static_assert(sizeof(Stats) % sizeof(unsigned long long) == 0, "the statistics block clears in 8-byte words");
+  clear_words<<<1, 256, 0, stream>>>(reinterpret_cast<unsigned long long*>(ctx->d_stats),
+                                     int(sizeof(Stats) / sizeof(unsigned long long)), d_counters,
+                                     kCountersPerPlan * int(plans.size()));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "clear stats and work counters");
   base = 0;
   int used = 0;
   int64_t ray_base = 0;  // where this plan's rays start in d_hits
@@ -610,6 +670,9 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       }
       if (tev) cudaEventRecord(tev[4 * p + 3], stream);
       used = kernel;
+    } else if (tev) {
+      // a plan with no rays: its timing events mark an empty interval
+      for (int k = 0; k < 4; ++k) cudaEventRecord(tev[4 * p + k], stream);
     }
     base += nv;
     ray_base += rays;
@@ -933,6 +996,10 @@ nd_status nd_ctx_destroy(nd_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->have_last) cudaEventSynchronize(ctx->last_done);
   if (ctx->d_views) cudaFree(ctx->d_views);
+  if (ctx->d_fviews) cudaFree(ctx->d_fviews);
+  if (ctx->upload) cudaStreamDestroy(ctx->upload);
+  for (int k = 0; k < 2; ++k)
+    if (ctx->uploaded[k]) cudaEventDestroy(ctx->uploaded[k]);
   if (ctx->d_counters) cudaFree(ctx->d_counters);
   if (ctx->d_stats) cudaFree(ctx->d_stats);
   if (ctx->d_thit) cudaFree(ctx->d_thit);
@@ -998,7 +1065,7 @@ nd_status forward_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, c
     if (!ctx->staged[k] && (e = cudaEventCreateWithFlags(&ctx->staged[k], cudaEventDisableTiming)) != cudaSuccess)
       return cuda_fail(ctx, e, "staging event");
   if (ctx->staged_valid[half]) cudaEventSynchronize(ctx->staged[half]);
-  if ((s = ensure_dev(ctx, &ctx->d_views, &ctx->views_cap, nviews, "view table")) != ND_OK) return s;
+  if ((s = ensure_forward_views(ctx, nviews)) != ND_OK) return s;
   if ((s = ensure_dev(ctx, &ctx->d_counters, &ctx->counters_cap, kCountersPerPlan * int(plans.size()),
                       "work counters")) != ND_OK)
     return s;
@@ -1024,18 +1091,7 @@ nd_status forward_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, c
     if (e != cudaSuccess) return cuda_fail(ctx, e, "hit buffers");
     ctx->thit_cap = total;
   }
-  if (ctx->h_views_cap < nviews) {
-    for (int k = 0; k < 2; ++k)
-      if (ctx->staged_valid[k]) cudaEventSynchronize(ctx->staged[k]);
-    if (ctx->have_last) cudaEventSynchronize(ctx->last_done);
-    if (ctx->h_views) cudaFreeHost(ctx->h_views);
-    ctx->h_views = nullptr;
-    ctx->h_views_cap = 0;
-    const int cap = std::max(nviews, 64);
-    e = cudaMallocHost((void**)&ctx->h_views, 2 * sizeof(DevView) * size_t(cap));
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "pinned view staging");
-    ctx->h_views_cap = cap;
-  }
+  if ((s = ensure_staging(ctx, nviews)) != ND_OK) return s;
   DevView* staging = ctx->h_views + size_t(half) * ctx->h_views_cap;
   int64_t voxels = 0;
   int accel_views = 0;
@@ -1061,14 +1117,22 @@ nd_status forward_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews, c
     if (e != cudaSuccess) return cuda_fail(ctx, e, "timing event");
     ctx->tev.push_back(ev);
   }
-  // a plan with no rays records no events: start from a clean slate
-  for (size_t i = 0; i < 4 * plans.size(); ++i) cudaEventRecord(ctx->tev[i], st);
   int kernel = 0;
   if (sc.nscenes > 0 && (s = ensure_dev(ctx, &ctx->d_scenes, &ctx->scenes_cap, sc.nscenes, "scene table")) != ND_OK)
     return s;
-  s = enqueue(ctx, views, nviews, opts, out, st, plans, ctx->d_views, staging, ctx->d_counters, ctx->d_thit,
-              ctx->d_hits, true, &kernel, ctx->tev.data(), sc, sc.nscenes > 0 ? ctx->d_scenes : nullptr,
-              ctx->d_accel, ctx->d_accel_jobs, nullptr, any_shadow ? ctx->d_shadowq : nullptr);
+  // the view table goes up on the upload stream as soon as this call is made: it
+  // then overlaps the previous call's march instead of waiting at the head of this
+  // call for the bus, where a caller's device-to-host read-back of the previous frame
+  // would slow it down
+  // (a caller capturing its stream into a graph gets the copy on that stream)
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if ((e = cudaStreamIsCapturing(st, &cap)) != cudaSuccess) return cuda_fail(ctx, e, "stream capture status");
+  const bool side = cap == cudaStreamCaptureStatusNone;
+  s = enqueue(ctx, views, nviews, opts, out, st, plans, ctx->d_fviews + size_t(half) * ctx->fviews_half, staging,
+              ctx->d_counters, ctx->d_thit, ctx->d_hits, true, &kernel, ctx->tev.data(), sc,
+              sc.nscenes > 0 ? ctx->d_scenes : nullptr, ctx->d_accel, ctx->d_accel_jobs, nullptr,
+              any_shadow ? ctx->d_shadowq : nullptr, side ? ctx->upload : nullptr,
+              side ? ctx->uploaded[half] : nullptr);
   ctx->tev_plans = s == ND_OK ? int(plans.size()) : 0;
   if (s != ND_OK) return s;
   e = cudaEventRecord(ctx->last_done, st);
@@ -1527,17 +1591,7 @@ nd_status shade_lite_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews
   if ((s = ensure_dev(ctx, &ctx->d_lite, &ctx->lite_cap, nlite, "lite descriptors")) != ND_OK) return s;
   if (sc.nscenes > 0 && (s = ensure_dev(ctx, &ctx->d_scenes, &ctx->scenes_cap, sc.nscenes, "scene table")) != ND_OK)
     return s;
-  if (ctx->h_views_cap < nviews) {
-    for (int k = 0; k < 2; ++k)
-      if (ctx->staged_valid[k]) cudaEventSynchronize(ctx->staged[k]);
-    if (ctx->h_views) cudaFreeHost(ctx->h_views);
-    ctx->h_views = nullptr;
-    ctx->h_views_cap = 0;
-    const int cap = std::max(nviews, 64);
-    e = cudaMallocHost((void**)&ctx->h_views, 2 * sizeof(DevView) * size_t(cap));
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "pinned view staging");
-    ctx->h_views_cap = cap;
-  }
+  if ((s = ensure_staging(ctx, nviews)) != ND_OK) return s;
   // views and descriptors in plan order; colour stops sorted by position
   std::vector<int64_t> out_off(nviews + 1, 0);
   for (int i = 0; i < nviews; ++i) out_off[i + 1] = out_off[i] + int64_t(views[i].spp) * views[i].tile_w * views[i].tile_h;
