@@ -306,6 +306,9 @@ nd_status nd_last_stats(nd_ctx* ctx, nd_stats* out); /* synchronises the last fo
 
 /* ---- marching ---- */
 nd_status nd_count_rays(const nd_view_desc* views, int32_t nviews, int64_t* total);
+/* Returns once the call's work is enqueued on `stream`.  A context keeps two calls'
+ * view tables, so a call blocks the host only until the call two back has finished on
+ * the device; calls on different streams run one after the other on the device. */
 nd_status nd_march_forward(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews,
                            const nd_march_opts* opts, const nd_gbuffer* out, void* stream);
 /* Times the launch configurations of the march on these views (writing into
