@@ -241,7 +241,8 @@ typedef struct nd_march_opts {
   int32_t block;             /* persistent march: threads per block, 64, 128 or 256 (0 = tuned, else 128) */
   int32_t blocks_per_sm;     /* persistent kernel residency: > 0 that many (at most what fits), < 0 that
                                 many fewer than fit, 0 = tuned default (as many as fit) */
-  int32_t refill_threshold;  /* persistent: refill a warp once this many lanes idle (0 = default) */
+  int32_t refill_threshold;  /* persistent: refill a warp once this many lanes idle (0 = tuned, else 6;
+                                2 for an FP64 DE) */
   int32_t de_precision;      /* 32 (default) or 64: float type of the DE itself */
   int32_t watchdog_ms;       /* device watchdog per launch (0 = 10000 ms) */
   int32_t accel_chain;       /* accelerator jumps a ray takes per pass of the persistent

@@ -573,7 +573,10 @@ nd_status enqueue(nd_ctx* ctx, const nd_view_desc* views, int nviews, const nd_m
       a.counter = d_counters + p;
       a.scenes = d_scenes;
       a.stats = ctx->d_stats;
-      a.refill_threshold = std::max(1, std::min(32, opts && opts->refill_threshold ? opts->refill_threshold : tu.refill_threshold));
+      // untuned, an FP64 DE (tens of FP64 iterations per evaluation) refills at 2 idle
+      // lanes: on the 4096^2 deep-zoom frame 416 ms against 437 at 6 and 490 at 12
+      const int thr_default = tu.tuned || prec != 64 ? tu.refill_threshold : 2;
+      a.refill_threshold = std::max(1, std::min(32, opts && opts->refill_threshold ? opts->refill_threshold : thr_default));
       // 4 jumps per pass measured fastest on batched views (1, 2, 4 and no limit tried)
       const int chain = opts ? opts->accel_chain : 0;
       a.accel_chain = chain > 0 ? chain : (chain < 0 ? 0 : 4);
