@@ -6,21 +6,27 @@
 A step is one forward march over the whole workload.  The default workload is the
 batched one: 64 views of mixed formulas (Mandelbulb, Mandelbox, Menger,
 pseudo-Kleinian) and uneven sizes (log-uniform 64..1024 per side, 7.2 M rays) in one
-persistent launch plus the trap pass, replayed as a CUDA graph.  The plain per-view
-launch of the same views is timed beside it, and the 1080p x 4 spp Mandelbox frame
-with shadow rays is timed as a second workload.  Rank 0 prints one JSON line.
+persistent launch plus the surface pass (normals, orbit trap), autotuned and replayed
+as a CUDA graph.  The plain per-view launch of the same views is timed beside it, and
+the 1080p x 4 spp Mandelbox frame with shadow rays is timed as a second workload.
+Rank 0 prints one JSON line.
 
 value         rays/s of the batched persistent march, device time (CUDA events on the
               launching stream), inputs resident; L2 is flushed between steps.
 e2e           the same metric through the public C ABI call (nd_march_forward) with
-              host view descriptors and the G-buffer read back to pinned host memory.
+              host view descriptors, and the G-buffer read back to pinned host memory
+              every step (two G-buffers: a frame's read-back overlaps the next march;
+              at least 20 frames, the last read-back inside the timed region).
 roofline      FP32-pipe roofline of the march kernel: algorithmic FLOPs per launch
               (DE evaluations x FLOPs per evaluation, counted by running the same ray
               program and formula code on the host with a counting float) / kernel
-              time, against the nominal FP32 FMA peak at the sampled SM clock.
-cpu_baseline  the oracle's FP32 march (same formulas, same march) on every host core
-              over a bounded, seeded sample of the workload's rays; the same sample in
-              FP64 gives the error figures against the GPU's output.
+              time, against the FP32 FMA peak measured on the GPU in the same run
+              (nominal at the sampled SM clock if that fails); DRAM traffic and the
+              issue-slot share from the committed ncu captures.
+cpu_baseline  the reference's own march code compiled for the host (see below), FP32,
+              on every host core over a bounded, seeded sample of the workload's rays,
+              with the oracle's FP32 restatement beside it; the oracle's FP64 run on
+              sampled rays gives the error figures against the GPU's output.
 
 --impl reference times the CPU implementation of the path on the host cores: the
 reference app itself only runs through WebGPU, which this machine cannot run, so its
