@@ -1651,7 +1651,12 @@ nd_status shade_lite_impl(nd_ctx* ctx, const nd_view_desc* views, int32_t nviews
     base += nv;
   }
   e = cudaEventRecord(ctx->last_done, st);
+  // the view table went up from the staging's first half: a forward call that reuses
+  // that half waits for this copy as for its own
+  if (e == cudaSuccess && !ctx->staged[0]) e = cudaEventCreateWithFlags(&ctx->staged[0], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->staged[0], st);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "record event");
+  ctx->staged_valid[0] = true;
   ctx->have_last = true;
   return ND_OK;
 }

@@ -46,3 +46,30 @@ def test_frames_enqueued_back_to_back_match_frames_marched_alone(ctx):
             got = bufs[i].numpy()
             for k in KEYS:
                 np.testing.assert_array_equal(got[k], want[k], err_msg=f"{nstreams} stream(s), frame {i}: {k}")
+
+
+def test_lite_shading_between_forward_calls(ctx):
+    # forward, lite shading of it, then the next frame's forward, nothing waited for:
+    # the lite call's view table goes up from the staging half the forward after next
+    # reuses, so each lite image must equal the one made with everything synchronised
+    import torch
+
+    stops = [((0.05, 0.05, 0.22), 0.0, 0.2, 1.3), ((1.0, 0.95, 0.82), 1.0, 0.8, 1.7)]
+    lights = [(abi.ND_LIGHT_GLOBAL, (0.4, 0.8, -0.45), (1.0, 0.95, 0.9), 1.2)]
+    opts = runtime.make_opts(kernel=abi.ND_KERNEL_PERSISTENT)
+    frames = _frames()
+    lites = [[abi.make_lite(stops, lights) for _ in v] for v in frames]
+    want = []
+    for views, lt in zip(frames, lites):
+        g = runtime.GBuffer.allocate(workloads.rays(views))
+        ctx.forward(views, g, opts)
+        want.append(ctx.shade_lite(views, lt, g).cpu().numpy())
+        torch.cuda.synchronize()
+    bufs = [runtime.GBuffer.allocate(workloads.rays(v)) for v in frames]
+    got = []
+    for views, lt, g in zip(frames, lites, bufs):
+        ctx.forward(views, g, opts)
+        got.append(ctx.shade_lite(views, lt, g))
+    torch.cuda.synchronize()
+    for i, (a, b) in enumerate(zip(got, want)):
+        np.testing.assert_array_equal(a.cpu().numpy(), b, err_msg=f"frame {i}")
