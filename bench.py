@@ -831,7 +831,9 @@ def main():
                          if measured_fp32 else "nominal: 148 SMs x 128 FP32 lanes x 2 x sampled SM clock",
                          "peak_nominal": nominal},
             "error_vs_fp64": err, "cpu_baseline": cpu, "clocks": clk,
-            "gpu_launches": 2 * args.steps,
+            # per replayed forward: the counter clear, the march, the surface pass, and
+            # the shadow pass when a view casts shadow rays
+            "gpu_launches": (3 + (1 if any(v.shadow for v in views) else 0)) * args.steps,
             "stats": {"de_evals": st.de_evals, "march": st.march_evals, "normal": st.normal_evals,
                       "shadow": st.shadow_evals, "trap": st.trap_evals, "hits": st.hits, "refills": st.refills},
             "tune": {"kernel": tune.kernel, "block": tune.block, "blocks_per_sm": tune.blocks_per_sm,
