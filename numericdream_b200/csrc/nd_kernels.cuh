@@ -241,8 +241,14 @@ __global__ void __launch_bounds__(kBlock, MarchBlocks<T, kBatched, kDefer>::valu
 // (the plain kernel) the pass computes the orbit trap of every ray that hit.  It
 // strides over its work with a resident grid, warp by warp (the queue appends are
 // warp-aggregated).
+#ifndef ND_SHADE_MIN_BLOCKS_F32
+#define ND_SHADE_MIN_BLOCKS_F32 7
+#endif
+template <class T> struct ShadeBlocks {
+  static constexpr int value = sizeof(T) == 4 ? ND_SHADE_MIN_BLOCKS_F32 : MinBlocks<T>::value;
+};
 template <class Set, class T, bool kDir64, bool kBatched, bool kScenes = false, bool kAccel = false>
-__global__ void __launch_bounds__(128, MinBlocks<T>::value)
+__global__ void __launch_bounds__(128, ShadeBlocks<T>::value)
     shade_kernel(const __grid_constant__ LaunchArgs a, const __grid_constant__ DevView single, int do_trap) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
