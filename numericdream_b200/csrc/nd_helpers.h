@@ -132,6 +132,15 @@ template <class T> ND_HD_INLINE IterCarry<T> bulb_power_step(IterCarry<T> c, v3<
 // template.wgsl:1033-1055: abs then sort components so that x >= y >= z.
 template <class T> ND_HD_INLINE v3<T> sort_desc_abs(v3<T> z) {
   v3<T> v = abs(z);
+#if defined(__CUDA_ARCH__) && !defined(ND_OPCOUNT_BUILD)
+  if constexpr (std::is_same<T, float>::value) {
+    // the same three compare-exchanges as a min/max network, so that a warp does not
+    // split on them (identical results for non-NaN components: abs gives no -0)
+    const float a = fmaxf(v.x, v.y), b = fminf(v.x, v.y);
+    const float x = fmaxf(a, v.z), c = fminf(a, v.z);
+    return v3<T>(x, fmaxf(b, c), fminf(b, c));
+  }
+#endif
   if (v.x < v.y) { const T t = v.x; v.x = v.y; v.y = t; }
   if (v.x < v.z) { const T t = v.x; v.x = v.z; v.z = t; }
   if (v.y < v.z) { const T t = v.y; v.y = v.z; v.z = t; }
