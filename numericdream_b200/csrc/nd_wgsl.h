@@ -17,6 +17,8 @@
 #include <math.h>
 #include <string.h>
 
+#include <type_traits>
+
 #if defined(__CUDACC__)
 #define ND_HD_INLINE __host__ __device__ __forceinline__
 #define ND_HD __host__ __device__
@@ -416,6 +418,25 @@ template <class S> ND_HD_INLINE v4<S> select(v4<S> f, v4<S> t, bool c) { return 
 template <class S> ND_HD_INLINE v2<S> select(v2<S> f, v2<S> t, v2<bool> c) { return v2<S>(c.x ? t.x : f.x, c.y ? t.y : f.y); }
 template <class S> ND_HD_INLINE v3<S> select(v3<S> f, v3<S> t, v3<bool> c) { return v3<S>(c.x ? t.x : f.x, c.y ? t.y : f.y, c.z ? t.z : f.z); }
 template <class S> ND_HD_INLINE v4<S> select(v4<S> f, v4<S> t, v4<bool> c) { return v4<S>(c.x ? t.x : f.x, c.y ? t.y : f.y, c.z ? t.z : f.z, c.w ? t.w : f.w); }
+
+// The scalar type of a value (a vector's component type).
+template <class X> struct scalar_of { typedef X type; };
+template <class S> struct scalar_of<v2<S>> { typedef S type; };
+template <class S> struct scalar_of<v3<S>> { typedef S type; };
+template <class S> struct scalar_of<v4<S>> { typedef S type; };
+
+// (a + b) + c where b and c are the same in every iteration of a formula's de_step
+// (built from pos and the parameters only).  The FP32 DE on the device adds b + c
+// first, so that the compiler computes it once per DE evaluation, outside the
+// iteration loop; the one rounding of that sum moves.  The FP64 DE, the dual numbers
+// and host code keep WGSL's left-to-right order.
+template <class A, class B, class C>
+ND_HD_INLINE auto add_inv(const A& a, const B& b, const C& c) -> decltype((a + b) + c) {
+#if defined(__CUDA_ARCH__) && !defined(ND_OPCOUNT_BUILD)
+  if constexpr (std::is_same<typename scalar_of<A>::type, float>::value) return a + (b + c);
+#endif
+  return (a + b) + c;
+}
 
 template <class S> ND_HD_INLINE S dot(v2<S> a, v2<S> b) { return a.x * b.x + a.y * b.y; }
 template <class S> ND_HD_INLINE S dot(v3<S> a, v3<S> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }

@@ -772,6 +772,7 @@ class TE:
     code: str
     const: object = None       # folded Python value for abstract/const expressions
     lvalue: bool = False
+    inv: bool = False          # de_step: the same in every iteration (no carry in it)
 
 
 def _wrap_trunc_div(a: int, b: int) -> int:
@@ -795,6 +796,7 @@ class FormulaCompiler:
         self.features: set[str] = set()
         self.calls: dict[str, set] = {}
         self.cur_fn = ""
+        self.inv_fn = False  # translating de_step: track what is the same in every iteration
         for f in fns:
             if f.name in self.fn_sigs:
                 raise TranslateError(f"function {f.name} defined twice", f.line)
@@ -1043,6 +1045,19 @@ class FormulaCompiler:
         return None
 
     def e_Binary(self, e):
+        te = self._e_binary(e)
+        # (a + b) + c in de_step with b and c the same in every iteration and a not:
+        # ndw::add_inv lets the FP32 DE on the device add b + c first, so that it is
+        # computed once per evaluation instead of once per iteration
+        if (e.op == "+" and self.inv_fn and isinstance(e.l, Binary) and e.l.op == "+" and
+                te.ty.kind in ("s", "v") and te.ty.scalar == "f32" and
+                self.is_inv(e.r) and self.is_inv(e.l.r) and not self.is_inv(e.l.l)):
+            x, y, z = self.expr(e.l.l), self.expr(e.l.r), self.expr(e.r)
+            if all(not is_abstract(t.ty) and t.ty.kind in ("s", "v") and t.ty.scalar == "f32" for t in (x, y, z)):
+                return TE(te.ty, f"ndw::add_inv({x.code}, {y.code}, {z.code})")
+        return te
+
+    def _e_binary(self, e):
         op = e.op
         a = self.expr(e.l)
         b = self.expr(e.r)
@@ -1542,7 +1557,8 @@ class FormulaCompiler:
             raise TranslateError(f"cannot declare a {ty}", s.line)
         mutable = s.kind == "var"
         cname = cpp_name(s.name)
-        self.declare(s.name, TE(ty, cname, None, lvalue=mutable), s.line)
+        inv = self.inv_fn and not mutable and s.init is not None and self.is_inv(s.init)
+        self.declare(s.name, TE(ty, cname, None, lvalue=mutable, inv=inv), s.line)
         qual = "" if mutable else "const "
         if init is None:
             return f"{qual}{cpp_type(ty)} {cname}{{}};"
@@ -1700,16 +1716,44 @@ class FormulaCompiler:
         ptys, rty = self.fn_sigs[f.name]
         self.cur_ret = rty
         self.cur_fn = f.name
+        # de_step(carry, pos, p): pos and the parameters are the same in every iteration
+        self.inv_fn = f.name == "de_step" and len(ptys) == 3
         self.push()
-        for (pn, pt) in ptys:
+        for k, (pn, pt) in enumerate(ptys):
             if pt.kind == "a" and pt.n == 8 and pt.elem == F32 and pn == "p":
                 pt = PARAMS
-            self.declare(pn, TE(pt, cpp_name(pn), None, lvalue=False), f.line)
+            self.declare(pn, TE(pt, cpp_name(pn), None, lvalue=False, inv=self.inv_fn and k > 0), f.line)
         body = []
         for s in f.body:
             body.extend(self.stmt(s, 1))
         self.pop()
+        self.inv_fn = False
         return body
+
+    def is_inv(self, e: Expr) -> bool:
+        """In de_step: does e have the same value in every iteration (built from pos, the
+        parameters, constants and `let`s of those, through pure operations)?"""
+        if isinstance(e, Num):
+            return True
+        if isinstance(e, Ident):
+            if e.name in ("true", "false"):
+                return True
+            for sc in reversed(self.scopes):
+                if e.name in sc:
+                    te = sc[e.name]
+                    return te.inv or te.const is not None
+            return e.name in self.module_consts_src or e.name in TEMPLATE_CONSTS
+        if isinstance(e, Unary):
+            return self.is_inv(e.e)
+        if isinstance(e, Binary):
+            return self.is_inv(e.l) and self.is_inv(e.r)
+        if isinstance(e, Call):
+            return all(self.is_inv(a) for a in e.args)
+        if isinstance(e, Index):
+            return self.is_inv(e.e) and self.is_inv(e.idx)
+        if isinstance(e, Member):
+            return self.is_inv(e.e)
+        return False
 
     def check_contract(self):
         need = {
