@@ -52,7 +52,7 @@ template <class T> struct MinBlocks {
 // The batched FP32 march that defers its shading (the forward calls) carries no
 // normal or shadow state and fits in fewer registers.
 #ifndef ND_MARCH_MIN_BLOCKS_F32
-#define ND_MARCH_MIN_BLOCKS_F32 7
+#define ND_MARCH_MIN_BLOCKS_F32 8
 #endif
 #ifndef ND_MARCH_MIN_BLOCKS_F64
 #define ND_MARCH_MIN_BLOCKS_F64 4
