@@ -55,11 +55,11 @@ METRIC = "Mrays/s & DE-evals/s on 1 B200, batched vs plain, at stated FP64 error
 # DRAM bytes (read + write) of one forward's kernels on each workload, from
 # ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum (one capture per workload;
 # the summary and its command are in profiles/).
-NCU_TRAFFIC = {"batched_64": {"march": 297.0e6, "surface": 402.2e6},
-               "mandelbox_1080p": {"march": 318.8e6, "surface": 502.9e6, "shadow": 333.7e6}}
+NCU_TRAFFIC = {"batched_64": {"march": 307.5e6, "surface": 391.7e6},
+               "mandelbox_1080p": {"march": 321.1e6, "surface": 499.8e6, "shadow": 330.3e6}}
 # The march kernel's share of issue slots busy on batched_64 (ncu --set full, one
 # capture; the summary and its command are in profiles/).
-NCU_ISSUE = {"batched_64": 0.836}
+NCU_ISSUE = {"batched_64": 0.865}
 
 
 def _dist_env():
