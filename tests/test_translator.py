@@ -169,3 +169,51 @@ def test_generated_build_translates_the_formula_set():
     for n in ("mandelbrot", "amazingbox_box", "menger3_ifs", "pseudokleinian_kleinian"):
         assert n in m["formulas"]
     assert set(m["rejected"]) <= {"heightmap_primitive"}
+
+
+INV_FORMULA = r"""
+fn de_iterations(p: Params) -> i32 { return 4; }
+fn de_step(carry: IterCarry, pos: vec3f, p: Params) -> IterCarry {
+    let julia = vec3f(p[1], p[2], p[3]);
+    var z = carry.z * p[0] + pos * p[4] + julia;
+    z = z + carry.dr + julia;
+    let w = carry.z + pos + julia;
+    return IterCarry(z + w, carry.dr * 2.0);
+}
+fn de_finalize(carry: IterCarry) -> f32 { return length(carry.z) / carry.dr; }
+"""
+
+
+def test_invariant_addends_are_grouped_only_in_de_step():
+    # (a + b) + c in de_step with b and c built from pos and the parameters alone is
+    # emitted as ndw::add_inv(a, b, c); a sum with an iteration-dependent b is not
+    cpp = translate(INV_FORMULA, "ndt_inv").cpp
+    lines = [l.strip() for l in cpp.split("\n")]
+    grouped = [l for l in lines if "add_inv" in l]
+    assert any(l.startswith("ndw::v3<T> z = ndw::add_inv((carry.z * ndw::param(p, int32_t(0)))") for l in grouped), grouped
+    assert any("const ndw::v3<T> w = ndw::add_inv(carry.z, pos, julia)" in l for l in grouped), grouped
+    assert not any(l.startswith("z = ndw::add_inv") for l in grouped), grouped  # carry.dr is not invariant
+    assert "add_inv" not in cpp.split("de_finalize(ndw::IterCarry<T> carry) {")[1]
+
+
+def test_add_inv_keeps_the_wgsl_order_on_the_host():
+    # host code (the oracle's, the op counter's) sums left to right like WGSL
+    src = r"""
+#include <stdio.h>
+#include "nd_wgsl.h"
+int main() {
+  const float a = 1.0f, b = 1e-8f, c = 1e-8f;
+  const ndw::v3<float> v(1.0f, 2.0f, 3.0f), u(1e-8f), w(1e-8f);
+  const ndw::v3<float> r = ndw::add_inv(v, u, w);
+  printf("%d %d\n", ndw::add_inv(a, b, c) == (a + b) + c, r.x == (1.0f + 1e-8f) + 1e-8f);
+  return 0;
+}
+"""
+    with tempfile.TemporaryDirectory() as d:
+        cpp = os.path.join(d, "t.cpp")
+        exe = os.path.join(d, "t")
+        with open(cpp, "w") as fh:
+            fh.write(src)
+        subprocess.run(["g++", "-std=c++17", "-O1", "-ffp-contract=off", "-I", CSRC, cpp, "-o", exe], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()
+    assert out == ["1", "1"]
